@@ -1,0 +1,164 @@
+// extern "C" surface of libcampfire_gas.so (include/campfire_gas.h): thin
+// wrappers over cfg::Engine that validate handles and translate exceptions and
+// CUDA failures into status codes.
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/campfire_gas.h"
+#include "engine.h"
+
+struct cfg_sim {
+  cfg::Engine* eng;
+  int scene;
+  bool owner;     // a single-scene FluidSim owns its engine; batch views do not
+};
+struct cfg_batch {
+  cfg::Engine* eng;
+  std::vector<std::unique_ptr<cfg_sim>> views;
+};
+
+namespace {
+template <class F> int guarded(F&& f) {
+  try { return f(); }
+  catch (const std::bad_alloc&) { return cfg::fail(CFG_ERR_NOMEM, "host allocation failed"); }
+  catch (const std::exception& e) { return cfg::fail(CFG_ERR_INVAL, e.what()); }
+}
+#define SIM_OK(sim) do { if (!(sim) || !(sim)->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_sim handle"); } while (0)
+#define OWNER_OK(sim) do { if (!(sim)->owner) return cfg::fail(CFG_ERR_INVAL, "this call steps a whole batch: use the cfg_batch_* entry point"); } while (0)
+}  // namespace
+
+extern "C" {
+
+int cfg_version(void) { return 10000; }
+
+int cfg_last_error(char* buf, size_t len) {
+  const std::string& e = cfg::last_error();
+  if (buf && len) { std::strncpy(buf, e.c_str(), len - 1); buf[len - 1] = 0; }
+  return (int)e.size();
+}
+
+int cfg_default_params(cfg_params* out) {
+  if (!out) return cfg::fail(CFG_ERR_INVAL, "null output");
+  cfg::default_params(out);
+  return CFG_OK;
+}
+
+int cfg_device_count(int* count) {
+  if (!count) return cfg::fail(CFG_ERR_INVAL, "null output");
+  int n = 0;
+  const cudaError_t e = cudaGetDeviceCount(&n);
+  *count = e == cudaSuccess ? n : 0;
+  return CFG_OK;
+}
+
+int cfg_create(int nx, int ny, double width, double dt, int device, cfg_sim** out) {
+  if (!out) return cfg::fail(CFG_ERR_INVAL, "null output");
+  *out = nullptr;
+  return guarded([&] {
+    auto eng = std::make_unique<cfg::Engine>();
+    CFG_TRY(eng->init(device, 1, &nx, &ny, &width, &dt));
+    *out = new cfg_sim{eng.release(), 0, true};
+    return CFG_OK;
+  });
+}
+
+int cfg_destroy(cfg_sim* sim) {
+  if (!sim) return CFG_OK;
+  if (!sim->owner) return cfg::fail(CFG_ERR_INVAL, "batch views are released with cfg_batch_destroy");
+  delete sim->eng;
+  delete sim;
+  return CFG_OK;
+}
+
+#define SCENE_CALL(sim, expr) SIM_OK(sim); return guarded([&] { return sim->eng->expr; })
+
+int cfg_reset(cfg_sim* sim) { SCENE_CALL(sim, reset(sim->scene)); }
+int cfg_set_param(cfg_sim* sim, const char* name, double v) { SCENE_CALL(sim, set_param(sim->scene, name, v)); }
+int cfg_get_param(cfg_sim* sim, const char* name, double* v) { SCENE_CALL(sim, get_param(sim->scene, name, v)); }
+int cfg_set_dt(cfg_sim* sim, double dt) { SCENE_CALL(sim, set_dt(sim->scene, dt)); }
+int cfg_write_params(cfg_sim* sim) { SCENE_CALL(sim, write_params(sim->scene)); }
+int cfg_upload_pieces(cfg_sim* sim, const float* data, int n) { SCENE_CALL(sim, upload_pieces(sim->scene, data, n)); }
+int cfg_clear_geometry(cfg_sim* sim) { SCENE_CALL(sim, clear_geometry(sim->scene)); }
+int cfg_geometry(cfg_sim* sim) { SCENE_CALL(sim, geometry(sim->scene)); }
+int cfg_radiation(cfg_sim* sim) { SCENE_CALL(sim, radiation(sim->scene)); }
+int cfg_set_frame(cfg_sim* sim, uint32_t frame) { SCENE_CALL(sim, set_frame(sim->scene, frame)); }
+int cfg_readback(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW) { SCENE_CALL(sim, readback(sim->scene, acc, rad, faceW)); }
+int cfg_field_size(cfg_sim* sim, const char* name, size_t* count) { SCENE_CALL(sim, field_size(sim->scene, name, count)); }
+int cfg_read_field(cfg_sim* sim, const char* name, float* out, size_t count) { SCENE_CALL(sim, read_field(sim->scene, name, out, count)); }
+int cfg_write_field(cfg_sim* sim, const char* name, const float* in, size_t count) { SCENE_CALL(sim, write_field(sim->scene, name, in, count)); }
+int cfg_read_p64(cfg_sim* sim, double* out, size_t count) { SCENE_CALL(sim, read_p64(sim->scene, out, count)); }
+int cfg_get_info(cfg_sim* sim, cfg_info* out) { SCENE_CALL(sim, info(sim->scene, out)); }
+int cfg_set_cfl(cfg_sim* sim, double cfl, double dt_cap) { SCENE_CALL(sim, set_cfl(sim->scene, cfl, dt_cap)); }
+int cfg_set_nray(cfg_sim* sim, int nray) { SCENE_CALL(sim, set_nray(sim->scene, nray)); }
+int cfg_pressure_residual(cfg_sim* sim, double* rel) { SCENE_CALL(sim, pressure_residual(sim->scene, rel)); }
+int cfg_budgets(cfg_sim* sim, double* out) { SCENE_CALL(sim, budgets(sim->scene, out)); }
+
+int cfg_step(cfg_sim* sim, int nsteps) { SIM_OK(sim); OWNER_OK(sim); return guarded([&] { return sim->eng->step(nsteps); }); }
+int cfg_step_profiled(cfg_sim* sim, float* ms) { SIM_OK(sim); OWNER_OK(sim); return guarded([&] { return sim->eng->step_profiled(ms); }); }
+int cfg_run_stage(cfg_sim* sim, const char* stage) { SIM_OK(sim); OWNER_OK(sim); return guarded([&] { return sim->eng->run_stage(stage); }); }
+int cfg_vcycle(cfg_sim* sim, int nu) { SIM_OK(sim); OWNER_OK(sim); return guarded([&] { return sim->eng->vcycle_once(nu); }); }
+int cfg_set_solver(cfg_sim* sim, int mode, int ncycles, double tol, int max_cycles) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->set_solver(mode, ncycles, tol, max_cycles); });
+}
+int cfg_set_stream(cfg_sim* sim, void* stream) { SIM_OK(sim); OWNER_OK(sim); return guarded([&] { return sim->eng->set_stream((cudaStream_t)stream); }); }
+int cfg_synchronize(cfg_sim* sim) { SIM_OK(sim); return guarded([&] { return sim->eng->synchronize(); }); }
+int cfg_set_graphs(cfg_sim* sim, int enable) { SIM_OK(sim); OWNER_OK(sim); return sim->eng->set_graphs(enable != 0); }
+int cfg_launch_count(cfg_sim* sim, int* per_step) {
+  SIM_OK(sim);
+  if (!per_step) return cfg::fail(CFG_ERR_INVAL, "null output");
+  *per_step = sim->eng->launches_per_step();
+  return CFG_OK;
+}
+
+// ---- batches
+int cfg_batch_create(int nscenes, const int* nx, const int* ny, const double* width, const double* dt, int device, cfg_batch** out) {
+  if (!out || !nx || !ny || !width || !dt) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  *out = nullptr;
+  return guarded([&] {
+    auto eng = std::make_unique<cfg::Engine>();
+    CFG_TRY(eng->init(device, nscenes, nx, ny, width, dt));
+    auto b = std::make_unique<cfg_batch>();
+    b->eng = eng.release();
+    for (int s = 0; s < nscenes; s++) b->views.emplace_back(new cfg_sim{b->eng, s, false});
+    *out = b.release();
+    return CFG_OK;
+  });
+}
+int cfg_batch_destroy(cfg_batch* b) {
+  if (!b) return CFG_OK;
+  delete b->eng;
+  delete b;
+  return CFG_OK;
+}
+#define BATCH_OK(b) do { if (!(b) || !(b)->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle"); } while (0)
+int cfg_batch_scene(cfg_batch* b, int i, cfg_sim** view) {
+  BATCH_OK(b);
+  if (!view || i < 0 || i >= (int)b->views.size()) return cfg::fail(CFG_ERR_INVAL, "scene index out of range");
+  *view = b->views[i].get();
+  return CFG_OK;
+}
+int cfg_batch_set_solver(cfg_batch* b, int mode, int ncycles, double tol, int max_cycles) {
+  BATCH_OK(b); return guarded([&] { return b->eng->set_solver(mode, ncycles, tol, max_cycles); });
+}
+int cfg_batch_set_active(cfg_batch* b, int i, int active) {
+  BATCH_OK(b);
+  if (i < 0 || i >= (int)b->views.size()) return cfg::fail(CFG_ERR_INVAL, "scene index out of range");
+  return guarded([&] { return b->eng->set_active(i, active != 0); });
+}
+int cfg_batch_step(cfg_batch* b, int nsteps) { BATCH_OK(b); return guarded([&] { return b->eng->step(nsteps); }); }
+int cfg_batch_set_stream(cfg_batch* b, void* stream) { BATCH_OK(b); return guarded([&] { return b->eng->set_stream((cudaStream_t)stream); }); }
+int cfg_batch_synchronize(cfg_batch* b) { BATCH_OK(b); return guarded([&] { return b->eng->synchronize(); }); }
+int cfg_batch_launch_count(cfg_batch* b, int* per_step) {
+  BATCH_OK(b);
+  if (!per_step) return cfg::fail(CFG_ERR_INVAL, "null output");
+  *per_step = b->eng->launches_per_step();
+  return CFG_OK;
+}
+int cfg_batch_write_params(cfg_batch* b) { BATCH_OK(b); return guarded([&] { return b->eng->write_params_all(); }); }
+int cfg_batch_geometry(cfg_batch* b) { BATCH_OK(b); return guarded([&] { return b->eng->geometry_all(); }); }
+
+}  // extern "C"

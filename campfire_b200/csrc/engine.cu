@@ -1,0 +1,800 @@
+// Host engine of the B200 gas step. See engine.h.
+//
+// One step (FluidSim.encodeStep, js/fluid.js:225-253) is enqueued as
+//   advect -> diffuse+sources -> forces+coef+rhs0 (+ coarse coefficients)
+//   -> [pressure loop: V(2,2) cycle -> residual norm / FP64 defect] -> project
+// and captured once in a CUDA graph whose pressure loop is a conditional WHILE
+// node: the kernel that finishes each residual reduction decides, per scene,
+// whether another cycle runs and sets the node's condition on the device, so a
+// step never waits on the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "kernels.h"
+
+namespace cfg {
+
+namespace {
+thread_local std::string g_err;
+
+const char* kParamNames[40] = {
+  "nx", "ny", "dx", "dt", "Tamb", "rhoAmb", "YOamb", "grav", "cp", "Pr", "viscMult", "diffMult",
+  "reactB", "reactTa", "dHc", "sO2", "sootFormA", "sootFormTa", "sootOxA", "sootOxTa",
+  "kappaSootC", "kappaGas", "exchAlpha", "depth", "charA", "charTa", "nPieces", "frame",
+  "heaterX0", "heaterX1", "heaterY1", "heaterT", "burnerX0", "burnerX1", "burnerFlux", "burnerT",
+  "sootDensity", "sigma", "charO2", "time"};
+
+__global__ void k_fill_f32(float* a, int pitch, int w, int h, float v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i < w && j < h) a[(size_t)j * pitch + i] = v;
+}
+__global__ void k_fill_f4(float4* a, int pitch, int w, int h, float4 v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i < w && j < h) a[(size_t)j * pitch + i] = v;
+}
+}  // namespace
+
+void set_error(const std::string& msg) { g_err = msg; }
+const std::string& last_error() { return g_err; }
+int fail(int code, const std::string& msg) { g_err = msg; return code; }
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInvalidDevice) return CFG_ERR_NODEV;
+  if (e == cudaErrorMemoryAllocation) return CFG_ERR_NOMEM;
+  return CFG_ERR_IO;
+}
+
+// FluidSim defaults (js/fluid.js:35-45) from PHYS (js/config.js:12-47)
+void default_params(cfg_params* p) {
+  std::memset(p, 0, sizeof *p);
+  const double rhoAmb = PhysConst::rhoAmb();
+  p->Tamb = (float)293.15; p->rhoAmb = (float)rhoAmb; p->YOamb = 0.232f; p->grav = 9.81f;
+  p->cp = 1300.f; p->Pr = 0.7f; p->viscMult = 1.f; p->diffMult = 1.f;
+  p->reactB = 2.0e10f; p->reactTa = 15000.f; p->dHc = 15.0e6f; p->sO2 = (float)(15.0e6 / 13.1e6);
+  p->sootFormA = 6.0e6f; p->sootFormTa = 25000.f; p->sootOxA = 5.4e8f; p->sootOxTa = 19800.f;
+  p->kappaSootC = 1862.f; p->kappaGas = 0.8f; p->exchAlpha = 0.05f; p->depth = 0.8f;
+  p->charA = 6.6f; p->charTa = 5800.f; p->burnerT = 600.f;
+  p->sootDensity = 1800.f; p->sigma = (float)5.670374e-8; p->charO2 = 2.667f;
+}
+
+int param_index(const char* name) {
+  if (!name) return -1;
+  for (int i = 0; i < 40; i++) if (std::strcmp(kParamNames[i], name) == 0) return i;
+  return -1;
+}
+
+// ------------------------------------------------------------------ lifetime
+Engine::~Engine() {
+  // nothing was allocated before the streams; keep the caller's error message intact
+  if (!stream_ || cudaSetDevice(device_) != cudaSuccess) return;
+  destroy_graph();
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& sc : scenes_) if (sc.arena) cudaFree(sc.arena);
+  for (auto& w : d_wl_) if (w) cudaFree(w);
+  if (d_scenes_) cudaFree(d_scenes_);
+  if (d_solve_) cudaFree(d_solve_);
+  if (d_ctl_) cudaFree(d_ctl_);
+  if (d_dxd_) cudaFree(d_dxd_);
+  if (d_alpha_) cudaFree(d_alpha_);
+  if (d_scratch_) cudaFree(d_scratch_);
+  if (h_ctl_pinned_) cudaFreeHost(h_ctl_pinned_);
+  if (stream_) cudaStreamDestroy(stream_);
+  if (body_stream_) cudaStreamDestroy(body_stream_);
+}
+
+int Engine::activate() const {
+  CFG_CUDA(cudaSetDevice(device_));
+  return CFG_OK;
+}
+
+int Engine::init(int device, int n, const int* nx, const int* ny, const double* width, const double* dt) {
+  if (n <= 0) return fail(CFG_ERR_INVAL, "scene count must be positive");
+  scenes_.resize(n);
+  for (int s = 0; s < n; s++) {
+    Scene& sc = scenes_[s];
+    if (nx[s] < 2 || ny[s] < 2 || nx[s] > 16384 || ny[s] > 16384) return fail(CFG_ERR_INVAL, "grid size out of range");
+    if (!(width[s] > 0) || !(dt[s] > 0)) return fail(CFG_ERR_INVAL, "width and dt must be positive");
+    sc.nx = nx[s]; sc.ny = ny[s]; sc.width = width[s];
+    sc.dxd = width[s] / nx[s]; sc.dtd = dt[s]; sc.dt_cap = dt[s];
+    default_params(&sc.host);
+    // multigrid hierarchy (js/fluid.js:70-91), at most MAX_LEVELS levels
+    int lx = sc.nx, ly = sc.ny, L = 0;
+    for (int l = 0; l < MAX_LEVELS; l++) {
+      sc.lnx[l] = lx; sc.lny[l] = ly; L = l + 1;
+      if (lx % 2 || ly % 2 || lx * ly <= 256) break;
+      lx /= 2; ly /= 2;
+    }
+    sc.nlev = L;
+    if (sc.lnx[L - 1] * sc.lny[L - 1] > 256) return fail(CFG_ERR_RANGE, "coarsest level too large");
+  }
+  int ndev = 0;
+  const cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(CFG_ERR_NODEV, "no CUDA device: the gas step has no CPU fallback");
+  if (device < 0 || device >= ndev) return fail(CFG_ERR_INVAL, "device index out of range");
+  device_ = device;
+  CFG_TRY(activate());
+  CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  CFG_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
+  CFG_CUDA(cudaMalloc(&d_scenes_, sizeof(SceneDesc) * n));
+  CFG_CUDA(cudaMalloc(&d_solve_, sizeof(SolveState) * n));
+  CFG_CUDA(cudaMemset(d_solve_, 0, sizeof(SolveState) * n));
+  CFG_CUDA(cudaMalloc(&d_ctl_, sizeof(SolveCtl)));
+  CFG_CUDA(cudaMallocHost(&h_ctl_pinned_, sizeof(SolveCtl)));
+  CFG_CUDA(cudaMalloc(&d_dxd_, sizeof(double) * n));
+  CFG_CUDA(cudaMalloc(&d_alpha_, sizeof(double) * n));
+  CFG_CUDA(cudaMalloc(&d_scratch_, sizeof(double) * 64));
+  for (int s = 0; s < n; s++) CFG_TRY(alloc_scene(scenes_[s]));
+  CFG_TRY(build_worklists());
+  for (int s = 0; s < n; s++) {
+    scenes_[s].desc.solve = d_solve_ + s;
+    CFG_TRY(write_params(s));
+    CFG_TRY(reset(s));
+  }
+  CFG_TRY(upload_ctl());
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+
+// One arena per scene; every array 256-byte aligned, rows pitched to 32 elements.
+int Engine::alloc_scene(Scene& sc) {
+  SceneDesc& d = sc.desc;
+  std::memset(&d, 0, sizeof d);
+  d.nx = sc.nx; d.ny = sc.ny;
+  d.pc = round_up(sc.nx, 32); d.pu = round_up(sc.nx + 1, 32);
+  d.nlev = sc.nlev; d.nray = sc.nray; d.enabled = 1;
+  const size_t C = (size_t)sc.ny * d.pc, Uf = (size_t)sc.ny * d.pu, Vf = (size_t)(sc.ny + 1) * d.pc;
+  const int nt_fr = ((sc.nx + FR_TX - 1) / FR_TX) * ((sc.ny + FR_TY - 1) / FR_TY);
+  const int nt_mg0 = ((sc.nx + MG_TX - 1) / MG_TX) * ((sc.ny + MG_TY - 1) / MG_TY);
+  d.nt_fr = nt_fr; d.nt_mg0 = nt_mg0;
+  struct Item { void** ptr; size_t bytes; };
+  std::vector<Item> items = {
+    {(void**)&d.U, Uf * 4}, {(void**)&d.U2, Uf * 4}, {(void**)&d.fx, Uf * 4},
+    {(void**)&d.V, Vf * 4}, {(void**)&d.V2, Vf * 4}, {(void**)&d.fy, Vf * 4},
+    {(void**)&d.T, C * 4}, {(void**)&d.T2, C * 4}, {(void**)&d.Tw, C * 4},
+    {(void**)&d.Y, C * 16}, {(void**)&d.Y2, C * 16}, {(void**)&d.Yw, C * 16},
+    {(void**)&d.SQ, C * 8}, {(void**)&d.cellG, C * 8},
+    {(void**)&d.acc, ACC_LEN * 4}, {(void**)&d.faceW, MAX_PIECES * 4 * 4},
+    {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4}, {(void**)&d.rad, RAD_LEN * 16},
+    {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
+    {(void**)&d.part, (size_t)std::max(nt_fr, nt_mg0) * 8},
+  };
+  double h = sc.dxd;
+  for (int l = 0; l < sc.nlev; l++) {
+    LevelDesc& L = d.lev[l];
+    L.nx = sc.lnx[l]; L.ny = sc.lny[l];
+    L.pc = round_up(L.nx, 32); L.pu = round_up(L.nx + 1, 32);
+    L.h2 = (float)(h * h);
+    h *= 2;
+    const size_t lc = (size_t)L.ny * L.pc;
+    items.push_back({(void**)&L.p, lc * 4});
+    items.push_back({(void**)&L.pb, lc * 4});
+    items.push_back({(void**)&L.rhs, lc * 4});
+    items.push_back({(void**)&L.ax, (size_t)L.ny * L.pu * 4});
+    items.push_back({(void**)&L.ay, (size_t)(L.ny + 1) * L.pc * 4});
+  }
+  size_t total = 0;
+  for (auto& it : items) total += (it.bytes + 255) / 256 * 256;
+  void* arena = nullptr;
+  cudaError_t e = cudaMalloc(&arena, total);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(scene arena)");
+  CFG_CUDA(cudaMemset(arena, 0, total));
+  sc.arena = arena; sc.arena_bytes = total;
+  size_t off = 0;
+  for (auto& it : items) { *it.ptr = (char*)arena + off; off += (it.bytes + 255) / 256 * 256; }
+  return CFG_OK;
+}
+
+int Engine::build_worklists() {
+  std::vector<Work> lists[WL_COUNT];
+  const int n = (int)scenes_.size();
+  auto tiles = [&](std::vector<Work>& v, int s, int w, int h, int TX, int TY) {
+    int t = 0;
+    for (int ty = 0; ty < (h + TY - 1) / TY; ty++)
+      for (int tx = 0; tx < (w + TX - 1) / TX; tx++) v.push_back(Work{s, tx, ty, t++});
+  };
+  for (int s = 0; s < n; s++) {
+    const Scene& sc = scenes_[s];
+    tiles(lists[WL_ADV], s, sc.nx, sc.ny, ADV_TX, ADV_TY);
+    tiles(lists[WL_DS], s, sc.nx, sc.ny, DS_TX, DS_TY);
+    tiles(lists[WL_FR], s, sc.nx, sc.ny, FR_TX, FR_TY);
+    tiles(lists[WL_PR], s, sc.nx, sc.ny, PR_TX, PR_TY);
+    tiles(lists[WL_GEO], s, sc.nx + 1, sc.ny + 1, GEO_TX, GEO_TY);
+    tiles(lists[WL_MG0], s, sc.nx, sc.ny, MG_TX, MG_TY);
+    for (int l = 0; l + 1 < sc.nlev; l++) {
+      tiles(lists[WL_MGV0 + l], s, sc.lnx[l], sc.lny[l], MG_TX, MG_TY);
+      tiles(lists[WL_MGC0 + l], s, sc.lnx[l + 1], sc.lny[l + 1], MG_TX, MG_TY);
+    }
+  }
+  for (int k = 0; k < WL_COUNT; k++) {
+    nwl_[k] = (int)lists[k].size();
+    if (nwl_[k] == 0) continue;
+    CFG_CUDA(cudaMalloc(&d_wl_[k], sizeof(Work) * lists[k].size()));
+    CFG_CUDA(cudaMemcpy(d_wl_[k], lists[k].data(), sizeof(Work) * lists[k].size(), cudaMemcpyHostToDevice));
+  }
+  return CFG_OK;
+}
+
+int Engine::upload_desc(int s) {
+  CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &scenes_[s].desc, sizeof(SceneDesc), cudaMemcpyHostToDevice, st()));
+  return CFG_OK;
+}
+int Engine::upload_descs() {
+  for (int s = 0; s < (int)scenes_.size(); s++) CFG_TRY(upload_desc(s));
+  return CFG_OK;
+}
+int Engine::upload_ctl() {
+  SolveCtl c{};
+  c.mode = mode_; c.ncycles = ncycles_; c.max_cycles = max_cycles_; c.min_cycles = 1; c.tol = tol_;
+  int en = 0;
+  for (auto& sc : scenes_) en += sc.enabled ? 1 : 0;
+  c.nscenes = en; c.nactive = en; c.any_active = 1; c.scenes_done = 0;
+  c.iter = 0; c.hard_cap = std::max(ncycles_, max_cycles_) + 1;
+  *h_ctl_pinned_ = c;
+  CFG_CUDA(cudaMemcpyAsync(d_ctl_, h_ctl_pinned_, sizeof(SolveCtl), cudaMemcpyHostToDevice, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+
+int Engine::max_sub() const {
+  int m = 1;
+  for (auto& sc : scenes_) if (sc.enabled) m = std::max(m, sc.diff_sub);
+  return m;
+}
+int Engine::max_levels() const {
+  int m = 1;
+  for (auto& sc : scenes_) m = std::max(m, sc.nlev);
+  return m;
+}
+
+// ------------------------------------------------------------------ FluidSim surface
+// reset() (js/fluid.js:162-176)
+int Engine::reset(int s) {
+  CFG_TRY(activate());
+  Scene& sc = scenes_[s];
+  SceneDesc& d = sc.desc;
+  cudaStream_t q = st();
+  const float Tamb = (float)PhysConst::Tamb;
+  auto fill = [&](float* a, int pitch, int w, int h, float v) {
+    k_fill_f32<<<dim3((w + 255) / 256, h), 256, 0, q>>>(a, pitch, w, h, v);
+  };
+  auto fill4 = [&](float4* a, int pitch, int w, int h, float4 v) {
+    k_fill_f4<<<dim3((w + 255) / 256, h), 256, 0, q>>>(a, pitch, w, h, v);
+  };
+  for (float* a : {d.T, d.T2, d.Tw}) fill(a, d.pc, sc.nx, sc.ny, Tamb);
+  const float4 y0 = make_float4(0.f, sc.host.YOamb, 0.f, 0.f);
+  for (float4* a : {d.Y, d.Y2, d.Yw}) fill4(a, d.pc, sc.nx, sc.ny, y0);
+  for (float* a : {d.U, d.U2}) fill(a, d.pu, sc.nx + 1, sc.ny, 0.f);
+  for (float* a : {d.V, d.V2}) fill(a, d.pc, sc.nx, sc.ny + 1, 0.f);
+  CFG_CUDA(cudaMemsetAsync(d.SQ, 0, (size_t)sc.ny * d.pc * 8, q));
+  CFG_CUDA(cudaMemsetAsync(d.acc, 0, ACC_LEN * 4, q));
+  CFG_CUDA(cudaMemsetAsync(d.rad, 0, RAD_LEN * 16, q));
+  for (int l = 0; l < sc.nlev; l++) {
+    CFG_CUDA(cudaMemsetAsync(d.lev[l].p, 0, (size_t)d.lev[l].ny * d.lev[l].pc * 4, q));
+    CFG_CUDA(cudaMemsetAsync(d.lev[l].pb, 0, (size_t)d.lev[l].ny * d.lev[l].pc * 4, q));
+  }
+  CFG_CUDA(cudaMemsetAsync(d.p64, 0, (size_t)sc.nx * sc.ny * 8, q));
+  CFG_CUDA(cudaGetLastError());
+  sc.time = 0;
+  return CFG_OK;
+}
+
+int Engine::set_param(int s, const char* name, double v) {
+  const int i = param_index(name);
+  if (i < 0) return fail(CFG_ERR_NOENT, std::string("unknown param ") + (name ? name : "(null)"));
+  char* base = reinterpret_cast<char*>(&scenes_[s].host) + 4 * i;
+  if (i == 0 || i == 1 || i == 26) { int32_t x = (int32_t)v; std::memcpy(base, &x, 4); }
+  else if (i == 27) { uint32_t x = (uint32_t)v; std::memcpy(base, &x, 4); }
+  else { float x = (float)v; std::memcpy(base, &x, 4); }
+  return CFG_OK;
+}
+int Engine::get_param(int s, const char* name, double* v) {
+  const int i = param_index(name);
+  if (i < 0) return fail(CFG_ERR_NOENT, std::string("unknown param ") + (name ? name : "(null)"));
+  if (!v) return fail(CFG_ERR_INVAL, "null output");
+  const char* base = reinterpret_cast<const char*>(&scenes_[s].host) + 4 * i;
+  if (i == 0 || i == 1 || i == 26) { int32_t x; std::memcpy(&x, base, 4); *v = x; }
+  else if (i == 27) { uint32_t x; std::memcpy(&x, base, 4); *v = x; }
+  else { float x; std::memcpy(&x, base, 4); *v = x; }
+  return CFG_OK;
+}
+int Engine::set_dt(int s, double dt) {
+  if (!(dt > 0)) return fail(CFG_ERR_INVAL, "dt must be positive");
+  scenes_[s].dtd = dt; scenes_[s].dt_cap = dt;
+  return CFG_OK;
+}
+
+// writeParams() (js/fluid.js:180-199)
+int Engine::write_params(int s) {
+  CFG_TRY(activate());
+  Scene& sc = scenes_[s];
+  if (sc.cfl > 0 && sc.desc.solve) {
+    // keep the device's CFL step: read it back before the upload overwrites it
+    float dt = 0.f;
+    CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
+                             cudaMemcpyDeviceToHost, st()));
+    CFG_CUDA(cudaStreamSynchronize(st()));
+    if (dt > 0.f) sc.dtd = (double)dt;
+  }
+  sc.host.nx = sc.nx; sc.host.ny = sc.ny; sc.host.dx = (float)sc.dxd; sc.host.dt = (float)sc.dtd;
+  sc.host.time = (float)sc.time; sc.host.frame = sc.frame;
+  sc.P = sc.host;
+  const double Tmax = 2200, mu = 1.716e-5 * std::pow(Tmax / 273.15, 1.5) * 383.55 / (Tmax + 110.4);
+  sc.alpha = mu / PhysConst::Pr * (double)sc.host.diffMult / (PhysConst::rhoAmb() * PhysConst::Tamb / Tmax);
+  int n = (int)std::ceil(sc.dtd / (sc.dxd * sc.dxd / (4.5 * sc.alpha)));
+  n = std::min(5, n % 2 ? n : n + 1);
+  if (n < 1) n = 1;
+  sc.diff_sub = n;
+  sc.diff_dt = (float)(sc.dtd / n);
+  SceneDesc& d = sc.desc;
+  d.P = sc.P; d.diff_sub = n; d.diff_dt = sc.diff_dt;
+  d.cfl = (float)sc.cfl; d.dt_cap = (float)sc.dt_cap; d.nray = sc.nray; d.enabled = sc.enabled ? 1 : 0;
+  CFG_TRY(upload_desc(s));
+  CFG_CUDA(cudaMemcpyAsync(d_dxd_ + s, &sc.dxd, 8, cudaMemcpyHostToDevice, st()));
+  CFG_CUDA(cudaMemcpyAsync(d_alpha_ + s, &sc.alpha, 8, cudaMemcpyHostToDevice, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  if (graph_sub_ >= 0 && max_sub() > graph_sub_) graph_dirty_ = true;
+  return CFG_OK;
+}
+int Engine::write_params_all() {
+  for (int s = 0; s < (int)scenes_.size(); s++) CFG_TRY(write_params(s));
+  return CFG_OK;
+}
+
+// uploadPieces(data, n) (js/fluid.js:201-204)
+int Engine::upload_pieces(int s, const float* data, int n) {
+  if (n < 0 || n > MAX_PIECES) return fail(CFG_ERR_INVAL, "piece count out of range");
+  if (!data && n > 0) return fail(CFG_ERR_INVAL, "null piece data");
+  CFG_TRY(activate());
+  Scene& sc = scenes_[s];
+  sc.host.nPieces = n;
+  std::memset(sc.pieces, 0, sizeof sc.pieces);
+  if (data) std::memcpy(sc.pieces, data, sizeof sc.pieces);
+  CFG_CUDA(cudaMemcpyAsync(sc.desc.pieces, sc.pieces, sizeof sc.pieces, cudaMemcpyHostToDevice, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+
+int Engine::clear_geometry(int s) {
+  CFG_TRY(activate());
+  CFG_CUDA(cudaMemsetAsync(scenes_[s].desc.faceW, 0, MAX_PIECES * 4 * 4, st()));
+  return CFG_OK;
+}
+
+int Engine::geometry(int s) {
+  CFG_TRY(activate());
+  // this scene's tiles are a contiguous run of the geometry work list
+  int off = 0;
+  for (int q = 0; q < s; q++) off += ((scenes_[q].nx + 1 + GEO_TX - 1) / GEO_TX) * ((scenes_[q].ny + 1 + GEO_TY - 1) / GEO_TY);
+  const int cnt = ((scenes_[s].nx + 1 + GEO_TX - 1) / GEO_TX) * ((scenes_[s].ny + 1 + GEO_TY - 1) / GEO_TY);
+  launch_geometry(d_scenes_, d_wl_[WL_GEO] + off, cnt, st());
+  CFG_CUDA(cudaGetLastError());
+  return CFG_OK;
+}
+int Engine::geometry_all() {
+  CFG_TRY(activate());
+  for (int s = 0; s < (int)scenes_.size(); s++) CFG_TRY(clear_geometry(s));
+  launch_geometry(d_scenes_, d_wl_[WL_GEO], nwl_[WL_GEO], st());
+  CFG_CUDA(cudaGetLastError());
+  return CFG_OK;
+}
+
+int Engine::radiation(int s) {
+  CFG_TRY(activate());
+  const Scene& sc = scenes_[s];
+  const int np = std::min(std::max(sc.desc.P.nPieces, 0), MAX_PIECES);
+  launch_radiation(d_scenes_, s, np * 4 + N_FLOOR, sc.nray, st());
+  CFG_CUDA(cudaGetLastError());
+  return CFG_OK;
+}
+int Engine::set_frame(int s, uint32_t f) { scenes_[s].frame = f; return CFG_OK; }
+int Engine::set_cfl(int s, double cfl, double dt_cap) {
+  if (cfl < 0 || !(dt_cap > 0)) return fail(CFG_ERR_INVAL, "cfl must be >= 0 and dt_cap > 0");
+  scenes_[s].cfl = cfl; scenes_[s].dt_cap = dt_cap;
+  graph_dirty_ = true;
+  return CFG_OK;
+}
+int Engine::set_nray(int s, int nray) {
+  if (nray < 1 || nray > 1024 || (nray & (nray - 1))) return fail(CFG_ERR_INVAL, "nray must be a power of two in [1, 1024]");
+  scenes_[s].nray = nray;
+  return CFG_OK;
+}
+
+// encodeReadback + afterSubmit (js/fluid.js:315-342), synchronous
+int Engine::readback(int s, int32_t* acc, float* rad, int32_t* faceW) {
+  CFG_TRY(activate());
+  const SceneDesc& d = scenes_[s].desc;
+  cudaStream_t q = st();
+  if (acc) CFG_CUDA(cudaMemcpyAsync(acc, d.acc, ACC_LEN * 4, cudaMemcpyDeviceToHost, q));
+  if (rad) CFG_CUDA(cudaMemcpyAsync(rad, d.rad, RAD_LEN * 16, cudaMemcpyDeviceToHost, q));
+  if (faceW) CFG_CUDA(cudaMemcpyAsync(faceW, d.faceW, MAX_PIECES * 16, cudaMemcpyDeviceToHost, q));
+  CFG_CUDA(cudaMemsetAsync(d.acc, 0, ACC_LEN * 4, q));
+  CFG_CUDA(cudaStreamSynchronize(q));
+  return CFG_OK;
+}
+
+int Engine::field_ptr(int s, const std::string& nm, char** base, size_t* elem, int* w, int* h, size_t* pitch) {
+  const Scene& sc = scenes_[s];
+  const SceneDesc& d = sc.desc;
+  auto set = [&](void* b, size_t e, int ww, int hh, int pe) { *base = (char*)b; *elem = e; *w = ww; *h = hh; *pitch = (size_t)pe * e; return CFG_OK; };
+  if (nm == "U") return set(d.U, 4, sc.nx + 1, sc.ny, d.pu);
+  if (nm == "U2") return set(d.U2, 4, sc.nx + 1, sc.ny, d.pu);
+  if (nm == "fx") return set(d.fx, 4, sc.nx + 1, sc.ny, d.pu);
+  if (nm == "V") return set(d.V, 4, sc.nx, sc.ny + 1, d.pc);
+  if (nm == "V2") return set(d.V2, 4, sc.nx, sc.ny + 1, d.pc);
+  if (nm == "fy") return set(d.fy, 4, sc.nx, sc.ny + 1, d.pc);
+  if (nm == "T") return set(d.T, 4, sc.nx, sc.ny, d.pc);
+  if (nm == "T2") return set(d.T2, 4, sc.nx, sc.ny, d.pc);
+  if (nm == "Y") return set(d.Y, 16, sc.nx, sc.ny, d.pc);
+  if (nm == "Y2") return set(d.Y2, 16, sc.nx, sc.ny, d.pc);
+  if (nm == "SQ") return set(d.SQ, 8, sc.nx, sc.ny, d.pc);
+  if (nm == "cellG") return set(d.cellG, 8, sc.nx, sc.ny, d.pc);
+  if (nm == "Uh" || nm == "Vh" || nm == "Th" || nm == "Yh")
+    return fail(CFG_ERR_NOENT, "field " + nm + " is not kept: the first-order advection values live in shared memory only");
+  std::string b = nm; int l = 0;
+  const size_t dot = nm.find('.');
+  if (dot != std::string::npos) { b = nm.substr(0, dot); l = std::atoi(nm.c_str() + dot + 1); }
+  if (l < 0 || l >= sc.nlev) return fail(CFG_ERR_NOENT, "no multigrid level in " + nm);
+  const LevelDesc& L = d.lev[l];
+  if (b == "p") return set(L.p, 4, L.nx, L.ny, L.pc);
+  if (b == "rhs") return set(L.rhs, 4, L.nx, L.ny, L.pc);
+  if (b == "ax") return set(L.ax, 4, L.nx + 1, L.ny, L.pu);
+  if (b == "ay") return set(L.ay, 4, L.nx, L.ny + 1, L.pc);
+  return fail(CFG_ERR_NOENT, "unknown field " + nm);
+}
+
+int Engine::field_size(int s, const char* name, size_t* count) {
+  if (!name || !count) return fail(CFG_ERR_INVAL, "null argument");
+  char* b; size_t e, p; int w, h;
+  CFG_TRY(field_ptr(s, name, &b, &e, &w, &h, &p));
+  *count = (size_t)w * h * (e / 4);
+  return CFG_OK;
+}
+
+// readBuffer(name) (js/fluid.js:345-355): dense copy of a field
+int Engine::read_field(int s, const char* name, float* out, size_t count) {
+  if (!name || !out) return fail(CFG_ERR_INVAL, "null argument");
+  CFG_TRY(activate());
+  char* b; size_t e, p; int w, h;
+  CFG_TRY(field_ptr(s, name, &b, &e, &w, &h, &p));
+  if (count != (size_t)w * h * (e / 4)) return fail(CFG_ERR_INVAL, std::string("field ") + name + ": expected " + std::to_string((size_t)w * h * (e / 4)) + " floats");
+  CFG_CUDA(cudaMemcpy2DAsync(out, (size_t)w * e, b, p, (size_t)w * e, h, cudaMemcpyDeviceToHost, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+int Engine::write_field(int s, const char* name, const float* in, size_t count) {
+  if (!name || !in) return fail(CFG_ERR_INVAL, "null argument");
+  CFG_TRY(activate());
+  char* b; size_t e, p; int w, h;
+  CFG_TRY(field_ptr(s, name, &b, &e, &w, &h, &p));
+  if (count != (size_t)w * h * (e / 4)) return fail(CFG_ERR_INVAL, std::string("field ") + name + ": expected " + std::to_string((size_t)w * h * (e / 4)) + " floats");
+  CFG_CUDA(cudaMemcpy2DAsync(b, p, in, (size_t)w * e, (size_t)w * e, h, cudaMemcpyHostToDevice, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+int Engine::read_p64(int s, double* out, size_t count) {
+  const Scene& sc = scenes_[s];
+  if (!out || count != (size_t)sc.nx * sc.ny) return fail(CFG_ERR_INVAL, "p64: expected nx*ny doubles");
+  CFG_TRY(activate());
+  CFG_CUDA(cudaMemcpyAsync(out, sc.desc.p64, count * 8, cudaMemcpyDeviceToHost, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+
+int Engine::info(int s, cfg_info* o) {
+  if (!o) return fail(CFG_ERR_INVAL, "null output");
+  CFG_TRY(activate());
+  const Scene& sc = scenes_[s];
+  SolveState ss{};
+  float dt = 0.f;
+  CFG_CUDA(cudaMemcpyAsync(&ss, d_solve_ + s, sizeof ss, cudaMemcpyDeviceToHost, st()));
+  CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
+                           cudaMemcpyDeviceToHost, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  std::memset(o, 0, sizeof *o);
+  o->nx = sc.nx; o->ny = sc.ny; o->levels = sc.nlev; o->diff_sub = sc.diff_sub;
+  o->dx = sc.dxd; o->dt = sc.cfl > 0 ? (double)dt : sc.dtd; o->height = sc.dxd * sc.ny; o->time = sc.time;
+  o->frame = sc.frame; o->last_cycles = ss.cycles; o->last_rel = ss.rel;
+  for (int l = 0; l < MAX_LEVELS; l++) { o->level_nx[l] = l < sc.nlev ? sc.lnx[l] : 0; o->level_ny[l] = l < sc.nlev ? sc.lny[l] : 0; }
+  return CFG_OK;
+}
+
+int Engine::pressure_residual(int s, double* rel) {
+  if (!rel) return fail(CFG_ERR_INVAL, "null output");
+  CFG_TRY(activate());
+  launch_residual_norms(d_scenes_, s, d_scratch_, st());
+  double o[2];
+  CFG_CUDA(cudaMemcpyAsync(o, d_scratch_, 16, cudaMemcpyDeviceToHost, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  *rel = o[1] > 0 ? std::sqrt(o[0] / o[1]) : 0.0;
+  return CFG_OK;
+}
+int Engine::budgets(int s, double* out) {
+  if (!out) return fail(CFG_ERR_INVAL, "null output");
+  CFG_TRY(activate());
+  launch_budgets(d_scenes_, s, d_scratch_, st());
+  CFG_CUDA(cudaMemcpyAsync(out, d_scratch_, 64, cudaMemcpyDeviceToHost, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+int Engine::set_active(int s, bool on) {
+  CFG_TRY(activate());
+  scenes_[s].enabled = on;
+  scenes_[s].desc.enabled = on ? 1 : 0;
+  const int v = on ? 1 : 0;
+  CFG_CUDA(cudaMemcpyAsync((char*)(d_scenes_ + s) + offsetof(SceneDesc, enabled), &v, 4, cudaMemcpyHostToDevice, st()));
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return upload_ctl();
+}
+
+// ------------------------------------------------------------------ the step
+int Engine::set_solver(int mode, int ncycles, double tol, int max_cycles) {
+  if (mode < CFG_SOLVE_FIXED || mode > CFG_SOLVE_FP64) return fail(CFG_ERR_INVAL, "unknown solver mode");
+  if (mode == CFG_SOLVE_FIXED && ncycles < 1) return fail(CFG_ERR_INVAL, "ncycles must be >= 1");
+  if (mode != CFG_SOLVE_FIXED && (!(tol > 0) || max_cycles < 1)) return fail(CFG_ERR_INVAL, "tol must be > 0 and max_cycles >= 1");
+  CFG_TRY(activate());
+  mode_ = mode; ncycles_ = ncycles; tol_ = tol; max_cycles_ = max_cycles;
+  graph_dirty_ = true;
+  return upload_ctl();
+}
+
+void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_cond) {
+  const bool fp64 = any_fp64();
+  launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s); launches_++;
+  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, s); launches_++;
+  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); launches_++;
+  for (int l = FR_KMAX; l + 1 < max_levels(); l++)
+    if (nwl_[WL_MGC0 + l] > 0) { launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s); launches_++; }
+  if (fp64) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s); launches_++; }
+  // the loop's cycle counter starts at zero in every step
+  cudaMemsetAsync(&d_ctl_->iter, 0, sizeof(int), s);
+  (void)h; (void)use_cond;
+}
+
+// FluidSim.vcycle (js/fluid.js:294-312), nu = 2
+void Engine::enqueue_vcycle(cudaStream_t s) {
+  const int L = max_levels();
+  for (int l = 0; l + 1 < L; l++) {
+    const int wv = WL_MGV0 + l;
+    if (nwl_[wv] == 0) continue;
+    for (int k = 0; k < 2; k++) {
+      launch_relax(d_scenes_, d_wl_[wv], nwl_[wv], l, 0, s);
+      launch_relax(d_scenes_, d_wl_[wv], nwl_[wv], l, 1, s);
+      vcycle_launches_ += 2;
+    }
+    launch_restrict_res(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
+    vcycle_launches_++;
+  }
+  launch_coarsest(d_scenes_, nscenes(), s);
+  vcycle_launches_++;
+  for (int l = L - 2; l >= 0; l--) {
+    const int wv = WL_MGV0 + l;
+    if (nwl_[wv] == 0) continue;
+    launch_prolong(d_scenes_, d_wl_[wv], nwl_[wv], l, s);
+    vcycle_launches_++;
+    for (int k = 0; k < 2; k++) {
+      launch_relax(d_scenes_, d_wl_[wv], nwl_[wv], l, 1, s);
+      launch_relax(d_scenes_, d_wl_[wv], nwl_[wv], l, 0, s);
+      vcycle_launches_ += 2;
+    }
+  }
+}
+
+void Engine::enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond) {
+  if (any_fp64()) {
+    launch_accum64(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], s);
+    launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, s);
+    vcycle_launches_ += 2;
+  } else {
+    launch_resnorm(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
+    vcycle_launches_++;
+  }
+  launch_loop_guard(d_ctl_, h, use_cond, s);
+  vcycle_launches_++;
+}
+
+void Engine::enqueue_post_solve(cudaStream_t s) {
+  launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], any_fp64(), s); launches_++;
+  bool cfl = false;
+  for (auto& sc : scenes_) cfl = cfl || sc.cfl > 0;
+  if (cfl) { launch_cfl_update(d_scenes_, nscenes(), d_dxd_, d_alpha_, s); launches_++; }
+}
+
+void Engine::enqueue_bnorm(cudaStream_t s) {
+  launch_bnorm(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, any_fp64(), s);
+}
+
+// Pressure loop driven from the host (launches outside a graph): the device
+// decides per cycle and mirrors the decision into SolveCtl::any_active.
+int Engine::host_pressure_loop() {
+  cudaStream_t s = st();
+  int guard = 0;
+  if (any_fp64()) {
+    launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s);
+  }
+  CFG_CUDA(cudaMemsetAsync(&d_ctl_->iter, 0, sizeof(int), s));
+  CFG_CUDA(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s));
+  CFG_CUDA(cudaStreamSynchronize(s));
+  int any = any_fp64() ? h_ctl_pinned_->any_active : 1;
+  while (any) {
+    enqueue_vcycle(s);
+    enqueue_cycle_tail(s, 0ull, 0);
+    CFG_CUDA(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s));
+    CFG_CUDA(cudaStreamSynchronize(s));
+    any = h_ctl_pinned_->any_active;
+    if (++guard > std::max(ncycles_, max_cycles_) + 2) return fail(CFG_ERR_TIMEDOUT, "pressure loop did not terminate");
+  }
+  return CFG_OK;
+}
+
+void Engine::destroy_graph() {
+  if (exec_) { cudaGraphExecDestroy(exec_); exec_ = nullptr; }
+  if (graph_) { cudaGraphDestroy(graph_); graph_ = nullptr; }
+}
+
+int Engine::ensure_graph() {
+  if (!graph_dirty_ && exec_ && graph_sub_ >= max_sub()) return CFG_OK;
+  destroy_graph();
+  cudaStream_t s = stream_;
+  CFG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaStreamCaptureStatus status;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  auto abort_capture = [&](cudaError_t e, const char* what) {
+    cudaGraph_t tmp = nullptr;
+    cudaStreamEndCapture(s, &tmp);
+    if (tmp) cudaGraphDestroy(tmp);
+    return cuda_fail(e, what);
+  };
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &status, nullptr, &g, nullptr, nullptr);
+  if (e != cudaSuccess) return abort_capture(e, "cudaStreamGetCaptureInfo");
+  cudaGraphConditionalHandle h = 0;
+  e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return abort_capture(e, "cudaGraphConditionalHandleCreate");
+  launches_ = 0;
+  enqueue_pre_solve(s, (unsigned long long)h, 1);
+  e = cudaStreamGetCaptureInfo(s, &status, nullptr, &g, &deps, &ndeps);
+  if (e != cudaSuccess) return abort_capture(e, "cudaStreamGetCaptureInfo");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
+  if (e != cudaSuccess) return abort_capture(e, "cudaGraphAddNode(while)");
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
+  if (e != cudaSuccess) return abort_capture(e, "cudaStreamUpdateCaptureDependencies");
+  e = cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return abort_capture(e, "cudaStreamBeginCaptureToGraph");
+  vcycle_launches_ = 0;
+  enqueue_vcycle(body_stream_);
+  enqueue_cycle_tail(body_stream_, (unsigned long long)h, 1);
+  e = cudaStreamEndCapture(body_stream_, &body);
+  if (e != cudaSuccess) return abort_capture(e, "cudaStreamEndCapture(body)");
+  enqueue_post_solve(s);
+  e = cudaStreamEndCapture(s, &g);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  graph_ = g;
+  e = cudaGraphInstantiate(&exec_, graph_, 0);
+  if (e != cudaSuccess) { destroy_graph(); return cuda_fail(e, "cudaGraphInstantiate"); }
+  graph_dirty_ = false;
+  graph_sub_ = max_sub();
+  return CFG_OK;
+}
+
+int Engine::step(int nsteps) {
+  if (nsteps < 0) return fail(CFG_ERR_INVAL, "negative step count");
+  CFG_TRY(activate());
+  for (int k = 0; k < nsteps; k++) {
+    if (use_graphs_) {
+      CFG_TRY(ensure_graph());
+      CFG_CUDA(cudaGraphLaunch(exec_, st()));
+    } else {
+      launches_ = 0; vcycle_launches_ = 0;
+      enqueue_pre_solve(st(), 0ull, 0);
+      CFG_CUDA(cudaGetLastError());
+      CFG_TRY(host_pressure_loop());
+      enqueue_post_solve(st());
+      CFG_CUDA(cudaGetLastError());
+    }
+    for (auto& sc : scenes_) if (sc.enabled) sc.time += sc.dtd;
+  }
+  CFG_CUDA(cudaGetLastError());
+  return CFG_OK;
+}
+
+int Engine::synchronize() {
+  CFG_TRY(activate());
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  // per-step launch count: kernels outside the loop + kernels per cycle x cycles (scene 0)
+  SolveState ss{};
+  CFG_CUDA(cudaMemcpy(&ss, d_solve_, sizeof ss, cudaMemcpyDeviceToHost));
+  launches_per_step_ = launches_ + vcycle_launches_ * std::max(ss.cycles, 1);
+  return CFG_OK;
+}
+
+int Engine::set_stream(cudaStream_t s) {
+  CFG_TRY(activate());
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  user_stream_ = s;
+  return CFG_OK;
+}
+
+// encodeStepProfiled (js/fluid.js:256-292): the unfused stage kernels between events
+int Engine::step_profiled(float* ms) {
+  if (!ms) return fail(CFG_ERR_INVAL, "null output");
+  CFG_TRY(activate());
+  cudaStream_t s = st();
+  cudaEvent_t ev[8];
+  for (auto& e : ev) CFG_CUDA(cudaEventCreate(&e));
+  CFG_CUDA(cudaEventRecord(ev[0], s));
+  launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s);
+  CFG_CUDA(cudaEventRecord(ev[1], s));
+  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), false, true, s);
+  CFG_CUDA(cudaEventRecord(ev[2], s));
+  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], 1, true, false, s);
+  CFG_CUDA(cudaEventRecord(ev[3], s));
+  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, false, any_fp64(), s);
+  CFG_CUDA(cudaEventRecord(ev[4], s));
+  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, false, true, any_fp64(), s);
+  for (int l = FR_KMAX; l + 1 < max_levels(); l++)
+    launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
+  CFG_CUDA(cudaEventRecord(ev[5], s));
+  CFG_TRY(host_pressure_loop());
+  CFG_CUDA(cudaEventRecord(ev[6], s));
+  enqueue_post_solve(s);
+  CFG_CUDA(cudaEventRecord(ev[7], s));
+  CFG_CUDA(cudaEventSynchronize(ev[7]));
+  for (int k = 0; k < 7; k++) CFG_CUDA(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (auto& sc : scenes_) if (sc.enabled) sc.time += sc.dtd;
+  return CFG_OK;
+}
+
+int Engine::run_stage(const char* stage) {
+  if (!stage) return fail(CFG_ERR_INVAL, "null stage");
+  CFG_TRY(activate());
+  const std::string st_(stage);
+  cudaStream_t s = st();
+  const bool fp64 = any_fp64();
+  if (st_ == "advect") launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s);
+  else if (st_ == "diffuse") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), false, true, s);
+  else if (st_ == "sources") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], 1, true, false, s);
+  else if (st_ == "diffuse_sources") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, s);
+  else if (st_ == "forces") launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, false, fp64, s);
+  else if (st_ == "coef_rhs") {
+    launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, false, true, fp64, s);
+    for (int l = FR_KMAX; l + 1 < max_levels(); l++)
+      launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
+  } else if (st_ == "pressure") {
+    enqueue_bnorm(s);
+    CFG_TRY(host_pressure_loop());
+  } else if (st_ == "project") launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s);
+  else if (st_ == "update_dt") launch_cfl_update(d_scenes_, nscenes(), d_dxd_, d_alpha_, s);
+  else return fail(CFG_ERR_NOENT, "unknown stage " + st_);
+  CFG_CUDA(cudaGetLastError());
+  CFG_CUDA(cudaStreamSynchronize(s));
+  return CFG_OK;
+}
+
+int Engine::vcycle_once(int nu) {
+  if (nu != 2) return fail(CFG_ERR_INVAL, "only V(2,2) cycles are provided (js/fluid.js:294 default nu = 2)");
+  CFG_TRY(activate());
+  cudaStream_t s = st();
+  enqueue_bnorm(s);   // arms every scene (active = 1)
+  enqueue_vcycle(s);
+  CFG_CUDA(cudaGetLastError());
+  CFG_CUDA(cudaStreamSynchronize(s));
+  return CFG_OK;
+}
+
+}  // namespace cfg

@@ -1,0 +1,151 @@
+// Host side of the B200 gas step: the FluidSim state of each scene, the batch
+// engine that owns device memory, work lists, streams and the CUDA graph of one
+// step, and the status/error plumbing of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "gas_dev.cuh"
+
+namespace cfg {
+
+void set_error(const std::string& msg);
+const std::string& last_error();
+
+// Status helper: CFG_OK or a negative CFG_ERR_*, with the message recorded.
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define CFG_CUDA(call)                                             \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return ::cfg::cuda_fail(e_, #call);     \
+  } while (0)
+#define CFG_TRY(call)                 \
+  do {                                \
+    int rc_ = (call);                 \
+    if (rc_ != CFG_OK) return rc_;    \
+  } while (0)
+
+// js/config.js:12-47 constants used on the host
+struct PhysConst {
+  static constexpr double Tamb = 293.15, p0 = 101325, Wmix = 0.0289, R = 8.314462, Pr = 0.7;
+  static double rhoAmb() { return p0 * Wmix / (R * Tamb); }
+};
+
+void default_params(cfg_params* p);
+int param_index(const char* name);   // -1 if unknown
+
+// One scene: FluidSim's host fields (js/fluid.js:27-47) and its device arrays.
+struct Scene {
+  int nx = 0, ny = 0, nlev = 0;
+  double width = 0, dxd = 0, dtd = 0, time = 0;
+  uint32_t frame = 0;
+  double cfl = 0, dt_cap = 0;
+  int nray = 64;
+  cfg_params host{};             // FluidSim.params (applied by write_params)
+  cfg_params P{};                // the uploaded uniform
+  float pieces[MAX_PIECES * PIECE_FLOATS] = {};
+  int diff_sub = 1;
+  float diff_dt = 0;
+  double alpha = 0;              // alpha(2200 K) of the diffusion sub-step rule
+  int lnx[MAX_LEVELS] = {}, lny[MAX_LEVELS] = {};
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  SceneDesc desc{};              // host mirror of the device descriptor
+  bool enabled = true;
+};
+
+enum WL { WL_ADV = 0, WL_DS, WL_FR, WL_PR, WL_GEO, WL_MG0, WL_MGV0, WL_MGC0 = WL_MGV0 + MAX_LEVELS,
+          WL_COUNT = WL_MGC0 + MAX_LEVELS };
+
+class Engine {
+ public:
+  ~Engine();
+  int init(int device, int nscenes, const int* nx, const int* ny, const double* width, const double* dt);
+
+  // per-scene FluidSim surface
+  int reset(int s);
+  int set_param(int s, const char* name, double v);
+  int get_param(int s, const char* name, double* v);
+  int set_dt(int s, double dt);
+  int write_params(int s);
+  int upload_pieces(int s, const float* data, int n);
+  int clear_geometry(int s);
+  int geometry(int s);
+  int radiation(int s);
+  int set_frame(int s, uint32_t f);
+  int set_cfl(int s, double cfl, double dt_cap);
+  int set_nray(int s, int nray);
+  int readback(int s, int32_t* acc, float* rad, int32_t* faceW);
+  int field_size(int s, const char* name, size_t* count);
+  int read_field(int s, const char* name, float* out, size_t count);
+  int write_field(int s, const char* name, const float* in, size_t count);
+  int read_p64(int s, double* out, size_t count);
+  int info(int s, cfg_info* out);
+  int pressure_residual(int s, double* rel);
+  int budgets(int s, double* out);
+  int set_active(int s, bool on);
+
+  // whole-batch operations
+  int set_solver(int mode, int ncycles, double tol, int max_cycles);
+  int step(int nsteps);
+  int step_profiled(float* stage_ms);
+  int run_stage(const char* stage);
+  int vcycle_once(int nu);
+  int set_stream(cudaStream_t s);
+  int synchronize();
+  int set_graphs(bool on) { use_graphs_ = on; graph_dirty_ = true; return CFG_OK; }
+  int launches_per_step() const { return launches_per_step_; }
+  int write_params_all();
+  int geometry_all();
+  int nscenes() const { return (int)scenes_.size(); }
+
+ private:
+  int alloc_scene(Scene& sc);
+  int upload_desc(int s);
+  int upload_descs();
+  int upload_ctl();
+  int build_worklists();
+  int ensure_graph();
+  void destroy_graph();
+  cudaStream_t st() const { return user_stream_ ? user_stream_ : stream_; }
+  int activate() const;
+  int field_ptr(int s, const std::string& name, char** base, size_t* elem, int* width, int* height, size_t* pitch);
+  int max_sub() const;
+  int max_levels() const;
+  bool any_fp64() const { return mode_ == CFG_SOLVE_FP64; }
+
+  // step pieces; launches counted in launches_
+  void enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_cond);
+  void enqueue_vcycle(cudaStream_t s);
+  void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
+  void enqueue_post_solve(cudaStream_t s);
+  int host_pressure_loop();
+  void enqueue_bnorm(cudaStream_t s);
+
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr, user_stream_ = nullptr, body_stream_ = nullptr;
+  std::vector<Scene> scenes_;
+  SceneDesc* d_scenes_ = nullptr;
+  SolveState* d_solve_ = nullptr;
+  SolveCtl* d_ctl_ = nullptr;
+  SolveCtl* h_ctl_pinned_ = nullptr;
+  double* d_dxd_ = nullptr;
+  double* d_alpha_ = nullptr;
+  double* d_scratch_ = nullptr;   // small FP64 outputs (budgets, norms)
+  Work* d_wl_[WL_COUNT] = {};
+  int nwl_[WL_COUNT] = {};
+  int mode_ = CFG_SOLVE_FIXED, ncycles_ = 1, max_cycles_ = 50;
+  double tol_ = 1e-6;
+  bool use_graphs_ = true, graph_dirty_ = true;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  int graph_sub_ = -1;
+  int launches_ = 0, launches_per_step_ = 0;
+  int vcycle_launches_ = 0;
+};
+
+}  // namespace cfg

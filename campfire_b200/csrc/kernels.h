@@ -1,0 +1,59 @@
+// Kernel launchers of the B200 gas step (host-callable, stream-ordered).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "gas_dev.cuh"
+
+namespace cfg {
+
+// Tile shapes (cells) of the level-0 kernels. Tiles are aligned to multiples of
+// 8 cells so the 8x8 blocks of the heat-release reduction match the WGSL
+// workgroups of sources.wgsl:34 exactly.
+constexpr int ADV_TX = 32, ADV_TY = 16, ADV_H = 2;   // advection (halo for |displacement| < 2 cells)
+constexpr int DS_TX = 32, DS_TY = 8;                 // diffusion + sources
+constexpr int FR_TX = 32, FR_TY = 16;                // forces + coef + rhs0 (+ coefficient hierarchy)
+constexpr int FR_KMAX = 4;                           // coarse coefficient levels built inside FR tiles
+constexpr int MG_TX = 32, MG_TY = 8;                 // single-pass multigrid kernels
+constexpr int PR_TX = 32, PR_TY = 8;                 // projection
+constexpr int GEO_TX = 32, GEO_TY = 8;               // geometry
+
+// Work-list kinds (tiles per scene are built by the engine)
+enum WorkKind { WK_ADV, WK_DS, WK_FR, WK_PR, WK_GEO, WK_MG0 };
+
+void launch_advect(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
+// diffusion sub-steps (diff_sub of each scene) fused with the sources pass
+void launch_diffuse_sources(const SceneDesc* scenes, const Work* work, int ntiles, int max_sub,
+                            bool with_sources, bool with_diffusion, cudaStream_t st);
+// forces (+ coef + rhs0 + coefficient levels 1..FR_KMAX + ||rhs|| reduction)
+void launch_forces(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool forces,
+                   bool coef_rhs, bool fp64, cudaStream_t st);
+// coefficient restriction of level l -> l+1 for levels the FR tiles did not build
+void launch_coef_restrict(const SceneDesc* scenes, const Work* work, int ntiles, int level, cudaStream_t st);
+// single-pass multigrid (pressure.wgsl:87-129)
+void launch_relax(const SceneDesc* scenes, const Work* work, int ntiles, int level, int color, cudaStream_t st);
+void launch_restrict_res(const SceneDesc* scenes, const Work* work, int ntiles, int level, cudaStream_t st);
+void launch_prolong(const SceneDesc* scenes, const Work* work, int ntiles, int level, cudaStream_t st);
+void launch_coarsest(const SceneDesc* scenes, int nscenes, cudaStream_t st);
+// level-0 residual norm + per-scene loop decision
+void launch_resnorm(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
+                    cudaStream_t st);
+// FP64 defect: r64 = rhs64 - A p64, rhs0 = f32(r64), p0 = 0, ||r64|| + loop decision
+void launch_defect64(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
+                     int first, cudaStream_t st);
+// end of a loop iteration: count it and set the WHILE node's condition (bounded by SolveCtl::hard_cap)
+void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_cond, cudaStream_t st);
+// ||rhs||^2 (FP64 mode: ||rhs64||^2) of level 0; arms the pressure loop
+void launch_bnorm(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool fp64, cudaStream_t st);
+// FP64: p64 += p0
+void launch_accum64(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
+// projection (+ max|u| and the CFL step for the next step)
+void launch_project(const SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st);
+void launch_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, const double* alpha, cudaStream_t st);
+void launch_geometry(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
+void launch_radiation(const SceneDesc* scenes, int scene, int ntargets, int nray, cudaStream_t st);
+// FP64 budgets of one scene into out[8] (device)
+void launch_budgets(const SceneDesc* scenes, int scene, double* out, cudaStream_t st);
+// ||r||2 and ||rhs||2 of level 0 of one scene into out[2] (device, FP64)
+void launch_residual_norms(const SceneDesc* scenes, int scene, double* out, cudaStream_t st);
+
+}  // namespace cfg

@@ -1,0 +1,69 @@
+// Deterministic FP64 block reductions and the per-scene "last CTA finishes"
+// protocol used by the norm reductions of the pressure solve.
+//
+// A reduction over the tiles of one scene: every CTA writes its partial to
+// scene.part[tile], fences, and bumps scene.solve->counter; the CTA that sees
+// the count reach the scene's tile count sums the partials in tile order (so
+// the total does not depend on CTA scheduling) and resets the counter.
+#pragma once
+#include "gas_dev.cuh"
+
+namespace cfg {
+
+// Sum over the block; the result is valid in thread 0. blockDim.x must be a
+// multiple of 32 and at most 1024. Fixed combination order -> deterministic.
+__device__ __forceinline__ double block_sum(double v, double* sh /* >= 32 doubles */) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (warp == 0) {
+    t = lane < nw ? sh[lane] : 0.0;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  return t;
+}
+
+__device__ __forceinline__ float block_max(float v, float* sh /* >= 32 floats */) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  float t = 0.f;
+  if (warp == 0) {
+    t = lane < nw ? sh[lane] : 0.f;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t = fmaxf(t, __shfl_down_sync(0xffffffffu, t, o));
+  }
+  return t;
+}
+
+// Publish this CTA's partial; returns true (in every thread) in the CTA that
+// completes the scene's reduction, which then holds the total in *total.
+__device__ __forceinline__ bool scene_reduce(const SceneDesc& S, int tile, int ntiles, double partial,
+                                             double* sh, double* total) {
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+    S.part[tile] = partial;
+    __threadfence();
+    const unsigned prev = atomicAdd(&S.solve->counter, 1u);
+    s_last = (prev == (unsigned)ntiles - 1u) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  double v = 0.0;
+  // each thread sums a fixed strided subset in order, then the fixed block tree
+  for (int k = threadIdx.x; k < ntiles; k += blockDim.x) v += __ldcg(S.part + k);
+  const double t = block_sum(v, sh);
+  if (threadIdx.x == 0) { *total = t; S.solve->counter = 0u; }
+  return true;
+}
+
+}  // namespace cfg

@@ -1,0 +1,328 @@
+"""FluidSim: the reference's gas-solver host interface over the B200 C ABI.
+
+Mirrors `class FluidSim` of js/fluid.js:26-356 (names, argument meaning and
+error behaviour) so a caller of the reference finds the same surface:
+
+    sim = FluidSim(device=0, mode={"nx": 224, "ny": 320, "dt": 0.003})
+    sim.init()                      # allocates; raises on 'coarsest level too large'
+    sim.setParam("heaterT", 1200)   # applied by the next writeParams()
+    sim.writeParams()
+    sim.uploadPieces(pieces, n)     # Float32Array(64*20) packing of js/main.js:196-199
+    sim.clearGeometry(); sim.encodeGeometry()
+    for _ in range(n): sim.encodeStep()
+    sim.encodeRadiation()
+    out = sim.readback()            # {acc, rad, faceW}, then acc is cleared
+    T = sim.readBuffer("T")
+
+WebGPU's encoder/pass arguments have no counterpart: each call enqueues CUDA
+work on the handle's stream in call order. Extensions beyond the reference
+(solver modes, CFL step, FP64 budgets, batches) are snake_case methods.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import CampfireError, CfgInfo, CfgParams, check
+
+SCENE_WIDTH = 0.7   # js/config.js:3
+STAGES = ("advect", "diffuse", "sources", "forces", "coef/rhs", "vcycle", "project")
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class _SceneOps:
+    """Per-scene FluidSim surface shared by FluidSim and batch scene views."""
+
+    _h: Optional[int]
+
+    # -- FluidSim methods
+    def reset(self):
+        check(_lib.lib().cfg_reset(self._h))
+        self.time = 0.0
+
+    def setParam(self, k: str, v: float):
+        check(_lib.lib().cfg_set_param(self._h, k.encode(), float(v)))
+
+    def getParam(self, k: str) -> float:
+        v = ctypes.c_double()
+        check(_lib.lib().cfg_get_param(self._h, k.encode(), ctypes.byref(v)))
+        return v.value
+
+    @property
+    def params(self) -> dict:
+        return {n: self.getParam(n) for n, _ in _lib.PARAM_FIELDS}
+
+    def writeParams(self):
+        check(_lib.lib().cfg_write_params(self._h))
+
+    def uploadPieces(self, data, n: int):
+        a = np.zeros(_lib.MAX_PIECES * _lib.PIECE_FLOATS, np.float32)
+        d = np.asarray(data, np.float32).ravel()
+        a[: min(d.size, a.size)] = d[: a.size]
+        check(_lib.lib().cfg_upload_pieces(self._h, _fp(a), int(n)))
+
+    def clearGeometry(self, encoder=None):
+        check(_lib.lib().cfg_clear_geometry(self._h))
+
+    def encodeGeometry(self, pass_=None):
+        check(_lib.lib().cfg_geometry(self._h))
+
+    def encodeRadiation(self, pass_=None):
+        check(_lib.lib().cfg_radiation(self._h))
+
+    def readback(self) -> dict:
+        """encodeReadback + afterSubmit: {acc: int32[528], rad: float32[320*4], faceW: int32[256]}."""
+        acc = np.zeros(_lib.ACC_LEN, np.int32)
+        rad = np.zeros(_lib.RAD_LEN * 4, np.float32)
+        fw = np.zeros(_lib.MAX_PIECES * 4, np.int32)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        check(_lib.lib().cfg_readback(self._h, acc.ctypes.data_as(i32p), _fp(rad), fw.ctypes.data_as(i32p)))
+        return {"acc": acc, "rad": rad, "faceW": fw}
+
+    def field_size(self, name: str) -> int:
+        n = ctypes.c_size_t()
+        check(_lib.lib().cfg_field_size(self._h, name.encode(), ctypes.byref(n)))
+        return n.value
+
+    def readBuffer(self, name: str) -> np.ndarray:
+        """Float32 copy of a field in the reference's dense layout (js/fluid.js:345-355)."""
+        n = self.field_size(name)
+        out = np.empty(n, np.float32)
+        check(_lib.lib().cfg_read_field(self._h, name.encode(), _fp(out), n))
+        return out
+
+    def writeBuffer(self, name: str, data) -> None:
+        a = np.ascontiguousarray(np.asarray(data, np.float32).ravel())
+        check(_lib.lib().cfg_write_field(self._h, name.encode(), _fp(a), a.size))
+
+    def read_p64(self) -> np.ndarray:
+        out = np.empty(self.nx * self.ny, np.float64)
+        check(_lib.lib().cfg_read_p64(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), out.size))
+        return out
+
+    def info(self) -> dict:
+        i = CfgInfo()
+        check(_lib.lib().cfg_get_info(self._h, ctypes.byref(i)))
+        return {"nx": i.nx, "ny": i.ny, "levels": i.levels, "diffSub": i.diff_sub, "dx": i.dx, "dt": i.dt,
+                "height": i.height, "time": i.time, "frame": i.frame, "last_cycles": i.last_cycles,
+                "last_rel": i.last_rel,
+                "level_dims": [(i.level_nx[l], i.level_ny[l]) for l in range(i.levels)]}
+
+    @property
+    def diffSub(self) -> int:
+        return self.info()["diffSub"]
+
+    @property
+    def levels(self) -> list:
+        return [{"nx": a, "ny": b} for a, b in self.info()["level_dims"]]
+
+    def setFrame(self, f: int):
+        self.frame = int(f)
+        check(_lib.lib().cfg_set_frame(self._h, int(f)))
+
+    # -- extensions
+    def set_dt(self, dt: float):
+        check(_lib.lib().cfg_set_dt(self._h, float(dt)))
+        self.dt = float(dt)
+
+    def set_cfl(self, cfl: float, dt_cap: float):
+        check(_lib.lib().cfg_set_cfl(self._h, float(cfl), float(dt_cap)))
+
+    def set_nray(self, n: int):
+        check(_lib.lib().cfg_set_nray(self._h, int(n)))
+
+    def pressure_residual(self) -> float:
+        v = ctypes.c_double()
+        check(_lib.lib().cfg_pressure_residual(self._h, ctypes.byref(v)))
+        return v.value
+
+    def budgets(self) -> np.ndarray:
+        o = np.zeros(8, np.float64)
+        check(_lib.lib().cfg_budgets(self._h, o.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return o
+
+
+class FluidSim(_SceneOps):
+    """new FluidSim(device, mode) + init() (js/fluid.js:27-160) on a CUDA device."""
+
+    def __init__(self, device: int = 0, mode: Optional[dict] = None, width: float = SCENE_WIDTH, **kw):
+        mode = dict(mode or {}, **kw)
+        self.device, self.nx, self.ny, self.dt = device, int(mode["nx"]), int(mode["ny"]), float(mode["dt"])
+        self.dx = width / self.nx
+        self.height = self.dx * self.ny
+        self.width = width
+        self.time = 0.0
+        self.frame = 0
+        self._h = None
+
+    def init(self):
+        h = ctypes.c_void_p()
+        check(_lib.lib().cfg_create(self.nx, self.ny, self.width, self.dt, self.device, ctypes.byref(h)))
+        self._h = h.value
+        return self
+
+    def close(self):
+        if self._h:
+            _lib.lib().cfg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def encodeStep(self, pass_=None, n: int = 1):
+        """One gas step (js/fluid.js:225-253); time += dt."""
+        check(_lib.lib().cfg_step(self._h, int(n)))
+        self.time += n * self.dt
+
+    def step(self, n: int = 1):
+        self.encodeStep(n=n)
+
+    def encodeStepProfiled(self) -> dict:
+        """One step with per-stage device ms, names of js/fluid.js:291."""
+        ms = np.zeros(7, np.float32)
+        check(_lib.lib().cfg_step_profiled(self._h, _fp(ms)))
+        self.time += self.dt
+        return dict(zip(STAGES, ms.tolist()))
+
+    def vcycle(self, pass_=None, nu: int = 2):
+        check(_lib.lib().cfg_vcycle(self._h, int(nu)))
+
+    def run_stage(self, name: str):
+        check(_lib.lib().cfg_run_stage(self._h, name.encode()))
+
+    def set_solver(self, mode: int = _lib.SOLVE_FIXED, ncycles: int = 1, tol: float = 1e-6, max_cycles: int = 50):
+        check(_lib.lib().cfg_set_solver(self._h, mode, ncycles, tol, max_cycles))
+
+    def set_stream(self, stream_ptr: int):
+        check(_lib.lib().cfg_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        check(_lib.lib().cfg_synchronize(self._h))
+
+    def set_graphs(self, on: bool):
+        check(_lib.lib().cfg_set_graphs(self._h, 1 if on else 0))
+
+    def launch_count(self) -> int:
+        n = ctypes.c_int()
+        check(_lib.lib().cfg_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+
+class _SceneView(_SceneOps):
+    def __init__(self, h, nx, ny, width):
+        self._h, self.nx, self.ny, self.width = h, nx, ny, width
+        self.dx = width / nx
+        self.time, self.frame = 0.0, 0
+
+
+class Batch:
+    """Many independent scenes of uneven size stepped together (one launch per kernel for all)."""
+
+    def __init__(self, dims, width=0.8, dts=None, device: int = 0):
+        n = len(dims)
+        nx = (ctypes.c_int * n)(*[d[0] for d in dims])
+        ny = (ctypes.c_int * n)(*[d[1] for d in dims])
+        widths = [width] * n if np.isscalar(width) else list(width)
+        dts = dts or [0.002] * n
+        wa = (ctypes.c_double * n)(*widths)
+        da = (ctypes.c_double * n)(*dts)
+        h = ctypes.c_void_p()
+        check(_lib.lib().cfg_batch_create(n, nx, ny, wa, da, device, ctypes.byref(h)))
+        self._h = h.value
+        self.scenes = []
+        for i in range(n):
+            v = ctypes.c_void_p()
+            check(_lib.lib().cfg_batch_scene(self._h, i, ctypes.byref(v)))
+            self.scenes.append(_SceneView(v.value, dims[i][0], dims[i][1], widths[i]))
+
+    def close(self):
+        if self._h:
+            _lib.lib().cfg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        check(_lib.lib().cfg_batch_step(self._h, int(n)))
+
+    def set_solver(self, mode=_lib.SOLVE_FIXED, ncycles=1, tol=1e-6, max_cycles=50):
+        check(_lib.lib().cfg_batch_set_solver(self._h, mode, ncycles, tol, max_cycles))
+
+    def set_active(self, i: int, on: bool):
+        check(_lib.lib().cfg_batch_set_active(self._h, i, 1 if on else 0))
+
+    def set_stream(self, stream_ptr: int):
+        check(_lib.lib().cfg_batch_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def synchronize(self):
+        check(_lib.lib().cfg_batch_synchronize(self._h))
+
+    def launch_count(self) -> int:
+        n = ctypes.c_int()
+        check(_lib.lib().cfg_batch_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    def write_params(self):
+        check(_lib.lib().cfg_batch_write_params(self._h))
+
+    def geometry(self):
+        check(_lib.lib().cfg_batch_geometry(self._h))
+
+
+def generate_scene(kind: int, nx: int, ny: int, width: float = 0.8, seed: int = 1234) -> dict:
+    """Seeded synthetic scene (cfg_scene_generate): initial fields, pieces, params, dt."""
+    T = np.empty(nx * ny, np.float32)
+    Y = np.empty(4 * nx * ny, np.float32)
+    U = np.empty((nx + 1) * ny, np.float32)
+    V = np.empty(nx * (ny + 1), np.float32)
+    pieces = np.zeros(_lib.MAX_PIECES * _lib.PIECE_FLOATS, np.float32)
+    npc = ctypes.c_int()
+    P = CfgParams()
+    dt = ctypes.c_double()
+    check(_lib.lib().cfg_scene_generate(kind, nx, ny, width, seed, _fp(T), _fp(Y), _fp(U), _fp(V), _fp(pieces),
+                                        ctypes.byref(npc), ctypes.byref(P), ctypes.byref(dt)))
+    params = {n: getattr(P, n) for n, _ in _lib.PARAM_FIELDS}
+    return {"T": T, "Y": Y, "U": U, "V": V, "pieces": pieces, "npieces": npc.value, "params": params,
+            "dt": dt.value, "nx": nx, "ny": ny, "width": width, "kind": kind, "seed": seed}
+
+
+# parameters that the scene sets; the rest keep FluidSim's defaults
+SCENE_PARAM_KEYS = ("Tamb", "rhoAmb", "YOamb", "reactB", "reactTa", "dHc", "Pr", "exchAlpha", "depth")
+
+
+def load_scene(sim, scene: dict) -> None:
+    """Apply a generated scene to a FluidSim-like object (product or oracle) and rasterise the wood."""
+    for k in SCENE_PARAM_KEYS:
+        sim_set = getattr(sim, "setParam", None) or getattr(sim, "set_param")
+        sim_set(k, scene["params"][k])
+    up = getattr(sim, "uploadPieces", None) or getattr(sim, "upload_pieces")
+    up(scene["pieces"], scene["npieces"])
+    (getattr(sim, "writeParams", None) or getattr(sim, "write_params"))()
+    (getattr(sim, "reset", None))()
+    wr = getattr(sim, "writeBuffer", None) or getattr(sim, "write")
+    for k in ("T", "Y", "U", "V"):
+        wr(k, scene[k])
+    # the advected copies start equal to the state (reset() fills them the same way)
+    wr("T2", scene["T"])
+    wr("Y2", scene["Y"])
+    (getattr(sim, "clearGeometry", None) or getattr(sim, "clear_geometry"))()
+    (getattr(sim, "encodeGeometry", None) or getattr(sim, "geometry"))()

@@ -1,0 +1,193 @@
+/*
+ * campfire_gas.h — C ABI of the B200 gas step (libcampfire_gas.so).
+ *
+ * Drop-in for the gas solver host of BoccheseGiacomo/campfire: `class FluidSim`
+ * in js/fluid.js:26-356, whose step runs the WGSL kernels of shaders/*.wgsl.
+ * Each entry point below names the FluidSim member (or WGSL entry point) it
+ * replaces. A JS host binds these through an N-API addon; any other host binds
+ * them through its FFI (ctypes, cgo, JNI).
+ *
+ * Conventions
+ *  - Every call returns an int status: CFG_OK (0) or a negative CFG_ERR_*.
+ *    cfg_last_error() gives the message of the calling thread's last failure.
+ *  - Handles are opaque. A handle is thread-compatible, not thread-safe: calls
+ *    on one handle must not overlap. Work is ordered on the handle's CUDA
+ *    stream; calls that return host data synchronise that stream.
+ *  - Host arrays use the reference's dense row-major layouts (js/fluid.js:51-68):
+ *    cells nx*ny (index j*nx+i), U faces (nx+1)*ny, V faces nx*(ny+1), Y 4 floats
+ *    per cell (fuel, O2, products, soot), SQ 2 floats per cell (S, heat release),
+ *    cellG 2 floats per cell (sdf, bitcast<f32>(piece*4+face)).
+ *  - There is no CPU fallback: every entry point that computes needs a CUDA
+ *    device and fails with CFG_ERR_NODEV / CFG_ERR_CUDA otherwise.
+ */
+#ifndef CAMPFIRE_GAS_H
+#define CAMPFIRE_GAS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Module constants, js/fluid.js:5-11 */
+#define CFG_MAX_PIECES 64
+#define CFG_PIECE_FLOATS 20
+#define CFG_ACC_GLOBAL 512
+#define CFG_ACC_LEN (CFG_ACC_GLOBAL + 16)
+#define CFG_E_SCALE 1e6
+#define CFG_M_SCALE 1e12
+#define CFG_G_SCALE 1e3
+#define CFG_N_FLOOR 64
+#define CFG_RAD_LEN (CFG_MAX_PIECES * 4 + CFG_N_FLOOR)
+#define CFG_MAX_LEVELS 7
+
+/* Status codes */
+#define CFG_OK 0
+#define CFG_ERR_NOENT (-2)     /* unknown parameter, field or stage name */
+#define CFG_ERR_IO (-5)        /* a CUDA call failed */
+#define CFG_ERR_NOMEM (-12)    /* device allocation failed or over the memory budget */
+#define CFG_ERR_BUSY (-16)     /* readback slot busy (js/fluid.js:317) */
+#define CFG_ERR_NODEV (-19)    /* no CUDA device */
+#define CFG_ERR_INVAL (-22)    /* bad argument */
+#define CFG_ERR_RANGE (-34)    /* 'coarsest level too large' (js/fluid.js:91) */
+#define CFG_ERR_TIMEDOUT (-110) /* a bounded device wait ran out */
+
+/* Pressure solve modes (extension; the reference runs one V(2,2) cycle, js/fluid.js:250) */
+#define CFG_SOLVE_FIXED 0      /* exactly ncycles V(2,2) cycles */
+#define CFG_SOLVE_TOL 1        /* V(2,2) cycles until ||r||2/||rhs||2 <= tol */
+#define CFG_SOLVE_FP64 2       /* FP32 V-cycles inside an FP64 defect-correction loop */
+
+/* The 40-field uniform of shaders/common.wgsl:4-15, in the upload order of js/fluid.js:13-24 */
+typedef struct cfg_params {
+  int32_t nx, ny; float dx, dt;
+  float Tamb, rhoAmb, YOamb, grav;
+  float cp, Pr, viscMult, diffMult;
+  float reactB, reactTa, dHc, sO2;
+  float sootFormA, sootFormTa, sootOxA, sootOxTa;
+  float kappaSootC, kappaGas, exchAlpha, depth;
+  float charA, charTa; int32_t nPieces; uint32_t frame;
+  float heaterX0, heaterX1, heaterY1, heaterT;
+  float burnerX0, burnerX1, burnerFlux, burnerT;
+  float sootDensity, sigma, charO2, time;
+} cfg_params;
+
+/* Read-only view of FluidSim's public scalars (js/fluid.js:29-46, 70-91) */
+typedef struct cfg_info {
+  int32_t nx, ny, levels, diff_sub;
+  double dx, dt, height, time;
+  uint32_t frame;
+  int32_t last_cycles;      /* V-cycles run by the last pressure solve */
+  double last_rel;          /* its final ||r||2/||rhs||2 (FP64 mode: of the FP64 defect) */
+  int32_t level_nx[CFG_MAX_LEVELS], level_ny[CFG_MAX_LEVELS];
+} cfg_info;
+
+typedef struct cfg_sim cfg_sim;
+typedef struct cfg_batch cfg_batch;
+
+int cfg_version(void);
+int cfg_last_error(char* buf, size_t len);
+/* FluidSim's default params (js/fluid.js:35-45 from js/config.js PHYS) */
+int cfg_default_params(cfg_params* out);
+int cfg_device_count(int* count);
+
+/* new FluidSim(device, {nx, ny, dt}) + await init()  (js/fluid.js:27-47, 49-160).
+ * dx = width/nx (the reference fixes width = SCENE_WIDTH = 0.7, js/config.js:3).
+ * Fails with CFG_ERR_RANGE when the coarsest multigrid level keeps more than 256
+ * cells after 7 halvings (the reference throws after 6, js/fluid.js:72, 91). */
+int cfg_create(int nx, int ny, double width, double dt, int device, cfg_sim** out);
+int cfg_destroy(cfg_sim* sim);
+/* reset(): ambient state, zero velocity/pressure/accumulators  (js/fluid.js:162-176) */
+int cfg_reset(cfg_sim* sim);
+/* setParam(k, v): stored, applied by the next cfg_write_params  (js/fluid.js:178) */
+int cfg_set_param(cfg_sim* sim, const char* name, double value);
+int cfg_get_param(cfg_sim* sim, const char* name, double* value);
+/* sim.dt = dt (public field; applied by the next cfg_write_params) */
+int cfg_set_dt(cfg_sim* sim, double dt);
+/* writeParams(): upload the 40-field uniform, recompute the diffusion sub-steps  (js/fluid.js:180-199) */
+int cfg_write_params(cfg_sim* sim);
+/* uploadPieces(Float32Array(64*20), n)  (js/fluid.js:201-204; packing js/main.js:190-199) */
+int cfg_upload_pieces(cfg_sim* sim, const float* data, int n);
+/* clearGeometry(enc)  (js/fluid.js:213): zero the per-face band weights */
+int cfg_clear_geometry(cfg_sim* sim);
+/* encodeGeometry(pass)  (js/fluid.js:215-218; shaders/geometry.wgsl) */
+int cfg_geometry(cfg_sim* sim);
+/* nsteps x encodeStep(pass)  (js/fluid.js:225-253), time += dt per step */
+int cfg_step(cfg_sim* sim, int nsteps);
+/* encodeStepProfiled: one step, per-stage device ms for the 7 stages
+ * 'advect','diffuse','sources','forces','coef/rhs','vcycle','project'  (js/fluid.js:256-292).
+ * Here 'diffuse' and 'sources' run fused; the fused time is reported under 'sources'. */
+int cfg_step_profiled(cfg_sim* sim, float* stage_ms);
+/* One stage of the step on the current state: "advect", "diffuse", "sources",
+ * "forces", "coef_rhs", "pressure", "project", "diffuse_sources" */
+int cfg_run_stage(cfg_sim* sim, const char* stage);
+/* vcycle(pass, nu): one V(nu,nu) cycle on the current level-0 rhs/p  (js/fluid.js:294-312); nu = 2 */
+int cfg_vcycle(cfg_sim* sim, int nu);
+/* encodeRadiation(pass)  (js/fluid.js:220-222; shaders/radiation.wgsl) */
+int cfg_radiation(cfg_sim* sim);
+/* sim.frame++ (js/main.js:282): the frame counter of the radiation jitter */
+int cfg_set_frame(cfg_sim* sim, uint32_t frame);
+/* encodeReadback + afterSubmit (js/fluid.js:315-342), synchronous: copies
+ * acc[528] (i32), rad[320*4] (f32), faceW[256] (i32), then clears acc. Any pointer may be NULL. */
+int cfg_readback(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW);
+/* readBuffer(name) (js/fluid.js:345-355) and its inverse. Names: U V T Y SQ cellG fx fy
+ * U2 V2 T2 Y2 p rhs ax ay, and p.L rhs.L ax.L ay.L for multigrid level L.
+ * Uh Vh Th Yh are not kept by the fused kernels and read as CFG_ERR_NOENT. */
+int cfg_field_size(cfg_sim* sim, const char* name, size_t* count);
+int cfg_read_field(cfg_sim* sim, const char* name, float* out, size_t count);
+int cfg_write_field(cfg_sim* sim, const char* name, const float* in, size_t count);
+/* FP64 level-0 pressure of CFG_SOLVE_FP64 (nx*ny doubles) */
+int cfg_read_p64(cfg_sim* sim, double* out, size_t count);
+int cfg_get_info(cfg_sim* sim, cfg_info* out);
+
+/* ---- extensions (no counterpart in the reference) ---- */
+/* Pressure solve mode; see CFG_SOLVE_*. Defaults: CFG_SOLVE_FIXED, 1 cycle (the reference). */
+int cfg_set_solver(cfg_sim* sim, int mode, int ncycles, double tol, int max_cycles);
+/* CFL step: after each step dt = min(dt_cap, cfl*dx/max|u|); cfl = 0 keeps dt fixed. */
+int cfg_set_cfl(cfg_sim* sim, double cfl, double dt_cap);
+/* Rays per wood face / floor probe of the radiation pass (radiation.wgsl:22 fixes 64) */
+int cfg_set_nray(cfg_sim* sim, int nray);
+/* ||r||2/||rhs||2 of the level-0 pressure equation now (FP64 sums) */
+int cfg_pressure_residual(cfg_sim* sim, double* rel);
+/* FP64 sums over gas cells, per m of depth: mass, energy (rho cp T), fuel, O2, products,
+ * soot masses, heat release rate, max T  (8 doubles) */
+int cfg_budgets(cfg_sim* sim, double* out);
+/* Run the handle's work on a caller-owned cudaStream_t (NULL: the handle's own stream) */
+int cfg_set_stream(cfg_sim* sim, void* cuda_stream);
+int cfg_synchronize(cfg_sim* sim);
+/* Capture each step in a CUDA graph (default on); off launches kernel by kernel */
+int cfg_set_graphs(cfg_sim* sim, int enable);
+/* Kernels launched by the last cfg_step (per step) */
+int cfg_launch_count(cfg_sim* sim, int* per_step);
+
+/* Synthetic scenes for the benchmark workloads (seeded, deterministic).
+ * kind 0: three square logs of half 0.025 at (0.35,0.025) (0.45,0.025) (0.40,0.068),
+ *         flux 5e-3 kg/m2/s at 600 K;  kind 1: five logs of half 0.05 in a seeded tepee,
+ *         flux 8e-3;  kind 2: 2-6 seeded floor logs of half 0.025 or 0.05 with B scaled
+ *         by log-uniform [0.5,2] and YOamb uniform in [0.18,0.233].
+ * Writes the initial T[nx*ny], Y[4*nx*ny], U[(nx+1)*ny], V[nx*(ny+1)], pieces[64*20],
+ * the piece count, the params and the CFL-limited dt. */
+int cfg_scene_generate(int kind, int nx, int ny, double width, uint64_t seed,
+                       float* T, float* Y, float* U, float* V, float* pieces, int* npieces,
+                       cfg_params* params, double* dt);
+
+/* ---- batches: many independent scenes of uneven size stepped together ---- */
+int cfg_batch_create(int nscenes, const int* nx, const int* ny, const double* width,
+                     const double* dt, int device, cfg_batch** out);
+int cfg_batch_destroy(cfg_batch* b);
+/* A non-owning cfg_sim view of scene i: every single-scene call above except
+ * cfg_step / cfg_step_profiled / cfg_vcycle / cfg_run_stage applies to that scene. */
+int cfg_batch_scene(cfg_batch* b, int i, cfg_sim** view);
+int cfg_batch_set_solver(cfg_batch* b, int mode, int ncycles, double tol, int max_cycles);
+int cfg_batch_set_active(cfg_batch* b, int i, int active);
+int cfg_batch_step(cfg_batch* b, int nsteps);
+int cfg_batch_set_stream(cfg_batch* b, void* cuda_stream);
+int cfg_batch_synchronize(cfg_batch* b);
+int cfg_batch_launch_count(cfg_batch* b, int* per_step);
+int cfg_batch_write_params(cfg_batch* b);
+int cfg_batch_geometry(cfg_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAMPFIRE_GAS_H */
