@@ -1,0 +1,300 @@
+"""Benchmark of the B200 gas step: cell-updates/s on the 256x384 plain scene.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload plain|fine]
+
+One step = one full gas step (advect -> diffuse -> sources -> forces ->
+pressure solve to the configured tolerance -> project) of the seeded synthetic
+scene: 256x384 MAC grid over 0.8 m x 1.2 m, three square logs of half-side
+2.5 cm injecting fuel at 5e-3 kg/m2/s, a 1800 K Gaussian hot spot; pressure by
+FP32 V(2,2) cycles inside an FP64 defect-correction loop to ||r||/||rhs|| <= 1e-6.
+The state (~25 MB) fits in L2, so L2 is flushed (a 256 MB write) before every
+timed step; each step is timed alone with CUDA events on the library's stream.
+
+N > 1 runs independent replicas (one scene per rank, seeds differ): the gas
+step has no data-path collective; value = all ranks' cell-updates / max-over-
+ranks time ("scaling": "weak").
+
+--impl reference times the reference's CPU implementation of the step on this
+box's host cores: the C++ restatement of the WGSL (the reference's WGSL needs a
+WebGPU stack that does not exist here), FP32, OpenMP over all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (nx, ny, scene kind, seed, solver mode, tol, max cycles)
+    "plain": (256, 384, 0, 1235, 2, 1e-6, 200),
+    "fine": (512, 768, 1, 1236, 2, 1e-10, 300),
+}
+METRIC = "cell-updates/s"
+# algorithmic bytes per cell-update (reference schedule, one read + one write per element at storage width):
+# advect 156, diffuse 48 per sub-step, sources 68, forces 28, coef 20, rhs0 28, coefRestrict 13.3, project 32,
+# V(2,2) cycle 216.8, FP64 defect-correction iteration 40, FP64 rhs assembly 12
+B_FIXED = 156 + 68 + 28 + 20 + 28 + 13.3 + 32
+
+
+def bytes_per_cell(diff_sub: int, cycles: float, fp64: bool) -> float:
+    b = B_FIXED + 48.0 * diff_sub + 216.8 * cycles
+    if fp64:
+        b += 40.0 * cycles + 12.0
+    return b
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.lines = index, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0])); mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_cpu(workload: str, steps: int, warmup: int, threads: int):
+    """The CPU restatement of the reference step (oracle, f32), same scene and solver."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    from oracle import oracle
+    nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
+    sc = cb.generate_scene(kind, nx, ny, 0.8, seed)
+    o = oracle.OracleSim(nx, ny, 0.8, sc["dt"])
+    load_scene(o, sc)
+    o.set_solver(mode, 1, tol, maxc)
+    o.step(warmup)
+    cyc = 0.0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(1)
+        cyc += o.info()["last_cycles"]
+    dt = time.perf_counter() - t0
+    return nx * ny * steps / dt, dt, cyc / max(steps, 1)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plain", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-sample", type=int, default=3, help="steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[a.workload]
+    config = {"workload": f"{a.workload} gas step {nx}x{ny}, 3 logs, FP32 V(2,2) in FP64 defect correction "
+                          f"to rel residual {tol:g}", "nx": nx, "ny": ny, "scene_seed": seed,
+              "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": maxc},
+              "l2": "flushed before every timed step (256 MB write)", "parallelism": f"replicas{world}"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        th = cpu_threads()
+        val, secs, cyc = run_cpu(a.workload, a.steps, a.warmup, th)
+        line = {"metric": METRIC, "value": val, "unit": METRIC, "impl": "reference", "n_gpus": a.gpus,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * secs / a.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(config, cycles_per_step=cyc),
+                "cpu_baseline": {"value": val, "unit": METRIC, "cores": th, "kind": "port",
+                                 "sample": f"{a.steps} steps of the {nx}x{ny} workload after {a.warmup} warm-up steps "
+                                           "(C++ restatement of the reference WGSL, f32, OpenMP)"},
+                "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    # one non-default stream shared by the library, the L2 flush and the timing events
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+
+    sc = cb.generate_scene(kind, nx, ny, 0.8, seed + 1000 * rank)
+    sim = cb.FluidSim(local, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(sim, sc)
+    sim.set_solver(mode, 1, tol, maxc)
+    sim.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    sim.step(a.warmup)
+    sim.synchronize()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    cycles = []
+    clocks = ClockSampler(local)
+    clocks.start()
+    for k in range(a.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        sim.step(1)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    info = sim.info()
+    sim.synchronize()
+    launches = sim.launch_count()
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * nx * ny * a.steps / (ms_max / 1e3)
+
+    # ---- end to end through the C ABI: per step upload params + pieces from pinned host
+    # memory, step, read the accumulators back (the frame data flow of js/main.js:266-283)
+    pin_pieces = torch.from_numpy(sc["pieces"].copy()).pin_memory()
+    acc = torch.zeros(528, dtype=torch.int32).pin_memory()
+    rad = torch.zeros(320 * 4, dtype=torch.float32).pin_memory()
+    fw = torch.zeros(256, dtype=torch.int32).pin_memory()
+    L = cb.lib()
+    fptr = ctypes.cast(pin_pieces.data_ptr(), ctypes.POINTER(ctypes.c_float))
+    i32 = ctypes.POINTER(ctypes.c_int32)
+    e2e_steps = max(5, a.steps // 4)
+    barrier()
+    e2e_s = 0.0
+    for k in range(e2e_steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        cb._lib.check(L.cfg_upload_pieces(sim._h, fptr, sc["npieces"]))
+        cb._lib.check(L.cfg_write_params(sim._h))
+        cb._lib.check(L.cfg_step(sim._h, 1))
+        cb._lib.check(L.cfg_readback(sim._h, ctypes.cast(acc.data_ptr(), i32),
+                                     ctypes.cast(rad.data_ptr(), ctypes.POINTER(ctypes.c_float)),
+                                     ctypes.cast(fw.data_ptr(), i32)))
+        e2e_s += time.perf_counter() - t0
+    t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * nx * ny * e2e_steps / float(t.item())
+
+    # ---- roofline of the dominant kernel (device time per step share), measured after the timed region
+    hbm, peak_kind = peaks()
+    kern = {}
+    for name in ("advect", "diffuse_sources", "forces", "relax0", "restrict0", "prolong0", "coarsest", "resnorm",
+                 "project"):
+        m, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        cb._lib.check(L.cfg_time_kernel(sim._h, name.encode(), 50, ctypes.byref(m), ctypes.byref(b), ctypes.byref(n)))
+        kern[name] = {"ms": m.value, "bytes": b.value, "per_step": n.value, "share_ms": m.value * n.value}
+    dom = max(kern, key=lambda k: kern[k]["share_ms"])
+    dk = kern[dom]
+    achieved = dk["bytes"] / (dk["ms"] / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
+            "traffic": None, "bytes_per_launch": dk["bytes"], "launch_ms": dk["ms"],
+            "step_bytes_per_cell": bytes_per_cell(info["diffSub"], info["last_cycles"], True),
+            "step_frac": (value / world) * bytes_per_cell(info["diffSub"], info["last_cycles"], True) / 1e9 / hbm,
+            "kernels": {k: {"ms": round(v["ms"], 5), "per_step": v["per_step"]} for k, v in kern.items()}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        th = cpu_threads()
+        val, secs, cyc = run_cpu(a.workload, a.cpu_sample, 1, th)
+        cpu = {"value": val, "unit": METRIC, "cores": th, "kind": "port",
+               "sample": f"{a.cpu_sample} steps of the same {nx}x{ny} workload after 1 warm-up step "
+                         f"(C++ restatement of the reference WGSL, f32, OpenMP; {cyc:.1f} V-cycles/step)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(config, cycles_last_step=info["last_cycles"], diff_sub=info["diffSub"],
+                               levels=info["levels"]),
+                # H2D: the piece buffer, the descriptor's parameter block (uniform + step controls, 204 B)
+                # and dx/alpha of the diffusion rule (16 B); D2H: acc + rad + faceW
+                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 204 + 16,
+                        "d2h_bytes_per_step": 528 * 4 + 320 * 16 + 256 * 4},
+                "gpu_launches": launches * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line))
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -97,6 +97,7 @@ def lib():
         "cfg_batch_set_active": [vp, ci, ci], "cfg_batch_step": [vp, ci], "cfg_batch_set_stream": [vp, vp],
         "cfg_batch_synchronize": [vp], "cfg_batch_launch_count": [vp, ip], "cfg_batch_write_params": [vp],
         "cfg_batch_geometry": [vp],
+        "cfg_time_kernel": [vp, cs, ci, dp, dp, dp],
     }
     for name, args in sigs.items():
         f = getattr(L, name)

@@ -162,3 +162,9 @@ int cfg_batch_write_params(cfg_batch* b) { BATCH_OK(b); return guarded([&] { ret
 int cfg_batch_geometry(cfg_batch* b) { BATCH_OK(b); return guarded([&] { return b->eng->geometry_all(); }); }
 
 }  // extern "C"
+
+extern "C" int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, double* mean_ms, double* bytes_per_launch,
+                               double* launches_per_step) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->time_kernel(kernel, iters, mean_ms, bytes_per_launch, launches_per_step); });
+}

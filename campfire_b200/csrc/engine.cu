@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -20,6 +21,9 @@
 #include "kernels.h"
 
 namespace cfg {
+
+// bench.py counts these bytes as the per-step parameter upload of cfg_write_params
+static_assert(kDescParamBytes == 204, "parameter block of SceneDesc");
 
 namespace {
 thread_local std::string g_err;
@@ -113,6 +117,10 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
     }
     sc.nlev = L;
     if (sc.lnx[L - 1] * sc.lny[L - 1] > 256) return fail(CFG_ERR_RANGE, "coarsest level too large");
+    sc.lc = L - 1;
+    for (int l = 0; l < L; l++)
+      if (sc.lnx[l] * sc.lny[l] <= COARSE_CELLS) { sc.lc = l; break; }
+    coarse_smem_ = std::max(coarse_smem_, coarse_smem_bytes(sc.lnx, sc.lny, sc.lc, sc.nlev));
   }
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -120,6 +128,7 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   if (device < 0 || device >= ndev) return fail(CFG_ERR_INVAL, "device index out of range");
   device_ = device;
   CFG_TRY(activate());
+  CFG_CUDA(prepare_mg_coarse(coarse_smem_));
   CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaMalloc(&d_scenes_, sizeof(SceneDesc) * n));
@@ -134,6 +143,7 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   CFG_TRY(build_worklists());
   for (int s = 0; s < n; s++) {
     scenes_[s].desc.solve = d_solve_ + s;
+    CFG_TRY(upload_desc(s));
     CFG_TRY(write_params(s));
     CFG_TRY(reset(s));
   }
@@ -152,7 +162,8 @@ int Engine::alloc_scene(Scene& sc) {
   const size_t C = (size_t)sc.ny * d.pc, Uf = (size_t)sc.ny * d.pu, Vf = (size_t)(sc.ny + 1) * d.pc;
   const int nt_fr = ((sc.nx + FR_TX - 1) / FR_TX) * ((sc.ny + FR_TY - 1) / FR_TY);
   const int nt_mg0 = ((sc.nx + MG_TX - 1) / MG_TX) * ((sc.ny + MG_TY - 1) / MG_TY);
-  d.nt_fr = nt_fr; d.nt_mg0 = nt_mg0;
+  const int nt_up0 = ((sc.nx + MGF_TX - 1) / MGF_TX) * ((sc.ny + MGF_TY - 1) / MGF_TY);
+  d.nt_fr = nt_fr; d.nt_mg0 = nt_mg0; d.nt_up0 = nt_up0; d.lc = sc.lc;
   struct Item { void** ptr; size_t bytes; };
   std::vector<Item> items = {
     {(void**)&d.U, Uf * 4}, {(void**)&d.U2, Uf * 4}, {(void**)&d.fx, Uf * 4},
@@ -163,7 +174,7 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.acc, ACC_LEN * 4}, {(void**)&d.faceW, MAX_PIECES * 4 * 4},
     {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4}, {(void**)&d.rad, RAD_LEN * 16},
     {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
-    {(void**)&d.part, (size_t)std::max(nt_fr, nt_mg0) * 8},
+    {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 8},
   };
   double h = sc.dxd;
   for (int l = 0; l < sc.nlev; l++) {
@@ -211,6 +222,7 @@ int Engine::build_worklists() {
       tiles(lists[WL_MGV0 + l], s, sc.lnx[l], sc.lny[l], MG_TX, MG_TY);
       tiles(lists[WL_MGC0 + l], s, sc.lnx[l + 1], sc.lny[l + 1], MG_TX, MG_TY);
     }
+    for (int l = 0; l < sc.lc; l++) tiles(lists[WL_MGD0 + l], s, sc.lnx[l], sc.lny[l], MGF_TX, MGF_TY);
   }
   for (int k = 0; k < WL_COUNT; k++) {
     nwl_[k] = (int)lists[k].size();
@@ -335,7 +347,8 @@ int Engine::write_params(int s) {
   SceneDesc& d = sc.desc;
   d.P = sc.P; d.diff_sub = n; d.diff_dt = sc.diff_dt;
   d.cfl = (float)sc.cfl; d.dt_cap = (float)sc.dt_cap; d.nray = sc.nray; d.enabled = sc.enabled ? 1 : 0;
-  CFG_TRY(upload_desc(s));
+  // only the leading scalar block changes here (the uniform and the step controls)
+  CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &d, kDescParamBytes, cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaMemcpyAsync(d_dxd_ + s, &sc.dxd, 8, cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaMemcpyAsync(d_alpha_ + s, &sc.alpha, 8, cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaStreamSynchronize(st()));
@@ -557,8 +570,34 @@ void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_con
   (void)h; (void)use_cond;
 }
 
-// FluidSim.vcycle (js/fluid.js:294-312), nu = 2
+int Engine::max_lc() const {
+  int m = 0;
+  for (auto& sc : scenes_) m = std::max(m, sc.lc);
+  return m;
+}
+
+// The step's V(2,2) cycle with the fused kernels (k_mgf.cu); the level-0 up
+// kernel (or the coarse block of scenes whose block starts at level 0) ends
+// the cycle with the residual norm (FP32 modes) or p64 += p (FP64 mode).
 void Engine::enqueue_vcycle(cudaStream_t s) {
+  const int LD = max_lc();
+  const int tail = any_fp64() ? 2 : 1;
+  for (int l = 0; l < LD; l++) {
+    if (nwl_[WL_MGD0 + l] == 0) continue;
+    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, s);
+    vcycle_launches_++;
+  }
+  launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, coarse_smem_, s);
+  vcycle_launches_++;
+  for (int l = LD - 1; l >= 0; l--) {
+    if (nwl_[WL_MGD0 + l] == 0) continue;
+    launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, l == 0 ? tail : 0, d_ctl_, s);
+    vcycle_launches_++;
+  }
+}
+
+// FluidSim.vcycle (js/fluid.js:294-312), nu = 2: one kernel per reference dispatch
+void Engine::enqueue_vcycle_ref(cudaStream_t s) {
   const int L = max_levels();
   for (int l = 0; l + 1 < L; l++) {
     const int wv = WL_MGV0 + l;
@@ -587,12 +626,9 @@ void Engine::enqueue_vcycle(cudaStream_t s) {
 }
 
 void Engine::enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond) {
+  // the fused cycle already ended with p64 += p (FP64) or the residual norm (FP32 modes)
   if (any_fp64()) {
-    launch_accum64(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], s);
     launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, s);
-    vcycle_launches_ += 2;
-  } else {
-    launch_resnorm(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
     vcycle_launches_++;
   }
   launch_loop_guard(d_ctl_, h, use_cond, s);
@@ -719,6 +755,12 @@ int Engine::synchronize() {
   SolveState ss{};
   CFG_CUDA(cudaMemcpy(&ss, d_solve_, sizeof ss, cudaMemcpyDeviceToHost));
   launches_per_step_ = launches_ + vcycle_launches_ * std::max(ss.cycles, 1);
+  int err = 0;
+  CFG_CUDA(cudaMemcpy(&err, &d_ctl_->err, sizeof err, cudaMemcpyDeviceToHost));
+  if (err) {
+    CFG_CUDA(cudaMemset(&d_ctl_->err, 0, sizeof err));
+    return fail(CFG_ERR_TIMEDOUT, "a bounded device wait ran out (TMA staging of the coarse multigrid levels)");
+  }
   return CFG_OK;
 }
 
@@ -786,12 +828,80 @@ int Engine::run_stage(const char* stage) {
   return CFG_OK;
 }
 
+// Mean device time of one kernel of the step on scene 0, with the algorithmic
+// bytes per launch of the reference schedule (one read + one write per array
+// element at storage width; the per-cell figures of each WGSL dispatch).
+int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, double* per_step) {
+  if (!name || !ms || !bytes || !per_step || iters < 1) return fail(CFG_ERR_INVAL, "bad argument");
+  CFG_TRY(activate());
+  const Scene& sc = scenes_[0];
+  const double cells = (double)sc.nx * sc.ny;
+  SolveState ss{};
+  CFG_CUDA(cudaMemcpy(&ss, d_solve_, sizeof ss, cudaMemcpyDeviceToHost));
+  const double cyc = std::max(ss.cycles, 1);
+  const bool fp64 = any_fp64();
+  cudaStream_t s = st();
+  const std::string n(name);
+  std::function<void(int)> go;
+  double b = 0, cnt = 1;
+  if (n == "advect") { go = [&](int) { launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s); }; b = 156 * cells; }
+  else if (n == "diffuse_sources") {
+    go = [&](int) { launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, s); };
+    b = (48.0 * sc.diff_sub + 68) * cells;
+  } else if (n == "forces") {
+    go = [&](int) { launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); };
+    b = (28 + 20 + 28 + 13.3) * cells;
+  } else if (n == "relax0") {
+    go = [&](int k) { launch_relax(d_scenes_, d_wl_[WL_MGV0], nwl_[WL_MGV0], 0, k & 1, s); };
+    b = 16 * cells; cnt = 8 * cyc;
+  } else if (n == "restrict0") {
+    go = [&](int) { launch_restrict_res(d_scenes_, d_wl_[WL_MGC0], nwl_[WL_MGC0], 0, s); };
+    b = 18 * cells; cnt = cyc;
+  } else if (n == "prolong0") {
+    go = [&](int) { launch_prolong(d_scenes_, d_wl_[WL_MGV0], nwl_[WL_MGV0], 0, s); };
+    b = 17 * cells; cnt = cyc;
+  } else if (n == "coarsest") {
+    go = [&](int) { launch_coarsest(d_scenes_, nscenes(), s); };
+    b = 0; cnt = cyc;
+  } else if (n == "mg_down0") {
+    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, s); };
+    b = (4 * 16 + 18) * cells; cnt = cyc;   // 4 colour passes + residual restriction
+  } else if (n == "mg_up0") {
+    go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 0, d_ctl_, s); };
+    b = (17 + 4 * 16) * cells; cnt = cyc;   // prolongation + 4 colour passes
+  } else if (n == "mg_coarse") {
+    go = [&](int) { launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, coarse_smem_, s); };
+    b = 0; cnt = cyc;
+  } else if (n == "resnorm") {
+    go = [&](int) { launch_resnorm(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
+    b = (fp64 ? 32 : 16) * cells; cnt = cyc;
+  } else if (n == "project") {
+    go = [&](int) { launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s); };
+    b = 32 * cells;
+  } else return fail(CFG_ERR_NOENT, "unknown kernel " + n);
+  launch_bnorm(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, false, s);   // arm the multigrid kernels
+  cudaEvent_t e0, e1;
+  CFG_CUDA(cudaEventCreate(&e0));
+  CFG_CUDA(cudaEventCreate(&e1));
+  go(0);   // warm-up
+  CFG_CUDA(cudaEventRecord(e0, s));
+  for (int k = 0; k < iters; k++) go(k);
+  CFG_CUDA(cudaEventRecord(e1, s));
+  CFG_CUDA(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CFG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  CFG_CUDA(cudaGetLastError());
+  *ms = (double)t / iters; *bytes = b; *per_step = cnt;
+  return CFG_OK;
+}
+
 int Engine::vcycle_once(int nu) {
   if (nu != 2) return fail(CFG_ERR_INVAL, "only V(2,2) cycles are provided (js/fluid.js:294 default nu = 2)");
   CFG_TRY(activate());
   cudaStream_t s = st();
   enqueue_bnorm(s);   // arms every scene (active = 1)
-  enqueue_vcycle(s);
+  enqueue_vcycle_ref(s);
   CFG_CUDA(cudaGetLastError());
   CFG_CUDA(cudaStreamSynchronize(s));
   return CFG_OK;

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <string>
 #include <vector>
 
@@ -52,14 +53,22 @@ struct Scene {
   float diff_dt = 0;
   double alpha = 0;              // alpha(2200 K) of the diffusion sub-step rule
   int lnx[MAX_LEVELS] = {}, lny[MAX_LEVELS] = {};
+  int lc = 0;                    // first level of the one-CTA coarse block
   void* arena = nullptr;
   size_t arena_bytes = 0;
   SceneDesc desc{};              // host mirror of the device descriptor
   bool enabled = true;
 };
 
+// Bytes of SceneDesc that cfg_write_params uploads: the uniform and the step
+// controls up to (not including) the tile counts and device pointers.
+constexpr size_t kDescParamBytes = offsetof(SceneDesc, nt_fr);
+
+// Work lists: per-kernel tiles of every scene. MGV/MGC: single-pass multigrid
+// tiles of level l / l+1 for scenes where l is not the coarsest level; MGD:
+// fused smoother tiles of level l for scenes where l is below the coarse block.
 enum WL { WL_ADV = 0, WL_DS, WL_FR, WL_PR, WL_GEO, WL_MG0, WL_MGV0, WL_MGC0 = WL_MGV0 + MAX_LEVELS,
-          WL_COUNT = WL_MGC0 + MAX_LEVELS };
+          WL_MGD0 = WL_MGC0 + MAX_LEVELS, WL_COUNT = WL_MGD0 + MAX_LEVELS };
 
 class Engine {
  public:
@@ -101,6 +110,7 @@ class Engine {
   int launches_per_step() const { return launches_per_step_; }
   int write_params_all();
   int geometry_all();
+  int time_kernel(const char* name, int iters, double* ms, double* bytes, double* per_step);
   int nscenes() const { return (int)scenes_.size(); }
 
  private:
@@ -120,7 +130,9 @@ class Engine {
 
   // step pieces; launches counted in launches_
   void enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_cond);
-  void enqueue_vcycle(cudaStream_t s);
+  void enqueue_vcycle(cudaStream_t s);       // fused kernels (the step's cycle)
+  void enqueue_vcycle_ref(cudaStream_t s);   // one kernel per reference dispatch (cfg_vcycle)
+  int max_lc() const;
   void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
   void enqueue_post_solve(cudaStream_t s);
   int host_pressure_loop();
@@ -146,6 +158,7 @@ class Engine {
   int graph_sub_ = -1;
   int launches_ = 0, launches_per_step_ = 0;
   int vcycle_launches_ = 0;
+  size_t coarse_smem_ = 0;
 };
 
 }  // namespace cfg

@@ -54,6 +54,8 @@ struct SceneDesc {
   int nray;                 // rays per target of the radiation pass
   int enabled;              // 0: scene skipped by every kernel (batch slot not in use)
   int nt_fr, nt_mg0;        // tiles of this scene in the forces and level-0 multigrid work lists
+  int nt_up0;               // tiles of this scene in the level-0 fused up-smoother work list
+  int lc;                   // first level of the one-CTA coarse block (levels lc..nlev-1)
   float *U, *V, *U2, *V2, *T, *T2, *Tw;   // Tw: diffusion ping-pong buffer
   float4 *Y, *Y2, *Yw;
   float2 *SQ, *cellG;
@@ -76,6 +78,8 @@ struct SolveCtl {
   int any_active;             // the loop decision of the last cycle
   int iter;                   // cycles run by the loop in this step (reset before the loop)
   int hard_cap;               // the loop stops after this many cycles whatever any_active says
+  int err;                    // set by a kernel whose bounded wait ran out (reported as CFG_ERR_TIMEDOUT)
+  int pad;
 };
 
 // One tile of a work list

@@ -14,6 +14,8 @@ constexpr int DS_TX = 32, DS_TY = 8;                 // diffusion + sources
 constexpr int FR_TX = 32, FR_TY = 16;                // forces + coef + rhs0 (+ coefficient hierarchy)
 constexpr int FR_KMAX = 4;                           // coarse coefficient levels built inside FR tiles
 constexpr int MG_TX = 32, MG_TY = 8;                 // single-pass multigrid kernels
+constexpr int MGF_TX = 32, MGF_TY = 16;              // fused (temporally blocked) multigrid kernels
+constexpr int COARSE_CELLS = 6144;                   // largest level handled by the one-CTA coarse block
 constexpr int PR_TX = 32, PR_TY = 8;                 // projection
 constexpr int GEO_TX = 32, GEO_TY = 8;               // geometry
 
@@ -42,6 +44,15 @@ void launch_defect64(const SceneDesc* scenes, int nscenes, const Work* work, int
                      int first, cudaStream_t st);
 // end of a loop iteration: count it and set the WHILE node's condition (bounded by SolveCtl::hard_cap)
 void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_cond, cudaStream_t st);
+// fused V(2,2) cycle: per fine level a down kernel (4 passes + restriction) and an
+// up kernel (prolongation + 4 passes; level 0 tail: 1 residual norm + decision,
+// 2 p64 += p), and one CTA per scene for levels lc..coarsest
+void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, cudaStream_t st);
+void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
+                  cudaStream_t st);
+void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, size_t smem, cudaStream_t st);
+size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);
+cudaError_t prepare_mg_coarse(size_t smem);
 // ||rhs||^2 (FP64 mode: ||rhs64||^2) of level 0; arms the pressure loop
 void launch_bnorm(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool fp64, cudaStream_t st);
 // FP64: p64 += p0

@@ -2,8 +2,12 @@
 //
 // Domain: width x (dx * ny) with dx = width / nx (0.8 m x 1.2 m at 2:3 grids).
 // Wood: the reference has square pieces only (common.wgsl:47-53), so a log of
-// radius r is a square of half-side r, frozen (alive, zero velocity), every face
-// at 600 K injecting fuel at the scene's flux (piece packing of js/main.js:196-199).
+// radius r becomes the square of equal cross-section area (half-side
+// r*sqrt(pi)/2) at the same centre: squares of half-side r would overlap where
+// the circles only come close, sealing cavities against the floor in which the
+// pressure equation has no solution. Pieces are frozen (alive, zero velocity),
+// every face at 600 K injecting fuel at the scene's flux (piece packing of
+// js/main.js:196-199).
 // Initial gas: T = 300 + 1500 exp(-r^2 / (2 * 0.05^2)) around (0.40, 0.12) m,
 // Y_F = 0.3 of the same Gaussian, Y_O = YOamb (1 - Y_F), Y_S = 0, Y_P the rest;
 // U, V uniform in [-0.01, 0.01] m/s from a counter-based hash of the seed.
@@ -66,7 +70,9 @@ bool inside(const Box& b, double W, double H) {
 }
 bool fits(const Box& b, const std::vector<Box>& placed, double W, double H) {
   if (!inside(b, W, H)) return false;
-  for (auto& q : placed) if (overlap(b, q, 0.002)) return false;
+  // keep 6 mm of gas between pieces: narrower seams close under the fractional
+  // faces of a 1.5 mm grid and would seal cavities
+  for (auto& q : placed) if (overlap(b, q, 0.006)) return false;
   return true;
 }
 
@@ -95,10 +101,12 @@ extern "C" int cfg_scene_generate(int kind, int nx, int ny, double width, uint64
   P.reactTa = 15000.f; P.dHc = 15.0e6f; P.Pr = 0.7f; P.exchAlpha = 0.05f; P.depth = 0.3f;
   // ---- wood
   std::vector<Box> boxes;
+  const double area_half = 0.5 * std::sqrt(3.14159265358979323846);   // half-side / radius at equal area
   if (kind == 0) {
-    boxes = {{0.35, 0.025, 0.0, 0.025}, {0.45, 0.025, 0.0, 0.025}, {0.40, 0.068, 0.0, 0.025}};
+    const double hf = 0.025 * area_half;
+    boxes = {{0.35, 0.025, 0.0, hf}, {0.45, 0.025, 0.0, hf}, {0.40, 0.068, 0.0, hf}};
   } else if (kind == 1) {
-    const double hf = 0.05, cx = 0.5 * width;
+    const double hf = 0.05 * area_half, cx = 0.5 * width;
     for (int k = 0; k < 5; k++) {
       for (int attempt = 0; attempt < 4000; attempt++) {
         Box b{};
@@ -112,7 +120,7 @@ extern "C" int cfg_scene_generate(int kind, int nx, int ny, double width, uint64
   } else {
     const int want = 2 + std::min(4, (int)(rng.u() * 5));
     for (int k = 0; k < want; k++) {
-      const double hf = rng.u() < 0.5 ? 0.025 : 0.05;
+      const double hf = (rng.u() < 0.5 ? 0.025 : 0.05) * area_half;
       for (int attempt = 0; attempt < 2000; attempt++) {
         Box b{rng.u(0.05 + hf, width - 0.05 - hf), hf, 0.0, hf};
         bool ok = fits(b, boxes, width, H);

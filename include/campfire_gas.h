@@ -159,6 +159,13 @@ int cfg_synchronize(cfg_sim* sim);
 int cfg_set_graphs(cfg_sim* sim, int enable);
 /* Kernels launched by the last cfg_step (per step) */
 int cfg_launch_count(cfg_sim* sim, int* per_step);
+/* Measurement: launch one kernel of the step `iters` times back to back on the
+ * current state and report its mean device time (CUDA events on the handle's
+ * stream), its algorithmic bytes per launch and its launches per step.
+ * Kernels: "advect", "diffuse_sources", "forces", "relax0", "restrict0",
+ * "prolong0", "coarsest", "resnorm", "project". The state changes as the kernel runs. */
+int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, double* mean_ms, double* bytes_per_launch,
+                    double* launches_per_step);
 
 /* Synthetic scenes for the benchmark workloads (seeded, deterministic).
  * kind 0: three square logs of half 0.025 at (0.35,0.025) (0.45,0.025) (0.40,0.068),

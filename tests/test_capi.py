@@ -69,10 +69,11 @@ def test_scene_generator_is_deterministic_and_matches_the_workload():
         assert np.array_equal(a[k], b[k])
     c = cb.generate_scene(0, 128, 192, 0.8, 1235)
     assert not np.array_equal(a["U"], c["U"])
-    # three logs of radius 2.5 cm at the stated centres, 600 K faces, 5e-3 kg/m2/s
+    # three logs of radius 2.5 cm at the stated centres as squares of equal area, 600 K faces, 5e-3 kg/m2/s
     P = a["pieces"].reshape(64, 20)
+    h = 0.025 * np.sqrt(np.pi) / 2
     assert a["npieces"] == 3
-    assert np.allclose(P[:3, :4], [[0.35, 0.025, 0, 0.025], [0.45, 0.025, 0, 0.025], [0.40, 0.068, 0, 0.025]])
+    assert np.allclose(P[:3, :4], [[0.35, 0.025, 0, h], [0.45, 0.025, 0, h], [0.40, 0.068, 0, h]])
     assert np.all(P[:3, 8:12] == 600) and np.allclose(P[:3, 12:16], 5e-3)
     # Gaussian hot spot 1800 K at (0.40, 0.12), velocities within +-0.01 m/s, dt = 2 ms by CFL cap
     T = a["T"].reshape(192, 128)
