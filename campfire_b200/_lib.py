@@ -98,6 +98,7 @@ def lib():
         "cfg_batch_synchronize": [vp], "cfg_batch_launch_count": [vp, ip], "cfg_batch_write_params": [vp],
         "cfg_batch_geometry": [vp],
         "cfg_time_kernel": [vp, cs, ci, dp, dp, dp],
+        "cfg_pressure_residual_noalloc": [vp, vp, vp, vp, ci, ci, cd, vp, dp],
     }
     for name, args in sigs.items():
         f = getattr(L, name)

@@ -149,6 +149,18 @@ int cfg_set_cfl(cfg_sim* sim, double cfl, double dt_cap);
 int cfg_set_nray(cfg_sim* sim, int nray);
 /* ||r||2/||rhs||2 of the level-0 pressure equation now (FP64 sums) */
 int cfg_pressure_residual(cfg_sim* sim, double* rel);
+/* ||r||2/||rhs||2 of a level-0 pressure field the caller owns, with no device allocation
+ * (no counterpart in the reference). For callers that cannot allocate at this point: a frame
+ * or serving loop whose device memory is already committed, or that must not stall on the
+ * device-wide synchronisation cudaMalloc/cudaFree can cause. Device arrays in the dense
+ * layouts of js/fluid.js:75-78: p, rhs nx*ny; ax (nx+1)*ny; ay nx*(ny+1); h2 = (cell size)^2,
+ * rounded to f32 as the level uniform. Per-block partial sums go to a fixed 64 KiB
+ * __device__ array held by every GPU that loads the library: at most 1,048,576 cells, larger
+ * grids fail with CFG_ERR_RANGE. The first call on each device looks up that array's device
+ * address; make it before any stream capture. All calls share the array: calls that overlap
+ * on the GPU race. Runs on `stream` (NULL: the legacy default stream) and waits for it. */
+int cfg_pressure_residual_noalloc(const float* p, const float* rhs, const float* ax, const float* ay, int nx, int ny,
+                                  double h2, void* stream, double* rel);
 /* FP64 sums over gas cells, per m of depth: mass, energy (rho cp T), fuel, O2, products,
  * soot masses, heat release rate, max T  (8 doubles) */
 int cfg_budgets(cfg_sim* sim, double* out);
