@@ -754,7 +754,8 @@ int Engine::synchronize() {
   // per-step launch count: kernels outside the loop + kernels per cycle x cycles (scene 0)
   SolveState ss{};
   CFG_CUDA(cudaMemcpy(&ss, d_solve_, sizeof ss, cudaMemcpyDeviceToHost));
-  launches_per_step_ = launches_ + vcycle_launches_ * std::max(ss.cycles, 1);
+  last_cycles_ = std::max(ss.cycles, 1);
+  launches_per_step_ = launches_ + vcycle_launches_ * last_cycles_;
   int err = 0;
   CFG_CUDA(cudaMemcpy(&err, &d_ctl_->err, sizeof err, cudaMemcpyDeviceToHost));
   if (err) {
@@ -838,7 +839,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   const double cells = (double)sc.nx * sc.ny;
   SolveState ss{};
   CFG_CUDA(cudaMemcpy(&ss, d_solve_, sizeof ss, cudaMemcpyDeviceToHost));
-  const double cyc = std::max(ss.cycles, 1);
+  const double cyc = std::max(std::max(ss.cycles, 1), last_cycles_);
   const bool fp64 = any_fp64();
   cudaStream_t s = st();
   const std::string n(name);
@@ -871,7 +872,13 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     b = (17 + 4 * 16) * cells; cnt = cyc;   // prolongation + 4 colour passes
   } else if (n == "mg_coarse") {
     go = [&](int) { launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, coarse_smem_, s); };
-    b = 0; cnt = cyc;
+    // the reference schedule's V-cycle bytes of the levels the block covers (163 B per level cell)
+    b = 0;
+    for (int l = sc.lc; l < sc.nlev; l++) b += 163.0 * sc.lnx[l] * sc.lny[l];
+    cnt = cyc;
+  } else if (n == "defect64") {
+    go = [&](int) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, s); };
+    b = 32 * cells; cnt = fp64 ? cyc : 0;
   } else if (n == "resnorm") {
     go = [&](int) { launch_resnorm(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
     b = (fp64 ? 32 : 16) * cells; cnt = cyc;

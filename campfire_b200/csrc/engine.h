@@ -157,6 +157,7 @@ class Engine {
   cudaGraphExec_t exec_ = nullptr;
   int graph_sub_ = -1;
   int launches_ = 0, launches_per_step_ = 0;
+  int last_cycles_ = 1;        // V-cycles of scene 0's last step, recorded by synchronize()
   int vcycle_launches_ = 0;
   size_t coarse_smem_ = 0;
 };

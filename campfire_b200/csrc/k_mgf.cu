@@ -16,7 +16,7 @@
 // Levels lc..coarsest run in one CTA per scene (coarse block): every level's
 // arrays staged into shared memory by TMA bulk copies, __syncthreads between
 // passes, and the coarsest level's 120 red-black sweeps (pressure.wgsl:132-156)
-// on 256 threads with a named barrier.
+// on 256 threads (one cell each) with a named barrier.
 #include "gas_dev.cuh"
 #include "kernels.h"
 #include "reduce.cuh"
@@ -232,8 +232,7 @@ namespace {
 constexpr int CB_THREADS = 1024;
 constexpr int CB_WARPS = CB_THREADS / 32;
 constexpr int COARSEST_THREADS = 256;   // the coarsest level has at most 256 cells
-// scratch floats: the residual of level lc, or the coarsest stencils (256 x 40 B + a zero slot)
-constexpr int COARSEST_SCRATCH = COARSEST_THREADS * 10 + 4;
+constexpr int COARSEST_SCRATCH = 0;     // the coarsest keeps its stencils in registers
 
 struct LvS { float *p, *rhs, *ax, *ay; int nx, ny, pc, pu; float h2; int pad; };
 
@@ -257,6 +256,7 @@ __device__ __forceinline__ void pass_d(const LvS& L, int color) {
       L.p[k] = diag > 0.f ? (off - L.rhs[k] * L.h2) / diag : 0.f;
     }
 }
+__device__ __forceinline__ void bar_coarsest() { asm volatile("bar.sync 1, %0;" ::"r"(COARSEST_THREADS) : "memory"); }
 }  // namespace
 
 __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __restrict__ scenes, int nscenes, SolveCtl* ctl, int tail) {
@@ -333,63 +333,44 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       }
     __syncthreads();
   }
-  // ---- coarsest (pressure.wgsl:132-156): 120 red-black sweeps from zero in one warp.
-  // The stencils are fixed during the sweeps: threads of the block build them once
-  // into shared memory (coefficients, neighbour slots, diagonal, rhs*h2); a missing
-  // neighbour reads a zero slot with coefficient 0, and adding 0*0 leaves the sum
-  // exactly as the WGSL's skipped term. Lane l then owns cells l, l+32, ... (<= 8).
-  {
+  // ---- coarsest (pressure.wgsl:132-156): 120 red-black sweeps from zero, one cell per thread
+  // of the first 256 (a named barrier keeps the other warps out); each thread's stencil is
+  // fixed during the sweeps and held in registers
+  if (threadIdx.x < COARSEST_THREADS) {
     const LvS L = lv[nl - 1];
-    const int n = L.nx * L.ny;
-    float4* cf = reinterpret_cast<float4*>(sres);               // n coefficient quads
-    int4* nb = reinterpret_cast<int4*>(cf + COARSEST_THREADS);  // n neighbour slots
-    float2* dr = reinterpret_cast<float2*>(nb + COARSEST_THREADS);
-    float* zero = reinterpret_cast<float*>(dr + COARSEST_THREADS);
-    const int zi = (int)(zero - L.p);
-    for (int k = threadIdx.x; k < n; k += CB_THREADS) {
-      const int i = k % L.nx, j = k / L.nx, kp = j * L.pc + i;
-      const float w = L.ax[j * L.pu + i], e = L.ax[j * L.pu + i + 1];
-      const float s = L.ay[j * L.pc + i], nn = L.ay[(j + 1) * L.pc + i];
-      float diag = 0.f;
-      float4 c4 = make_float4(0.f, 0.f, 0.f, 0.f);
-      int4 n4 = make_int4(zi, zi, zi, zi);
-      if (i > 0) { c4.x = w; n4.x = kp - 1; diag += w; } else { diag += 2.f * w; }
-      if (i < L.nx - 1) { c4.y = e; n4.y = kp + 1; diag += e; } else { diag += 2.f * e; }
-      if (j > 0) { c4.z = s; n4.z = kp - L.pc; diag += s; }
-      if (j < L.ny - 1) { c4.w = nn; n4.w = kp + L.pc; diag += nn; } else { diag += 2.f * nn; }
-      cf[k] = c4; nb[k] = n4; dr[k] = make_float2(diag, L.rhs[kp] * L.h2);
+    const int k = threadIdx.x, n = L.nx * L.ny;
+    const int i = k % L.nx, j = k / L.nx;
+    const bool act = k < n;
+    const int kp = j * L.pc + i;
+    float w = 0.f, e = 0.f, s = 0.f, nn = 0.f, diag = 0.f, rh = 0.f;
+    int col = -1;
+    if (act) {
+      w = L.ax[j * L.pu + i]; e = L.ax[j * L.pu + i + 1];
+      s = L.ay[j * L.pc + i]; nn = L.ay[(j + 1) * L.pc + i];
+      if (i > 0) diag += w; else diag += 2.f * w;
+      if (i < L.nx - 1) diag += e; else diag += 2.f * e;
+      if (j > 0) diag += s;
+      if (j < L.ny - 1) diag += nn; else diag += 2.f * nn;
+      rh = L.rhs[kp] * L.h2;
+      col = (i + j) & 1;
       L.p[kp] = 0.f;
     }
-    if (threadIdx.x == 0) *zero = 0.f;
-    __syncthreads();
-    if (warp == 0) {
-      constexpr int M = COARSEST_THREADS / 32;
-      int kp[M], col[M];
+    const bool hw = act && i > 0, he = act && i < L.nx - 1, hs = act && j > 0, hn = act && j < L.ny - 1;
+    float* p = L.p;
+    bar_coarsest();
+    #pragma unroll 1
+    for (int it = 0; it < 120; it++) {
       #pragma unroll
-      for (int m = 0; m < M; m++) {
-        const int k = lane + 32 * m;
-        const int i = k % L.nx, j = k / L.nx;
-        kp[m] = j * L.pc + i;
-        col[m] = k < n ? ((i + j) & 1) : -1;
-      }
-      float* p = L.p;
-      #pragma unroll 1
-      for (int it = 0; it < 120; it++) {
-        #pragma unroll
-        for (int c = 0; c < 2; c++) {
-          #pragma unroll
-          for (int m = 0; m < M; m++) {
-            if (col[m] == c) {
-              const int k = lane + 32 * m;
-              const float4 c4 = cf[k];
-              const int4 n4 = nb[k];
-              const float2 d2 = dr[k];
-              const float off = (((0.f + c4.x * p[n4.x]) + c4.y * p[n4.y]) + c4.z * p[n4.z]) + c4.w * p[n4.w];
-              p[kp[m]] = d2.x > 0.f ? (off - d2.y) / d2.x : 0.f;
-            }
-          }
-          __syncwarp();
+      for (int c = 0; c < 2; c++) {
+        if (col == c) {
+          float off = 0.f;
+          if (hw) off += w * p[kp - 1];
+          if (he) off += e * p[kp + 1];
+          if (hs) off += s * p[kp - L.pc];
+          if (hn) off += nn * p[kp + L.pc];
+          p[kp] = diag > 0.f ? (off - rh) / diag : 0.f;
         }
+        bar_coarsest();
       }
     }
   }
