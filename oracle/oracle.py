@@ -1,11 +1,14 @@
 """ORACLE — test infrastructure, not product code.
 
-ctypes wrapper over oracle/liboracle_gas.so: the CPU restatement of the
-reference WGSL gas step (gas_ref.hpp) and the 1D flame restatement
-(flame1d.c). Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
-leg import this module, as the checker. The method names follow
-js/fluid.js's FluidSim so the parity tests read like the reference's own
-harness (dev/gas_test.html).
+ctypes wrappers over the CPU checkers:
+  * oracle/liboracle_gas.so  — the C++ restatement of the reference WGSL gas step
+    (gas_ref.hpp) and the 1D flame restatement (flame1d.c);
+  * oracle/_ref/libwgslref.so — the reference's own WGSL translated mechanically
+    to C++ (wgsl2cpp.py) under the FluidSim harness (wgsl_harness.cpp); built
+    only where the reference checkout exists.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this
+module, as the checker. Method names follow js/fluid.js's FluidSim so the parity
+tests read like the reference's own harness (dev/gas_test.html).
 """
 from __future__ import annotations
 
@@ -17,56 +20,74 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboracle_gas.so")
+REF_LIB_PATH = os.path.join(_HERE, "_ref", "libwgslref.so")
+REFERENCE_ROOT = "/root/reference"
 
 SOLVE_FIXED, SOLVE_TOL, SOLVE_FP64 = 0, 1, 2
 STAGES = ("advect", "diffuse", "sources", "forces", "coef_rhs", "pressure", "project")
 
 
 def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (g++ -O3 -fopenmp -ffp-contract=off)."""
+    """Compile the restatement with its Makefile (g++ -O3 -fopenmp -ffp-contract=off)."""
     if force or not os.path.exists(LIB_PATH):
-        subprocess.run(["make", "-C", _HERE, "-B" if force else "all"], check=True,
-                       stdout=subprocess.DEVNULL)
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "all"], check=True, stdout=subprocess.DEVNULL)
     return LIB_PATH
 
 
-_lib = None
+def build_ref() -> str | None:
+    """Translate and compile the reference WGSL (only where the reference checkout exists)."""
+    if os.path.isdir(os.path.join(REFERENCE_ROOT, "shaders")):
+        subprocess.run(["make", "-C", _HERE, "ref"], check=True, stdout=subprocess.DEVNULL)
+    return REF_LIB_PATH if os.path.exists(REF_LIB_PATH) else None
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
-        L = ctypes.CDLL(LIB_PATH)
-        vp, ci, cd, cs = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_char_p
-        dp = ctypes.POINTER(ctypes.c_double)
-        L.orc_error.restype = cs
-        L.orc_create.restype = vp
-        L.orc_create.argtypes = [ci, ci, cd, cd, ci]
-        for name, args in {
-            "orc_destroy": [vp], "orc_reset": [vp], "orc_write_params": [vp],
-            "orc_set_param": [vp, cs, cd], "orc_get_param": [vp, cs, dp],
-            "orc_set_dt": [vp, cd], "orc_set_cfl": [vp, cd, cd], "orc_set_frame": [vp, ctypes.c_uint],
-            "orc_set_nray": [vp, ci], "orc_set_solver": [vp, ci, ci, cd, ci],
-            "orc_upload_pieces": [vp, ctypes.POINTER(ctypes.c_float), ci],
-            "orc_clear_geometry": [vp], "orc_geometry": [vp], "orc_radiation": [vp],
-            "orc_step": [vp, ci], "orc_vcycle": [vp, ci], "orc_stage": [vp, cs],
-            "orc_read_field": [vp, cs, dp, ctypes.c_size_t],
-            "orc_write_field": [vp, cs, dp, ctypes.c_size_t],
-            "orc_readback": [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float),
-                             ctypes.POINTER(ctypes.c_int32)],
-            "orc_budgets": [vp, dp], "orc_info": [vp, dp],
-            "orc_level_dims": [vp, ci, ctypes.POINTER(ctypes.c_int)],
-            "orc_pressure_residual": [vp, dp],
-        }.items():
-            fn = getattr(L, name)
+def _declare(L, pfx):
+    vp, ci, cd, cs = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_char_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    getattr(L, pfx + "error").restype = cs
+    getattr(L, pfx + "create").restype = vp
+    getattr(L, pfx + "create").argtypes = [ci, ci, cd, cd, ci]
+    sigs = {
+        "destroy": [vp], "reset": [vp], "write_params": [vp],
+        "set_param": [vp, cs, cd], "get_param": [vp, cs, dp],
+        "set_dt": [vp, cd], "set_cfl": [vp, cd, cd], "set_frame": [vp, ctypes.c_uint],
+        "set_nray": [vp, ci], "set_solver": [vp, ci, ci, cd, ci],
+        "upload_pieces": [vp, ctypes.POINTER(ctypes.c_float), ci],
+        "clear_geometry": [vp], "geometry": [vp], "radiation": [vp],
+        "step": [vp, ci], "vcycle": [vp, ci], "stage": [vp, cs],
+        "read_field": [vp, cs, dp, ctypes.c_size_t], "write_field": [vp, cs, dp, ctypes.c_size_t],
+        "readback": [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float),
+                     ctypes.POINTER(ctypes.c_int32)],
+        "budgets": [vp, dp], "info": [vp, dp], "level_dims": [vp, ci, ctypes.POINTER(ctypes.c_int)],
+        "pressure_residual": [vp, dp],
+    }
+    for name, args in sigs.items():
+        fn = getattr(L, pfx + name, None)
+        if fn is not None:
             fn.restype = ci
             fn.argtypes = args
-        L.flame1d_speed.restype = cd
-        L.flame1d_speed.argtypes = [cd] * 7 + [dp]
-        _lib = L
-    return _lib
+
+
+_libs = {}
+
+
+def lib(which: str = "restatement"):
+    """The restatement ("restatement") or the translated reference WGSL ("wgsl")."""
+    if which not in _libs:
+        if which == "restatement":
+            if not os.path.exists(LIB_PATH):
+                build()
+            L = ctypes.CDLL(LIB_PATH)
+            _declare(L, "orc_")
+            L.flame1d_speed.restype = ctypes.c_double
+            L.flame1d_speed.argtypes = [ctypes.c_double] * 7 + [ctypes.POINTER(ctypes.c_double)]
+        else:
+            if not os.path.exists(REF_LIB_PATH):
+                raise OracleError("oracle/_ref/libwgslref.so is not built (needs the reference checkout)")
+            L = ctypes.CDLL(REF_LIB_PATH)
+            _declare(L, "wref_")
+        _libs[which] = L
+    return _libs[which]
 
 
 def flame_speed(B=2e10, Ta=15000.0, dx=5e-5, F=1.0, phi=1.0, L=0.03, tEnd=1.0):
@@ -80,25 +101,40 @@ class OracleError(RuntimeError):
     pass
 
 
-def _chk(rc):
-    if rc != 0:
-        raise OracleError(lib().orc_error().decode())
+class _Fns:
+    def __init__(self, L, pfx):
+        self._L, self._pfx = L, pfx
+
+    def __getattr__(self, name):
+        fn = getattr(self._L, self._pfx + name, None)
+        if fn is None:
+            raise OracleError(f"{self._pfx}{name} is not provided by this checker")
+        return fn
 
 
 class OracleSim:
-    """FluidSim-shaped wrapper over the CPU oracle (fp64=False: f32 parity oracle)."""
+    """FluidSim-shaped CPU checker.
 
-    def __init__(self, nx: int, ny: int, width: float, dt: float, fp64: bool = False):
-        self._L = lib()
-        h = self._L.orc_create(nx, ny, width, dt, 1 if fp64 else 0)
+    impl="restatement": the C++ restatement (fp64=False: f32 parity oracle, True: FP64).
+    impl="wgsl": the reference's WGSL, mechanically translated (f32, one V-cycle per step).
+    """
+
+    def __init__(self, nx: int, ny: int, width: float, dt: float, fp64: bool = False, impl: str = "restatement"):
+        L = lib(impl)
+        self._f = _Fns(L, "orc_" if impl == "restatement" else "wref_")
+        h = self._f.create(nx, ny, width, dt, 1 if fp64 else 0)
         if not h:
-            raise OracleError(self._L.orc_error().decode())
+            raise OracleError(self._f.error().decode())
         self._h = h
-        self.nx, self.ny, self.fp64 = nx, ny, fp64
+        self.nx, self.ny, self.fp64, self.impl = nx, ny, fp64, impl
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise OracleError(self._f.error().decode())
 
     def close(self):
-        if self._h:
-            self._L.orc_destroy(self._h)
+        if getattr(self, "_h", None):
+            self._f.destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -108,35 +144,35 @@ class OracleSim:
             pass
 
     # -- FluidSim surface
-    def reset(self): _chk(self._L.orc_reset(self._h))
-    def set_param(self, k, v): _chk(self._L.orc_set_param(self._h, k.encode(), float(v)))
+    def reset(self): self._chk(self._f.reset(self._h))
+    def set_param(self, k, v): self._chk(self._f.set_param(self._h, k.encode(), float(v)))
 
     def get_param(self, k):
         v = ctypes.c_double()
-        _chk(self._L.orc_get_param(self._h, k.encode(), ctypes.byref(v)))
+        self._chk(self._f.get_param(self._h, k.encode(), ctypes.byref(v)))
         return v.value
 
-    def write_params(self): _chk(self._L.orc_write_params(self._h))
-    def set_dt(self, dt): _chk(self._L.orc_set_dt(self._h, dt))
-    def set_cfl(self, cfl, dt_cap): _chk(self._L.orc_set_cfl(self._h, cfl, dt_cap))
-    def set_frame(self, f): _chk(self._L.orc_set_frame(self._h, f))
-    def set_nray(self, n): _chk(self._L.orc_set_nray(self._h, n))
+    def write_params(self): self._chk(self._f.write_params(self._h))
+    def set_dt(self, dt): self._chk(self._f.set_dt(self._h, dt))
+    def set_cfl(self, cfl, dt_cap): self._chk(self._f.set_cfl(self._h, cfl, dt_cap))
+    def set_frame(self, f): self._chk(self._f.set_frame(self._h, f))
+    def set_nray(self, n): self._chk(self._f.set_nray(self._h, n))
 
     def set_solver(self, mode=SOLVE_FIXED, ncycles=1, tol=1e-6, max_cycles=50):
-        _chk(self._L.orc_set_solver(self._h, mode, ncycles, tol, max_cycles))
+        self._chk(self._f.set_solver(self._h, mode, ncycles, tol, max_cycles))
 
     def upload_pieces(self, data, n):
         a = np.zeros(64 * 20, np.float32)
         d = np.asarray(data, np.float32).ravel()
         a[: d.size] = d
-        _chk(self._L.orc_upload_pieces(self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n))
+        self._chk(self._f.upload_pieces(self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n))
 
-    def clear_geometry(self): _chk(self._L.orc_clear_geometry(self._h))
-    def geometry(self): _chk(self._L.orc_geometry(self._h))
-    def radiation(self): _chk(self._L.orc_radiation(self._h))
-    def step(self, n=1): _chk(self._L.orc_step(self._h, n))
-    def vcycle(self, nu=2): _chk(self._L.orc_vcycle(self._h, nu))
-    def stage(self, name): _chk(self._L.orc_stage(self._h, name.encode()))
+    def clear_geometry(self): self._chk(self._f.clear_geometry(self._h))
+    def geometry(self): self._chk(self._f.geometry(self._h))
+    def radiation(self): self._chk(self._f.radiation(self._h))
+    def step(self, n=1): self._chk(self._f.step(self._h, n))
+    def vcycle(self, nu=2): self._chk(self._f.vcycle(self._h, nu))
+    def stage(self, name): self._chk(self._f.stage(self._h, name.encode()))
 
     def field_size(self, name):
         nx, ny = self.nx, self.ny
@@ -153,42 +189,42 @@ class OracleSim:
         if name in ("SQ", "cellG"):
             return 2 * nx * ny
         d = (ctypes.c_int * 2)()
-        _chk(self._L.orc_level_dims(self._h, lvl, d))
+        self._chk(self._f.level_dims(self._h, lvl, d))
         lx, ly = d[0], d[1]
         return {"p": lx * ly, "rhs": lx * ly, "ax": (lx + 1) * ly, "ay": lx * (ly + 1)}[base]
 
     def read(self, name):
         n = self.field_size(name)
         out = np.empty(n, np.float64)
-        _chk(self._L.orc_read_field(self._h, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+        self._chk(self._f.read_field(self._h, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
         return out
 
     def write(self, name, arr):
         a = np.ascontiguousarray(np.asarray(arr, np.float64).ravel())
-        _chk(self._L.orc_write_field(self._h, name.encode(), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size))
+        self._chk(self._f.write_field(self._h, name.encode(), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size))
 
     def readback(self):
         acc = np.zeros(528, np.int32)
         rad = np.zeros(320 * 4, np.float32)
         fw = np.zeros(256, np.int32)
-        _chk(self._L.orc_readback(self._h, acc.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
-                                  rad.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
-                                  fw.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        self._chk(self._f.readback(self._h, acc.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                   rad.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                   fw.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
         return {"acc": acc, "rad": rad, "faceW": fw}
 
     def budgets(self):
         o = np.zeros(8, np.float64)
-        _chk(self._L.orc_budgets(self._h, o.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        self._chk(self._f.budgets(self._h, o.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return o
 
     def info(self):
         o = np.zeros(16, np.float64)
-        _chk(self._L.orc_info(self._h, o.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        self._chk(self._f.info(self._h, o.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         keys = ["nx", "ny", "dx", "dt", "time", "frame", "diffSub", "levels", "last_cycles",
                 "last_rel", "height", "last_rel0"]
         return dict(zip(keys, o[: len(keys)].tolist()))
 
     def pressure_residual(self):
         v = ctypes.c_double()
-        _chk(self._L.orc_pressure_residual(self._h, ctypes.byref(v)))
+        self._chk(self._f.pressure_residual(self._h, ctypes.byref(v)))
         return v.value

@@ -1,0 +1,157 @@
+"""Generates the golden fixtures of the gas step (tests/golden/*.npz).
+
+The outputs come from the reference itself: its WGSL kernels (shaders/*.wgsl and
+the sampler text of js/gpu.js) translated mechanically to C++ by
+oracle/wgsl2cpp.py and driven in FluidSim's dispatch order (js/fluid.js) by
+oracle/wgsl_harness.cpp, built by `make -C oracle ref` into oracle/_ref/.
+Needs the reference checkout (default /root/reference, or $CAMPFIRE_REF) and
+the product library for the scene generator; the fixtures themselves are
+self-contained (inputs and outputs), so the tests read only the .npz files.
+
+Each fixture holds, for one seeded scene:
+  in_*      the scene: parameter names/values, pieces, npieces, T, Y, U, V
+  geo_*     encodeGeometry: cellG (sdf, piece id), fx, fy, faceW
+  acc       the acc readback after each of `steps` steps (frame = step index)
+  fin_*     the state after those steps
+  st_<stage>_<field>
+            the fields each stage writes, stage by stage, during one more step
+  rad       encodeRadiation after that step
+
+    python tests/golden/make_golden.py            # rewrite the fixtures
+"""
+from __future__ import annotations
+
+import glob
+import hashlib
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+REF = os.environ.get("CAMPFIRE_REF", "/root/reference")
+STATE = ("T", "Y", "U", "V", "T2", "Y2", "U2", "V2", "SQ", "p")
+STAGE_OUT = {
+    "advect": ("T2", "Y2", "U2", "V2"),
+    "diffuse": ("T", "Y"),
+    "sources": ("T", "Y", "SQ"),
+    "forces": ("U", "V"),
+    "coef_rhs": ("rhs", "ax", "ay"),
+    "pressure": ("p",),
+    "project": ("U", "V"),
+}
+STAGES = tuple(STAGE_OUT)
+
+# name, scene kind, nx, ny, width, seed, steps, extra parameters
+CASES = [
+    ("logs_32x48", 0, 32, 48, 0.8, 101, 12, {}),
+    ("tepee_diff3_40x64", 1, 40, 64, 0.5, 102, 10, {"diffMult": 40.0}),
+    ("floor_heater_burner_32x48", 2, 32, 48, 0.4, 103, 10,
+     {"diffMult": 200.0, "heaterX0": 0.1, "heaterX1": 0.2, "heaterY1": 0.03, "heaterT": 900.0,
+      "burnerX0": 0.25, "burnerX1": 0.3, "burnerFlux": 0.02, "burnerT": 600.0}),
+]
+
+
+def shader_digest(ref: str) -> str:
+    h = hashlib.sha256()
+    for f in sorted(glob.glob(os.path.join(ref, "shaders", "*.wgsl"))) + [os.path.join(ref, "js", "gpu.js")]:
+        with open(f, "rb") as fh:
+            h.update(os.path.relpath(f, ref).encode())
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def level_fields(sim, base):
+    nl = int(sim.info()["levels"])
+    return [base if l == 0 else f"{base}.{l}" for l in range(nl)]
+
+
+def stage_fields(sim, stage):
+    out = []
+    for f in STAGE_OUT[stage]:
+        out += level_fields(sim, f) if f in ("ax", "ay") else [f]
+    return out
+
+
+def make_case(om, cb, name, kind, nx, ny, width, seed, steps, extra):
+    from campfire_b200.fluid import SCENE_PARAM_KEYS
+    sc = cb.generate_scene(kind, nx, ny, width, seed)
+    s = om.OracleSim(nx, ny, width, sc["dt"], impl="wgsl")
+    names = list(SCENE_PARAM_KEYS) + list(extra)
+    vals = [sc["params"][k] for k in SCENE_PARAM_KEYS] + [extra[k] for k in extra]
+    d = {
+        "meta_name": np.array(name), "meta_dims": np.array([nx, ny], np.int32), "meta_width": np.float64(width),
+        "meta_dt": np.float64(sc["dt"]), "meta_steps": np.int32(steps), "meta_shaders_sha256": np.array(shader_digest(REF)),
+        "in_param_names": np.array(names), "in_param_values": np.array(vals, np.float64),
+        "in_pieces": np.asarray(sc["pieces"], np.float32).ravel(), "in_npieces": np.int32(sc["npieces"]),
+    }
+    for k in ("T", "Y", "U", "V"):
+        d["in_" + k] = np.asarray(sc[k], np.float32).ravel()
+    apply_inputs(s, d)
+    d["meta_levels"] = np.int32(s.info()["levels"])
+    d["meta_diffsub"] = np.int32(s.info()["diffSub"])
+    cg = s.read("cellG").reshape(-1, 2)
+    d["geo_cellG_sdf"] = cg[:, 0].astype(np.float32)
+    d["geo_cellG_id"] = cg[:, 1].astype(np.uint32)
+    d["geo_fx"] = s.read("fx").astype(np.float32)
+    d["geo_fy"] = s.read("fy").astype(np.float32)
+    d["geo_faceW"] = s.readback()["faceW"].astype(np.int32)
+    acc = []
+    for i in range(steps):
+        s.set_frame(i)
+        s.write_params()
+        s.step()
+        acc.append(s.readback()["acc"].copy())
+    d["acc"] = np.stack(acc).astype(np.int32)
+    for f in STATE:
+        d["fin_" + f] = s.read(f).astype(np.float32)
+    for f in ("rhs", "ax", "ay"):
+        for lf in level_fields(s, f):
+            d["fin_" + lf] = s.read(lf).astype(np.float32)
+    for lf in level_fields(s, "p")[1:]:
+        d["fin_" + lf] = s.read(lf).astype(np.float32)
+    s.set_frame(steps)
+    s.write_params()
+    for st in STAGES:
+        s.stage(st)
+        for f in stage_fields(s, st):
+            d[f"st_{st}_{f}"] = s.read(f).astype(np.float32)
+    d["st_acc"] = s.readback()["acc"].astype(np.int32)
+    s.radiation()
+    d["rad"] = s.readback()["rad"].astype(np.float32)
+    s.close()
+    return d
+
+
+def apply_inputs(sim, d):
+    """Scene set-up in FluidSim's order: params, pieces, writeParams, reset, fields, geometry."""
+    for k, v in zip(d["in_param_names"].tolist(), d["in_param_values"].tolist()):
+        sim.set_param(k, v)
+    sim.upload_pieces(d["in_pieces"], int(d["in_npieces"]))
+    sim.write_params()
+    sim.reset()
+    for k in ("T", "Y", "U", "V"):
+        sim.write(k, d["in_" + k])
+    sim.write("T2", d["in_T"])
+    sim.write("Y2", d["in_Y"])
+    sim.clear_geometry()
+    sim.geometry()
+
+
+def main():
+    from oracle import oracle as om
+    import campfire_b200 as cb
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
+    for case in CASES:
+        d = make_case(om, cb, *case)
+        path = os.path.join(HERE, case[0] + ".npz")
+        np.savez_compressed(path, **d)
+        print(f"{path}: {os.path.getsize(path)} bytes, levels {int(d['meta_levels'])}, diffSub {int(d['meta_diffsub'])}")
+
+
+if __name__ == "__main__":
+    main()
