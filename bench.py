@@ -45,6 +45,10 @@ METRIC = "cell-updates/s"
 B_FIXED = 156 + 68 + 28 + 20 + 28 + 13.3 + 32
 
 
+# DRAM bytes (read + write) per launch of a kernel, from one ncu capture of the workload
+NCU_TRAFFIC = {("plain", "mg_coarse"): 164096, ("plain", "mg_down0"): 1651712}
+
+
 def bytes_per_cell(diff_sub: int, cycles: float, fp64: bool) -> float:
     b = B_FIXED + 48.0 * diff_sub + 216.8 * cycles
     if fp64:
@@ -137,6 +141,78 @@ def run_cpu(workload: str, steps: int, warmup: int, threads: int):
     return nx * ny * steps / dt, dt, cyc / max(steps, 1)
 
 
+BATCH_CLASSES = ((96, 144), (128, 192), (192, 288), (256, 384))
+
+
+def batch_scenes(n: int = 64, seed: int = 2000):
+    """64 floor-log scenes of uneven size: size class uniform, 2-6 logs, B x logU[0.5,2], YOamb ~ U[0.18,0.233]."""
+    import numpy as np
+    import campfire_b200 as cb
+    idx = np.random.default_rng(seed).integers(0, len(BATCH_CLASSES), n)
+    return [cb.generate_scene(2, *BATCH_CLASSES[i], 0.8, seed + k) for k, i in enumerate(idx)]
+
+
+def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cycles: int, plain_steps: int):
+    """Batched gas step of 64 uneven scenes (one launch per kernel for all scenes, one graph per step)
+    against the same scenes stepped one by one with the plain single-scene step."""
+    import torch
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    scenes = batch_scenes()
+    cells = sum(s["nx"] * s["ny"] for s in scenes)
+    b = cb.Batch([(s["nx"], s["ny"]) for s in scenes], 0.8, [s["dt"] for s in scenes], device=dev.index)
+    for v, s in zip(b.scenes, scenes):
+        load_scene(v, s)
+    b.set_solver(cb.SOLVE_FP64, 1, tol, max_cycles)
+    b.set_stream(stream.cuda_stream)
+    b.step(warmup)
+    b.synchronize()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        b.step(1)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    b.synchronize()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    cyc = [v.info()["last_cycles"] for v in b.scenes]
+    rel = max(v.info()["last_rel"] for v in b.scenes)
+    launches = b.launch_count()
+    b.close()
+    batched = cells * steps / (ms / 1e3)
+
+    # the same scenes, one by one, through the plain single-scene step (same solver, same tolerance)
+    plain_ms, plain_cells = 0.0, 0
+    for s in scenes:
+        g = cb.FluidSim(dev.index, {"nx": s["nx"], "ny": s["ny"], "dt": s["dt"]}, width=0.8).init()
+        load_scene(g, s)
+        g.set_solver(cb.SOLVE_FP64, 1, tol, max_cycles)
+        g.set_stream(stream.cuda_stream)
+        g.step(warmup)
+        g.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(0.0)
+        e0.record(stream)
+        g.step(plain_steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        g.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        plain_cells += s["nx"] * s["ny"] * plain_steps
+        g.close()
+    plain = plain_cells / (plain_ms / 1e3)
+    return {"value": batched, "unit": METRIC, "scenes": len(scenes), "cells": cells, "steps": steps,
+            "ms_per_step": ms / steps, "launches_per_step": launches,
+            "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": max_cycles,
+                         "cycles_last_step": {"min": min(cyc), "max": max(cyc)}, "max_rel_residual": rel},
+            "sizes": {f"{nx}x{ny}": sum(1 for s in scenes if (s["nx"], s["ny"]) == (nx, ny))
+                      for nx, ny in BATCH_CLASSES},
+            "plain_one_by_one": {"value": plain, "unit": METRIC, "steps_per_scene": plain_steps},
+            "batched_over_plain": batched / plain}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -146,6 +222,8 @@ def main():
     ap.add_argument("--workload", default="plain", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-steps", type=int, default=10,
+                    help="timed steps of the 64-scene batched measurement added to the line (0: skip)")
     ap.add_argument("--launch", default="graph", choices=["graph", "stream"],
                     help="graph: one CUDA graph per step (pressure loop as a device-side WHILE node); "
                          "stream: kernel by kernel, the host polling the loop decision (for profilers that "
@@ -271,10 +349,16 @@ def main():
     achieved = dk["bytes"] / (dk["ms"] / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
-            "traffic": None, "bytes_per_launch": dk["bytes"], "launch_ms": dk["ms"],
+            "traffic": NCU_TRAFFIC.get((a.workload, dom)), "traffic_source": "ncu dram__bytes_read.sum + "
+            "dram__bytes_write.sum, one capture of this workload (--set full)",
+            "bytes_per_launch": dk["bytes"], "launch_ms": dk["ms"],
             "step_bytes_per_cell": bytes_per_cell(info["diffSub"], info["last_cycles"], True),
             "step_frac": (value / world) * bytes_per_cell(info["diffSub"], info["last_cycles"], True) / 1e9 / hbm,
             "kernels": {k: {"ms": round(v["ms"], 5), "per_step": v["per_step"]} for k, v in kern.items()}}
+
+    batched = None
+    if a.batched_steps > 0:
+        batched = run_batched(dev, stream, flush, a.batched_steps, 3, 1e-10, 300, 3)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -294,7 +378,8 @@ def main():
                 # and dx/alpha of the diffusion rule (16 B); D2H: acc + rad + faceW
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 204 + 16,
                         "d2h_bytes_per_step": 528 * 4 + 320 * 16 + 256 * 4},
-                "gpu_launches": launches * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+                "gpu_launches": launches * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "batched": batched}
         print(json.dumps(line))
     sim.close()
     if world > 1:
