@@ -25,7 +25,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompile
                      "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
 SOURCES = ["k_advect.cu", "k_diffsrc.cu", "k_forces.cu", "k_mg.cu", "k_mgf.cu", "k_misc.cu", "noalloc.cu", "engine.cu",
            "capi.cpp", "scene.cpp"]
-HEADERS = ["gas_dev.cuh", "kernels.h", "reduce.cuh", "engine.h"]
+HEADERS = ["gas_dev.cuh", "kernels.h", "reduce.cuh", "engine.h", "tma.cuh"]
 
 
 def nvcc() -> str:

@@ -7,6 +7,8 @@
 // node: the kernel that finishes each residual reduction decides, per scene,
 // whether another cycle runs and sets the node's condition on the device, so a
 // step never waits on the host.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,6 +16,7 @@
 #include <cstddef>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -153,6 +156,59 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
 }
 
 // One arena per scene; every array 256-byte aligned, rows pitched to 32 elements.
+namespace {
+// cuTensorMapEncodeTiled from the driver (through the runtime's entry-point query,
+// so the library links against cudart only)
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 2D f32 map of a pitched array (w x h elements, rows `pitch` elements apart) with a
+// bw x bh box; out-of-range elements read as zero
+int encode_map(CUtensorMap* m, const float* base, int w, int h, int pitch, int bw, int bh) {
+  auto fn = tmap_encoder();
+  if (!fn) return fail(CFG_ERR_NODEV, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)h};
+  const cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  const cuuint32_t es[2] = {1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(CFG_ERR_INVAL, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return CFG_OK;
+}
+}  // namespace
+
+// Tensor maps of every level for the fused smoother kernels, copied into the arena.
+int Engine::build_tmaps(Scene& sc) {
+  static_assert(sizeof(CUtensorMap) == TMAP_BYTES, "CUtensorMap is 128 bytes");
+  const SceneDesc& d = sc.desc;
+  std::vector<CUtensorMap> maps((size_t)MAX_LEVELS * TM_PER_LEVEL);
+  std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+  for (int l = 0; l < sc.nlev; l++) {
+    const LevelDesc& L = d.lev[l];
+    CUtensorMap* m = &maps[(size_t)l * TM_PER_LEVEL];
+    CFG_TRY(encode_map(&m[TM_P], L.p, L.nx, L.ny, L.pc, MGF_BW, MGF_BH));
+    CFG_TRY(encode_map(&m[TM_PB], L.pb, L.nx, L.ny, L.pc, MGF_BW, MGF_BH));
+    CFG_TRY(encode_map(&m[TM_RHS], L.rhs, L.nx, L.ny, L.pc, MGF_BW, MGF_BH));
+    CFG_TRY(encode_map(&m[TM_AX], L.ax, L.nx + 1, L.ny, L.pu, MGF_BW, MGF_BH));
+    CFG_TRY(encode_map(&m[TM_AY], L.ay, L.nx, L.ny + 1, L.pc, MGF_BW, MGF_BH + 1));
+    CFG_TRY(encode_map(&m[TM_PC], L.p, L.nx, L.ny, L.pc, MGF_CBW, MGF_CBH));
+  }
+  CFG_CUDA(cudaMemcpy(const_cast<char*>(d.tmap), maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+  return CFG_OK;
+}
+
 int Engine::alloc_scene(Scene& sc) {
   SceneDesc& d = sc.desc;
   std::memset(&d, 0, sizeof d);
@@ -175,6 +231,7 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4}, {(void**)&d.rad, RAD_LEN * 16},
     {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 8},
+    {(void**)&d.tmap, (size_t)MAX_LEVELS * TM_PER_LEVEL * TMAP_BYTES},
   };
   double h = sc.dxd;
   for (int l = 0; l < sc.nlev; l++) {
@@ -199,7 +256,7 @@ int Engine::alloc_scene(Scene& sc) {
   sc.arena = arena; sc.arena_bytes = total;
   size_t off = 0;
   for (auto& it : items) { *it.ptr = (char*)arena + off; off += (it.bytes + 255) / 256 * 256; }
-  return CFG_OK;
+  return build_tmaps(sc);
 }
 
 int Engine::build_worklists() {
@@ -584,7 +641,7 @@ void Engine::enqueue_vcycle(cudaStream_t s) {
   const int tail = any_fp64() ? 2 : 1;
   for (int l = 0; l < LD; l++) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
-    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, s);
+    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, s);
     vcycle_launches_++;
   }
   launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, coarse_smem_, s);
@@ -865,7 +922,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     go = [&](int) { launch_coarsest(d_scenes_, nscenes(), s); };
     b = 0; cnt = cyc;
   } else if (n == "mg_down0") {
-    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, s); };
+    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, s); };
     b = (4 * 16 + 18) * cells; cnt = cyc;   // 4 colour passes + residual restriction
   } else if (n == "mg_up0") {
     go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 0, d_ctl_, s); };

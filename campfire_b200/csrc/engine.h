@@ -115,6 +115,7 @@ class Engine {
 
  private:
   int alloc_scene(Scene& sc);
+  int build_tmaps(Scene& sc);
   int upload_desc(int s);
   int upload_descs();
   int upload_ctl();

@@ -65,6 +65,7 @@ struct SceneDesc {
   float4 *rad;
   double *p64, *rhs64, *part;   // FP64 pressure, FP64 rhs, per-CTA partial sums
   SolveState* solve;
+  const char* tmap;         // TMA tensor maps of the levels (TM_PER_LEVEL per level, 128 bytes each)
   LevelDesc lev[MAX_LEVELS];
 };
 

@@ -2,13 +2,14 @@
 // js/fluid.js:294-312) with temporal blocking.
 //
 // Each fine level l < lc is handled by two kernels per cycle:
-//   down: load p, rhs, ax, ay on the tile plus a 5-cell halo into shared
-//         memory, run the 4 colour passes (red, black, red, black), each one
-//         cell narrower than the last, then the residual of the tile's cells
-//         and its restriction to the coarse rhs (coarse p = 0);
-//   up:   the same halo load, bilinear prolongation of the coarse correction,
-//         4 colour passes (black, red, black, red); on level 0 also the
-//         residual norm (FP32 modes) or p64 += p (FP64 defect correction).
+//   down: stage p, rhs, ax, ay of the tile plus a 5-cell halo into shared
+//         memory with TMA tensor copies, run the 4 colour passes (red, black,
+//         red, black), each one cell narrower than the last, then the residual
+//         of the tile's cells and its restriction to the coarse rhs (coarse p = 0);
+//   up:   the same staging (and the coarse p under the tile), bilinear
+//         prolongation of the coarse correction, 4 colour passes (black, red,
+//         black, red); on level 0 also the residual norm (FP32 modes) or
+//         p64 += p (FP64 defect correction).
 // A cell update reads exactly the neighbour values the separate dispatches
 // would read, so the result equals the reference schedule bit for bit.
 // Down kernels read p and write pb; up kernels read pb and write p, so no CTA
@@ -16,7 +17,7 @@
 // Levels lc..coarsest run in one CTA per scene (coarse block): every level's
 // arrays staged into shared memory by TMA bulk copies, __syncthreads between
 // passes, and the coarsest level's 120 red-black sweeps (pressure.wgsl:132-156)
-// on 256 threads (one cell each) with a named barrier.
+// on one thread per red/black cell pair with a named barrier.
 #include "gas_dev.cuh"
 #include "kernels.h"
 #include "reduce.cuh"
@@ -28,30 +29,28 @@ namespace cfg {
 
 namespace {
 
-constexpr int H_DOWN = 5;   // 4 passes + the residual's neighbours
-constexpr int H_UP = 5;     // 4 passes + the level-0 residual's neighbours
-
+// Shared tile of the fused kernels: every array staged as an MGF_BW-wide box whose
+// column 0 is level column sx and row 0 is level row sy (ay has one more row).
 struct Tile {
-  // shared arrays of a (RW x RH) cell region at origin (rx0, ry0)
   float *p, *rhs, *ax, *ay;
-  int RW, RH, rx0, ry0;
-  __device__ __forceinline__ int c(int i, int j) const { return (j - ry0) * RW + (i - rx0); }
-  __device__ __forceinline__ int u(int i, int j) const { return (j - ry0) * (RW + 1) + (i - rx0); }
+  int sx, sy;
+  __device__ __forceinline__ int c(int i, int j) const { return (j - sy) * MGF_BW + (i - sx); }
 };
 
-// pressure.wgsl:77-85 on the shared tile (i, j in level coordinates)
+// pressure.wgsl:77-85 on the shared tile (i, j in level coordinates); ax[c] is the
+// west face of cell c, ay[c] its south face
 __device__ __forceinline__ void stencil_s(const Tile& t, int nx, int ny, int i, int j, float& off, float& diag) {
   off = 0.f; diag = 0.f;
-  const int k = t.c(i, j), ku = t.u(i, j);
-  const float w = t.ax[ku], e = t.ax[ku + 1], s = t.ay[k], n = t.ay[k + t.RW];
+  const int k = t.c(i, j);
+  const float w = t.ax[k], e = t.ax[k + 1], s = t.ay[k], n = t.ay[k + MGF_BW];
   if (i > 0) { off += w * t.p[k - 1]; diag += w; } else { diag += 2.f * w; }
   if (i < nx - 1) { off += e * t.p[k + 1]; diag += e; } else { diag += 2.f * e; }
-  if (j > 0) { off += s * t.p[k - t.RW]; diag += s; }
-  if (j < ny - 1) { off += n * t.p[k + t.RW]; diag += n; } else { diag += 2.f * n; }
+  if (j > 0) { off += s * t.p[k - MGF_BW]; diag += s; }
+  if (j < ny - 1) { off += n * t.p[k + MGF_BW]; diag += n; } else { diag += 2.f * n; }
 }
 __device__ __forceinline__ float diag_s(const Tile& t, int nx, int ny, int i, int j) {
-  const int k = t.c(i, j), ku = t.u(i, j);
-  const float w = t.ax[ku], e = t.ax[ku + 1], s = t.ay[k], n = t.ay[k + t.RW];
+  const int k = t.c(i, j);
+  const float w = t.ax[k], e = t.ax[k + 1], s = t.ay[k], n = t.ay[k + MGF_BW];
   float diag = 0.f;
   if (i > 0) diag += w; else diag += 2.f * w;
   if (i < nx - 1) diag += e; else diag += 2.f * e;
@@ -60,38 +59,62 @@ __device__ __forceinline__ float diag_s(const Tile& t, int nx, int ny, int i, in
   return diag;
 }
 
-// load p (from src), rhs, ax, ay of the region, clipped to the level
-__device__ __forceinline__ void load_tile(const Tile& t, const LevelDesc& L, const float* src) {
-  const int RW = t.RW, RH = t.RH;
-  for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
-    const int i = t.rx0 + e % RW, j = t.ry0 + e / RW;
-    if (i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
-    t.p[e] = src[j * L.pc + i];
-    t.rhs[e] = __ldg(L.rhs + j * L.pc + i);
+constexpr uint32_t BOX_BYTES = MGF_BW * MGF_BH * 4, BOX_AY_BYTES = MGF_BW * (MGF_BH + 1) * 4;
+constexpr uint32_t CBOX_BYTES = MGF_CBW * MGF_CBH * 4;
+
+__device__ __forceinline__ const void* tmap_of(const SceneDesc& S, int level, int kind) {
+  return S.tmap + (size_t)(level * TM_PER_LEVEL + kind) * TMAP_BYTES;
+}
+
+// one thread issues the tile's tensor copies (p from map `pkind`), all threads wait
+// (bounded); false if the copies did not land, after recording the error and
+// waiting once more for the copies still in flight
+__device__ __forceinline__ bool stage_tile(const SceneDesc& S, int level, int pkind, const Tile& t, float* cp, int cx,
+                                           int cy, uint64_t* bar, SolveCtl* ctl) {
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, 3 * BOX_BYTES + BOX_AY_BYTES + (cp ? CBOX_BYTES : 0u));
+    tma_load_2d(t.p, tmap_of(S, level, pkind), t.sx, t.sy, bar);
+    tma_load_2d(t.rhs, tmap_of(S, level, TM_RHS), t.sx, t.sy, bar);
+    tma_load_2d(t.ax, tmap_of(S, level, TM_AX), t.sx, t.sy, bar);
+    tma_load_2d(t.ay, tmap_of(S, level, TM_AY), t.sx, t.sy, bar);
+    if (cp) tma_load_2d(cp, tmap_of(S, level + 1, TM_PC), cx, cy, bar);
   }
-  for (int e = threadIdx.x; e < RH * (RW + 1); e += blockDim.x) {
-    const int i = t.rx0 + e % (RW + 1), j = t.ry0 + e / (RW + 1);
-    if (i < 0 || i > L.nx || j < 0 || j >= L.ny) continue;
-    t.ax[e] = __ldg(L.ax + j * L.pu + i);
+  __syncthreads();
+  const bool ok = mbar_wait(bar, 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(&ctl->err, 1);
+    mbar_wait(bar, 0);
+    return false;
   }
-  for (int e = threadIdx.x; e < (RH + 1) * RW; e += blockDim.x) {
-    const int i = t.rx0 + e % RW, j = t.ry0 + e / RW;
-    if (i < 0 || i >= L.nx || j < 0 || j > L.ny) continue;
-    t.ay[e] = __ldg(L.ay + j * L.pc + i);
-  }
+  return true;
 }
 
 // one red-black colour pass (pressure.wgsl:87-94) over cells [xa,xb) x [ya,yb) of colour
-// `color`: warps take rows, lanes every other cell (the region is at most 64 cells wide)
+// `color`: warps take rows, lanes every other cell (the region is at most 64 cells wide).
+// A pass reads only cells of the other colour, so each thread computes all its cells
+// before it stores any (their shared-memory loads overlap).
+template <int NW, int RH>
 __device__ __forceinline__ void colour_pass(const Tile& t, const LevelDesc& L, int xa, int xb, int ya, int yb, int color) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int j = ya + warp; j < yb; j += nw) {
+  constexpr int M = (RH + NW - 1) / NW;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float v[M];
+  int kk[M];
+  #pragma unroll
+  for (int m = 0; m < M; m++) {
+    const int j = ya + warp + NW * m;
     const int i = xa + ((xa + j + color) & 1) + 2 * lane;
-    if (i >= xb) continue;
-    float off, diag; stencil_s(t, L.nx, L.ny, i, j, off, diag);
-    const int k = t.c(i, j);
-    t.p[k] = diag > 0.f ? (off - t.rhs[k] * L.h2) / diag : 0.f;
+    kk[m] = -1;
+    if (j < yb && i < xb) {
+      float off, diag; stencil_s(t, L.nx, L.ny, i, j, off, diag);
+      const int k = t.c(i, j);
+      v[m] = diag > 0.f ? (off - t.rhs[k] * L.h2) / diag : 0.f;
+      kk[m] = k;
+    }
   }
+  #pragma unroll
+  for (int m = 0; m < M; m++)
+    if (kk[m] >= 0) t.p[kk[m]] = v[m];
 }
 
 __device__ __forceinline__ bool scene_live(const SceneDesc& S) { return S.enabled && S.solve->active; }
@@ -100,22 +123,26 @@ __device__ __forceinline__ bool scene_live(const SceneDesc& S) { return S.enable
 
 // ------------------------------------------------------------------ down: 4 passes + restrict
 template <int TX, int TY>
-__global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work, int level) {
-  constexpr int RW = TX + 2 * H_DOWN, RH = TY + 2 * H_DOWN;
-  __shared__ float sp[RH * RW], srhs[RH * RW], sax[RH * (RW + 1)], say[(RH + 1) * RW];
+__global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work, int level,
+                                                 SolveCtl* ctl) {
+  static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
+  __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
+  __shared__ __align__(128) float srhs[MGF_BH * MGF_BW];
+  __shared__ __align__(128) float sax[MGF_BH * MGF_BW];
+  __shared__ __align__(128) float say[(MGF_BH + 1) * MGF_BW];
   __shared__ float sr[TY * TX];
+  __shared__ __align__(8) uint64_t bar;
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
   if (!scene_live(S)) return;
   const LevelDesc L = S.lev[level], C = S.lev[level + 1];
   const int x0 = w.tx * TX, y0 = w.ty * TY;
-  const Tile t{sp, srhs, sax, say, RW, RH, x0 - H_DOWN, y0 - H_DOWN};
-  load_tile(t, L, L.p);
-  __syncthreads();
+  const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
+  if (!stage_tile(S, level, TM_P, t, nullptr, 0, 0, &bar, ctl)) return;
   #pragma unroll 1
   for (int k = 1; k <= 4; k++) {   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
-    colour_pass(t, L, max(x0 - H_DOWN + k, 0), min(x0 + TX + H_DOWN - k, L.nx), max(y0 - H_DOWN + k, 0),
-                min(y0 + TY + H_DOWN - k, L.ny), (k - 1) & 1);
+    colour_pass<8, MGF_BH>(t, L, max(x0 - MGF_H + k, 0), min(x0 + TX + MGF_H - k, L.nx), max(y0 - MGF_H + k, 0),
+                           min(y0 + TY + MGF_H - k, L.ny), (k - 1) & 1);
     __syncthreads();
   }
   // residual of the tile cells (pressure.wgsl:96-101) and the smoothed p
@@ -174,33 +201,41 @@ __device__ void solve_decide_f(const SceneDesc* scenes, int nscenes, const Scene
 template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, int tail, SolveCtl* ctl) {
-  constexpr int RW = TX + 2 * H_UP, RH = TY + 2 * H_UP;
-  __shared__ float sp[RH * RW], srhs[RH * RW], sax[RH * (RW + 1)], say[(RH + 1) * RW];
+  static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
+  constexpr int RW = TX + 2 * MGF_H, RH = TY + 2 * MGF_H;
+  __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
+  __shared__ __align__(128) float srhs[MGF_BH * MGF_BW];
+  __shared__ __align__(128) float sax[MGF_BH * MGF_BW];
+  __shared__ __align__(128) float say[(MGF_BH + 1) * MGF_BW];
+  __shared__ __align__(128) float scp[MGF_CBH * MGF_CBW];
   __shared__ double red[32];
+  __shared__ __align__(8) uint64_t bar;
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
   if (!scene_live(S)) return;
   const LevelDesc L = S.lev[level], C = S.lev[level + 1];
   const int x0 = w.tx * TX, y0 = w.ty * TY;
-  const Tile t{sp, srhs, sax, say, RW, RH, x0 - H_UP, y0 - H_UP};
-  load_tile(t, L, L.pb);
-  __syncthreads();
+  const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
+  // coarse p under the region: columns x0/2-4 .. x0/2+TX/2+3, rows y0/2-4 .. y0/2+TY/2+3
+  const int cx = x0 / 2 - 8, cy = y0 / 2 - 4;
+  if (!stage_tile(S, level, TM_PB, t, scp, cx, cy, &bar, ctl)) return;
   // prolongation (pressure.wgsl:116-129) on the whole region
   for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
-    const int i = t.rx0 + e % RW, j = t.ry0 + e / RW;
+    const int i = x0 - MGF_H + e % RW, j = y0 - MGF_H + e / RW;
     if (i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
     const int I = i / 2, J = j / 2;
     const int I2 = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), C.nx - 1);
     const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), C.ny - 1);
-    const float* cp = C.p;
-    const float c = 0.5625f * cp[J * C.pc + I] + 0.1875f * (cp[J * C.pc + I2] + cp[J2 * C.pc + I]) + 0.0625f * cp[J2 * C.pc + I2];
-    t.p[e] += diag_s(t, L.nx, L.ny, i, j) > 0.f ? c : 0.f;
+    const int r0 = (J - cy) * MGF_CBW, r1 = (J2 - cy) * MGF_CBW;
+    const float c = 0.5625f * scp[r0 + I - cx] + 0.1875f * (scp[r0 + I2 - cx] + scp[r1 + I - cx]) +
+                    0.0625f * scp[r1 + I2 - cx];
+    t.p[t.c(i, j)] += diag_s(t, L.nx, L.ny, i, j) > 0.f ? c : 0.f;
   }
   __syncthreads();
   #pragma unroll 1
   for (int k = 1; k <= 4; k++) {   // colours 1, 0, 1, 0 (js/fluid.js:307-310)
-    colour_pass(t, L, max(x0 - H_UP + k, 0), min(x0 + TX + H_UP - k, L.nx), max(y0 - H_UP + k, 0),
-                min(y0 + TY + H_UP - k, L.ny), k & 1);
+    colour_pass<8, MGF_BH>(t, L, max(x0 - MGF_H + k, 0), min(x0 + TX + MGF_H - k, L.nx), max(y0 - MGF_H + k, 0),
+                           min(y0 + TY + MGF_H - k, L.ny), k & 1);
     __syncthreads();
   }
   double part = 0.0;
@@ -231,7 +266,6 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
 namespace {
 constexpr int CB_THREADS = 1024;
 constexpr int CB_WARPS = CB_THREADS / 32;
-constexpr int COARSEST_THREADS = 256;   // the coarsest level has at most 256 cells
 constexpr int COARSEST_SCRATCH = 0;     // the coarsest keeps its stencils in registers
 
 struct LvS { float *p, *rhs, *ax, *ay; int nx, ny, pc, pu; float h2; int pad; };
@@ -247,16 +281,76 @@ __device__ __forceinline__ void stencil_d(const LvS& L, int i, int j, float& off
   if (j < L.ny - 1) { off += n * p[(j + 1) * L.pc + i]; diag += n; } else { diag += 2.f * n; }
 }
 // one colour pass: warps take rows, lanes take every other cell of the row
+// A pass reads only cells of the other colour: up to 4 rows of a thread are computed
+// before any is stored, so their shared-memory loads overlap.
 __device__ __forceinline__ void pass_d(const LvS& L, int color) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int j = warp; j < L.ny; j += CB_WARPS)
-    for (int i = 2 * lane + ((j + color) & 1); i < L.nx; i += 64) {
-      float off, diag; stencil_d(L, i, j, off, diag);
-      const int k = j * L.pc + i;
-      L.p[k] = diag > 0.f ? (off - L.rhs[k] * L.h2) / diag : 0.f;
+  for (int i0 = 0; i0 < L.nx; i0 += 64)
+    for (int j0 = warp; j0 < L.ny; j0 += 4 * CB_WARPS) {
+      float v[4];
+      int kk[4];
+      #pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const int j = j0 + m * CB_WARPS, i = i0 + 2 * lane + ((j + color) & 1);
+        kk[m] = -1;
+        if (j < L.ny && i < L.nx) {
+          float off, diag; stencil_d(L, i, j, off, diag);
+          const int k = j * L.pc + i;
+          v[m] = diag > 0.f ? (off - L.rhs[k] * L.h2) / diag : 0.f;
+          kk[m] = k;
+        }
+      }
+      #pragma unroll
+      for (int m = 0; m < 4; m++)
+        if (kk[m] >= 0) L.p[kk[m]] = v[m];
     }
 }
-__device__ __forceinline__ void bar_coarsest() { asm volatile("bar.sync 1, %0;" ::"r"(COARSEST_THREADS) : "memory"); }
+__device__ __forceinline__ void bar_coarsest(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
+
+// x / d rounded to nearest from r = RN(1/d): q0 = RN(x r), q = RN(q0 + r (x - d q0)),
+// the residual x - d q0 exact by FMA (Markstein, IBM J. Res. Dev. 34(1), 1990). Equal
+// to the IEEE quotient for quotients in the normal range; it replaces the division
+// subroutine on the coarsest level, whose diagonals stay fixed for all its sweeps.
+__device__ __forceinline__ float div_by_rcp(float x, float d, float r) {
+  const float q0 = __fmul_rn(x, r);
+  const float e = __fmaf_rn(-q0, d, x);
+  return __fmaf_rn(e, r, q0);
+}
+
+// One coarsest-level cell with its fixed stencil (pressure.wgsl:132-156).
+struct CCell {
+  float w, e, s, n, rh, diag, rcp;
+  int kp;
+  bool act, hw, he, hs, hn;
+};
+__device__ __forceinline__ CCell coarsest_cell(const LvS& L, int k) {
+  CCell c{};
+  c.act = k < L.nx * L.ny;
+  if (!c.act) return c;
+  const int i = k % L.nx, j = k / L.nx;
+  c.kp = j * L.pc + i;
+  c.w = L.ax[j * L.pu + i]; c.e = L.ax[j * L.pu + i + 1];
+  c.s = L.ay[j * L.pc + i]; c.n = L.ay[(j + 1) * L.pc + i];
+  float diag = 0.f;
+  if (i > 0) diag += c.w; else diag += 2.f * c.w;
+  if (i < L.nx - 1) diag += c.e; else diag += 2.f * c.e;
+  if (j > 0) diag += c.s;
+  if (j < L.ny - 1) diag += c.n; else diag += 2.f * c.n;
+  c.diag = diag;
+  c.rcp = diag > 0.f ? __frcp_rn(diag) : 0.f;
+  c.rh = L.rhs[c.kp] * L.h2;
+  c.hw = i > 0; c.he = i < L.nx - 1; c.hs = j > 0; c.hn = j < L.ny - 1;
+  return c;
+}
+__device__ __forceinline__ void coarsest_update(float* p, int pc, const CCell& c) {
+  if (!c.act) return;
+  float off = 0.f;
+  if (c.hw) off += c.w * p[c.kp - 1];
+  if (c.he) off += c.e * p[c.kp + 1];
+  if (c.hs) off += c.s * p[c.kp - pc];
+  if (c.hn) off += c.n * p[c.kp + pc];
+  p[c.kp] = c.diag > 0.f ? div_by_rcp(off - c.rh, c.diag, c.rcp) : 0.f;
+}
 }  // namespace
 
 __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __restrict__ scenes, int nscenes, SolveCtl* ctl, int tail) {
@@ -333,44 +427,32 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       }
     __syncthreads();
   }
-  // ---- coarsest (pressure.wgsl:132-156): 120 red-black sweeps from zero, one cell per thread
-  // of the first 256 (a named barrier keeps the other warps out); each thread's stencil is
-  // fixed during the sweeps and held in registers
-  if (threadIdx.x < COARSEST_THREADS) {
+  // ---- coarsest (pressure.wgsl:132-156): 120 red-black sweeps from zero. Row-major
+  // cells 2t and 2t+1 have opposite colours for any nx (even nx: same row, adjacent;
+  // odd nx: colour = index parity), so thread t owns one cell of each colour and every
+  // thread works in every pass; the ceil(n/2) threads (<= 128, rounded up to warps)
+  // sync on a named barrier while the other warps wait at the block barrier below.
+  // Stencils, diagonals and their reciprocals stay in registers for all sweeps.
+  {
     const LvS L = lv[nl - 1];
-    const int k = threadIdx.x, n = L.nx * L.ny;
-    const int i = k % L.nx, j = k / L.nx;
-    const bool act = k < n;
-    const int kp = j * L.pc + i;
-    float w = 0.f, e = 0.f, s = 0.f, nn = 0.f, diag = 0.f, rh = 0.f;
-    int col = -1;
-    if (act) {
-      w = L.ax[j * L.pu + i]; e = L.ax[j * L.pu + i + 1];
-      s = L.ay[j * L.pc + i]; nn = L.ay[(j + 1) * L.pc + i];
-      if (i > 0) diag += w; else diag += 2.f * w;
-      if (i < L.nx - 1) diag += e; else diag += 2.f * e;
-      if (j > 0) diag += s;
-      if (j < L.ny - 1) diag += nn; else diag += 2.f * nn;
-      rh = L.rhs[kp] * L.h2;
-      col = (i + j) & 1;
-      L.p[kp] = 0.f;
-    }
-    const bool hw = act && i > 0, he = act && i < L.nx - 1, hs = act && j > 0, hn = act && j < L.ny - 1;
-    float* p = L.p;
-    bar_coarsest();
-    #pragma unroll 1
-    for (int it = 0; it < 120; it++) {
-      #pragma unroll
-      for (int c = 0; c < 2; c++) {
-        if (col == c) {
-          float off = 0.f;
-          if (hw) off += w * p[kp - 1];
-          if (he) off += e * p[kp + 1];
-          if (hs) off += s * p[kp - L.pc];
-          if (hn) off += nn * p[kp + L.pc];
-          p[kp] = diag > 0.f ? (off - rh) / diag : 0.f;
-        }
-        bar_coarsest();
+    const int npair = (L.nx * L.ny + 1) >> 1;
+    const int nthr = (npair + 31) & ~31;
+    if ((int)threadIdx.x < nthr) {
+      const CCell a = coarsest_cell(L, 2 * threadIdx.x), b = coarsest_cell(L, 2 * threadIdx.x + 1);
+      if (a.act) L.p[a.kp] = 0.f;
+      if (b.act) L.p[b.kp] = 0.f;
+      // colour of cell 2t: (i + j) & 1
+      const int k0 = 2 * threadIdx.x;
+      const bool a_red = ((k0 % L.nx + k0 / L.nx) & 1) == 0;
+      const CCell c0 = a_red ? a : b, c1 = a_red ? b : a;
+      float* p = L.p;
+      bar_coarsest(nthr);
+      #pragma unroll 1
+      for (int it = 0; it < 120; it++) {
+        coarsest_update(p, L.pc, c0);
+        bar_coarsest(nthr);
+        coarsest_update(p, L.pc, c1);
+        bar_coarsest(nthr);
       }
     }
   }
@@ -423,8 +505,8 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
   return f * 4;
 }
 
-void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, cudaStream_t st) {
-  if (ntiles > 0) k_mg_down<MGF_TX, MGF_TY><<<ntiles, 256, 0, st>>>(scenes, work, level);
+void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, cudaStream_t st) {
+  if (ntiles > 0) k_mg_down<MGF_TX, MGF_TY><<<ntiles, 256, 0, st>>>(scenes, work, level, ctl);
 }
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {

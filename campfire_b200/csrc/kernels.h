@@ -15,6 +15,16 @@ constexpr int FR_TX = 32, FR_TY = 16;                // forces + coef + rhs0 (+ 
 constexpr int FR_KMAX = 4;                           // coarse coefficient levels built inside FR tiles
 constexpr int MG_TX = 32, MG_TY = 8;                 // single-pass multigrid kernels
 constexpr int MGF_TX = 32, MGF_TY = 16;              // fused (temporally blocked) multigrid kernels
+constexpr int MGF_H = 5;                             // their halo: 4 colour passes + the residual's neighbours
+// The fused kernels stage their tiles with TMA tensor copies. A box starts MGF_SX
+// cells left of the tile so that its x coordinate stays 16-byte aligned, and the
+// level's boundary is zero-filled by the copy.
+constexpr int MGF_SX = 8;
+constexpr int MGF_BW = MGF_TX + 2 * MGF_SX, MGF_BH = MGF_TY + 2 * MGF_H;   // p, pb, rhs, ax box (ay: one more row)
+constexpr int MGF_CBW = MGF_TX / 2 + 16, MGF_CBH = MGF_TY / 2 + 8;        // coarse p box of the up kernel
+// tensor maps per level, in the scene arena (CUtensorMap: 128 bytes, 64-byte aligned)
+enum TmapKind { TM_P = 0, TM_PB, TM_RHS, TM_AX, TM_AY, TM_PC, TM_PER_LEVEL };
+constexpr int TMAP_BYTES = 128;
 constexpr int COARSE_CELLS = 6144;                   // largest level handled by the one-CTA coarse block
 constexpr int PR_TX = 32, PR_TY = 8;                 // projection
 constexpr int GEO_TX = 32, GEO_TY = 8;               // geometry
@@ -47,7 +57,7 @@ void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_co
 // fused V(2,2) cycle: per fine level a down kernel (4 passes + restriction) and an
 // up kernel (prolongation + 4 passes; level 0 tail: 1 residual norm + decision,
 // 2 p64 += p), and one CTA per scene for levels lc..coarsest
-void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, cudaStream_t st);
+void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, cudaStream_t st);
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st);
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, size_t smem, cudaStream_t st);
