@@ -164,6 +164,9 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     for v, s in zip(b.scenes, scenes):
         load_scene(v, s)
     b.set_solver(cb.SOLVE_FP64, 1, tol, max_cycles)
+    b.set_coarse_solve(True)
+    tune = cb.autotune([(s["nx"], s["ny"]) for s in scenes], iters=10, device=dev.index, coarse_direct=True)
+    b.set_coarse_cells(tune["best"])
     b.set_stream(stream.cuda_stream)
     b.step(warmup)
     b.synchronize()
@@ -185,10 +188,13 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
 
     # the same scenes, one by one, through the plain single-scene step (same solver, same tolerance)
     plain_ms, plain_cells = 0.0, 0
+    best = {d: cb.autotune([d], iters=10, device=dev.index, coarse_direct=True)["best"] for d in BATCH_CLASSES}
     for s in scenes:
         g = cb.FluidSim(dev.index, {"nx": s["nx"], "ny": s["ny"], "dt": s["dt"]}, width=0.8).init()
         load_scene(g, s)
         g.set_solver(cb.SOLVE_FP64, 1, tol, max_cycles)
+        g.set_coarse_solve(True)
+        g.set_coarse_cells(best[(s["nx"], s["ny"])])
         g.set_stream(stream.cuda_stream)
         g.step(warmup)
         g.synchronize()
@@ -204,6 +210,8 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
         g.close()
     plain = plain_cells / (plain_ms / 1e3)
     return {"value": batched, "unit": METRIC, "scenes": len(scenes), "cells": cells, "steps": steps,
+            "schedule": {"coarse_cells": tune["best"],
+                         "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}},
             "ms_per_step": ms / steps, "launches_per_step": launches,
             "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": max_cycles,
                          "cycles_last_step": {"min": min(cyc), "max": max(cyc)}, "max_rel_residual": rel},
@@ -274,6 +282,13 @@ def main():
     sim = cb.FluidSim(local, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
     load_scene(sim, sc)
     sim.set_solver(mode, 1, tol, maxc)
+    sim.set_coarse_solve(True)
+    config["pressure"]["coarsest"] = "direct (inverse per step)"
+    # smoother schedule picked by the autotuner (fused V-cycles timed on a scratch scene of this size)
+    tune = cb.autotune([(nx, ny)], iters=20, device=local, coarse_direct=True)
+    sim.set_coarse_cells(tune["best"])
+    config["schedule"] = {"coarse_cells": tune["best"],
+                          "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}}
     sim.set_stream(stream.cuda_stream)
     sim.set_graphs(a.launch == "graph")
     config["launch"] = a.launch

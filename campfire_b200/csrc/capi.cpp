@@ -1,6 +1,7 @@
 // extern "C" surface of libcampfire_gas.so (include/campfire_gas.h): thin
 // wrappers over cfg::Engine that validate handles and translate exceptions and
 // CUDA failures into status codes.
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -167,4 +168,95 @@ extern "C" int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, doub
                                double* launches_per_step) {
   SIM_OK(sim); OWNER_OK(sim);
   return guarded([&] { return sim->eng->time_kernel(kernel, iters, mean_ms, bytes_per_launch, launches_per_step); });
+}
+
+extern "C" int cfg_set_coarse_cells(cfg_sim* sim, int cells) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->set_coarse_cells(cells); });
+}
+extern "C" int cfg_batch_set_coarse_cells(cfg_batch* b, int cells) {
+  if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
+  return guarded([&] { return b->eng->set_coarse_cells(cells); });
+}
+
+namespace {
+// a generated scene loaded into scene s of an engine, in FluidSim's set-up order
+int load_generated(cfg::Engine& eng, int s, int kind, int nx, int ny, double width, uint64_t seed) {
+  const size_t n = (size_t)nx * ny;
+  std::vector<float> T(n), Y(4 * n), U((size_t)(nx + 1) * ny), V((size_t)nx * (ny + 1)),
+      pieces((size_t)CFG_MAX_PIECES * CFG_PIECE_FLOATS);
+  int np = 0;
+  cfg_params P;
+  double dt = 0;
+  CFG_TRY(cfg_scene_generate(kind, nx, ny, width, seed, T.data(), Y.data(), U.data(), V.data(), pieces.data(), &np, &P,
+                             &dt));
+  for (const char* k : {"Tamb", "rhoAmb", "YOamb", "reactB", "reactTa", "dHc", "Pr", "exchAlpha", "depth"}) {
+    float f;
+    std::memcpy(&f, reinterpret_cast<const char*>(&P) + 4 * cfg::param_index(k), 4);
+    CFG_TRY(eng.set_param(s, k, f));
+  }
+  CFG_TRY(eng.upload_pieces(s, pieces.data(), np));
+  CFG_TRY(eng.write_params(s));
+  CFG_TRY(eng.reset(s));
+  CFG_TRY(eng.write_field(s, "T", T.data(), T.size()));
+  CFG_TRY(eng.write_field(s, "Y", Y.data(), Y.size()));
+  CFG_TRY(eng.write_field(s, "U", U.data(), U.size()));
+  CFG_TRY(eng.write_field(s, "V", V.data(), V.size()));
+  CFG_TRY(eng.write_field(s, "T2", T.data(), T.size()));
+  CFG_TRY(eng.write_field(s, "Y2", Y.data(), Y.size()));
+  CFG_TRY(eng.clear_geometry(s));
+  return eng.geometry(s);
+}
+}  // namespace
+
+extern "C" int cfg_autotune(int device, int nscenes, const int* nx, const int* ny, int coarse_direct, int iters,
+                            int* best_cells, int* cand_cells, double* cand_ms, int* ncand) {
+  if (nscenes < 1 || !nx || !ny || iters < 1 || !best_cells || !cand_cells || !cand_ms || !ncand || *ncand < 1)
+    return cfg::fail(CFG_ERR_INVAL, "bad argument");
+  return guarded([&] {
+    std::vector<double> width(nscenes, 0.8), dt(nscenes, 0.002);
+    cfg::Engine eng;
+    CFG_TRY(eng.init(device, nscenes, nx, ny, width.data(), dt.data()));
+    for (int s = 0; s < nscenes; s++) CFG_TRY(load_generated(eng, s, 0, nx[s], ny[s], 0.8, 1234 + s));
+    if (coarse_direct) {
+      CFG_TRY(eng.set_solver(CFG_SOLVE_FP64, 1, 1e-6, 4));
+      CFG_TRY(eng.set_coarse_solve(1));
+    } else {
+      CFG_TRY(eng.set_solver(CFG_SOLVE_FIXED, 1, 1e-6, 1));
+    }
+    CFG_TRY(eng.step(1));
+    CFG_TRY(eng.synchronize());
+    // candidate thresholds: the level sizes below level 0, largest first
+    std::vector<int> cells;
+    for (int s = 0; s < nscenes; s++) {
+      cfg_info inf;
+      CFG_TRY(eng.info(s, &inf));
+      for (int l = 1; l < inf.levels; l++) cells.push_back(inf.level_nx[l] * inf.level_ny[l]);
+    }
+    std::sort(cells.begin(), cells.end(), [](int a, int b) { return a > b; });
+    cells.erase(std::unique(cells.begin(), cells.end()), cells.end());
+    int k = 0;
+    double best = 1e300;
+    *best_cells = 0;
+    for (int c : cells) {
+      if (k >= *ncand) break;
+      if (eng.set_coarse_cells(c) != CFG_OK) continue;   // does not fit in shared memory
+      double ms = 0, bytes = 0, per = 0;
+      CFG_TRY(eng.time_kernel("vcycle", iters, &ms, &bytes, &per));
+      cand_cells[k] = c; cand_ms[k] = ms; k++;
+      if (ms < best) { best = ms; *best_cells = c; }
+    }
+    *ncand = k;
+    if (k == 0) return cfg::fail(CFG_ERR_RANGE, "no smoother schedule fits these sizes");
+    return CFG_OK;
+  });
+}
+
+extern "C" int cfg_set_coarse_solve(cfg_sim* sim, int direct) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->set_coarse_solve(direct); });
+}
+extern "C" int cfg_batch_set_coarse_solve(cfg_batch* b, int direct) {
+  if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
+  return guarded([&] { return b->eng->set_coarse_solve(direct); });
 }

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -101,6 +102,14 @@ int Engine::activate() const {
   return CFG_OK;
 }
 
+// The coarse block starts at the first level with at most `cells` cells whose
+// arrays fit in one CTA's shared memory (else at the coarsest level).
+int Engine::choose_lc(const Scene& sc, int cells) {
+  for (int l = 0; l < sc.nlev; l++)
+    if (sc.lnx[l] * sc.lny[l] <= cells && coarse_smem_bytes(sc.lnx, sc.lny, l, sc.nlev) <= kCoarseSmemMax) return l;
+  return sc.nlev - 1;
+}
+
 int Engine::init(int device, int n, const int* nx, const int* ny, const double* width, const double* dt) {
   if (n <= 0) return fail(CFG_ERR_INVAL, "scene count must be positive");
   scenes_.resize(n);
@@ -120,9 +129,7 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
     }
     sc.nlev = L;
     if (sc.lnx[L - 1] * sc.lny[L - 1] > 256) return fail(CFG_ERR_RANGE, "coarsest level too large");
-    sc.lc = L - 1;
-    for (int l = 0; l < L; l++)
-      if (sc.lnx[l] * sc.lny[l] <= COARSE_CELLS) { sc.lc = l; break; }
+    sc.lc = choose_lc(sc, coarse_cells_);
     coarse_smem_ = std::max(coarse_smem_, coarse_smem_bytes(sc.lnx, sc.lny, sc.lc, sc.nlev));
   }
   int ndev = 0;
@@ -131,7 +138,10 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   if (device < 0 || device >= ndev) return fail(CFG_ERR_INVAL, "device index out of range");
   device_ = device;
   CFG_TRY(activate());
+  // CAMPFIRE_PDL=0 launches the pressure-loop kernels without programmatic dependent launch
+  if (const char* v = std::getenv("CAMPFIRE_PDL")) set_pdl(v[0] != '0');
   CFG_CUDA(prepare_mg_coarse(coarse_smem_));
+  CFG_CUDA(prepare_coarse_factor());
   CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaMalloc(&d_scenes_, sizeof(SceneDesc) * n));
@@ -232,6 +242,7 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 8},
     {(void**)&d.tmap, (size_t)MAX_LEVELS * TM_PER_LEVEL * TMAP_BYTES},
+    {(void**)&d.cinv, (size_t)sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * 4},
   };
   double h = sc.dxd;
   for (int l = 0; l < sc.nlev; l++) {
@@ -290,6 +301,37 @@ int Engine::build_worklists() {
   return CFG_OK;
 }
 
+int Engine::set_coarse_cells(int cells) {
+  if (cells < 1) return fail(CFG_ERR_INVAL, "coarse cells must be >= 1");
+  CFG_TRY(activate());
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  size_t smem = 0;
+  std::vector<int> lcs(scenes_.size());
+  for (size_t s = 0; s < scenes_.size(); s++) {
+    const Scene& sc = scenes_[s];
+    lcs[s] = choose_lc(sc, cells);
+    smem = std::max(smem, coarse_smem_bytes(sc.lnx, sc.lny, lcs[s], sc.nlev));
+  }
+  if (smem > kCoarseSmemMax) return fail(CFG_ERR_RANGE, "the coarsest level does not fit in one CTA's shared memory");
+  CFG_CUDA(prepare_mg_coarse(smem));
+  coarse_cells_ = cells;
+  coarse_smem_ = smem;
+  for (size_t s = 0; s < scenes_.size(); s++) {
+    scenes_[s].lc = lcs[s];
+    scenes_[s].desc.lc = lcs[s];
+    CFG_TRY(upload_desc((int)s));
+  }
+  for (int k = 0; k < WL_COUNT; k++) {
+    if (d_wl_[k]) cudaFree(d_wl_[k]);
+    d_wl_[k] = nullptr;
+    nwl_[k] = 0;
+  }
+  CFG_TRY(build_worklists());
+  graph_dirty_ = true;
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+
 int Engine::upload_desc(int s) {
   CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &scenes_[s].desc, sizeof(SceneDesc), cudaMemcpyHostToDevice, st()));
   return CFG_OK;
@@ -305,6 +347,7 @@ int Engine::upload_ctl() {
   for (auto& sc : scenes_) en += sc.enabled ? 1 : 0;
   c.nscenes = en; c.nactive = en; c.any_active = 1; c.scenes_done = 0;
   c.iter = 0; c.hard_cap = std::max(ncycles_, max_cycles_) + 1;
+  c.coarse_direct = (mode_ != CFG_SOLVE_FIXED && coarse_direct_) ? 1 : 0;
   *h_ctl_pinned_ = c;
   CFG_CUDA(cudaMemcpyAsync(d_ctl_, h_ctl_pinned_, sizeof(SolveCtl), cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaStreamSynchronize(st()));
@@ -621,10 +664,24 @@ void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_con
   launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); launches_++;
   for (int l = FR_KMAX; l + 1 < max_levels(); l++)
     if (nwl_[WL_MGC0 + l] > 0) { launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s); launches_++; }
+  if (direct_coarse()) { launch_coarse_factor(d_scenes_, nscenes(), max_coarsest_cells(), s); launches_++; }
   if (fp64) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s); launches_++; }
   // the loop's cycle counter starts at zero in every step
   cudaMemsetAsync(&d_ctl_->iter, 0, sizeof(int), s);
   (void)h; (void)use_cond;
+}
+
+int Engine::max_coarsest_cells() const {
+  int m = 1;
+  for (auto& sc : scenes_) m = std::max(m, sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1]);
+  return m;
+}
+int Engine::set_coarse_solve(int direct) {
+  if (direct != 0 && direct != 1) return fail(CFG_ERR_INVAL, "coarse solve must be 0 (sweeps) or 1 (direct)");
+  CFG_TRY(activate());
+  coarse_direct_ = direct;
+  graph_dirty_ = true;
+  return upload_ctl();
 }
 
 int Engine::max_lc() const {
@@ -636,9 +693,8 @@ int Engine::max_lc() const {
 // The step's V(2,2) cycle with the fused kernels (k_mgf.cu); the level-0 up
 // kernel (or the coarse block of scenes whose block starts at level 0) ends
 // the cycle with the residual norm (FP32 modes) or p64 += p (FP64 mode).
-void Engine::enqueue_vcycle(cudaStream_t s) {
+void Engine::enqueue_vcycle(cudaStream_t s, int tail) {
   const int LD = max_lc();
-  const int tail = any_fp64() ? 2 : 1;
   for (int l = 0; l < LD; l++) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
     launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, s);
@@ -716,7 +772,7 @@ int Engine::host_pressure_loop() {
   CFG_CUDA(cudaStreamSynchronize(s));
   int any = any_fp64() ? h_ctl_pinned_->any_active : 1;
   while (any) {
-    enqueue_vcycle(s);
+    enqueue_vcycle(s, any_fp64() ? 2 : 1);
     enqueue_cycle_tail(s, 0ull, 0);
     CFG_CUDA(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s));
     CFG_CUDA(cudaStreamSynchronize(s));
@@ -769,7 +825,7 @@ int Engine::ensure_graph() {
   e = cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamBeginCaptureToGraph");
   vcycle_launches_ = 0;
-  enqueue_vcycle(body_stream_);
+  enqueue_vcycle(body_stream_, any_fp64() ? 2 : 1);
   enqueue_cycle_tail(body_stream_, (unsigned long long)h, 1);
   e = cudaStreamEndCapture(body_stream_, &body);
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamEndCapture(body)");
@@ -789,7 +845,14 @@ int Engine::step(int nsteps) {
   CFG_TRY(activate());
   for (int k = 0; k < nsteps; k++) {
     if (use_graphs_) {
-      CFG_TRY(ensure_graph());
+      if (ensure_graph() != CFG_OK) {
+        // a driver that cannot capture programmatic launches into the loop body: capture without them
+        if (!pdl_enabled()) return fail(CFG_ERR_INVAL, last_error());
+        cudaGetLastError();
+        set_pdl(false);
+        graph_dirty_ = true;
+        CFG_TRY(ensure_graph());
+      }
       CFG_CUDA(cudaGraphLaunch(exec_, st()));
     } else {
       launches_ = 0; vcycle_launches_ = 0;
@@ -876,6 +939,7 @@ int Engine::run_stage(const char* stage) {
     for (int l = FR_KMAX; l + 1 < max_levels(); l++)
       launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   } else if (st_ == "pressure") {
+    if (direct_coarse()) launch_coarse_factor(d_scenes_, nscenes(), max_coarsest_cells(), s);
     enqueue_bnorm(s);
     CFG_TRY(host_pressure_loop());
   } else if (st_ == "project") launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s);
@@ -932,6 +996,12 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     // the reference schedule's V-cycle bytes of the levels the block covers (163 B per level cell)
     b = 0;
     for (int l = sc.lc; l < sc.nlev; l++) b += 163.0 * sc.lnx[l] * sc.lny[l];
+    cnt = cyc;
+  } else if (n == "vcycle") {
+    // one fused V(2,2) cycle without its tail (the smoother schedule's cost)
+    go = [&](int) { enqueue_vcycle(s, 0); };
+    b = 0;
+    for (int l = 0; l + 1 < sc.nlev; l++) b += 163.0 * sc.lnx[l] * sc.lny[l];
     cnt = cyc;
   } else if (n == "defect64") {
     go = [&](int) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, s); };

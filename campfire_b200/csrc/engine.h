@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "gas_dev.cuh"
+#include "kernels.h"
 
 namespace cfg {
 
@@ -111,9 +112,17 @@ class Engine {
   int write_params_all();
   int geometry_all();
   int time_kernel(const char* name, int iters, double* ms, double* bytes, double* per_step);
+  // smoother schedule: the one-CTA coarse block starts at the first level with at
+  // most `cells` cells (levels above it run as tiled down/up kernels)
+  int set_coarse_cells(int cells);
+  int coarse_cells() const { return coarse_cells_; }
+  // coarsest level of the TOL/FP64 modes: 0 the reference's 120 sweeps, 1 its inverse
+  int set_coarse_solve(int direct);
+  int scene_lc(int s) const { return scenes_[s].lc; }
   int nscenes() const { return (int)scenes_.size(); }
 
  private:
+  static int choose_lc(const Scene& sc, int cells);
   int alloc_scene(Scene& sc);
   int build_tmaps(Scene& sc);
   int upload_desc(int s);
@@ -131,9 +140,11 @@ class Engine {
 
   // step pieces; launches counted in launches_
   void enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_cond);
-  void enqueue_vcycle(cudaStream_t s);       // fused kernels (the step's cycle)
+  void enqueue_vcycle(cudaStream_t s, int tail);   // fused kernels (the step's cycle); tail as k_mg_up
   void enqueue_vcycle_ref(cudaStream_t s);   // one kernel per reference dispatch (cfg_vcycle)
   int max_lc() const;
+  int max_coarsest_cells() const;
+  bool direct_coarse() const { return mode_ != CFG_SOLVE_FIXED && coarse_direct_ != 0; }
   void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
   void enqueue_post_solve(cudaStream_t s);
   int host_pressure_loop();
@@ -161,6 +172,8 @@ class Engine {
   int last_cycles_ = 1;        // V-cycles of scene 0's last step, recorded by synchronize()
   int vcycle_launches_ = 0;
   size_t coarse_smem_ = 0;
+  int coarse_cells_ = COARSE_CELLS;
+  int coarse_direct_ = 0;
 };
 
 }  // namespace cfg

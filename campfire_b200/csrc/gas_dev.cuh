@@ -43,6 +43,8 @@ struct SolveState {
   int active;               // 1 while this scene keeps cycling
   unsigned int counter;     // CTAs finished in the current reduction
   unsigned int maxu;        // max |u| over faces after projection (f32 bits; CFL step)
+  int direct_ok;            // the coarsest operator's inverse of this step is valid (direct coarse solve)
+  int pad;
 };
 
 struct SceneDesc {
@@ -66,6 +68,7 @@ struct SceneDesc {
   double *p64, *rhs64, *part;   // FP64 pressure, FP64 rhs, per-CTA partial sums
   SolveState* solve;
   const char* tmap;         // TMA tensor maps of the levels (TM_PER_LEVEL per level, 128 bytes each)
+  float* cinv;              // inverse of the coarsest operator (n x n, n = its cells), direct coarse solve
   LevelDesc lev[MAX_LEVELS];
 };
 
@@ -80,7 +83,7 @@ struct SolveCtl {
   int iter;                   // cycles run by the loop in this step (reset before the loop)
   int hard_cap;               // the loop stops after this many cycles whatever any_active says
   int err;                    // set by a kernel whose bounded wait ran out (reported as CFG_ERR_TIMEDOUT)
-  int pad;
+  int coarse_direct;          // TOL/FP64 modes: solve the coarsest level with its inverse instead of 120 sweeps
 };
 
 // One tile of a work list
@@ -89,6 +92,15 @@ struct Work { int scene, tx, ty, tile; };
 __host__ __device__ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 #ifdef __CUDACC__
+// Programmatic dependent launch (kernels of the pressure loop): a kernel launched
+// with programmatic stream serialization may start while its predecessor is still
+// running. pdl_wait() blocks until the predecessor grid has completed and its
+// writes are visible; everything before it may read only data no kernel of the
+// step writes (descriptors, work lists, tensor maps). pdl_trigger() lets the
+// successor begin launching. Both are no-ops for an ordinary launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 
 // ------------------------------------------------------------- common.wgsl
 __device__ __forceinline__ float rhoOf(const cfg_params& P, float T) { return P.rhoAmb * P.Tamb / T; }   // :33

@@ -3,6 +3,8 @@
 // as in FluidSim.vcycle (js/fluid.js:294-312); plus the loop control of the
 // pressure solve (residual norms, FP64 defect correction) that decides, per
 // scene, whether another V-cycle runs.
+#include <atomic>
+
 #include "gas_dev.cuh"
 #include "kernels.h"
 #include "reduce.cuh"
@@ -73,6 +75,7 @@ __device__ void solve_decide(const SceneDesc* scenes, int nscenes, const SceneDe
 // Last node of each loop iteration: count the cycle and set the WHILE node's
 // condition. The count bounds the loop even if a decision were never recorded.
 __global__ void k_loop_guard(SolveCtl* ctl, unsigned long long h, int use_cond) {
+  pdl_wait();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int it = ctl->iter + 1;
   ctl->iter = it;
@@ -201,8 +204,10 @@ __global__ void __launch_bounds__(256) k_defect64(const SceneDesc* __restrict__ 
   __shared__ double red[32];
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
-  if (!scene_live(S)) return;
+  pdl_trigger();
   const LevelDesc L = S.lev[0];
+  pdl_wait();
+  if (!scene_live(S)) return;
   const int nx = L.nx;
   const int i = w.tx * MG_TX + (threadIdx.x % MG_TX), j = w.ty * MG_TY + (threadIdx.x / MG_TX);
   double v = 0.0;
@@ -304,11 +309,18 @@ void launch_resnorm(const SceneDesc* scenes, int nscenes, const Work* work, int 
 }
 void launch_defect64(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
                      int first, cudaStream_t st) {
-  if (ntiles > 0) k_defect64<<<ntiles, MG_TX * MG_TY, 0, st>>>(scenes, nscenes, work, ctl, first);
+  if (ntiles > 0)
+    launch_pdl(pdl_enabled(), k_defect64, dim3(ntiles), dim3(MG_TX * MG_TY), 0, st, scenes, nscenes, work, ctl, first);
 }
 void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_cond, cudaStream_t st) {
-  k_loop_guard<<<1, 32, 0, st>>>(ctl, cond_handle, use_cond);
+  launch_pdl(pdl_enabled(), k_loop_guard, dim3(1), dim3(32), 0, st, ctl, cond_handle, use_cond);
 }
+
+namespace {
+std::atomic<bool> g_pdl{true};
+}
+void set_pdl(bool on) { g_pdl.store(on); }
+bool pdl_enabled() { return g_pdl.load(); }
 void launch_accum64(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st) {
   if (ntiles > 0) k_accum64<<<ntiles, MG_TX * MG_TY, 0, st>>>(scenes, work);
 }

@@ -134,10 +134,12 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
   __shared__ __align__(8) uint64_t bar;
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
-  if (!scene_live(S)) return;
+  pdl_trigger();
   const LevelDesc L = S.lev[level], C = S.lev[level + 1];
   const int x0 = w.tx * TX, y0 = w.ty * TY;
   const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
+  pdl_wait();
+  if (!scene_live(S)) return;
   if (!stage_tile(S, level, TM_P, t, nullptr, 0, 0, &bar, ctl)) return;
   #pragma unroll 1
   for (int k = 1; k <= 4; k++) {   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
@@ -212,12 +214,14 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   __shared__ __align__(8) uint64_t bar;
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
-  if (!scene_live(S)) return;
+  pdl_trigger();
   const LevelDesc L = S.lev[level], C = S.lev[level + 1];
   const int x0 = w.tx * TX, y0 = w.ty * TY;
   const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
   // coarse p under the region: columns x0/2-4 .. x0/2+TX/2+3, rows y0/2-4 .. y0/2+TY/2+3
   const int cx = x0 / 2 - 8, cy = y0 / 2 - 4;
+  pdl_wait();
+  if (!scene_live(S)) return;
   if (!stage_tile(S, level, TM_PB, t, scp, cx, cy, &bar, ctl)) return;
   // prolongation (pressure.wgsl:116-129) on the whole region
   for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
   const SceneDesc& S = scenes[blockIdx.x];
-  if (!scene_live(S)) return;
+  pdl_trigger();
   const int lc = S.lc, nl = S.nlev;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -378,6 +382,8 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     mbar_init(&bar, 1);
   }
   __syncthreads();
+  pdl_wait();
+  if (!scene_live(S)) return;
   const LvS V0 = lv[lc];
   float* sres = lv[nl - 1].ay + (lv[nl - 1].ny + 1) * lv[nl - 1].pc;   // residual scratch (level lc size)
   // ---- stage the arrays with TMA bulk copies (one per array; sizes are multiples of 128 bytes)
@@ -433,7 +439,30 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // thread works in every pass; the ceil(n/2) threads (<= 128, rounded up to warps)
   // sync on a named barrier while the other warps wait at the block barrier below.
   // Stencils, diagonals and their reciprocals stay in registers for all sweeps.
-  {
+  if (ctl->coarse_direct && S.solve->direct_ok) {
+    // direct coarse solve (TOL/FP64 modes): p = A^-1 b with b = -rhs h2 (0 in closed cells),
+    // each row's dot product as 8 strided partial sums combined pairwise (the oracle's order)
+    const LvS L = lv[nl - 1];
+    const int n = L.nx * L.ny;
+    for (int k = threadIdx.x; k < n; k += CB_THREADS) {
+      const int i = k % L.nx, j = k / L.nx;
+      float off, diag; stencil_d(L, i, j, off, diag);
+      sres[k] = diag > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
+    }
+    __syncthreads();
+    const float* A = S.cinv;
+    const int q = lane & 7;
+    for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
+      const int k = base + (lane >> 3);
+      float sum = 0.f;
+      if (k < n)
+        for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(A + (size_t)k * n + m), sres[m], sum);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+      if (k < n && q == 0) L.p[(k / L.nx) * L.pc + k % L.nx] = sum;
+    }
+  } else {
     const LvS L = lv[nl - 1];
     const int npair = (L.nx * L.ny + 1) >> 1;
     const int nthr = (npair + 31) & ~31;
@@ -494,6 +523,90 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   }
 }
 
+// ------------------------------------------------------------------ direct coarse solve: the coarsest inverse
+// Gauss-Jordan inversion in f32 without pivoting of the coarsest operator A (A_kk =
+// the stencil's diagonal, A_km = -face coefficient; a closed cell gets the row
+// dmax e_k and b_k = 0), once per step after the coefficients are built. A is
+// symmetric and, with an open boundary in reach of every gas cell, positive
+// definite; a pivot <= 1e-6 dmax (a sealed gas pocket: pure Neumann) leaves
+// direct_ok = 0 and the coarse block keeps the 120 sweeps for this step. Per pivot
+// k: r = 1/a_kk; row k scaled by r (a_kk -> r); every other row i updated as
+// a_ij = fma(-a_ik, row_k[j], a_ij) with a_ik first set to 0.
+__global__ void __launch_bounds__(1024) k_coarse_factor(const SceneDesc* __restrict__ scenes, int ncap) {
+  extern __shared__ float a[];
+  __shared__ float s_dmax;
+  __shared__ int s_ok;
+  const SceneDesc& S = scenes[blockIdx.x];
+  if (!S.enabled) return;
+  const LevelDesc L = S.lev[S.nlev - 1];
+  const int n = L.nx * L.ny;
+  if (n > ncap) {
+    if (threadIdx.x == 0) S.solve->direct_ok = 0;
+    return;
+  }
+  float* fcol = a + n * n;
+  float* rowk = fcol + n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[e] = 0.f;
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const int i = k % L.nx, j = k / L.nx;
+    const float w = L.ax[j * L.pu + i], e = L.ax[j * L.pu + i + 1];
+    const float so = L.ay[j * L.pc + i], no = L.ay[(j + 1) * L.pc + i];
+    float diag = 0.f;
+    if (i > 0) diag += w; else diag += 2.f * w;
+    if (i < L.nx - 1) diag += e; else diag += 2.f * e;
+    if (j > 0) diag += so;
+    if (j < L.ny - 1) diag += no; else diag += 2.f * no;
+    fcol[k] = diag;
+    if (diag > 0.f) {
+      a[k * n + k] = diag;
+      if (i > 0) a[k * n + k - 1] = -w;
+      if (i < L.nx - 1) a[k * n + k + 1] = -e;
+      if (j > 0) a[k * n + k - L.nx] = -so;
+      if (j < L.ny - 1) a[k * n + k + L.nx] = -no;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int k = 0; k < n; k++) m = fmaxf(m, fcol[k]);
+    s_dmax = m;
+    s_ok = m > 0.f ? 1 : 0;
+  }
+  __syncthreads();
+  const float dmax = s_dmax, thr = 1e-6f * dmax;
+  for (int k = threadIdx.x; k < n; k += blockDim.x)
+    if (!(fcol[k] > 0.f)) a[k * n + k] = dmax;
+  __syncthreads();
+  for (int k = 0; k < n && s_ok; k++) {
+    const float p = a[k * n + k];
+    if (!(p > thr)) {   // uniform: every thread read the same pivot
+      if (threadIdx.x == 0) s_ok = 0;
+      break;
+    }
+    const float r = 1.0f / p;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      fcol[t] = a[t * n + k];
+      rowk[t] = (t == k ? 1.0f : a[k * n + t]) * r;
+    }
+    __syncthreads();
+    for (int i = warp; i < n; i += nw) {
+      const float f = fcol[i];
+      for (int j = lane; j < n; j += 32) {
+        const int e = i * n + j;
+        a[e] = i == k ? rowk[j] : __fmaf_rn(-f, rowk[j], j == k ? 0.f : a[e]);
+      }
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  const int ok = s_ok;
+  if (ok)
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) S.cinv[e] = a[e];
+  if (threadIdx.x == 0) S.solve->direct_ok = ok;
+}
+
 // shared bytes of the coarse block for one scene (the layout built by k_mg_coarse)
 size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
   size_t f = 0;
@@ -506,14 +619,31 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
 }
 
 void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, cudaStream_t st) {
-  if (ntiles > 0) k_mg_down<MGF_TX, MGF_TY><<<ntiles, 256, 0, st>>>(scenes, work, level, ctl);
+  if (ntiles > 0)
+    launch_pdl(pdl_enabled(), k_mg_down<MGF_TX, MGF_TY>, dim3(ntiles), dim3(256), 0, st, scenes, work, level, ctl);
 }
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {
-  if (ntiles > 0) k_mg_up<MGF_TX, MGF_TY><<<ntiles, 256, 0, st>>>(scenes, nscenes, work, level, tail, ctl);
+  if (ntiles > 0)
+    launch_pdl(pdl_enabled(), k_mg_up<MGF_TX, MGF_TY>, dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, tail,
+               ctl);
 }
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, size_t smem, cudaStream_t st) {
-  if (nscenes > 0) k_mg_coarse<<<nscenes, CB_THREADS, smem, st>>>(scenes, nscenes, ctl, tail);
+  if (nscenes > 0) launch_pdl(pdl_enabled(), k_mg_coarse, dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail);
+}
+size_t coarse_factor_smem(int ncap) { return ((size_t)ncap * ncap + 2 * (size_t)ncap) * 4; }
+int coarse_factor_cap() {
+  int n = 256;
+  while (coarse_factor_smem(n) > kCoarseSmemMax) n--;
+  return n;
+}
+void launch_coarse_factor(const SceneDesc* scenes, int nscenes, int nmax, cudaStream_t st) {
+  const int ncap = std::min(nmax, coarse_factor_cap());
+  if (nscenes > 0) k_coarse_factor<<<nscenes, 1024, coarse_factor_smem(ncap), st>>>(scenes, ncap);
+}
+cudaError_t prepare_coarse_factor() {
+  return cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)coarse_factor_smem(coarse_factor_cap()));
 }
 cudaError_t prepare_mg_coarse(size_t smem) {
   return cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

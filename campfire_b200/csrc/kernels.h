@@ -25,9 +25,32 @@ constexpr int MGF_CBW = MGF_TX / 2 + 16, MGF_CBH = MGF_TY / 2 + 8;        // coa
 // tensor maps per level, in the scene arena (CUtensorMap: 128 bytes, 64-byte aligned)
 enum TmapKind { TM_P = 0, TM_PB, TM_RHS, TM_AX, TM_AY, TM_PC, TM_PER_LEVEL };
 constexpr int TMAP_BYTES = 128;
-constexpr int COARSE_CELLS = 6144;                   // largest level handled by the one-CTA coarse block
+constexpr int COARSE_CELLS = 6144;                   // default: largest level handled by the one-CTA coarse block
+constexpr size_t kCoarseSmemMax = 232448 - 2048;     // dynamic shared memory of the coarse block (227 KB less static)
 constexpr int PR_TX = 32, PR_TY = 8;                 // projection
 constexpr int GEO_TX = 32, GEO_TY = 8;               // geometry
+
+// Launch with programmatic stream serialization (the kernel must call pdl_wait()
+// before it touches data an earlier kernel of the step writes) when `pdl`, else an
+// ordinary launch.
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = pdl ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+// programmatic dependent launch for the pressure-loop kernels (set by the engine)
+void set_pdl(bool on);
+bool pdl_enabled();
 
 // Work-list kinds (tiles per scene are built by the engine)
 enum WorkKind { WK_ADV, WK_DS, WK_FR, WK_PR, WK_GEO, WK_MG0 };
@@ -63,6 +86,11 @@ void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int nt
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, size_t smem, cudaStream_t st);
 size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);
 cudaError_t prepare_mg_coarse(size_t smem);
+// direct coarse solve: the inverse of each scene's coarsest operator (scenes whose
+// coarsest level has more than coarse_factor_cap() cells keep the sweeps)
+void launch_coarse_factor(const SceneDesc* scenes, int nscenes, int nmax, cudaStream_t st);
+int coarse_factor_cap();
+cudaError_t prepare_coarse_factor();
 // ||rhs||^2 (FP64 mode: ||rhs64||^2) of level 0; arms the pressure loop
 void launch_bnorm(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool fp64, cudaStream_t st);
 // FP64: p64 += p0

@@ -205,6 +205,14 @@ class FluidSim(_SceneOps):
     def run_stage(self, name: str):
         check(_lib.lib().cfg_run_stage(self._h, name.encode()))
 
+    def set_coarse_cells(self, cells: int):
+        """Smoother schedule: the one-CTA coarse block starts at the first level with <= cells cells."""
+        check(_lib.lib().cfg_set_coarse_cells(self._h, int(cells)))
+
+    def set_coarse_solve(self, direct: bool):
+        """TOL/FP64 modes: solve the coarsest level with its inverse (True) or 120 sweeps (False)."""
+        check(_lib.lib().cfg_set_coarse_solve(self._h, 1 if direct else 0))
+
     def set_solver(self, mode: int = _lib.SOLVE_FIXED, ncycles: int = 1, tol: float = 1e-6, max_cycles: int = 50):
         check(_lib.lib().cfg_set_solver(self._h, mode, ncycles, tol, max_cycles))
 
@@ -267,6 +275,12 @@ class Batch:
     def set_solver(self, mode=_lib.SOLVE_FIXED, ncycles=1, tol=1e-6, max_cycles=50):
         check(_lib.lib().cfg_batch_set_solver(self._h, mode, ncycles, tol, max_cycles))
 
+    def set_coarse_cells(self, cells: int):
+        check(_lib.lib().cfg_batch_set_coarse_cells(self._h, int(cells)))
+
+    def set_coarse_solve(self, direct: bool):
+        check(_lib.lib().cfg_batch_set_coarse_solve(self._h, 1 if direct else 0))
+
     def set_active(self, i: int, on: bool):
         check(_lib.lib().cfg_batch_set_active(self._h, i, 1 if on else 0))
 
@@ -286,6 +300,22 @@ class Batch:
 
     def geometry(self):
         check(_lib.lib().cfg_batch_geometry(self._h))
+
+
+def autotune(dims, iters: int = 20, device: int = 0, coarse_direct: bool = False) -> dict:
+    """Time the fused V-cycle under every coarse-block threshold on a scratch batch of these
+    sizes (cfg_autotune); {"best": cells, "ms_per_cycle": {cells: ms}}."""
+    n = len(dims)
+    nx = (ctypes.c_int * n)(*[d[0] for d in dims])
+    ny = (ctypes.c_int * n)(*[d[1] for d in dims])
+    cap = 16
+    cells = (ctypes.c_int * cap)()
+    ms = (ctypes.c_double * cap)()
+    k = ctypes.c_int(cap)
+    best = ctypes.c_int()
+    check(_lib.lib().cfg_autotune(device, n, nx, ny, 1 if coarse_direct else 0, iters, ctypes.byref(best), cells, ms,
+                                  ctypes.byref(k)))
+    return {"best": best.value, "ms_per_cycle": {cells[i]: ms[i] for i in range(k.value)}}
 
 
 def generate_scene(kind: int, nx: int, ny: int, width: float = 0.8, seed: int = 1234) -> dict:

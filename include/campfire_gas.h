@@ -175,9 +175,31 @@ int cfg_launch_count(cfg_sim* sim, int* per_step);
  * current state and report its mean device time (CUDA events on the handle's
  * stream), its algorithmic bytes per launch and its launches per step.
  * Kernels: "advect", "diffuse_sources", "forces", "relax0", "restrict0",
- * "prolong0", "coarsest", "resnorm", "project". The state changes as the kernel runs. */
+ * "prolong0", "coarsest", "resnorm", "mg_down0", "mg_up0", "mg_coarse", "vcycle"
+ * (one fused V-cycle), "defect64", "project". The state changes as the kernel runs. */
 int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, double* mean_ms, double* bytes_per_launch,
                     double* launches_per_step);
+
+/* Smoother schedule (no counterpart in the reference, whose schedule is fixed): the levels
+ * from the first one with at most `cells` cells down to the coarsest run in one CTA per
+ * scene, the levels above as tiled down/up kernels. Results are bit-identical for every
+ * choice; only the time changes. Default 6144. Batch views: use cfg_batch_set_coarse_cells. */
+int cfg_set_coarse_cells(cfg_sim* sim, int cells);
+/* Coarsest-level solve of the TOL and FP64 modes (no counterpart in the reference, which runs
+ * one fixed cycle): 0 (default) the reference's 120 red-black sweeps; 1 the level's operator
+ * inverted once per step (f32 Gauss-Jordan, after the coefficients are built) and applied
+ * in every cycle. Scenes whose coarsest level has more than 239 cells, or a sealed gas pocket
+ * (no open boundary in reach: singular operator), keep the sweeps. FIXED mode ignores it. */
+int cfg_set_coarse_solve(cfg_sim* sim, int direct);
+int cfg_batch_set_coarse_solve(cfg_batch* b, int direct);
+/* Autotuner of that schedule (no counterpart in the reference): builds a scratch batch of
+ * these sizes on `device` with generated scenes, runs one step to build the coefficients
+ * (and, with coarse_direct, the coarsest inverse), then times `iters` fused V-cycles for
+ * every threshold that fits (the level sizes). On entry *ncand is the capacity of
+ * cand_cells/cand_ms; on return, the candidates timed (ms per cycle) and *best_cells the
+ * fastest. */
+int cfg_autotune(int device, int nscenes, const int* nx, const int* ny, int coarse_direct, int iters,
+                 int* best_cells, int* cand_cells, double* cand_ms, int* ncand);
 
 /* Synthetic scenes for the benchmark workloads (seeded, deterministic).
  * kind 0: three square logs of half 0.025 at (0.35,0.025) (0.45,0.025) (0.40,0.068),
@@ -205,6 +227,7 @@ int cfg_batch_synchronize(cfg_batch* b);
 int cfg_batch_launch_count(cfg_batch* b, int* per_step);
 int cfg_batch_write_params(cfg_batch* b);
 int cfg_batch_geometry(cfg_batch* b);
+int cfg_batch_set_coarse_cells(cfg_batch* b, int cells);
 
 #ifdef __cplusplus
 }

@@ -160,6 +160,11 @@ struct Sim {
   int mode = SOLVE_FIXED, ncycles = 1, max_cycles = 50, min_cycles = 1;
   double tol = 1e-6;
   int last_cycles = 0; double last_rel = 0, last_rel0 = 0;
+  // direct coarse solve of the TOL/FP64 modes (extension of the library; the reference
+  // runs one fixed cycle with the 120-sweep coarsest level)
+  int coarse_direct = 0;
+  std::vector<R> cinv;
+  bool cinv_ok = false;
   std::vector<double> p64, rhs64;   // FP64 defect correction state (level 0)
 
   // converted parameters (R)
@@ -754,14 +759,86 @@ struct Sim {
         }
     for (int k = 0; k < n; k++) L.p[k] = wp[k];
   }
-  // js/fluid.js:294-312
-  void vcycle(int nu = 2) {
+  // Inverse of the coarsest operator by Gauss-Jordan without pivoting (A_kk the
+  // stencil diagonal, A_km = -face coefficient, closed cells the row dmax e_k), in
+  // the library's operation order: per pivot k, r = 1/a_kk, row k scaled by r, every
+  // other row a_ij = fma(-a_ik, row_k[j], a_ij) with a_ik taken as 0. A pivot <= 1e-6
+  // dmax (singular: a sealed gas pocket) leaves cinv_ok false. Levels over 239 cells
+  // are not inverted (the library's shared-memory bound).
+  void coarse_factor() {
+    const Level& L = lv.back();
+    const int n = L.nx * L.ny;
+    cinv_ok = false;
+    if (n > 239) return;
+    std::vector<R> a((size_t)n * n, R(0)), dg(n), fcol(n), rowk(n);
+    for (int k = 0; k < n; k++) {
+      const int i = k % L.nx, j = k / L.nx;
+      const R w = L.ax[j * (L.nx + 1) + i], e = L.ax[j * (L.nx + 1) + i + 1];
+      const R so = L.ay[j * L.nx + i], no = L.ay[(j + 1) * L.nx + i];
+      R diag = R(0);
+      if (i > 0) diag += w; else diag += R(2) * w;
+      if (i < L.nx - 1) diag += e; else diag += R(2) * e;
+      if (j > 0) diag += so;
+      if (j < L.ny - 1) diag += no; else diag += R(2) * no;
+      dg[k] = diag;
+      if (diag > R(0)) {
+        a[(size_t)k * n + k] = diag;
+        if (i > 0) a[(size_t)k * n + k - 1] = -w;
+        if (i < L.nx - 1) a[(size_t)k * n + k + 1] = -e;
+        if (j > 0) a[(size_t)k * n + k - L.nx] = -so;
+        if (j < L.ny - 1) a[(size_t)k * n + k + L.nx] = -no;
+      }
+    }
+    R dmax = R(0);
+    for (int k = 0; k < n; k++) dmax = std::max(dmax, dg[k]);
+    if (!(dmax > R(0))) return;
+    const R thr = R(1e-6f) * dmax;
+    for (int k = 0; k < n; k++)
+      if (!(dg[k] > R(0))) a[(size_t)k * n + k] = dmax;
+    for (int k = 0; k < n; k++) {
+      const R p = a[(size_t)k * n + k];
+      if (!(p > thr)) return;
+      const R r = R(1) / p;
+      for (int t = 0; t < n; t++) {
+        fcol[t] = a[(size_t)t * n + k];
+        rowk[t] = (t == k ? R(1) : a[(size_t)k * n + t]) * r;
+      }
+      for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+          R& x = a[(size_t)i * n + j];
+          x = i == k ? rowk[j] : std::fma(-fcol[i], rowk[j], j == k ? R(0) : x);
+        }
+    }
+    cinv = std::move(a);
+    cinv_ok = true;
+  }
+  // p = A^-1 b, b = -rhs h2 (0 in closed cells); each row as 8 strided partial sums
+  // (fma, increasing index) combined ((s0+s1)+(s2+s3))+((s4+s5)+(s6+s7))
+  void coarsest_direct(int l) {
+    Level& L = lv[l];
+    const int n = L.nx * L.ny;
+    std::vector<R> b(n);
+    for (int k = 0; k < n; k++) {
+      R off, diag; stencil(L, L.p.data(), k % L.nx, k / L.nx, off, diag);
+      b[k] = diag > R(0) ? -(L.rhs[k] * L.h2) : R(0);
+    }
+    for (int k = 0; k < n; k++) {
+      R sq[8];
+      for (int q = 0; q < 8; q++) {
+        sq[q] = R(0);
+        for (int m = q; m < n; m += 8) sq[q] = std::fma(cinv[(size_t)k * n + m], b[m], sq[q]);
+      }
+      L.p[k] = ((sq[0] + sq[1]) + (sq[2] + sq[3])) + ((sq[4] + sq[5]) + (sq[6] + sq[7]));
+    }
+  }
+  // js/fluid.js:294-312 (direct: the solve loop's cycles with the inverted coarsest level)
+  void vcycle(int nu = 2, bool direct = false) {
     const int NL = (int)lv.size();
     for (int l = 0; l < NL - 1; l++) {
       for (int s = 0; s < nu; s++) { relax(l, 0); relax(l, 1); }
       restrictRes(l);
     }
-    coarsest(NL - 1);
+    if (direct) coarsest_direct(NL - 1); else coarsest(NL - 1);
     for (int l = NL - 2; l >= 0; l--) {
       prolong(l);
       for (int s = 0; s < nu; s++) { relax(l, 1); relax(l, 0); }
@@ -865,10 +942,12 @@ struct Sim {
       const double b = rhs_norm(); last_rel = b > 0 ? res_norm() / b : 0.0;
       return;
     }
+    if (coarse_direct) coarse_factor();
+    const bool direct = coarse_direct && cinv_ok;
     if (mode == SOLVE_TOL) {
       const double b = rhs_norm();
       int c = 0; double rel = 0;
-      do { vcycle(); c++; rel = b > 0 ? res_norm() / b : 0.0; } while (rel > tol && c < max_cycles);
+      do { vcycle(2, direct); c++; rel = b > 0 ? res_norm() / b : 0.0; } while (rel > tol && c < max_cycles);
       last_cycles = c; last_rel = rel;
       return;
     }
@@ -882,7 +961,7 @@ struct Sim {
     Level& L0 = lv[0];
     while (b > 0 && rn / b > tol && c < max_cycles) {
       for (size_t k = 0; k < r.size(); k++) { L0.rhs[k] = R((float)r[k]); L0.p[k] = R(0); }
-      vcycle(); c++;
+      vcycle(2, direct); c++;
       for (size_t k = 0; k < r.size(); k++) p64[k] += (double)L0.p[k];
       rn = res64(r);
     }

@@ -59,7 +59,7 @@ def _declare(L, pfx):
         "readback": [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float),
                      ctypes.POINTER(ctypes.c_int32)],
         "budgets": [vp, dp], "info": [vp, dp], "level_dims": [vp, ci, ctypes.POINTER(ctypes.c_int)],
-        "pressure_residual": [vp, dp],
+        "pressure_residual": [vp, dp], "set_coarse_solve": [vp, ci],
     }
     for name, args in sigs.items():
         fn = getattr(L, pfx + name, None)
@@ -160,6 +160,9 @@ class OracleSim:
 
     def set_solver(self, mode=SOLVE_FIXED, ncycles=1, tol=1e-6, max_cycles=50):
         self._chk(self._f.set_solver(self._h, mode, ncycles, tol, max_cycles))
+
+    def set_coarse_solve(self, direct):
+        self._chk(self._f.set_coarse_solve(self._h, 1 if direct else 0))
 
     def upload_pieces(self, data, n):
         a = np.zeros(64 * 20, np.float32)

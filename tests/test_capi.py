@@ -100,3 +100,18 @@ def test_tepee_and_floor_scenes_have_no_overlaps():
         if kind == 2:
             assert 0.5 * 2e10 <= s["params"]["reactB"] <= 2 * 2e10 * 1.0001
             assert 0.18 <= s["params"]["YOamb"] <= 0.233
+
+
+def test_autotuner_needs_a_device_and_valid_arguments():
+    import ctypes
+    L = cb.lib()
+    one = (ctypes.c_int * 1)(64)
+    cells = (ctypes.c_int * 4)()
+    ms = (ctypes.c_double * 4)()
+    best = ctypes.c_int()
+    k = ctypes.c_int(0)
+    assert L.cfg_autotune(0, 1, one, one, 0, 5, ctypes.byref(best), cells, ms, ctypes.byref(k)) == -22   # no capacity
+    if cb.device_count() == 0:
+        with pytest.raises(cb.CampfireError) as e:
+            cb.autotune([(64, 96)], iters=2)
+        assert e.value.code == -19

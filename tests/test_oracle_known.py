@@ -141,3 +141,31 @@ def test_fp64_projection_is_divergence_consistent(oracle_mod):
     openc = (fx[:, 1:] + fx[:, :-1] + fy[1:] + fy[:-1]) > 0
     err = np.abs(div - S)[openc]
     assert err.max() < 1e-6 * max(1.0, np.abs(S).max())
+
+
+def test_direct_coarsest_falls_back_to_sweeps_when_singular(oracle_mod):
+    """Direct coarsest solve (TOL/FP64 extension): a pocket sealed on the coarsest level
+    makes the operator singular; the oracle then keeps the 120 sweeps, bit for bit."""
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    sc = cb.generate_scene(0, 64, 96, 0.8, 1234)
+    res = {}
+    for direct, seal in ((False, True), (True, True), (False, False), (True, False)):
+        o = oracle_mod.OracleSim(64, 96, 0.8, sc["dt"])
+        load_scene(o, sc)
+        o.set_solver(oracle_mod.SOLVE_FIXED, 1)
+        o.step(3)
+        o.set_solver(oracle_mod.SOLVE_TOL, 1, 1e-30, 2)
+        o.set_coarse_solve(direct)
+        o.stage("coef_rhs")
+        L = int(o.info()["levels"]) - 1
+        if seal:
+            ax, ay = o.read(f"ax.{L}"), o.read(f"ay.{L}")
+            cnx, cny = 8, 12   # the coarsest level of 64x96
+            ax = ax.reshape(cny, cnx + 1).copy(); ay = ay.reshape(cny + 1, cnx).copy()
+            ax[2:4, 2] = 0.0; ax[2:4, 4] = 0.0; ay[2, 2:4] = 0.0; ay[4, 2:4] = 0.0
+            o.write(f"ax.{L}", ax.ravel()); o.write(f"ay.{L}", ay.ravel())
+        o.stage("pressure")
+        res[(direct, seal)] = o.read("p")
+    assert np.array_equal(res[(True, True)], res[(False, True)])        # singular: sweeps
+    assert not np.array_equal(res[(True, False)], res[(False, False)])  # regular: the inverse
