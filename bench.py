@@ -221,6 +221,77 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
             "batched_over_plain": batched / plain}
 
 
+SERVE_CLASSES = ((96, 144), (128, 192), (192, 288), (256, 384), (512, 768))
+
+
+def served_jobs(lam: float, njobs: int, steps_lo: int, steps_hi: int, seed: int):
+    """Poisson arrivals at rate lam; size class uniform; tepee scenes (scene kind 1); N uniform."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t, jobs = 0.0, []
+    for k in range(njobs):
+        t += float(rng.exponential(1.0 / lam))
+        jobs.append({"size_class": int(rng.integers(0, len(SERVE_CLASSES))), "kind": 1, "seed": 9000 + k,
+                     "nsteps": int(rng.integers(steps_lo, steps_hi + 1)), "arrival_s": t})
+    return jobs
+
+
+def run_served(dev, stream, lams, njobs: int, steps_lo: int, steps_hi: int, slots: int, budget: float, tol: float):
+    """The serving loop (continuous batching, HBM-budget admission) at several arrival rates, against the
+    same jobs served one by one by the plain single-scene step (FIFO; each job's time from the measured
+    plain ms/step of its size class)."""
+    import numpy as np
+    import torch
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    # plain per-step time of each size class (same solver), for the one-by-one schedule
+    plain_ms = {}
+    for c, (nx, ny) in enumerate(SERVE_CLASSES):
+        sc = cb.generate_scene(1, nx, ny, 0.8, 9000)
+        g = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+        load_scene(g, sc)
+        g.set_solver(cb.SOLVE_FP64, 1, tol, 300)
+        g.set_coarse_solve(True)
+        g.set_stream(stream.cuda_stream)
+        g.step(3)
+        g.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step(5)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_ms[c] = e0.elapsed_time(e1) / 5
+        g.close()
+    srv = cb.Server(SERVE_CLASSES, [slots] * len(SERVE_CLASSES), budget, device=dev.index)
+    srv.set_solver(cb.SOLVE_FP64, 1, tol, 300, True)
+    out = []
+    for lam in lams:
+        jobs = served_jobs(lam, njobs, steps_lo, steps_hi, seed=int(lam) + 17)
+        res, wall, cu = srv.run(jobs)
+        lat = np.array([r["done_s"] - r["arrival_s"] for r in res])
+        # one by one, first come first served, with the plain step
+        t_free, lat1 = 0.0, []
+        for j in sorted(jobs, key=lambda q: q["arrival_s"]):
+            start = max(j["arrival_s"], t_free)
+            t_free = start + j["nsteps"] * plain_ms[j["size_class"]] / 1e3
+            lat1.append(t_free - j["arrival_s"])
+        lat1 = np.array(lat1)
+        cells = sum(SERVE_CLASSES[j["size_class"]][0] * SERVE_CLASSES[j["size_class"]][1] * j["nsteps"] for j in jobs)
+        out.append({"lambda_jobs_per_s": lam, "jobs": njobs, "value": cu / wall, "unit": METRIC,
+                    "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                    "wall_s": wall, "max_rel_residual": max(r["last_rel"] for r in res),
+                    "one_by_one": {"value": cells / t_free if t_free > 0 else None, "unit": METRIC,
+                                   "p50_latency_s": float(np.percentile(lat1, 50)),
+                                   "p99_latency_s": float(np.percentile(lat1, 99))}})
+    srv.close()
+    return {"classes": [f"{a}x{b}" for a, b in SERVE_CLASSES], "slots_per_class": slots, "budget_bytes": budget,
+            "steps_per_job": [steps_lo, steps_hi], "scene": "tepee (five logs of half 5 cm), FP64 defect correction "
+            f"to {tol:g}, direct coarsest", "one_by_one_model": "FIFO over the same jobs with each class's measured "
+            "plain single-scene ms/step", "plain_ms_per_step": {f"{a}x{b}": plain_ms[c] for c, (a, b) in
+                                                                enumerate(SERVE_CLASSES)},
+            "runs": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -232,6 +303,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=10,
                     help="timed steps of the 64-scene batched measurement added to the line (0: skip)")
+    ap.add_argument("--served-jobs", type=int, default=40,
+                    help="jobs per arrival rate of the serving measurement added to the line (0: skip)")
+    ap.add_argument("--served-steps", type=int, nargs=2, default=(20, 200), metavar=("LO", "HI"),
+                    help="steps per served job, uniform in [LO, HI]")
+    ap.add_argument("--served-rates", type=float, nargs="+", default=(10.0, 100.0, 1000.0))
     ap.add_argument("--launch", default="graph", choices=["graph", "stream"],
                     help="graph: one CUDA graph per step (pressure loop as a device-side WHILE node); "
                          "stream: kernel by kernel, the host polling the loop decision (for profilers that "
@@ -375,6 +451,11 @@ def main():
     if a.batched_steps > 0:
         batched = run_batched(dev, stream, flush, a.batched_steps, 3, 1e-10, 300, 3)
 
+    served = None
+    if a.served_jobs > 0:
+        served = run_served(dev, stream, a.served_rates, a.served_jobs, a.served_steps[0], a.served_steps[1],
+                            slots=12, budget=150e9, tol=1e-10)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         th = cpu_threads()
@@ -394,7 +475,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 204 + 16,
                         "d2h_bytes_per_step": 528 * 4 + 320 * 16 + 256 * 4},
                 "gpu_launches": launches * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "batched": batched}
+                "batched": batched, "served": served}
         print(json.dumps(line))
     sim.close()
     if world > 1:

@@ -50,6 +50,18 @@ class CfgInfo(ctypes.Structure):
                 ("level_nx", ctypes.c_int32 * MAX_LEVELS), ("level_ny", ctypes.c_int32 * MAX_LEVELS)]
 
 
+class CfgJob(ctypes.Structure):
+    _fields_ = [("size_class", ctypes.c_int32), ("kind", ctypes.c_int32), ("seed", ctypes.c_uint64),
+                ("nsteps", ctypes.c_int32), ("pad", ctypes.c_int32), ("arrival_s", ctypes.c_double)]
+
+
+class CfgJobResult(ctypes.Structure):
+    _fields_ = [("arrival_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double),
+                ("slot", ctypes.c_int32), ("steps", ctypes.c_int32), ("last_cycles", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("last_rel", ctypes.c_double), ("hash", ctypes.c_uint64),
+                ("t_sum", ctypes.c_double)]
+
+
 class CampfireError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -102,6 +114,10 @@ def lib():
         "cfg_set_coarse_cells": [vp, ci], "cfg_batch_set_coarse_cells": [vp, ci],
         "cfg_autotune": [ci, ci, ip, ip, ci, ci, ip, ip, dp, ip],
         "cfg_set_coarse_solve": [vp, ci], "cfg_batch_set_coarse_solve": [vp, ci],
+        "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
+        "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci],
+        "cfg_server_slot_bytes": [vp, ci, ctypes.POINTER(sz)],
+        "cfg_server_run": [vp, ctypes.POINTER(CfgJob), ci, ctypes.POINTER(CfgJobResult), dp, dp],
     }
     for name, args in sigs.items():
         f = getattr(L, name)

@@ -179,9 +179,8 @@ extern "C" int cfg_batch_set_coarse_cells(cfg_batch* b, int cells) {
   return guarded([&] { return b->eng->set_coarse_cells(cells); });
 }
 
-namespace {
-// a generated scene loaded into scene s of an engine, in FluidSim's set-up order
-int load_generated(cfg::Engine& eng, int s, int kind, int nx, int ny, double width, uint64_t seed) {
+int cfg::load_generated_scene(cfg::Engine& eng, int s, int kind, double width, uint64_t seed) {
+  const int nx = eng.scene_nx(s), ny = eng.scene_ny(s);
   const size_t n = (size_t)nx * ny;
   std::vector<float> T(n), Y(4 * n), U((size_t)(nx + 1) * ny), V((size_t)nx * (ny + 1)),
       pieces((size_t)CFG_MAX_PIECES * CFG_PIECE_FLOATS);
@@ -195,9 +194,12 @@ int load_generated(cfg::Engine& eng, int s, int kind, int nx, int ny, double wid
     std::memcpy(&f, reinterpret_cast<const char*>(&P) + 4 * cfg::param_index(k), 4);
     CFG_TRY(eng.set_param(s, k, f));
   }
+  CFG_TRY(eng.set_dt(s, dt));
+  CFG_TRY(eng.set_frame(s, 0));
+  // reset before writeParams so that a reused batch slot uploads time 0, as a fresh one does
+  CFG_TRY(eng.reset(s));
   CFG_TRY(eng.upload_pieces(s, pieces.data(), np));
   CFG_TRY(eng.write_params(s));
-  CFG_TRY(eng.reset(s));
   CFG_TRY(eng.write_field(s, "T", T.data(), T.size()));
   CFG_TRY(eng.write_field(s, "Y", Y.data(), Y.size()));
   CFG_TRY(eng.write_field(s, "U", U.data(), U.size()));
@@ -207,7 +209,6 @@ int load_generated(cfg::Engine& eng, int s, int kind, int nx, int ny, double wid
   CFG_TRY(eng.clear_geometry(s));
   return eng.geometry(s);
 }
-}  // namespace
 
 extern "C" int cfg_autotune(int device, int nscenes, const int* nx, const int* ny, int coarse_direct, int iters,
                             int* best_cells, int* cand_cells, double* cand_ms, int* ncand) {
@@ -217,7 +218,7 @@ extern "C" int cfg_autotune(int device, int nscenes, const int* nx, const int* n
     std::vector<double> width(nscenes, 0.8), dt(nscenes, 0.002);
     cfg::Engine eng;
     CFG_TRY(eng.init(device, nscenes, nx, ny, width.data(), dt.data()));
-    for (int s = 0; s < nscenes; s++) CFG_TRY(load_generated(eng, s, 0, nx[s], ny[s], 0.8, 1234 + s));
+    for (int s = 0; s < nscenes; s++) CFG_TRY(cfg::load_generated_scene(eng, s, 0, 0.8, 1234 + s));
     if (coarse_direct) {
       CFG_TRY(eng.set_solver(CFG_SOLVE_FP64, 1, 1e-6, 4));
       CFG_TRY(eng.set_coarse_solve(1));

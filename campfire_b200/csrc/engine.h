@@ -40,6 +40,12 @@ struct PhysConst {
 void default_params(cfg_params* p);
 int param_index(const char* name);   // -1 if unknown
 
+class Engine;
+// A seeded synthetic scene (cfg_scene_generate) loaded into scene s of an engine in
+// FluidSim's set-up order (params, pieces, writeParams, reset, fields, geometry),
+// with the scene's own dt; frame 0.
+int load_generated_scene(Engine& eng, int s, int kind, double width, uint64_t seed);
+
 // One scene: FluidSim's host fields (js/fluid.js:27-47) and its device arrays.
 struct Scene {
   int nx = 0, ny = 0, nlev = 0;
@@ -119,6 +125,10 @@ class Engine {
   // coarsest level of the TOL/FP64 modes: 0 the reference's 120 sweeps, 1 its inverse
   int set_coarse_solve(int direct);
   int scene_lc(int s) const { return scenes_[s].lc; }
+  size_t arena_bytes(int s) const { return scenes_[s].arena_bytes; }
+  int scene_nx(int s) const { return scenes_[s].nx; }
+  int scene_ny(int s) const { return scenes_[s].ny; }
+  cudaStream_t stream() const { return st(); }
   int nscenes() const { return (int)scenes_.size(); }
 
  private:

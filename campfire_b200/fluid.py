@@ -302,6 +302,63 @@ class Batch:
         check(_lib.lib().cfg_batch_geometry(self._h))
 
 
+class Server:
+    """Continuous-batching server of gas-step jobs (cfg_server_*): resident slots per size
+    class, admission by an HBM budget, one batched step per loop iteration."""
+
+    def __init__(self, classes, slots, budget_bytes: float, device: int = 0, width: float = 0.8):
+        n = len(classes)
+        nx = (ctypes.c_int * n)(*[c[0] for c in classes])
+        ny = (ctypes.c_int * n)(*[c[1] for c in classes])
+        sl = (ctypes.c_int * n)(*slots)
+        h = ctypes.c_void_p()
+        check(_lib.lib().cfg_server_create(device, n, nx, ny, sl, float(budget_bytes), width, ctypes.byref(h)))
+        self._h = h.value
+        self.classes = list(classes)
+
+    def close(self):
+        if self._h:
+            _lib.lib().cfg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_solver(self, mode=_lib.SOLVE_FP64, ncycles=1, tol=1e-10, max_cycles=300, coarse_direct=True,
+                   coarse_cells=0):
+        check(_lib.lib().cfg_server_set_solver(self._h, mode, ncycles, tol, max_cycles, 1 if coarse_direct else 0,
+                                               coarse_cells))
+
+    def slot_bytes(self, size_class: int) -> int:
+        b = ctypes.c_size_t()
+        check(_lib.lib().cfg_server_slot_bytes(self._h, size_class, ctypes.byref(b)))
+        return b.value
+
+    def run(self, jobs):
+        """jobs: dicts with size_class, kind, seed, nsteps, arrival_s. Returns (results, wall_s, cell_updates)."""
+        n = len(jobs)
+        arr = (_lib.CfgJob * max(n, 1))()
+        for i, j in enumerate(jobs):
+            arr[i] = _lib.CfgJob(j["size_class"], j.get("kind", 1), j["seed"], j["nsteps"], 0, j["arrival_s"])
+        res = (_lib.CfgJobResult * max(n, 1))()
+        wall, cu = ctypes.c_double(), ctypes.c_double()
+        check(_lib.lib().cfg_server_run(self._h, arr, n, res, ctypes.byref(wall), ctypes.byref(cu)))
+        out = [{k: getattr(res[i], k) for k, _ in _lib.CfgJobResult._fields_ if k != "pad"} for i in range(n)]
+        return out, wall.value, cu.value
+
+
+def field_hash(sim) -> int:
+    """FNV-1a 64 of the dense T, Y, U, V float32 bytes (the hash cfg_server_run reports)."""
+    h = 1469598103934665603
+    for f in ("T", "Y", "U", "V"):
+        for b in np.ascontiguousarray(sim.readBuffer(f), np.float32).tobytes():
+            h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
 def autotune(dims, iters: int = 20, device: int = 0, coarse_direct: bool = False) -> dict:
     """Time the fused V-cycle under every coarse-block threshold on a scratch batch of these
     sizes (cfg_autotune); {"best": cells, "ms_per_cycle": {cells: ms}}."""

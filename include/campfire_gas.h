@@ -229,6 +229,40 @@ int cfg_batch_write_params(cfg_batch* b);
 int cfg_batch_geometry(cfg_batch* b);
 int cfg_batch_set_coarse_cells(cfg_batch* b, int cells);
 
+/* ---- serving: jobs of several grid sizes in resident batch slots (no counterpart in the
+ * reference). One batch holds slots[c] scenes of size class c (nx[c] x ny[c]); a job is
+ * admitted into a free slot of its class once it has arrived and the bytes of the slots in
+ * use plus its own fit in budget_bytes. Admitted jobs advance together, one batched step per
+ * loop iteration, and leave after their own step count (continuous batching). */
+typedef struct cfg_server cfg_server;
+typedef struct cfg_job {
+  int32_t size_class;       /* index into the server's classes */
+  int32_t kind;             /* scene generator kind (cfg_scene_generate) */
+  uint64_t seed;            /* scene seed */
+  int32_t nsteps;           /* gas steps to run */
+  int32_t pad;
+  double arrival_s;         /* arrival time, seconds after cfg_server_run starts */
+} cfg_job;
+typedef struct cfg_job_result {
+  double arrival_s, admit_s, done_s;   /* seconds after cfg_server_run starts */
+  int32_t slot, steps, last_cycles, pad;
+  double last_rel;          /* final relative residual of the last pressure solve */
+  uint64_t hash;            /* FNV-1a 64 of the final dense T, Y, U, V bytes */
+  double t_sum;             /* sum of the final T */
+} cfg_job_result;
+int cfg_server_create(int device, int nclasses, const int* nx, const int* ny, const int* slots, double budget_bytes,
+                      double width, cfg_server** out);
+int cfg_server_destroy(cfg_server* s);
+/* solver of every slot (as cfg_set_solver, cfg_set_coarse_solve, cfg_set_coarse_cells; cells <= 0 keeps it) */
+int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int max_cycles, int coarse_direct,
+                          int coarse_cells);
+/* device bytes of one slot of a size class */
+int cfg_server_slot_bytes(cfg_server* s, int size_class, size_t* bytes);
+/* run the jobs to completion in real time (arrivals are honoured by the host clock);
+ * results[j] for jobs[j]; *wall_s the run's duration, *cell_updates the cells stepped */
+int cfg_server_run(cfg_server* s, const cfg_job* jobs, int njobs, cfg_job_result* results, double* wall_s,
+                   double* cell_updates);
+
 #ifdef __cplusplus
 }
 #endif

@@ -115,3 +115,13 @@ def test_autotuner_needs_a_device_and_valid_arguments():
         with pytest.raises(cb.CampfireError) as e:
             cb.autotune([(64, 96)], iters=2)
         assert e.value.code == -19
+
+
+def test_server_structs_match_the_header():
+    import ctypes
+    assert ctypes.sizeof(cb._lib.CfgJob) == 32
+    assert ctypes.sizeof(cb._lib.CfgJobResult) == 64
+    if cb.device_count() == 0:
+        with pytest.raises(cb.CampfireError) as e:
+            cb.Server([(64, 96)], [1], 1e9)
+        assert e.value.code == -19
