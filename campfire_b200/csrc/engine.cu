@@ -141,7 +141,6 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   // CAMPFIRE_PDL=0 launches the pressure-loop kernels without programmatic dependent launch
   if (const char* v = std::getenv("CAMPFIRE_PDL")) set_pdl(v[0] != '0');
   CFG_CUDA(prepare_mg_coarse(coarse_smem_));
-  CFG_CUDA(prepare_coarse_factor());
   CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaMalloc(&d_scenes_, sizeof(SceneDesc) * n));
@@ -664,18 +663,13 @@ void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_con
   launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); launches_++;
   for (int l = FR_KMAX; l + 1 < max_levels(); l++)
     if (nwl_[WL_MGC0 + l] > 0) { launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s); launches_++; }
-  if (direct_coarse()) { launch_coarse_factor(d_scenes_, nscenes(), max_coarsest_cells(), s); launches_++; }
+  if (direct_coarse()) { launch_coarse_factor(d_scenes_, nscenes(), s); launches_++; }
   if (fp64) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s); launches_++; }
   // the loop's cycle counter starts at zero in every step
   cudaMemsetAsync(&d_ctl_->iter, 0, sizeof(int), s);
   (void)h; (void)use_cond;
 }
 
-int Engine::max_coarsest_cells() const {
-  int m = 1;
-  for (auto& sc : scenes_) m = std::max(m, sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1]);
-  return m;
-}
 int Engine::set_coarse_solve(int direct) {
   if (direct != 0 && direct != 1) return fail(CFG_ERR_INVAL, "coarse solve must be 0 (sweeps) or 1 (direct)");
   CFG_TRY(activate());
@@ -939,7 +933,7 @@ int Engine::run_stage(const char* stage) {
     for (int l = FR_KMAX; l + 1 < max_levels(); l++)
       launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   } else if (st_ == "pressure") {
-    if (direct_coarse()) launch_coarse_factor(d_scenes_, nscenes(), max_coarsest_cells(), s);
+    if (direct_coarse()) launch_coarse_factor(d_scenes_, nscenes(), s);
     enqueue_bnorm(s);
     CFG_TRY(host_pressure_loop());
   } else if (st_ == "project") launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s);

@@ -153,7 +153,6 @@ class Engine {
   void enqueue_vcycle(cudaStream_t s, int tail);   // fused kernels (the step's cycle); tail as k_mg_up
   void enqueue_vcycle_ref(cudaStream_t s);   // one kernel per reference dispatch (cfg_vcycle)
   int max_lc() const;
-  int max_coarsest_cells() const;
   bool direct_coarse() const { return mode_ != CFG_SOLVE_FIXED && coarse_direct_ != 0; }
   void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
   void enqueue_post_solve(cudaStream_t s);

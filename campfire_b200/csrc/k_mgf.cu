@@ -524,32 +524,38 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
 }
 
 // ------------------------------------------------------------------ direct coarse solve: the coarsest inverse
-// Gauss-Jordan inversion in f32 without pivoting of the coarsest operator A (A_kk =
-// the stencil's diagonal, A_km = -face coefficient; a closed cell gets the row
-// dmax e_k and b_k = 0), once per step after the coefficients are built. A is
-// symmetric and, with an open boundary in reach of every gas cell, positive
-// definite; a pivot <= 1e-6 dmax (a sealed gas pocket: pure Neumann) leaves
-// direct_ok = 0 and the coarse block keeps the 120 sweeps for this step. Per pivot
-// k: r = 1/a_kk; row k scaled by r (a_kk -> r); every other row i updated as
-// a_ij = fma(-a_ik, row_k[j], a_ij) with a_ik first set to 0.
-__global__ void __launch_bounds__(1024) k_coarse_factor(const SceneDesc* __restrict__ scenes, int ncap) {
-  extern __shared__ float a[];
+// The coarsest operator A (A_kk = the stencil's diagonal, A_km = -face coefficient;
+// a closed cell gets the row dmax e_k) is symmetric with half-bandwidth nx in
+// row-major cell order. Once per step: banded Cholesky A = L L^T (right-looking,
+// one warp: per column jc, L_jcjc = sqrt(a_jcjc), L_ijc = a_ijc / L_jcjc, then
+// a_ik = fma(-L_ijc, L_kjc, a_ik) for jc < k <= i <= jc + nx), then column c of
+// A^-1 by forward and back substitution on thread c (y_i = (e_ic - sum L_ik y_k) *
+// (1/L_ii) with k ascending, then x_i = (y_i - sum L_ki x_k) * (1/L_ii), k ascending).
+// A pivot a_jcjc <= 1e-6 dmax (a sealed gas pocket: singular) or a level wider than
+// CF_MAXBW cells leaves direct_ok = 0, and the coarse block keeps the 120 sweeps.
+namespace {
+constexpr int CF_THREADS = 256;   // the coarsest level has at most 256 cells
+constexpr int CF_MAXBW = 32;
+}
+
+__global__ void __launch_bounds__(CF_THREADS) k_coarse_factor(const SceneDesc* __restrict__ scenes) {
+  __shared__ float band[CF_THREADS * (CF_MAXBW + 1)];
+  __shared__ float rinv[CF_THREADS];
   __shared__ float s_dmax;
   __shared__ int s_ok;
   const SceneDesc& S = scenes[blockIdx.x];
   if (!S.enabled) return;
   const LevelDesc L = S.lev[S.nlev - 1];
-  const int n = L.nx * L.ny;
-  if (n > ncap) {
+  const int n = L.nx * L.ny, bw = L.nx, W = bw + 1;
+  if (n > CF_THREADS || bw > CF_MAXBW) {
     if (threadIdx.x == 0) S.solve->direct_ok = 0;
     return;
   }
-  float* fcol = a + n * n;
-  float* rowk = fcol + n;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) a[e] = 0.f;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < n * W; e += CF_THREADS) band[e] = 0.f;
   __syncthreads();
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+  // lower band: band[k*W + d] = A[k][k-d]; the diagonal is kept in rinv[] until dmax is known
+  for (int k = tid; k < n; k += CF_THREADS) {
     const int i = k % L.nx, j = k / L.nx;
     const float w = L.ax[j * L.pu + i], e = L.ax[j * L.pu + i + 1];
     const float so = L.ay[j * L.pc + i], no = L.ay[(j + 1) * L.pc + i];
@@ -558,53 +564,71 @@ __global__ void __launch_bounds__(1024) k_coarse_factor(const SceneDesc* __restr
     if (i < L.nx - 1) diag += e; else diag += 2.f * e;
     if (j > 0) diag += so;
     if (j < L.ny - 1) diag += no; else diag += 2.f * no;
-    fcol[k] = diag;
+    rinv[k] = diag;
     if (diag > 0.f) {
-      a[k * n + k] = diag;
-      if (i > 0) a[k * n + k - 1] = -w;
-      if (i < L.nx - 1) a[k * n + k + 1] = -e;
-      if (j > 0) a[k * n + k - L.nx] = -so;
-      if (j < L.ny - 1) a[k * n + k + L.nx] = -no;
+      band[k * W] = diag;
+      if (i > 0) band[k * W + 1] = -w;
+      if (j > 0) band[k * W + bw] = -so;
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     float m = 0.f;
-    for (int k = 0; k < n; k++) m = fmaxf(m, fcol[k]);
+    for (int k = 0; k < n; k++) m = fmaxf(m, rinv[k]);
     s_dmax = m;
     s_ok = m > 0.f ? 1 : 0;
   }
   __syncthreads();
   const float dmax = s_dmax, thr = 1e-6f * dmax;
-  for (int k = threadIdx.x; k < n; k += blockDim.x)
-    if (!(fcol[k] > 0.f)) a[k * n + k] = dmax;
+  for (int k = tid; k < n; k += CF_THREADS)
+    if (!(rinv[k] > 0.f)) band[k * W] = dmax;
   __syncthreads();
-  for (int k = 0; k < n && s_ok; k++) {
-    const float p = a[k * n + k];
-    if (!(p > thr)) {   // uniform: every thread read the same pivot
-      if (threadIdx.x == 0) s_ok = 0;
-      break;
-    }
-    const float r = 1.0f / p;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      fcol[t] = a[t * n + k];
-      rowk[t] = (t == k ? 1.0f : a[k * n + t]) * r;
-    }
-    __syncthreads();
-    for (int i = warp; i < n; i += nw) {
-      const float f = fcol[i];
-      for (int j = lane; j < n; j += 32) {
-        const int e = i * n + j;
-        a[e] = i == k ? rowk[j] : __fmaf_rn(-f, rowk[j], j == k ? 0.f : a[e]);
+  if (warp == 0 && s_ok) {
+    for (int jc = 0; jc < n; jc++) {
+      const float piv = band[jc * W];
+      if (!(piv > thr)) {   // every lane read the same pivot
+        if (lane == 0) s_ok = 0;
+        break;
       }
+      const float ljj = sqrtf(piv);
+      const int i = jc + 1 + lane;
+      const bool mine = lane < bw && i < n;
+      float lij = 0.f;
+      if (mine) lij = band[i * W + (i - jc)] / ljj;
+      __syncwarp();
+      if (lane == 0) band[jc * W] = ljj;
+      if (mine) band[i * W + (i - jc)] = lij;
+      __syncwarp();
+      if (mine)
+        for (int k = jc + 1; k <= i; k++) band[i * W + (i - k)] = __fmaf_rn(-lij, band[k * W + (k - jc)], band[i * W + (i - k)]);
+      __syncwarp();
     }
-    __syncthreads();
   }
   __syncthreads();
-  const int ok = s_ok;
-  if (ok)
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) S.cinv[e] = a[e];
-  if (threadIdx.x == 0) S.solve->direct_ok = ok;
+  if (!s_ok) {
+    if (tid == 0) S.solve->direct_ok = 0;
+    return;
+  }
+  for (int k = tid; k < n; k += CF_THREADS) rinv[k] = 1.0f / band[k * W];
+  __syncthreads();
+  const int c = tid;
+  if (c < n) {
+    float y[CF_THREADS];
+    for (int i = 0; i < c; i++) y[i] = 0.f;
+    for (int i = c; i < n; i++) {
+      float sum = i == c ? 1.f : 0.f;
+      for (int k = max(c, i - bw); k < i; k++) sum = __fmaf_rn(-band[i * W + (i - k)], y[k], sum);
+      y[i] = sum * rinv[i];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      float sum = y[i];
+      const int kend = min(n - 1, i + bw);
+      for (int k = i + 1; k <= kend; k++) sum = __fmaf_rn(-band[k * W + (k - i)], y[k], sum);
+      y[i] = sum * rinv[i];
+    }
+    for (int i = 0; i < n; i++) S.cinv[(size_t)i * n + c] = y[i];
+  }
+  if (tid == 0) S.solve->direct_ok = 1;
 }
 
 // shared bytes of the coarse block for one scene (the layout built by k_mg_coarse)
@@ -631,19 +655,8 @@ void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int nt
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, size_t smem, cudaStream_t st) {
   if (nscenes > 0) launch_pdl(pdl_enabled(), k_mg_coarse, dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail);
 }
-size_t coarse_factor_smem(int ncap) { return ((size_t)ncap * ncap + 2 * (size_t)ncap) * 4; }
-int coarse_factor_cap() {
-  int n = 256;
-  while (coarse_factor_smem(n) > kCoarseSmemMax) n--;
-  return n;
-}
-void launch_coarse_factor(const SceneDesc* scenes, int nscenes, int nmax, cudaStream_t st) {
-  const int ncap = std::min(nmax, coarse_factor_cap());
-  if (nscenes > 0) k_coarse_factor<<<nscenes, 1024, coarse_factor_smem(ncap), st>>>(scenes, ncap);
-}
-cudaError_t prepare_coarse_factor() {
-  return cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)coarse_factor_smem(coarse_factor_cap()));
+void launch_coarse_factor(const SceneDesc* scenes, int nscenes, cudaStream_t st) {
+  if (nscenes > 0) k_coarse_factor<<<nscenes, CF_THREADS, 0, st>>>(scenes);
 }
 cudaError_t prepare_mg_coarse(size_t smem) {
   return cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -87,10 +87,8 @@ void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int t
 size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);
 cudaError_t prepare_mg_coarse(size_t smem);
 // direct coarse solve: the inverse of each scene's coarsest operator (scenes whose
-// coarsest level has more than coarse_factor_cap() cells keep the sweeps)
-void launch_coarse_factor(const SceneDesc* scenes, int nscenes, int nmax, cudaStream_t st);
-int coarse_factor_cap();
-cudaError_t prepare_coarse_factor();
+// coarsest level is wider than 32 cells keep the sweeps)
+void launch_coarse_factor(const SceneDesc* scenes, int nscenes, cudaStream_t st);
 // ||rhs||^2 (FP64 mode: ||rhs64||^2) of level 0; arms the pressure loop
 void launch_bnorm(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool fp64, cudaStream_t st);
 // FP64: p64 += p0

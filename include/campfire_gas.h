@@ -187,9 +187,10 @@ int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, double* mean_ms
 int cfg_set_coarse_cells(cfg_sim* sim, int cells);
 /* Coarsest-level solve of the TOL and FP64 modes (no counterpart in the reference, which runs
  * one fixed cycle): 0 (default) the reference's 120 red-black sweeps; 1 the level's operator
- * inverted once per step (f32 Gauss-Jordan, after the coefficients are built) and applied
- * in every cycle. Scenes whose coarsest level has more than 239 cells, or a sealed gas pocket
- * (no open boundary in reach: singular operator), keep the sweeps. FIXED mode ignores it. */
+ * inverted once per step (f32 banded Cholesky and column solves, after the coefficients are
+ * built) and applied in every cycle. Scenes whose coarsest level is wider than 32 cells, or
+ * has a sealed gas pocket (no open boundary in reach: singular operator), keep the sweeps.
+ * FIXED mode ignores it. */
 int cfg_set_coarse_solve(cfg_sim* sim, int direct);
 int cfg_batch_set_coarse_solve(cfg_batch* b, int direct);
 /* Autotuner of that schedule (no counterpart in the reference): builds a scratch batch of

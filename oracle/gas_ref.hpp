@@ -759,18 +759,19 @@ struct Sim {
         }
     for (int k = 0; k < n; k++) L.p[k] = wp[k];
   }
-  // Inverse of the coarsest operator by Gauss-Jordan without pivoting (A_kk the
-  // stencil diagonal, A_km = -face coefficient, closed cells the row dmax e_k), in
-  // the library's operation order: per pivot k, r = 1/a_kk, row k scaled by r, every
-  // other row a_ij = fma(-a_ik, row_k[j], a_ij) with a_ik taken as 0. A pivot <= 1e-6
-  // dmax (singular: a sealed gas pocket) leaves cinv_ok false. Levels over 239 cells
-  // are not inverted (the library's shared-memory bound).
+  // Inverse of the coarsest operator in the library's operation order: A's lower
+  // band (half-bandwidth nx, row-major cells; closed cells the row dmax e_k);
+  // right-looking banded Cholesky (per column jc: L_jcjc = sqrt(a_jcjc), L_ijc =
+  // a_ijc / L_jcjc, then a_ik = fma(-L_ijc, L_kjc, a_ik) for jc < k <= i <= jc+nx);
+  // then column c of the inverse by forward and back substitution with the
+  // reciprocal diagonal, k ascending. A pivot <= 1e-6 dmax (singular: a sealed gas
+  // pocket) or a level wider than 32 cells leaves cinv_ok false.
   void coarse_factor() {
     const Level& L = lv.back();
-    const int n = L.nx * L.ny;
+    const int n = L.nx * L.ny, bw = L.nx, W = bw + 1;
     cinv_ok = false;
-    if (n > 239) return;
-    std::vector<R> a((size_t)n * n, R(0)), dg(n), fcol(n), rowk(n);
+    if (n > 256 || bw > 32) return;
+    std::vector<R> band((size_t)n * W, R(0)), dg(n), rinv(n);
     for (int k = 0; k < n; k++) {
       const int i = k % L.nx, j = k / L.nx;
       const R w = L.ax[j * (L.nx + 1) + i], e = L.ax[j * (L.nx + 1) + i + 1];
@@ -782,11 +783,9 @@ struct Sim {
       if (j < L.ny - 1) diag += no; else diag += R(2) * no;
       dg[k] = diag;
       if (diag > R(0)) {
-        a[(size_t)k * n + k] = diag;
-        if (i > 0) a[(size_t)k * n + k - 1] = -w;
-        if (i < L.nx - 1) a[(size_t)k * n + k + 1] = -e;
-        if (j > 0) a[(size_t)k * n + k - L.nx] = -so;
-        if (j < L.ny - 1) a[(size_t)k * n + k + L.nx] = -no;
+        band[(size_t)k * W] = diag;
+        if (i > 0) band[(size_t)k * W + 1] = -w;
+        if (j > 0) band[(size_t)k * W + bw] = -so;
       }
     }
     R dmax = R(0);
@@ -794,20 +793,44 @@ struct Sim {
     if (!(dmax > R(0))) return;
     const R thr = R(1e-6f) * dmax;
     for (int k = 0; k < n; k++)
-      if (!(dg[k] > R(0))) a[(size_t)k * n + k] = dmax;
-    for (int k = 0; k < n; k++) {
-      const R p = a[(size_t)k * n + k];
-      if (!(p > thr)) return;
-      const R r = R(1) / p;
-      for (int t = 0; t < n; t++) {
-        fcol[t] = a[(size_t)t * n + k];
-        rowk[t] = (t == k ? R(1) : a[(size_t)k * n + t]) * r;
+      if (!(dg[k] > R(0))) band[(size_t)k * W] = dmax;
+    auto B = [&](int i, int d) -> R& { return band[(size_t)i * W + d]; };
+    std::vector<R> lij(bw);
+    for (int jc = 0; jc < n; jc++) {
+      const R piv = B(jc, 0);
+      if (!(piv > thr)) return;
+      const R ljj = std::sqrt(piv);
+      for (int l = 0; l < bw; l++) {
+        const int i = jc + 1 + l;
+        if (i < n) lij[l] = B(i, i - jc) / ljj;
       }
-      for (int i = 0; i < n; i++)
-        for (int j = 0; j < n; j++) {
-          R& x = a[(size_t)i * n + j];
-          x = i == k ? rowk[j] : std::fma(-fcol[i], rowk[j], j == k ? R(0) : x);
-        }
+      B(jc, 0) = ljj;
+      for (int l = 0; l < bw; l++) {
+        const int i = jc + 1 + l;
+        if (i < n) B(i, i - jc) = lij[l];
+      }
+      for (int l = 0; l < bw; l++) {
+        const int i = jc + 1 + l;
+        if (i >= n) continue;
+        for (int k = jc + 1; k <= i; k++) B(i, i - k) = std::fma(-lij[l], B(k, k - jc), B(i, i - k));
+      }
+    }
+    for (int k = 0; k < n; k++) rinv[k] = R(1) / B(k, 0);
+    std::vector<R> a((size_t)n * n), y(n);
+    for (int c = 0; c < n; c++) {
+      for (int i = 0; i < c; i++) y[i] = R(0);
+      for (int i = c; i < n; i++) {
+        R sum = i == c ? R(1) : R(0);
+        for (int k = std::max(c, i - bw); k < i; k++) sum = std::fma(-B(i, i - k), y[k], sum);
+        y[i] = sum * rinv[i];
+      }
+      for (int i = n - 1; i >= 0; i--) {
+        R sum = y[i];
+        const int kend = std::min(n - 1, i + bw);
+        for (int k = i + 1; k <= kend; k++) sum = std::fma(-B(k, k - i), y[k], sum);
+        y[i] = sum * rinv[i];
+      }
+      for (int i = 0; i < n; i++) a[(size_t)i * n + c] = y[i];
     }
     cinv = std::move(a);
     cinv_ok = true;
