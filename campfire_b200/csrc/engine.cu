@@ -347,6 +347,8 @@ int Engine::upload_ctl() {
   c.nscenes = en; c.nactive = en; c.any_active = 1; c.scenes_done = 0;
   c.iter = 0; c.hard_cap = std::max(ncycles_, max_cycles_) + 1;
   c.coarse_direct = (mode_ != CFG_SOLVE_FIXED && coarse_direct_) ? 1 : 0;
+  c.use_cond = ctl_use_cond_ == 1 ? 1 : 0;
+  c.cond = cond_handle_;
   *h_ctl_pinned_ = c;
   CFG_CUDA(cudaMemcpyAsync(d_ctl_, h_ctl_pinned_, sizeof(SolveCtl), cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaStreamSynchronize(st()));
@@ -670,6 +672,15 @@ void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_con
   (void)h; (void)use_cond;
 }
 
+// The loop decision sets the graph's WHILE condition only while steps run as that
+// graph; every launch outside it (host loop, stages, timing) runs with use_cond = 0.
+int Engine::set_cond_mode(bool graph) {
+  const int want = graph ? 1 : 0;
+  if (ctl_use_cond_ == want) return CFG_OK;
+  ctl_use_cond_ = want;
+  return upload_ctl();
+}
+
 int Engine::set_coarse_solve(int direct) {
   if (direct != 0 && direct != 1) return fail(CFG_ERR_INVAL, "coarse solve must be 0 (sweeps) or 1 (direct)");
   CFG_TRY(activate());
@@ -687,14 +698,15 @@ int Engine::max_lc() const {
 // The step's V(2,2) cycle with the fused kernels (k_mgf.cu); the level-0 up
 // kernel (or the coarse block of scenes whose block starts at level 0) ends
 // the cycle with the residual norm (FP32 modes) or p64 += p (FP64 mode).
-void Engine::enqueue_vcycle(cudaStream_t s, int tail) {
+void Engine::enqueue_vcycle(cudaStream_t s, int tail, int count_iter) {
   const int LD = max_lc();
   for (int l = 0; l < LD; l++) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
-    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, s);
+    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, count_iter, s);
+    count_iter = 0;
     vcycle_launches_++;
   }
-  launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, coarse_smem_, s);
+  launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, count_iter, coarse_smem_, s);
   vcycle_launches_++;
   for (int l = LD - 1; l >= 0; l--) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
@@ -766,7 +778,7 @@ int Engine::host_pressure_loop() {
   CFG_CUDA(cudaStreamSynchronize(s));
   int any = any_fp64() ? h_ctl_pinned_->any_active : 1;
   while (any) {
-    enqueue_vcycle(s, any_fp64() ? 2 : 1);
+    enqueue_vcycle(s, any_fp64() ? 2 : 1, 0);
     enqueue_cycle_tail(s, 0ull, 0);
     CFG_CUDA(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s));
     CFG_CUDA(cudaStreamSynchronize(s));
@@ -819,8 +831,13 @@ int Engine::ensure_graph() {
   e = cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamBeginCaptureToGraph");
   vcycle_launches_ = 0;
-  enqueue_vcycle(body_stream_, any_fp64() ? 2 : 1);
-  enqueue_cycle_tail(body_stream_, (unsigned long long)h, 1);
+  // the first kernel of the body counts the iteration and the cycle's decision sets the
+  // condition (loop_count / loop_decide): no guard kernel in the body
+  enqueue_vcycle(body_stream_, any_fp64() ? 2 : 1, 1);
+  if (any_fp64()) {
+    launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, body_stream_);
+    vcycle_launches_++;
+  }
   e = cudaStreamEndCapture(body_stream_, &body);
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamEndCapture(body)");
   enqueue_post_solve(s);
@@ -829,6 +846,8 @@ int Engine::ensure_graph() {
   graph_ = g;
   e = cudaGraphInstantiate(&exec_, graph_, 0);
   if (e != cudaSuccess) { destroy_graph(); return cuda_fail(e, "cudaGraphInstantiate"); }
+  cond_handle_ = (unsigned long long)h;
+  ctl_use_cond_ = -1;   // upload the new handle before the next launch
   graph_dirty_ = false;
   graph_sub_ = max_sub();
   return CFG_OK;
@@ -847,8 +866,10 @@ int Engine::step(int nsteps) {
         graph_dirty_ = true;
         CFG_TRY(ensure_graph());
       }
+      CFG_TRY(set_cond_mode(true));
       CFG_CUDA(cudaGraphLaunch(exec_, st()));
     } else {
+      CFG_TRY(set_cond_mode(false));
       launches_ = 0; vcycle_launches_ = 0;
       enqueue_pre_solve(st(), 0ull, 0);
       CFG_CUDA(cudaGetLastError());
@@ -906,6 +927,8 @@ int Engine::step_profiled(float* ms) {
   for (int l = FR_KMAX; l + 1 < max_levels(); l++)
     launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   CFG_CUDA(cudaEventRecord(ev[5], s));
+  CFG_TRY(set_cond_mode(false));
+  if (direct_coarse()) launch_coarse_factor(d_scenes_, nscenes(), s);
   CFG_TRY(host_pressure_loop());
   CFG_CUDA(cudaEventRecord(ev[6], s));
   enqueue_post_solve(s);
@@ -933,6 +956,7 @@ int Engine::run_stage(const char* stage) {
     for (int l = FR_KMAX; l + 1 < max_levels(); l++)
       launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   } else if (st_ == "pressure") {
+    CFG_TRY(set_cond_mode(false));
     if (direct_coarse()) launch_coarse_factor(d_scenes_, nscenes(), s);
     enqueue_bnorm(s);
     CFG_TRY(host_pressure_loop());
@@ -980,20 +1004,20 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     go = [&](int) { launch_coarsest(d_scenes_, nscenes(), s); };
     b = 0; cnt = cyc;
   } else if (n == "mg_down0") {
-    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, s); };
+    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, 0, s); };
     b = (4 * 16 + 18) * cells; cnt = cyc;   // 4 colour passes + residual restriction
   } else if (n == "mg_up0") {
     go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 0, d_ctl_, s); };
     b = (17 + 4 * 16) * cells; cnt = cyc;   // prolongation + 4 colour passes
   } else if (n == "mg_coarse") {
-    go = [&](int) { launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, coarse_smem_, s); };
+    go = [&](int) { launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, 0, coarse_smem_, s); };
     // the reference schedule's V-cycle bytes of the levels the block covers (163 B per level cell)
     b = 0;
     for (int l = sc.lc; l < sc.nlev; l++) b += 163.0 * sc.lnx[l] * sc.lny[l];
     cnt = cyc;
   } else if (n == "vcycle") {
     // one fused V(2,2) cycle without its tail (the smoother schedule's cost)
-    go = [&](int) { enqueue_vcycle(s, 0); };
+    go = [&](int) { enqueue_vcycle(s, 0, 0); };
     b = 0;
     for (int l = 0; l + 1 < sc.nlev; l++) b += 163.0 * sc.lnx[l] * sc.lny[l];
     cnt = cyc;
@@ -1007,6 +1031,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     go = [&](int) { launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s); };
     b = 32 * cells;
   } else return fail(CFG_ERR_NOENT, "unknown kernel " + n);
+  CFG_TRY(set_cond_mode(false));
   launch_bnorm(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, false, s);   // arm the multigrid kernels
   cudaEvent_t e0, e1;
   CFG_CUDA(cudaEventCreate(&e0));
@@ -1028,6 +1053,7 @@ int Engine::vcycle_once(int nu) {
   if (nu != 2) return fail(CFG_ERR_INVAL, "only V(2,2) cycles are provided (js/fluid.js:294 default nu = 2)");
   CFG_TRY(activate());
   cudaStream_t s = st();
+  CFG_TRY(set_cond_mode(false));
   enqueue_bnorm(s);   // arms every scene (active = 1)
   enqueue_vcycle_ref(s);
   CFG_CUDA(cudaGetLastError());

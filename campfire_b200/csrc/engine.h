@@ -150,7 +150,8 @@ class Engine {
 
   // step pieces; launches counted in launches_
   void enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_cond);
-  void enqueue_vcycle(cudaStream_t s, int tail);   // fused kernels (the step's cycle); tail as k_mg_up
+  // fused kernels (the step's cycle); tail as k_mg_up; count_iter: the first kernel opens a graph iteration
+  void enqueue_vcycle(cudaStream_t s, int tail, int count_iter);
   void enqueue_vcycle_ref(cudaStream_t s);   // one kernel per reference dispatch (cfg_vcycle)
   int max_lc() const;
   bool direct_coarse() const { return mode_ != CFG_SOLVE_FIXED && coarse_direct_ != 0; }
@@ -183,6 +184,9 @@ class Engine {
   size_t coarse_smem_ = 0;
   int coarse_cells_ = COARSE_CELLS;
   int coarse_direct_ = 0;
+  unsigned long long cond_handle_ = 0;   // the step graph's WHILE-node handle
+  int ctl_use_cond_ = 0;                 // SolveCtl::use_cond on the device (-1: stale)
+  int set_cond_mode(bool graph);
 };
 
 }  // namespace cfg

@@ -84,6 +84,9 @@ struct SolveCtl {
   int hard_cap;               // the loop stops after this many cycles whatever any_active says
   int err;                    // set by a kernel whose bounded wait ran out (reported as CFG_ERR_TIMEDOUT)
   int coarse_direct;          // TOL/FP64 modes: solve the coarsest level with its inverse instead of 120 sweeps
+  int use_cond;               // 1 while the step runs as a graph: the loop decision sets the WHILE node's condition
+  int pad2;
+  unsigned long long cond;    // that node's cudaGraphConditionalHandle
 };
 
 // One tile of a work list
@@ -100,6 +103,21 @@ __host__ __device__ inline int round_up(int x, int m) { return (x + m - 1) / m *
 // successor begin launching. Both are no-ops for an ordinary launch.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Pressure loop as a graph WHILE node: the first kernel of each iteration counts it
+// (one thread; at the hard cap the loop ends after this iteration even if no
+// decision is ever recorded), and the last scene's decision of the iteration sets
+// the node's condition. Outside a graph (use_cond = 0) the host reads any_active.
+__device__ __forceinline__ void loop_count(SolveCtl* ctl) {
+  const int it = ctl->iter + 1;
+  ctl->iter = it;
+  if (it >= ctl->hard_cap && ctl->use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond, 0u);
+}
+__device__ __forceinline__ void loop_decide(SolveCtl* ctl, int nactive) {
+  const int go = (nactive > 0 && ctl->iter < ctl->hard_cap) ? 1 : 0;
+  ctl->any_active = go;
+  if (ctl->use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond, (unsigned)go);
+}
 
 
 // ------------------------------------------------------------- common.wgsl

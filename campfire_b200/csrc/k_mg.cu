@@ -43,8 +43,8 @@ __device__ __forceinline__ float residual(const LevelDesc& L, int i, int j) {
 __device__ __forceinline__ bool scene_live(const SceneDesc& S) { return S.enabled && S.solve->active; }
 
 // Per-scene loop decision after a norm reduction (thread 0 of the finishing CTA);
-// the last scene of this round records whether any scene cycles again. The
-// graph's loop condition itself is set by k_loop_guard, which always runs.
+// the last scene of this round records whether any scene cycles again and, in a
+// graph, sets the loop's condition (loop_decide).
 __device__ void solve_decide(const SceneDesc* scenes, int nscenes, const SceneDesc& S, SolveCtl* ctl, double r2,
                              bool count_cycle) {
   SolveState* ss = S.solve;
@@ -66,14 +66,14 @@ __device__ void solve_decide(const SceneDesc* scenes, int nscenes, const SceneDe
       if (scenes[s].enabled && *((volatile int*)&scenes[s].solve->active)) na++;
     ctl->scenes_done = 0u;
     ctl->nactive = na;
-    ctl->any_active = na > 0 ? 1 : 0;
+    loop_decide(ctl, na);
   }
 }
 
 }  // namespace
 
-// Last node of each loop iteration: count the cycle and set the WHILE node's
-// condition. The count bounds the loop even if a decision were never recorded.
+// Last kernel of each iteration of the host-driven loop (launches outside a graph):
+// count the cycle and fold in the hard cap.
 __global__ void k_loop_guard(SolveCtl* ctl, unsigned long long h, int use_cond) {
   pdl_wait();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;

@@ -124,7 +124,7 @@ __device__ __forceinline__ bool scene_live(const SceneDesc& S) { return S.enable
 // ------------------------------------------------------------------ down: 4 passes + restrict
 template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work, int level,
-                                                 SolveCtl* ctl) {
+                                                 SolveCtl* ctl, int count_iter) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
   __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
   __shared__ __align__(128) float srhs[MGF_BH * MGF_BW];
@@ -139,6 +139,7 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
   const int x0 = w.tx * TX, y0 = w.ty * TY;
   const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
   pdl_wait();
+  if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!scene_live(S)) return;
   if (!stage_tile(S, level, TM_P, t, nullptr, 0, 0, &bar, ctl)) return;
   #pragma unroll 1
@@ -195,7 +196,7 @@ __device__ void solve_decide_f(const SceneDesc* scenes, int nscenes, const Scene
       if (scenes[s].enabled && *((volatile int*)&scenes[s].solve->active)) na++;
     ctl->scenes_done = 0u;
     ctl->nactive = na;
-    ctl->any_active = na > 0 ? 1 : 0;
+    loop_decide(ctl, na);
   }
 }
 }  // namespace
@@ -357,7 +358,8 @@ __device__ __forceinline__ void coarsest_update(float* p, int pc, const CCell& c
 }
 }  // namespace
 
-__global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __restrict__ scenes, int nscenes, SolveCtl* ctl, int tail) {
+__global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __restrict__ scenes, int nscenes, SolveCtl* ctl, int tail,
+                                                         int count_iter) {
   extern __shared__ __align__(128) float smem[];
   __shared__ double red[32];
   __shared__ LvS lv[MAX_LEVELS];
@@ -383,6 +385,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   }
   __syncthreads();
   pdl_wait();
+  if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!scene_live(S)) return;
   const LvS V0 = lv[lc];
   float* sres = lv[nl - 1].ay + (lv[nl - 1].ny + 1) * lv[nl - 1].pc;   // residual scratch (level lc size)
@@ -642,9 +645,11 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
   return f * 4;
 }
 
-void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, cudaStream_t st) {
+void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, int count_iter,
+                    cudaStream_t st) {
   if (ntiles > 0)
-    launch_pdl(pdl_enabled(), k_mg_down<MGF_TX, MGF_TY>, dim3(ntiles), dim3(256), 0, st, scenes, work, level, ctl);
+    launch_pdl(pdl_enabled(), k_mg_down<MGF_TX, MGF_TY>, dim3(ntiles), dim3(256), 0, st, scenes, work, level, ctl,
+               count_iter);
 }
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {
@@ -652,8 +657,11 @@ void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int nt
     launch_pdl(pdl_enabled(), k_mg_up<MGF_TX, MGF_TY>, dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, tail,
                ctl);
 }
-void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, size_t smem, cudaStream_t st) {
-  if (nscenes > 0) launch_pdl(pdl_enabled(), k_mg_coarse, dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail);
+void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
+                      cudaStream_t st) {
+  if (nscenes > 0)
+    launch_pdl(pdl_enabled(), k_mg_coarse, dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail,
+               count_iter);
 }
 void launch_coarse_factor(const SceneDesc* scenes, int nscenes, cudaStream_t st) {
   if (nscenes > 0) k_coarse_factor<<<nscenes, CF_THREADS, 0, st>>>(scenes);

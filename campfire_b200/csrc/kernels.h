@@ -80,10 +80,13 @@ void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_co
 // fused V(2,2) cycle: per fine level a down kernel (4 passes + restriction) and an
 // up kernel (prolongation + 4 passes; level 0 tail: 1 residual norm + decision,
 // 2 p64 += p), and one CTA per scene for levels lc..coarsest
-void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, cudaStream_t st);
+// count_iter: the kernel opens a graph loop iteration (loop_count)
+void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, int count_iter,
+                    cudaStream_t st);
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st);
-void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, size_t smem, cudaStream_t st);
+void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
+                      cudaStream_t st);
 size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);
 cudaError_t prepare_mg_coarse(size_t smem);
 // direct coarse solve: the inverse of each scene's coarsest operator (scenes whose
