@@ -221,6 +221,47 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
             "batched_over_plain": batched / plain}
 
 
+def field_errors(g, ref):
+    """max|gpu - ref| / max|ref| of T, u (U and V faces), Y_F and Y_S."""
+    import numpy as np
+    out = {}
+    for name, get in (("T", lambda s, r: (s("T"),)), ("u", lambda s, r: (s("U"), s("V"))),
+                      ("Y_F", lambda s, r: (s("Y").reshape(-1, 4)[:, 0],)),
+                      ("Y_S", lambda s, r: (s("Y").reshape(-1, 4)[:, 3],))):
+        a = np.concatenate([np.asarray(x, np.float64).ravel() for x in get(g.readBuffer, None)])
+        b = np.concatenate([np.asarray(x, np.float64).ravel() for x in get(ref.read, None)])
+        scale = float(np.max(np.abs(b))) or 1.0
+        out[name] = float(np.max(np.abs(a - b))) / scale
+    return out
+
+
+def run_fp64_error(dev, workload: str, steps: int, every: int, threads: int):
+    """The GPU step (FP32, FP64 defect correction) and the FP64 oracle (the same algorithm in
+    double precision) from the same scene, side by side; errors every `every` steps."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    from oracle import oracle
+    nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
+    sc = cb.generate_scene(kind, nx, ny, 0.8, seed)
+    g = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(g, sc)
+    g.set_solver(mode, 1, tol, maxc)
+    g.set_coarse_solve(True)
+    o = oracle.OracleSim(nx, ny, 0.8, sc["dt"], fp64=True)
+    load_scene(o, sc)
+    o.set_solver(mode, 1, tol, maxc)
+    rows = []
+    for k in range(1, steps + 1):
+        g.step(1)
+        o.step(1)
+        if k % every == 0 or k == 1:
+            rows.append(dict(step=k, **field_errors(g, o)))
+    g.close()
+    return {"workload": workload, "steps": steps, "every": every, "errors": rows,
+            "metric": "max|gpu - fp64 oracle| / max|fp64 oracle| per field"}
+
+
 SERVE_CLASSES = ((96, 144), (128, 192), (192, 288), (256, 384), (512, 768))
 
 
@@ -308,6 +349,10 @@ def main():
     ap.add_argument("--served-steps", type=int, nargs=2, default=(20, 200), metavar=("LO", "HI"),
                     help="steps per served job, uniform in [LO, HI]")
     ap.add_argument("--served-rates", type=float, nargs="+", default=(10.0, 100.0, 1000.0))
+    ap.add_argument("--fp64-error-every", type=int, default=0,
+                    help="with --fp64-error-steps S: run the workload beside the FP64 oracle for S steps and "
+                         "report the field errors every this many steps (0: skip)")
+    ap.add_argument("--fp64-error-steps", type=int, default=2000)
     ap.add_argument("--launch", default="graph", choices=["graph", "stream"],
                     help="graph: one CUDA graph per step (pressure loop as a device-side WHILE node); "
                          "stream: kernel by kernel, the host polling the loop decision (for profilers that "
@@ -451,6 +496,10 @@ def main():
     if a.batched_steps > 0:
         batched = run_batched(dev, stream, flush, a.batched_steps, 3, 1e-10, 300, 3)
 
+    fp64_error = None
+    if a.fp64_error_every > 0 and rank == 0:
+        fp64_error = run_fp64_error(dev, a.workload, a.fp64_error_steps, a.fp64_error_every, cpu_threads())
+
     served = None
     if a.served_jobs > 0:
         served = run_served(dev, stream, a.served_rates, a.served_jobs, a.served_steps[0], a.served_steps[1],
@@ -475,7 +524,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 204 + 16,
                         "d2h_bytes_per_step": 528 * 4 + 320 * 16 + 256 * 4},
                 "gpu_launches": launches * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "batched": batched, "served": served}
+                "batched": batched, "served": served, "fp64_oracle_error": fp64_error}
         print(json.dumps(line))
     sim.close()
     if world > 1:

@@ -114,6 +114,7 @@ def lib():
         "cfg_set_coarse_cells": [vp, ci], "cfg_batch_set_coarse_cells": [vp, ci],
         "cfg_autotune": [ci, ci, ip, ip, ci, ci, ip, ip, dp, ip],
         "cfg_set_coarse_solve": [vp, ci], "cfg_batch_set_coarse_solve": [vp, ci],
+        "cfg_checkpoint_save": [vp, cs], "cfg_checkpoint_load": [vp, cs],
         "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
         "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci],
         "cfg_server_slot_bytes": [vp, ci, ctypes.POINTER(sz)],

@@ -261,3 +261,12 @@ extern "C" int cfg_batch_set_coarse_solve(cfg_batch* b, int direct) {
   if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
   return guarded([&] { return b->eng->set_coarse_solve(direct); });
 }
+
+extern "C" int cfg_checkpoint_save(cfg_sim* sim, const char* path) {
+  SIM_OK(sim);
+  return guarded([&] { return sim->eng->checkpoint_save(sim->scene, path); });
+}
+extern "C" int cfg_checkpoint_load(cfg_sim* sim, const char* path) {
+  SIM_OK(sim);
+  return guarded([&] { return sim->eng->checkpoint_load(sim->scene, path); });
+}

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -265,8 +266,150 @@ int Engine::alloc_scene(Scene& sc) {
   CFG_CUDA(cudaMemset(arena, 0, total));
   sc.arena = arena; sc.arena_bytes = total;
   size_t off = 0;
-  for (auto& it : items) { *it.ptr = (char*)arena + off; off += (it.bytes + 255) / 256 * 256; }
+  sc.items.clear();
+  for (auto& it : items) {
+    *it.ptr = (char*)arena + off;
+    off += (it.bytes + 255) / 256 * 256;
+    const bool scratch = it.ptr == (void**)&d.tmap || it.ptr == (void**)&d.part || it.ptr == (void**)&d.cinv;
+    sc.items.push_back({*it.ptr, it.bytes, !scratch});
+  }
   return build_tmaps(sc);
+}
+
+// ------------------------------------------------------------------ checkpoints
+// File: "CFGCKPT1", u32 version 1, nx, ny, nlev, nitems; f64 time, dt, dt_cap, cfl,
+// width; u32 frame, nray; the host params (cfg_params); the host pieces
+// (64 x 20 f32); the device's parameter block (the uniform and step controls,
+// which the CFL step updates on the device); the scene's SolveState; then per
+// state array of the arena (allocation order, pitched as allocated) u64 bytes +
+// the bytes; last u64 FNV-1a of everything after the magic.
+namespace {
+constexpr char kCkptMagic[8] = {'C', 'F', 'G', 'C', 'K', 'P', 'T', '1'};
+struct CkptHead {
+  uint32_t version, nx, ny, nlev, nitems, frame, nray, pad;
+  double time, dt, dt_cap, cfl, width;
+};
+struct Fnv64 {
+  uint64_t h = 1469598103934665603ull;
+  void add(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ull; }
+  }
+};
+struct File {
+  FILE* f = nullptr;
+  ~File() { if (f) std::fclose(f); }
+};
+}  // namespace
+
+int Engine::checkpoint_save(int s, const char* path) {
+  if (!path) return fail(CFG_ERR_INVAL, "null path");
+  CFG_TRY(activate());
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  const Scene& sc = scenes_[s];
+  int nstate = 0;
+  for (auto& it : sc.items) nstate += it.state ? 1 : 0;
+  CkptHead h{1u, (uint32_t)sc.nx, (uint32_t)sc.ny, (uint32_t)sc.nlev, (uint32_t)nstate, sc.frame, (uint32_t)sc.nray, 0u,
+             sc.time, sc.dtd, sc.dt_cap, sc.cfl, sc.width};
+  std::vector<char> dparams(kDescParamBytes);
+  SolveState ss{};
+  CFG_CUDA(cudaMemcpy(dparams.data(), d_scenes_ + s, kDescParamBytes, cudaMemcpyDeviceToHost));
+  CFG_CUDA(cudaMemcpy(&ss, sc.desc.solve, sizeof ss, cudaMemcpyDeviceToHost));
+  File out;
+  out.f = std::fopen(path, "wb");
+  if (!out.f) return fail(CFG_ERR_IO, std::string("cannot write ") + path);
+  Fnv64 sum;
+  auto put = [&](const void* p, size_t n) {
+    sum.add(p, n);
+    return std::fwrite(p, 1, n, out.f) == n;
+  };
+  bool ok = std::fwrite(kCkptMagic, 1, 8, out.f) == 8;
+  ok = ok && put(&h, sizeof h) && put(&sc.host, sizeof sc.host) && put(sc.pieces, sizeof sc.pieces) &&
+       put(dparams.data(), dparams.size()) && put(&ss, sizeof ss);
+  std::vector<char> buf;
+  for (auto& it : sc.items) {
+    if (!ok) break;
+    if (!it.state) continue;
+    buf.resize(it.bytes);
+    CFG_CUDA(cudaMemcpy(buf.data(), it.ptr, it.bytes, cudaMemcpyDeviceToHost));
+    const uint64_t n = it.bytes;
+    ok = put(&n, 8) && put(buf.data(), it.bytes);
+  }
+  const uint64_t digest = sum.h;
+  ok = ok && std::fwrite(&digest, 1, 8, out.f) == 8;
+  if (!ok) return fail(CFG_ERR_IO, std::string("short write to ") + path);
+  return CFG_OK;
+}
+
+int Engine::checkpoint_load(int s, const char* path) {
+  if (!path) return fail(CFG_ERR_INVAL, "null path");
+  CFG_TRY(activate());
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  Scene& sc = scenes_[s];
+  File in;
+  in.f = std::fopen(path, "rb");
+  if (!in.f) return fail(CFG_ERR_NOENT, std::string("cannot read ") + path);
+  Fnv64 sum;
+  auto get = [&](void* p, size_t n) {
+    if (std::fread(p, 1, n, in.f) != n) return false;
+    sum.add(p, n);
+    return true;
+  };
+  char magic[8];
+  if (std::fread(magic, 1, 8, in.f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0)
+    return fail(CFG_ERR_INVAL, std::string(path) + " is not a gas-step checkpoint");
+  CkptHead h;
+  cfg_params host;
+  float pieces[MAX_PIECES * PIECE_FLOATS];
+  std::vector<char> dparams(kDescParamBytes);
+  SolveState ss;
+  if (!get(&h, sizeof h) || !get(&host, sizeof host) || !get(pieces, sizeof pieces) ||
+      !get(dparams.data(), dparams.size()) || !get(&ss, sizeof ss))
+    return fail(CFG_ERR_IO, std::string("truncated checkpoint ") + path);
+  int nstate = 0;
+  for (auto& it : sc.items) nstate += it.state ? 1 : 0;
+  if (h.version != 1u) return fail(CFG_ERR_INVAL, "unsupported checkpoint version");
+  if ((int)h.nx != sc.nx || (int)h.ny != sc.ny || (int)h.nlev != sc.nlev || (int)h.nitems != nstate)
+    return fail(CFG_ERR_RANGE, "checkpoint grid " + std::to_string(h.nx) + "x" + std::to_string(h.ny) +
+                                   " does not match this scene");
+  // read every array before touching the scene, so a bad file leaves it unchanged
+  std::vector<std::vector<char>> arrays;
+  for (auto& it : sc.items) {
+    if (!it.state) continue;
+    uint64_t n = 0;
+    if (!get(&n, 8) || n != it.bytes) return fail(CFG_ERR_INVAL, "checkpoint array sizes do not match this scene");
+    arrays.emplace_back(it.bytes);
+    if (!get(arrays.back().data(), it.bytes)) return fail(CFG_ERR_IO, std::string("truncated checkpoint ") + path);
+  }
+  uint64_t digest = 0;
+  const uint64_t expect = sum.h;
+  if (std::fread(&digest, 1, 8, in.f) != 8 || digest != expect)
+    return fail(CFG_ERR_INVAL, std::string("checkpoint checksum mismatch in ") + path);
+  size_t k = 0;
+  for (auto& it : sc.items) {
+    if (!it.state) continue;
+    CFG_CUDA(cudaMemcpy(it.ptr, arrays[k].data(), it.bytes, cudaMemcpyHostToDevice));
+    k++;
+  }
+  sc.host = host;
+  std::memcpy(sc.pieces, pieces, sizeof pieces);
+  sc.time = h.time; sc.dtd = h.dt; sc.dt_cap = h.dt_cap; sc.cfl = h.cfl; sc.frame = h.frame; sc.nray = (int)h.nray;
+  const double cfl = sc.cfl;
+  sc.cfl = 0;   // write_params must not read the device's step back: it is restored below
+  CFG_TRY(write_params(s));
+  sc.cfl = cfl;
+  // the device's parameter block as saved (CFL step included); this slot's enabled flag kept
+  SceneDesc tmp = sc.desc;
+  std::memcpy(&tmp, dparams.data(), kDescParamBytes);
+  tmp.enabled = sc.enabled ? 1 : 0;
+  std::memcpy(&sc.desc, &tmp, kDescParamBytes);
+  sc.P = sc.desc.P;
+  sc.diff_sub = sc.desc.diff_sub;
+  sc.diff_dt = sc.desc.diff_dt;
+  CFG_CUDA(cudaMemcpy(d_scenes_ + s, &sc.desc, kDescParamBytes, cudaMemcpyHostToDevice));
+  CFG_CUDA(cudaMemcpy(sc.desc.solve, &ss, sizeof ss, cudaMemcpyHostToDevice));
+  graph_dirty_ = true;
+  return CFG_OK;
 }
 
 int Engine::build_worklists() {

@@ -65,6 +65,10 @@ struct Scene {
   size_t arena_bytes = 0;
   SceneDesc desc{};              // host mirror of the device descriptor
   bool enabled = true;
+  // the arena's arrays in allocation order; `state`: part of a checkpoint (not the
+  // tensor maps, which hold this arena's addresses, nor per-step scratch)
+  struct Item { void* ptr; size_t bytes; bool state; };
+  std::vector<Item> items;
 };
 
 // Bytes of SceneDesc that cfg_write_params uploads: the uniform and the step
@@ -104,6 +108,9 @@ class Engine {
   int pressure_residual(int s, double* rel);
   int budgets(int s, double* out);
   int set_active(int s, bool on);
+  // the scene's state to / from a file (same grid size on load)
+  int checkpoint_save(int s, const char* path);
+  int checkpoint_load(int s, const char* path);
 
   // whole-batch operations
   int set_solver(int mode, int ncycles, double tol, int max_cycles);

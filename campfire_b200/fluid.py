@@ -21,6 +21,7 @@ work on the handle's stream in call order. Extensions beyond the reference
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Optional
 
 import numpy as np
@@ -141,6 +142,16 @@ class _SceneOps:
         v = ctypes.c_double()
         check(_lib.lib().cfg_pressure_residual(self._h, ctypes.byref(v)))
         return v.value
+
+    def save_checkpoint(self, path: str):
+        """The scene's state to a file (cfg_checkpoint_save)."""
+        check(_lib.lib().cfg_checkpoint_save(self._h, os.fsencode(path)))
+
+    def load_checkpoint(self, path: str):
+        """Resume from a checkpoint of a scene of the same grid size (cfg_checkpoint_load)."""
+        check(_lib.lib().cfg_checkpoint_load(self._h, os.fsencode(path)))
+        inf = self.info()
+        self.time, self.frame = inf["time"], inf["frame"]
 
     def budgets(self) -> np.ndarray:
         o = np.zeros(8, np.float64)

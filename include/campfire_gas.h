@@ -202,6 +202,15 @@ int cfg_batch_set_coarse_solve(cfg_batch* b, int direct);
 int cfg_autotune(int device, int nscenes, const int* nx, const int* ny, int coarse_direct, int iters,
                  int* best_cells, int* cand_cells, double* cand_ms, int* ncand);
 
+/* Checkpoint / resume of one scene (no counterpart in the reference, which only resets,
+ * js/fluid.js:162-176): every state array of the scene (fields, advected copies, sources,
+ * geometry, pressure levels, FP64 pressure, accumulators, pieces), its host clock, dt and
+ * parameters, the device's parameter block (the CFL step) and its solve state, with an
+ * FNV-1a checksum. Loading needs a scene of the same grid size (batch views included);
+ * a step after loading continues bit for bit as the saved scene would have. */
+int cfg_checkpoint_save(cfg_sim* sim, const char* path);
+int cfg_checkpoint_load(cfg_sim* sim, const char* path);
+
 /* Synthetic scenes for the benchmark workloads (seeded, deterministic).
  * kind 0: three square logs of half 0.025 at (0.35,0.025) (0.45,0.025) (0.40,0.068),
  *         flux 5e-3 kg/m2/s at 600 K;  kind 1: five logs of half 0.05 in a seeded tepee,
