@@ -116,7 +116,8 @@ def lib():
         "cfg_set_coarse_solve": [vp, ci], "cfg_batch_set_coarse_solve": [vp, ci],
         "cfg_checkpoint_save": [vp, cs], "cfg_checkpoint_load": [vp, cs],
         "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
-        "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci],
+        "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci, ci],
+        "cfg_set_krylov": [vp, ci], "cfg_batch_set_krylov": [vp, ci],
         "cfg_server_slot_bytes": [vp, ci, ctypes.POINTER(sz)],
         "cfg_server_run": [vp, ctypes.POINTER(CfgJob), ci, ctypes.POINTER(CfgJobResult), dp, dp],
     }

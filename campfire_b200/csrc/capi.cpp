@@ -270,3 +270,12 @@ extern "C" int cfg_checkpoint_load(cfg_sim* sim, const char* path) {
   SIM_OK(sim);
   return guarded([&] { return sim->eng->checkpoint_load(sim->scene, path); });
 }
+
+extern "C" int cfg_set_krylov(cfg_sim* sim, int on) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->set_krylov(on); });
+}
+extern "C" int cfg_batch_set_krylov(cfg_batch* b, int on) {
+  if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
+  return guarded([&] { return b->eng->set_krylov(on); });
+}

@@ -240,7 +240,9 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.acc, ACC_LEN * 4}, {(void**)&d.faceW, MAX_PIECES * 4 * 4},
     {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4}, {(void**)&d.rad, RAD_LEN * 16},
     {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
-    {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 8},
+    {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 16},
+    {(void**)&d.r64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.dA, (size_t)sc.nx * sc.ny * 8},
+    {(void**)&d.dB, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.q64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.tmap, (size_t)MAX_LEVELS * TM_PER_LEVEL * TMAP_BYTES},
     {(void**)&d.cinv, (size_t)sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * 4},
   };
@@ -491,6 +493,7 @@ int Engine::upload_ctl() {
   c.iter = 0; c.hard_cap = std::max(ncycles_, max_cycles_) + 1;
   c.coarse_direct = (mode_ != CFG_SOLVE_FIXED && coarse_direct_) ? 1 : 0;
   c.use_cond = ctl_use_cond_ == 1 ? 1 : 0;
+  c.krylov = krylov() ? 1 : 0;
   c.cond = cond_handle_;
   *h_ctl_pinned_ = c;
   CFG_CUDA(cudaMemcpyAsync(d_ctl_, h_ctl_pinned_, sizeof(SolveCtl), cudaMemcpyHostToDevice, st()));
@@ -824,6 +827,14 @@ int Engine::set_cond_mode(bool graph) {
   return upload_ctl();
 }
 
+int Engine::set_krylov(int on) {
+  if (on != 0 && on != 1) return fail(CFG_ERR_INVAL, "krylov must be 0 or 1");
+  CFG_TRY(activate());
+  krylov_ = on;
+  graph_dirty_ = true;
+  return upload_ctl();
+}
+
 int Engine::set_coarse_solve(int direct) {
   if (direct != 0 && direct != 1) return fail(CFG_ERR_INVAL, "coarse solve must be 0 (sweeps) or 1 (direct)");
   CFG_TRY(activate());
@@ -887,12 +898,23 @@ void Engine::enqueue_vcycle_ref(cudaStream_t s) {
   }
 }
 
-void Engine::enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond) {
-  // the fused cycle already ended with p64 += p (FP64) or the residual norm (FP32 modes)
-  if (any_fp64()) {
+// FP64 mode after the fused cycle: the defect of the corrected p64 (plain correction),
+// or the Krylov direction and update (the cycle ended with the direction update beta)
+void Engine::enqueue_fp64_tail(cudaStream_t s) {
+  if (!any_fp64()) return;
+  if (krylov()) {
+    launch_pcg_dir(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
+    launch_pcg_update(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
+    vcycle_launches_ += 2;
+  } else {
     launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, s);
     vcycle_launches_++;
   }
+}
+
+void Engine::enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond) {
+  // the fused cycle already ended with p64 += p / the direction update (FP64) or the residual norm
+  enqueue_fp64_tail(s);
   launch_loop_guard(d_ctl_, h, use_cond, s);
   vcycle_launches_++;
 }
@@ -921,7 +943,7 @@ int Engine::host_pressure_loop() {
   CFG_CUDA(cudaStreamSynchronize(s));
   int any = any_fp64() ? h_ctl_pinned_->any_active : 1;
   while (any) {
-    enqueue_vcycle(s, any_fp64() ? 2 : 1, 0);
+    enqueue_vcycle(s, cycle_tail(), 0);
     enqueue_cycle_tail(s, 0ull, 0);
     CFG_CUDA(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s));
     CFG_CUDA(cudaStreamSynchronize(s));
@@ -976,11 +998,8 @@ int Engine::ensure_graph() {
   vcycle_launches_ = 0;
   // the first kernel of the body counts the iteration and the cycle's decision sets the
   // condition (loop_count / loop_decide): no guard kernel in the body
-  enqueue_vcycle(body_stream_, any_fp64() ? 2 : 1, 1);
-  if (any_fp64()) {
-    launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, body_stream_);
-    vcycle_launches_++;
-  }
+  enqueue_vcycle(body_stream_, cycle_tail(), 1);
+  enqueue_fp64_tail(body_stream_);
   e = cudaStreamEndCapture(body_stream_, &body);
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamEndCapture(body)");
   enqueue_post_solve(s);

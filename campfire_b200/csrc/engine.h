@@ -131,6 +131,8 @@ class Engine {
   int coarse_cells() const { return coarse_cells_; }
   // coarsest level of the TOL/FP64 modes: 0 the reference's 120 sweeps, 1 its inverse
   int set_coarse_solve(int direct);
+  // FP64 mode: flexible preconditioned CG around the V-cycle (1) or plain defect correction (0)
+  int set_krylov(int on);
   int scene_lc(int s) const { return scenes_[s].lc; }
   size_t arena_bytes(int s) const { return scenes_[s].arena_bytes; }
   int scene_nx(int s) const { return scenes_[s].nx; }
@@ -162,6 +164,9 @@ class Engine {
   void enqueue_vcycle_ref(cudaStream_t s);   // one kernel per reference dispatch (cfg_vcycle)
   int max_lc() const;
   bool direct_coarse() const { return mode_ != CFG_SOLVE_FIXED && coarse_direct_ != 0; }
+  bool krylov() const { return mode_ == CFG_SOLVE_FP64 && krylov_ != 0; }
+  int cycle_tail() const { return any_fp64() ? (krylov() ? 3 : 2) : 1; }
+  void enqueue_fp64_tail(cudaStream_t s);
   void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
   void enqueue_post_solve(cudaStream_t s);
   int host_pressure_loop();
@@ -191,6 +196,7 @@ class Engine {
   size_t coarse_smem_ = 0;
   int coarse_cells_ = COARSE_CELLS;
   int coarse_direct_ = 0;
+  int krylov_ = 0;
   unsigned long long cond_handle_ = 0;   // the step graph's WHILE-node handle
   int ctl_use_cond_ = 0;                 // SolveCtl::use_cond on the device (-1: stale)
   int set_cond_mode(bool graph);

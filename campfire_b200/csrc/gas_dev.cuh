@@ -45,6 +45,7 @@ struct SolveState {
   unsigned int maxu;        // max |u| over faces after projection (f32 bits; CFL step)
   int direct_ok;            // the coarsest operator's inverse of this step is valid (direct coarse solve)
   int pad;
+  double delta, alpha, beta;   // Krylov FP64 mode: r.z of this cycle, the step length, the direction update
 };
 
 struct SceneDesc {
@@ -65,7 +66,8 @@ struct SceneDesc {
   int32_t *acc, *faceW;
   float *pieces;
   float4 *rad;
-  double *p64, *rhs64, *part;   // FP64 pressure, FP64 rhs, per-CTA partial sums
+  double *p64, *rhs64, *part;   // FP64 pressure, FP64 rhs, per-CTA partial sums (2 per tile)
+  double *r64, *dA, *dB, *q64;  // Krylov FP64 mode: residual, search directions (ping-pong), L d
   SolveState* solve;
   const char* tmap;         // TMA tensor maps of the levels (TM_PER_LEVEL per level, 128 bytes each)
   float* cinv;              // inverse of the coarsest operator (n x n, n = its cells), direct coarse solve
@@ -85,7 +87,7 @@ struct SolveCtl {
   int err;                    // set by a kernel whose bounded wait ran out (reported as CFG_ERR_TIMEDOUT)
   int coarse_direct;          // TOL/FP64 modes: solve the coarsest level with its inverse instead of 120 sweeps
   int use_cond;               // 1 while the step runs as a graph: the loop decision sets the WHILE node's condition
-  int pad2;
+  int krylov;                 // FP64 mode: preconditioned (flexible) CG around the V-cycle instead of plain correction
   unsigned long long cond;    // that node's cudaGraphConditionalHandle
 };
 

@@ -171,7 +171,8 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
 }
 
 // ------------------------------------------------------------------ up: prolong + 4 passes (+ level-0 tail)
-// tail: 0 none, 1 residual norm + loop decision (FP32 modes), 2 p64 += p (FP64 defect correction)
+// tail: 0 none, 1 residual norm + loop decision (FP32 modes), 2 p64 += p (FP64 defect correction),
+// 3 r.z and q.z -> the direction update (Krylov FP64 mode)
 template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, int tail, SolveCtl* ctl);
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
                            min(y0 + TY + MGF_H - k, L.ny), k & 1);
     __syncthreads();
   }
-  double part = 0.0;
+  double part = 0.0, part2 = 0.0;
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
     if (i >= L.nx || j >= L.ny) continue;
@@ -255,7 +256,19 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
       part += r * r;
     } else if (tail == 2) {
       S.p64[j * L.nx + i] += (double)t.p[k];
+    } else if (tail == 3) {
+      const int kk = j * L.nx + i;
+      const double z = (double)t.p[k];
+      part += S.r64[kk] * z;
+      part2 += S.q64[kk] * z;
     }
+  }
+  if (tail == 3) {
+    const double pa = block_sum(part, red);
+    const double pb = block_sum(part2, red);
+    double ta = 0.0, tb = 0.0;
+    if (scene_reduce2(S, w.tile, S.nt_up0, pa, pb, red, &ta, &tb) && threadIdx.x == 0) pcg_beta(S, ta, tb);
+    return;
   }
   if (tail != 1) return;
   const double bp = block_sum(part, red);
@@ -507,7 +520,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   }
   // ---- write level lc back; when the block covers level 0, finish the cycle here
   const LevelDesc& G = S.lev[lc];
-  double part = 0.0;
+  double part = 0.0, part2 = 0.0;
   for (int j = warp; j < G.ny; j += CB_WARPS)
     for (int i = lane; i < G.nx; i += 32) {
       const int e = j * V0.pc + i;
@@ -518,11 +531,19 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
         part += r * r;
       } else if (lc == 0 && tail == 2) {
         S.p64[j * G.nx + i] += (double)V0.p[e];
+      } else if (lc == 0 && tail == 3) {
+        const double z = (double)V0.p[e];
+        part += S.r64[j * G.nx + i] * z;
+        part2 += S.q64[j * G.nx + i] * z;
       }
     }
   if (lc == 0 && tail == 1) {
     const double t = block_sum(part, red);
     if (threadIdx.x == 0) solve_decide_f(scenes, nscenes, S, ctl, t);
+  } else if (lc == 0 && tail == 3) {
+    const double ta = block_sum(part, red);
+    const double tb = block_sum(part2, red);
+    if (threadIdx.x == 0) pcg_beta(S, ta, tb);
   }
 }
 

@@ -66,4 +66,38 @@ __device__ __forceinline__ bool scene_reduce(const SceneDesc& S, int tile, int n
   return true;
 }
 
+// Two sums at once (partials at part[2 tile], part[2 tile + 1]); same protocol.
+__device__ __forceinline__ bool scene_reduce2(const SceneDesc& S, int tile, int ntiles, double a, double b,
+                                              double* sh, double* ta, double* tb) {
+  __shared__ int s_last2;
+  if (threadIdx.x == 0) {
+    S.part[2 * tile] = a;
+    S.part[2 * tile + 1] = b;
+    __threadfence();
+    const unsigned prev = atomicAdd(&S.solve->counter, 1u);
+    s_last2 = (prev == (unsigned)ntiles - 1u) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last2) return false;
+  __threadfence();
+  double va = 0.0, vb = 0.0;
+  for (int k = threadIdx.x; k < ntiles; k += blockDim.x) {
+    va += __ldcg(S.part + 2 * k);
+    vb += __ldcg(S.part + 2 * k + 1);
+  }
+  const double sa = block_sum(va, sh);
+  const double sb = block_sum(vb, sh);
+  if (threadIdx.x == 0) { *ta = sa; *tb = sb; S.solve->counter = 0u; }
+  return true;
+}
+
+// Krylov FP64 mode, after the V-cycle: delta = r.z and eta = q_prev.z give the
+// direction update beta = -alpha_prev eta / delta_prev (0 in the first cycle)
+__device__ __forceinline__ void pcg_beta(const SceneDesc& S, double delta, double eta) {
+  SolveState* ss = S.solve;
+  const double prev = ss->delta;
+  ss->beta = (ss->cycles > 0 && prev != 0.0) ? -ss->alpha * eta / prev : 0.0;
+  ss->delta = delta;
+}
+
 }  // namespace cfg

@@ -108,10 +108,11 @@ int cfg_server_destroy(cfg_server* s) {
 }
 
 int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int max_cycles, int coarse_direct,
-                          int coarse_cells) {
+                          int coarse_cells, int krylov) {
   if (!s) return cfg::fail(CFG_ERR_INVAL, "null cfg_server handle");
   CFG_TRY(s->eng.set_solver(mode, ncycles, tol, max_cycles));
   CFG_TRY(s->eng.set_coarse_solve(coarse_direct ? 1 : 0));
+  CFG_TRY(s->eng.set_krylov(krylov ? 1 : 0));
   if (coarse_cells > 0) CFG_TRY(s->eng.set_coarse_cells(coarse_cells));
   return CFG_OK;
 }

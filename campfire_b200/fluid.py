@@ -224,6 +224,10 @@ class FluidSim(_SceneOps):
         """TOL/FP64 modes: solve the coarsest level with its inverse (True) or 120 sweeps (False)."""
         check(_lib.lib().cfg_set_coarse_solve(self._h, 1 if direct else 0))
 
+    def set_krylov(self, on: bool):
+        """FP64 mode: preconditioned CG around the V-cycle (True) or plain defect correction (False)."""
+        check(_lib.lib().cfg_set_krylov(self._h, 1 if on else 0))
+
     def set_solver(self, mode: int = _lib.SOLVE_FIXED, ncycles: int = 1, tol: float = 1e-6, max_cycles: int = 50):
         check(_lib.lib().cfg_set_solver(self._h, mode, ncycles, tol, max_cycles))
 
@@ -292,6 +296,9 @@ class Batch:
     def set_coarse_solve(self, direct: bool):
         check(_lib.lib().cfg_batch_set_coarse_solve(self._h, 1 if direct else 0))
 
+    def set_krylov(self, on: bool):
+        check(_lib.lib().cfg_batch_set_krylov(self._h, 1 if on else 0))
+
     def set_active(self, i: int, on: bool):
         check(_lib.lib().cfg_batch_set_active(self._h, i, 1 if on else 0))
 
@@ -339,9 +346,9 @@ class Server:
             pass
 
     def set_solver(self, mode=_lib.SOLVE_FP64, ncycles=1, tol=1e-10, max_cycles=300, coarse_direct=True,
-                   coarse_cells=0):
+                   coarse_cells=0, krylov=False):
         check(_lib.lib().cfg_server_set_solver(self._h, mode, ncycles, tol, max_cycles, 1 if coarse_direct else 0,
-                                               coarse_cells))
+                                               coarse_cells, 1 if krylov else 0))
 
     def slot_bytes(self, size_class: int) -> int:
         b = ctypes.c_size_t()

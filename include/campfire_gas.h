@@ -193,6 +193,12 @@ int cfg_set_coarse_cells(cfg_sim* sim, int cells);
  * FIXED mode ignores it. */
 int cfg_set_coarse_solve(cfg_sim* sim, int direct);
 int cfg_batch_set_coarse_solve(cfg_batch* b, int direct);
+/* FP64 mode outer loop (no counterpart in the reference): 0 (default) plain defect correction
+ * (p64 += V-cycle(f32(r)) per cycle); 1 flexible preconditioned conjugate gradients on the
+ * level-0 operator in FP64 with the same FP32 V-cycle as preconditioner (Polak-Ribiere
+ * direction update), which needs about half the cycles for the same tolerance. */
+int cfg_set_krylov(cfg_sim* sim, int on);
+int cfg_batch_set_krylov(cfg_batch* b, int on);
 /* Autotuner of that schedule (no counterpart in the reference): builds a scratch batch of
  * these sizes on `device` with generated scenes, runs one step to build the coefficients
  * (and, with coarse_direct, the coarsest inverse), then times `iters` fused V-cycles for
@@ -263,9 +269,10 @@ typedef struct cfg_job_result {
 int cfg_server_create(int device, int nclasses, const int* nx, const int* ny, const int* slots, double budget_bytes,
                       double width, cfg_server** out);
 int cfg_server_destroy(cfg_server* s);
-/* solver of every slot (as cfg_set_solver, cfg_set_coarse_solve, cfg_set_coarse_cells; cells <= 0 keeps it) */
+/* solver of every slot (as cfg_set_solver, cfg_set_coarse_solve, cfg_set_coarse_cells (cells <= 0
+ * keeps it) and cfg_set_krylov) */
 int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int max_cycles, int coarse_direct,
-                          int coarse_cells);
+                          int coarse_cells, int krylov);
 /* device bytes of one slot of a size class */
 int cfg_server_slot_bytes(cfg_server* s, int size_class, size_t* bytes);
 /* run the jobs to completion in real time (arrivals are honoured by the host clock);

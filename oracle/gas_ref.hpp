@@ -163,6 +163,7 @@ struct Sim {
   // direct coarse solve of the TOL/FP64 modes (extension of the library; the reference
   // runs one fixed cycle with the 120-sweep coarsest level)
   int coarse_direct = 0;
+  int krylov = 0;   // FP64 mode: flexible preconditioned CG around the FP32 V-cycle (extension)
   std::vector<R> cinv;
   bool cinv_ok = false;
   std::vector<double> p64, rhs64;   // FP64 defect correction state (level 0)
@@ -923,6 +924,57 @@ struct Sim {
       }
     return std::sqrt(s);
   }
+  // q = L d at level 0 in FP64: (sum a d_nb - diag d) / h2 (0 in closed cells)
+  void lap64(const std::vector<double>& d, std::vector<double>& q) const {
+    const Level& L = lv[0]; const double h2 = (double)L.h2;
+    q.assign((size_t)L.nx * L.ny, 0.0);
+    for (int j = 0; j < L.ny; j++)
+      for (int i = 0; i < L.nx; i++) {
+        const double w = L.ax[j * (L.nx + 1) + i], e = L.ax[j * (L.nx + 1) + i + 1];
+        const double so = L.ay[j * L.nx + i], n = L.ay[(j + 1) * L.nx + i];
+        double off = 0, diag = 0;
+        if (i > 0) { off += w * d[j * L.nx + i - 1]; diag += w; } else diag += 2 * w;
+        if (i < L.nx - 1) { off += e * d[j * L.nx + i + 1]; diag += e; } else diag += 2 * e;
+        if (j > 0) { off += so * d[(j - 1) * L.nx + i]; diag += so; }
+        if (j < L.ny - 1) { off += n * d[(j + 1) * L.nx + i]; diag += n; } else diag += 2 * n;
+        const int k = j * L.nx + i;
+        q[k] = diag > 0 ? (off - diag * d[k]) / h2 : 0.0;
+      }
+  }
+  // FP64 mode, Krylov variant: flexible (Polak-Ribiere) preconditioned CG on the level-0
+  // operator, one FP32 V-cycle on f32(r) per iteration as the preconditioner z ~ L^-1 r:
+  // delta = r.z; beta = -alpha_prev (q_prev.z) / delta_prev; d = z + beta d; q = L d;
+  // alpha = delta / (d.q); p64 += alpha d; r -= alpha q; stop on ||r|| / ||rhs64||.
+  void pressure_pcg(bool direct) {
+    rhs0_64();
+    double b = 0; for (double v : rhs64) b += v * v; b = std::sqrt(b);
+    std::vector<double> r, z, d, q;
+    double rn = res64(r);
+    last_rel0 = b > 0 ? rn / b : 0.0;
+    Level& L0 = lv[0];
+    const size_t n = r.size();
+    d.assign(n, 0.0); q.assign(n, 0.0); z.assign(n, 0.0);
+    double alpha = 0, delta_prev = 0;
+    int c = 0;
+    while (b > 0 && rn / b > tol && c < max_cycles) {
+      for (size_t k = 0; k < n; k++) { L0.rhs[k] = R((float)r[k]); L0.p[k] = R(0); }
+      vcycle(2, direct); c++;
+      for (size_t k = 0; k < n; k++) z[k] = (double)L0.p[k];
+      double delta = 0, eta = 0;
+      for (size_t k = 0; k < n; k++) { delta += r[k] * z[k]; eta += q[k] * z[k]; }
+      const double beta = c > 1 && delta_prev != 0 ? -alpha * eta / delta_prev : 0.0;
+      for (size_t k = 0; k < n; k++) d[k] = z[k] + beta * d[k];
+      lap64(d, q);
+      double pi = 0;
+      for (size_t k = 0; k < n; k++) pi += d[k] * q[k];
+      alpha = pi != 0 ? delta / pi : 0.0;
+      delta_prev = delta;
+      double s2 = 0;
+      for (size_t k = 0; k < n; k++) { p64[k] += alpha * d[k]; r[k] -= alpha * q[k]; s2 += r[k] * r[k]; }
+      rn = std::sqrt(s2);
+    }
+    last_cycles = c; last_rel = b > 0 ? rn / b : 0.0;
+  }
   // FP64 divergence-source assembly (the FP64 counterpart of rhs0)
   void rhs0_64() {
     const double ddx = (double)dx, ddt = (double)dt;
@@ -974,6 +1026,7 @@ struct Sim {
       last_cycles = c; last_rel = rel;
       return;
     }
+    if (krylov) { pressure_pcg(direct); return; }
     // SOLVE_FP64: FP32 V-cycles on the defect inside an FP64 loop
     rhs0_64();
     double b = 0; for (double v : rhs64) b += v * v; b = std::sqrt(b);

@@ -59,7 +59,7 @@ def _declare(L, pfx):
         "readback": [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float),
                      ctypes.POINTER(ctypes.c_int32)],
         "budgets": [vp, dp], "info": [vp, dp], "level_dims": [vp, ci, ctypes.POINTER(ctypes.c_int)],
-        "pressure_residual": [vp, dp], "set_coarse_solve": [vp, ci],
+        "pressure_residual": [vp, dp], "set_coarse_solve": [vp, ci], "set_krylov": [vp, ci],
     }
     for name, args in sigs.items():
         fn = getattr(L, pfx + name, None)
@@ -163,6 +163,9 @@ class OracleSim:
 
     def set_coarse_solve(self, direct):
         self._chk(self._f.set_coarse_solve(self._h, 1 if direct else 0))
+
+    def set_krylov(self, on):
+        self._chk(self._f.set_krylov(self._h, 1 if on else 0))
 
     def upload_pieces(self, data, n):
         a = np.zeros(64 * 20, np.float32)
