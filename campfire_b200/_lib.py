@@ -62,6 +62,12 @@ class CfgJobResult(ctypes.Structure):
                 ("t_sum", ctypes.c_double)]
 
 
+class CfgWoodPiece(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("side", "rhoV", "rhoC", "mv", "mc", "Tc", "gasRate")] + \
+               [(n, ctypes.c_double * 4) for n in ("Ts", "Tp", "d", "mflux", "charCov", "exposure")] + \
+               [("dead", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
 class CampfireError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -115,6 +121,13 @@ def lib():
         "cfg_autotune": [ci, ci, ip, ip, ci, ci, ip, ip, dp, ip],
         "cfg_set_coarse_solve": [vp, ci], "cfg_batch_set_coarse_solve": [vp, ci],
         "cfg_checkpoint_save": [vp, cs], "cfg_checkpoint_load": [vp, cs],
+        "cfg_wood_piece_init": [ctypes.POINTER(CfgWoodPiece), cd, cd, cd],
+        "cfg_wood_piece_preheat": [ctypes.POINTER(CfgWoodPiece), cd, cd, cd, cd],
+        "cfg_wood_piece_step": [ctypes.POINTER(CfgWoodPiece), cd, dp, dp, dp, cd, cd],
+        "cfg_wood_create": [vp, cd, cd, ctypes.POINTER(vp)], "cfg_wood_destroy": [vp],
+        "cfg_wood_add": [vp, cd, cd, cd, cd, cd, dp, dp, ip], "cfg_wood_remove": [vp, ci],
+        "cfg_wood_frame": [vp, cd, ip], "cfg_wood_get": [vp, ci, ctypes.POINTER(CfgWoodPiece), dp, dp],
+        "cfg_wood_stats": [vp, dp, dp, dp],
         "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
         "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci, ci],
         "cfg_set_krylov": [vp, ci], "cfg_batch_set_krylov": [vp, ci],

@@ -24,8 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
                      "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
 SOURCES = ["k_advect.cu", "k_diffsrc.cu", "k_forces.cu", "k_mg.cu", "k_mgf.cu", "k_misc.cu", "noalloc.cu", "engine.cu",
-           "capi.cpp", "scene.cpp", "serve.cpp"]
-HEADERS = ["gas_dev.cuh", "kernels.h", "reduce.cuh", "engine.h", "tma.cuh"]
+           "capi.cpp", "scene.cpp", "serve.cpp", "wood.cpp"]
+HEADERS = ["gas_dev.cuh", "kernels.h", "reduce.cuh", "engine.h", "tma.cuh", "wood.h"]
 
 
 def nvcc() -> str:
@@ -47,7 +47,8 @@ def _compile(src: str, force: bool, extra: list[str]) -> str:
         return obj
     cmd = [nvcc()] + NVCC_FLAGS + extra + ["-x", "cu" if src.endswith(".cu") else "c++", "-c", path, "-o", obj]
     if src.endswith(".cpp"):
-        cmd = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-x", "c++", "-c", path, "-o", obj]
+        cmd = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off", "-I" + os.path.join(HERE, "..", "include"),
+               "-x", "c++", "-c", path, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")

@@ -10,6 +10,7 @@
 
 #include "../../include/campfire_gas.h"
 #include "engine.h"
+#include "wood.h"
 
 struct cfg_sim {
   cfg::Engine* eng;
@@ -279,3 +280,108 @@ extern "C" int cfg_batch_set_krylov(cfg_batch* b, int on) {
   if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
   return guarded([&] { return b->eng->set_krylov(on); });
 }
+
+// ------------------------------------------------------------------ wood
+struct cfg_wood {
+  cfg::Engine* eng;
+  std::unique_ptr<cfg::WoodScene> scene;
+};
+
+namespace {
+void to_c(const cfg::WoodPiece& w, cfg_wood_piece* o) {
+  o->side = w.side; o->rhoV = w.rhoV; o->rhoC = w.rhoC; o->mv = w.mv; o->mc = w.mc; o->Tc = w.Tc; o->gasRate = w.gasRate;
+  for (int f = 0; f < 4; f++) {
+    o->Ts[f] = w.Ts[f]; o->Tp[f] = w.Tp[f]; o->d[f] = w.d[f]; o->mflux[f] = w.mflux[f];
+    o->charCov[f] = w.charCov[f]; o->exposure[f] = w.exposure[f];
+  }
+  o->dead = w.dead ? 1 : 0;
+  o->pad = 0;
+}
+cfg::WoodPiece from_c(const cfg_wood_piece* o) {
+  cfg::WoodPiece w;
+  w.side = o->side; w.rhoV = o->rhoV; w.rhoC = o->rhoC; w.mv = o->mv; w.mc = o->mc; w.Tc = o->Tc; w.gasRate = o->gasRate;
+  for (int f = 0; f < 4; f++) {
+    w.Ts[f] = o->Ts[f]; w.Tp[f] = o->Tp[f]; w.d[f] = o->d[f]; w.mflux[f] = o->mflux[f];
+    w.charCov[f] = o->charCov[f]; w.exposure[f] = o->exposure[f];
+  }
+  w.dead = o->dead != 0;
+  return w;
+}
+std::array<double, 4> a4(const double* p) { return {p[0], p[1], p[2], p[3]}; }
+}  // namespace
+
+extern "C" {
+int cfg_wood_piece_init(cfg_wood_piece* w, double side, double density, double T0) {
+  if (!w || !(side > 0) || !(density > 0) || !(T0 > 0)) return cfg::fail(CFG_ERR_INVAL, "bad wood piece arguments");
+  to_c(cfg::WoodPiece(side, density, T0), w);
+  return CFG_OK;
+}
+int cfg_wood_piece_preheat(cfg_wood_piece* w, double Tsurf, double char_depth, double Tcore, double char_yield) {
+  if (!w) return cfg::fail(CFG_ERR_INVAL, "null piece");
+  cfg::WoodPiece p = from_c(w);
+  p.preheat(Tsurf, char_depth, Tcore, char_yield);
+  to_c(p, w);
+  return CFG_OK;
+}
+int cfg_wood_piece_step(cfg_wood_piece* w, double dt, const double* qConv4, const double* qInc4,
+                        const double* charBurnt4, double char_yield, double pyro_mult) {
+  if (!w || !qConv4 || !qInc4 || !charBurnt4 || !(dt > 0)) return cfg::fail(CFG_ERR_INVAL, "bad wood step arguments");
+  cfg::WoodPiece p = from_c(w);
+  cfg::WoodCtl ctl;
+  ctl.charYield = char_yield;
+  ctl.pyroMult = pyro_mult;
+  p.step(dt, a4(qConv4), a4(qInc4), a4(charBurnt4), ctl);
+  to_c(p, w);
+  return CFG_OK;
+}
+int cfg_wood_create(cfg_sim* sim, double char_yield, double pyro_mult, cfg_wood** out) {
+  SIM_OK(sim); OWNER_OK(sim);
+  if (!out) return cfg::fail(CFG_ERR_INVAL, "null output");
+  return guarded([&] {
+    cfg::WoodCtl ctl;
+    ctl.charYield = char_yield;
+    ctl.pyroMult = pyro_mult;
+    auto* w = new cfg_wood{sim->eng, std::make_unique<cfg::WoodScene>(sim->eng, sim->scene, ctl)};
+    *out = w;
+    return CFG_OK;
+  });
+}
+int cfg_wood_destroy(cfg_wood* w) {
+  delete w;
+  return CFG_OK;
+}
+int cfg_wood_add(cfg_wood* w, double x, double y, double angle, double side, double density, const double* preheat3,
+                 const double* face_T4, int* slot) {
+  if (!w || !slot) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  return guarded([&] {
+    const int s = w->scene->add(x, y, angle, side, density, preheat3, face_T4);
+    if (s < 0) return s;
+    *slot = s;
+    return CFG_OK;
+  });
+}
+int cfg_wood_remove(cfg_wood* w, int slot) {
+  if (!w) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  return guarded([&] { return w->scene->remove(slot); });
+}
+int cfg_wood_frame(cfg_wood* w, double sim_dt, int* nsteps) {
+  if (!w) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  return guarded([&] { return w->scene->frame(sim_dt, nsteps); });
+}
+int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, double* qInc4) {
+  if (!w || !out) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  const cfg::WoodSlot* p = w->scene->slot(slot);
+  if (!p) return cfg::fail(CFG_ERR_NOENT, "no piece in this slot");
+  to_c(p->wood, out);
+  if (qConv4) for (int f = 0; f < 4; f++) qConv4[f] = p->qConv[f];
+  if (qInc4) for (int f = 0; f < 4; f++) qInc4[f] = p->qInc[f];
+  return CFG_OK;
+}
+int cfg_wood_stats(cfg_wood* w, double* hrr, double* rad, double* tmax) {
+  if (!w) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  if (hrr) *hrr = w->scene->hrr;
+  if (rad) *rad = w->scene->rad;
+  if (tmax) *tmax = w->scene->tmax;
+  return CFG_OK;
+}
+}  // extern "C"

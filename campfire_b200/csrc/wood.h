@@ -1,0 +1,71 @@
+// Host-side wood model and the per-frame wood <-> gas coupling of the campfire
+// app, around the GPU gas step.
+//
+// WoodPiece restates js/wood.js (WOOD constants :12-31, the class :33-182) in
+// double precision, as the reference computes it in JS numbers. WoodScene
+// restates the frame loop of js/main.js for frozen bodies (the rigid-body world
+// and contacts are out of this path): addPiece :103-119 (slots, per-piece
+// qConv/qInc/vis/charPending), uploadPieces :190-207, onReadback :209-230,
+// stepWood :232-243 and the gas part of frame() :247-283.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <vector>
+
+namespace cfg {
+
+class Engine;
+
+struct WoodCtl {
+  double charYield = 0.25, pyroMult = 1.0;   // js/config.js:55-57 CONTROL_DEFAULTS
+};
+
+struct WoodPiece {
+  double rhoV = 500, rhoC = 150, mv = 0, mc = 0, Tc = 293.15, gasRate = 0, side = 0;
+  std::array<double, 4> Ts{}, Tp{}, d{}, mflux{}, charCov{}, exposure{1, 1, 1, 1};
+  bool dead = false;
+
+  WoodPiece() = default;
+  WoodPiece(double side, double rhoV, double T0 = 293.15);   // js/wood.js:34-49
+  double half() const { return 0.5 * side; }
+  void updateSide();                                          // :60
+  double charFraction() const;                                // :61
+  void preheat(double Tsurf, double charDepth, double Tcore, double charYield);   // :64-76
+  // :82-181: heat inputs per face (qConv W/m, qInc W/m^2, char burnt kg/m)
+  void step(double dt, const std::array<double, 4>& qConv, const std::array<double, 4>& qInc,
+            const std::array<double, 4>& charBurnt, const WoodCtl& ctl);
+};
+
+// A piece of the scene: its body (frozen: position and angle fixed, size from the wood)
+struct WoodSlot {
+  bool used = false;
+  double x = 0, y = 0, angle = 0;
+  WoodPiece wood;
+  std::array<double, 4> qConv{}, qInc{}, vis{}, charPending{};
+};
+
+class WoodScene {
+ public:
+  WoodScene(Engine* eng, int scene, WoodCtl ctl) : eng_(eng), scene_(scene), ctl_(ctl) {}
+  // :103-119 (returns the slot, or a negative status when all 64 are taken)
+  int add(double x, double y, double angle, double side, double density, const double* preheat3,
+          const double* faceT4);
+  int remove(int slot);
+  // one frame of main.js frame() with `sim_dt` of gas time: the wood steps on the
+  // last readback, pieces are uploaded, geometry rebuilt, floor(sim_dt/dt) gas steps
+  // (at most ceil(0.034/dt)) and radiation run, and the readback applied
+  int frame(double sim_dt, int* nsteps);
+  const WoodSlot* slot(int s) const { return (s >= 0 && s < (int)slots_.size() && slots_[s].used) ? &slots_[s] : nullptr; }
+  double hrr = 0, rad = 0, tmax = 0;   // stats of the last readback (main.js:225-229, before smoothing)
+
+ private:
+  int upload();
+  int readback(double sim_dt);
+  Engine* eng_;
+  int scene_;
+  WoodCtl ctl_;
+  std::vector<WoodSlot> slots_ = std::vector<WoodSlot>(64);
+  double sim_acc_ = 0;
+};
+
+}  // namespace cfg

@@ -1,0 +1,97 @@
+"""The campfire app's wood model and frame coupling around the gas step, through
+the C ABI (cfg_wood_*): WoodPiece mirrors js/wood.js's class, WoodScene the
+frame loop of js/main.js for pieces frozen in place."""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+from ._lib import CfgWoodPiece, check
+
+
+def _d4(v):
+    return (ctypes.c_double * 4)(*[float(x) for x in v])
+
+
+class WoodPiece:
+    """new WoodPiece(side, rhoV, T0) of js/wood.js; fields as attributes (Ts, Tp, d, ...)."""
+
+    def __init__(self, side: float, rhoV: float, T0: float = 293.15):
+        self._s = CfgWoodPiece()
+        check(_lib.lib().cfg_wood_piece_init(ctypes.byref(self._s), side, rhoV, T0))
+
+    def __getattr__(self, name):
+        s = object.__getattribute__(self, "_s")
+        v = getattr(s, name)
+        return list(v) if isinstance(v, ctypes.Array) else v
+
+    @property
+    def half(self):
+        return 0.5 * self._s.side
+
+    @property
+    def dead(self):
+        return bool(self._s.dead)
+
+    def set_exposure(self, ex):
+        for f in range(4):
+            self._s.exposure[f] = ex[f]
+
+    def preheat(self, Tsurf, charDepth, Tcore, charYield=0.25):
+        check(_lib.lib().cfg_wood_piece_preheat(ctypes.byref(self._s), Tsurf, charDepth, Tcore, charYield))
+
+    def step(self, dt, qConv, qInc, charBurnt, charYield=0.25, pyroMult=1.0):
+        check(_lib.lib().cfg_wood_piece_step(ctypes.byref(self._s), dt, _d4(qConv), _d4(qInc), _d4(charBurnt),
+                                             charYield, pyroMult))
+
+
+class WoodScene:
+    """The pieces of a FluidSim and the per-frame coupling (cfg_wood_frame)."""
+
+    def __init__(self, sim, charYield: float = 0.25, pyroMult: float = 1.0):
+        h = ctypes.c_void_p()
+        check(_lib.lib().cfg_wood_create(sim._h, charYield, pyroMult, ctypes.byref(h)))
+        self._h = h.value
+
+    def close(self):
+        if self._h:
+            _lib.lib().cfg_wood_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, x, y, angle, side, density=500.0, preheat=None, faceT=None) -> int:
+        slot = ctypes.c_int()
+        pre = (ctypes.c_double * 3)(*preheat) if preheat else None
+        ft = _d4(faceT) if faceT else None
+        check(_lib.lib().cfg_wood_add(self._h, x, y, angle, side, density, pre, ft, ctypes.byref(slot)))
+        return slot.value
+
+    def remove(self, slot: int):
+        check(_lib.lib().cfg_wood_remove(self._h, slot))
+
+    def frame(self, sim_dt: float) -> int:
+        n = ctypes.c_int()
+        check(_lib.lib().cfg_wood_frame(self._h, sim_dt, ctypes.byref(n)))
+        return n.value
+
+    def piece(self, slot: int):
+        """(state dict, qConv[4], qInc[4]) or None for an empty slot."""
+        st = CfgWoodPiece()
+        qc, qi = (ctypes.c_double * 4)(), (ctypes.c_double * 4)()
+        rc = _lib.lib().cfg_wood_get(self._h, slot, ctypes.byref(st), qc, qi)
+        if rc == -2:
+            return None
+        check(rc)
+        d = {k: (list(getattr(st, k)) if isinstance(getattr(st, k), ctypes.Array) else getattr(st, k))
+             for k, _ in CfgWoodPiece._fields_ if k != "pad"}
+        return d, list(qc), list(qi)
+
+    def stats(self):
+        h, r, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(_lib.lib().cfg_wood_stats(self._h, ctypes.byref(h), ctypes.byref(r), ctypes.byref(t)))
+        return {"hrr": h.value, "rad": r.value, "tmax": t.value}

@@ -245,6 +245,37 @@ int cfg_batch_write_params(cfg_batch* b);
 int cfg_batch_geometry(cfg_batch* b);
 int cfg_batch_set_coarse_cells(cfg_batch* b, int cells);
 
+/* ---- wood: the CPU wood model (js/wood.js WoodPiece) and the per-frame coupling of the
+ * campfire app (js/main.js frame(): stepWood, uploadPieces, geometry, gas steps, radiation,
+ * readback) around the GPU gas step, for pieces frozen in place (no rigid-body motion). */
+typedef struct cfg_wood_piece {
+  double side, rhoV, rhoC, mv, mc, Tc, gasRate;
+  double Ts[4], Tp[4], d[4], mflux[4], charCov[4], exposure[4];
+  int32_t dead, pad;
+} cfg_wood_piece;
+/* new WoodPiece(side, rhoV, T0) (js/wood.js:34-49) */
+int cfg_wood_piece_init(cfg_wood_piece* w, double side, double density, double T0);
+/* WoodPiece.preheat (js/wood.js:64-76) */
+int cfg_wood_piece_preheat(cfg_wood_piece* w, double Tsurf, double char_depth, double Tcore, double char_yield);
+/* WoodPiece.step (js/wood.js:82-181): per face qConv (W/m), qInc (W/m^2), char burnt (kg/m) */
+int cfg_wood_piece_step(cfg_wood_piece* w, double dt, const double* qConv4, const double* qInc4,
+                        const double* charBurnt4, double char_yield, double pyro_mult);
+typedef struct cfg_wood cfg_wood;
+/* the pieces of a single-scene handle (not a batch view) and their coupling state */
+int cfg_wood_create(cfg_sim* sim, double char_yield, double pyro_mult, cfg_wood** out);
+int cfg_wood_destroy(cfg_wood* w);
+/* addPiece (js/main.js:103-119): optional preheat {Tsurf, char depth, Tcore} and face
+ * temperatures (0: keep); *slot receives the piece slot (0..63) */
+int cfg_wood_add(cfg_wood* w, double x, double y, double angle, double side, double density, const double* preheat3,
+                 const double* face_T4, int* slot);
+int cfg_wood_remove(cfg_wood* w, int slot);
+/* one frame with `sim_dt` seconds of gas time (js/main.js:247-283); *nsteps gas steps run */
+int cfg_wood_frame(cfg_wood* w, double sim_dt, int* nsteps);
+/* a piece's state and its last heat inputs (qConv W/m, qInc W/m^2); CFG_ERR_NOENT if the slot is empty */
+int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, double* qInc4);
+/* heat release rate and radiative loss (W per m depth) and max T of the last frame (js/main.js:225-229) */
+int cfg_wood_stats(cfg_wood* w, double* hrr, double* rad, double* tmax);
+
 /* ---- serving: jobs of several grid sizes in resident batch slots (no counterpart in the
  * reference). One batch holds slots[c] scenes of size class c (nx[c] x ny[c]); a job is
  * admitted into a free slot of its class once it has arrived and the bytes of the slots in

@@ -1,0 +1,85 @@
+"""The frame coupling of js/main.js (wood step on the last readback, piece upload,
+geometry, gas steps, radiation, readback) on the GPU gas step (cfg_wood_frame)
+against the oracle's restatement of the same loop over the CPU gas step.
+
+The gas fields agree within 1e-4 per step, so after a frame of ~8 steps the
+radiative (T^4) and convective heat inputs of a face agree within a few 1e-3
+and the wood state, which integrates them slowly, within 1e-4. The flame
+amplifies ulp-level differences (the CPU FP32 restatement itself drifts ~10% in
+T from the FP64 oracle within 40 steps), so from the third frame on the face
+inputs are compared by their totals per piece and the wood within 1e-3."""
+import pytest
+
+import campfire_b200 as cb
+from campfire_b200.fluid import load_scene
+from campfire_b200.wood import WoodScene
+from oracle.wood_ref import WoodScene as RefScene
+
+pytestmark = pytest.mark.gpu
+
+
+def pieces():
+    # two preheated logs on the floor and a stick above them (frozen)
+    return [(0.33, 0.03, 0.0, 0.05, 500.0, (900.0, 0.004, 500.0)),
+            (0.47, 0.03, 0.0, 0.05, 500.0, (900.0, 0.004, 500.0)),
+            (0.40, 0.085, 0.3, 0.025, 500.0, None)]
+
+
+def rel(a, b, floor):
+    return abs(a - b) / max(abs(b), floor)
+
+
+def test_frames_match_the_oracle(oracle_mod):
+    nx, ny = 96, 144
+    sc = cb.generate_scene(0, nx, ny, 0.8, 4242)
+    sc["npieces"] = 0
+    g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(g, sc)
+    o = oracle_mod.OracleSim(nx, ny, 0.8, sc["dt"])
+    load_scene(o, sc)
+    ws, rs = WoodScene(g), RefScene(o)
+    for p in pieces():
+        assert ws.add(*p[:5], preheat=p[5]) == rs.add(*p[:5], preheat=p[5])
+    for k in range(6):
+        n = ws.frame(1 / 60)
+        assert n == rs.frame(1 / 60) and n >= 1
+        got = [ws.piece(s) for s in range(3)]
+        # heat inputs: error relative to the largest input of the frame (as the field errors)
+        sc_c = max(abs(q) for r in rs.slots[:3] for q in r["qConv"])
+        sc_i = max(abs(q) for r in rs.slots[:3] for q in r["qInc"])
+        early = k < 2
+        for s in range(3):
+            a, qc, qi = got[s]
+            r = rs.slots[s]
+            w = r["wood"]
+            for f in range(4):
+                assert rel(a["Ts"][f], w.Ts[f], 1.0) <= (1e-4 if early else 1e-3), (k, s, f, a["Ts"][f], w.Ts[f])
+                if early:
+                    assert abs(a["mflux"][f] - w.mflux[f]) <= 1e-3 * max(max(w.mflux), 1e-6), (k, s, f)
+                    assert abs(qi[f] - r["qInc"][f]) <= 5e-3 * sc_i, (k, s, f, qi[f], r["qInc"][f])
+                    assert abs(qc[f] - r["qConv"][f]) <= 5e-3 * sc_c, (k, s, f, qc[f], r["qConv"][f])
+            if not early:   # the flame near the wood has begun to drift: the piece's totals
+                assert rel(sum(qi), sum(r["qInc"]), 1.0) <= 3e-2, (k, s)
+                assert abs(sum(qc) - sum(r["qConv"])) <= 3e-2 * 4 * sc_c, (k, s)
+            assert rel(a["mv"], w.mv, 1e-12) <= 1e-5
+    st = ws.stats()
+    assert rel(st["hrr"], rs.hrr, 1.0) <= 5e-3
+    assert abs(st["tmax"] - rs.tmax) <= 2
+    ws.close(); g.close()
+
+
+def test_slots_and_errors():
+    sc = cb.generate_scene(0, 64, 96, 0.8, 1)
+    g = cb.FluidSim(0, {"nx": 64, "ny": 96, "dt": sc["dt"]}, width=0.8).init()
+    ws = WoodScene(g)
+    s0 = ws.add(0.3, 0.03, 0.0, 0.05)
+    s1 = ws.add(0.5, 0.03, 0.0, 0.05)
+    assert (s0, s1) == (0, 1)
+    ws.remove(s0)
+    assert ws.piece(s0) is None
+    assert ws.add(0.2, 0.03, 0.0, 0.03) == 0
+    with pytest.raises(cb.CampfireError):
+        ws.remove(7)
+    with pytest.raises(cb.CampfireError):
+        ws.add(0.2, 0.03, 0.0, -1.0)
+    ws.close(); g.close()
