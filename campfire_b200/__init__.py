@@ -4,6 +4,7 @@ shaders/*.wgsl) as hand-written sm_100a CUDA kernels behind a C ABI
 reference's FluidSim interface."""
 from ._lib import (CampfireError, SOLVE_FIXED, SOLVE_FP64, SOLVE_TOL, declared_symbols, device_count, lib)
 from .fluid import SCENE_WIDTH, STAGES, Batch, FluidSim, Server, autotune, field_hash, generate_scene, load_scene
+from .render import GROUND, VIEWS, Renderer, write_png
 
 __all__ = ["CampfireError", "FluidSim", "Batch", "Server", "autotune", "field_hash", "generate_scene", "load_scene", "lib", "device_count",
-           "declared_symbols", "SOLVE_FIXED", "SOLVE_TOL", "SOLVE_FP64", "SCENE_WIDTH", "STAGES"]
+           "declared_symbols", "Renderer", "VIEWS", "GROUND", "write_png", "SOLVE_FIXED", "SOLVE_TOL", "SOLVE_FP64", "SCENE_WIDTH", "STAGES"]

@@ -68,6 +68,13 @@ class CfgWoodPiece(ctypes.Structure):
                [("dead", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
+class CfgRenderParams(ctypes.Structure):
+    """The uniform RP of shaders/render.wgsl:13-17 (js/render.js:41-53)."""
+    _fields_ = [("view", ctypes.c_int32), ("nPieces", ctypes.c_int32)] + \
+               [(n, ctypes.c_float) for n in ("exposure", "width", "height", "ground", "time", "tmax", "chemi",
+                                               "camX", "camY", "zoom")]
+
+
 class CampfireError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -127,7 +134,9 @@ def lib():
         "cfg_wood_create": [vp, cd, cd, ctypes.POINTER(vp)], "cfg_wood_destroy": [vp],
         "cfg_wood_add": [vp, cd, cd, cd, cd, cd, dp, dp, ip], "cfg_wood_remove": [vp, ci],
         "cfg_wood_frame": [vp, cd, ip], "cfg_wood_get": [vp, ci, ctypes.POINTER(CfgWoodPiece), dp, dp],
-        "cfg_wood_stats": [vp, dp, dp, dp],
+        "cfg_wood_stats": [vp, dp, dp, dp], "cfg_wood_render_data": [vp, fp],
+        "cfg_render_defaults": [vp, ctypes.POINTER(CfgRenderParams)],
+        "cfg_render": [vp, ctypes.POINTER(CfgRenderParams), fp, ci, ci, fp],
         "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
         "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci, ci],
         "cfg_set_krylov": [vp, ci], "cfg_batch_set_krylov": [vp, ci],

@@ -88,6 +88,12 @@ int cfg_geometry(cfg_sim* sim) { SCENE_CALL(sim, geometry(sim->scene)); }
 int cfg_radiation(cfg_sim* sim) { SCENE_CALL(sim, radiation(sim->scene)); }
 int cfg_set_frame(cfg_sim* sim, uint32_t frame) { SCENE_CALL(sim, set_frame(sim->scene, frame)); }
 int cfg_readback(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW) { SCENE_CALL(sim, readback(sim->scene, acc, rad, faceW)); }
+int cfg_render_defaults(cfg_sim* sim, cfg_render_params* rp) { SCENE_CALL(sim, render_defaults(sim->scene, rp)); }
+int cfg_render(cfg_sim* sim, const cfg_render_params* rp, const float* wood, int width, int height, float* rgba) {
+  SIM_OK(sim);
+  if (!rp) return cfg::fail(CFG_ERR_INVAL, "rp is null");
+  return guarded([&] { return sim->eng->render(sim->scene, *rp, wood, width, height, rgba); });
+}
 int cfg_field_size(cfg_sim* sim, const char* name, size_t* count) { SCENE_CALL(sim, field_size(sim->scene, name, count)); }
 int cfg_read_field(cfg_sim* sim, const char* name, float* out, size_t count) { SCENE_CALL(sim, read_field(sim->scene, name, out, count)); }
 int cfg_write_field(cfg_sim* sim, const char* name, const float* in, size_t count) { SCENE_CALL(sim, write_field(sim->scene, name, in, count)); }
@@ -375,6 +381,12 @@ int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, dou
   to_c(p->wood, out);
   if (qConv4) for (int f = 0; f < 4; f++) qConv4[f] = p->qConv[f];
   if (qInc4) for (int f = 0; f < 4; f++) qInc4[f] = p->qInc[f];
+  return CFG_OK;
+}
+int cfg_wood_render_data(cfg_wood* w, float* wood) {
+  if (!w || !wood) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  const auto& r = w->scene->render_wood();
+  std::copy(r.begin(), r.end(), wood);
   return CFG_OK;
 }
 int cfg_wood_stats(cfg_wood* w, double* hrr, double* rad, double* tmax) {

@@ -93,6 +93,8 @@ Engine::~Engine() {
   if (d_dxd_) cudaFree(d_dxd_);
   if (d_alpha_) cudaFree(d_alpha_);
   if (d_scratch_) cudaFree(d_scratch_);
+  if (d_rwood_) cudaFree(d_rwood_);
+  if (d_image_) cudaFree(d_image_);
   if (h_ctl_pinned_) cudaFreeHost(h_ctl_pinned_);
   if (stream_) cudaStreamDestroy(stream_);
   if (body_stream_) cudaStreamDestroy(body_stream_);
@@ -679,6 +681,55 @@ int Engine::readback(int s, int32_t* acc, float* rad, int32_t* faceW) {
   return CFG_OK;
 }
 
+// Renderer.encode (js/render.js:57-70) into a device image instead of the canvas:
+// the wood buffer (Renderer.writeWood, :55) is uploaded, one thread per pixel runs
+// the fragment stage, and the image is copied back.
+int Engine::render(int s, const cfg_render_params& rp, const float* wood, int width, int height, float* rgba) {
+  if (width < 1 || height < 1 || width > 16384 || height > 16384)
+    return fail(CFG_ERR_INVAL, "image size must be in [1, 16384] x [1, 16384]");
+  if (rp.nPieces < 0 || rp.nPieces > MAX_PIECES) return fail(CFG_ERR_INVAL, "nPieces must be in [0, 64]");
+  if (!rgba) return fail(CFG_ERR_INVAL, "rgba is null");
+  CFG_TRY(activate());
+  cudaStream_t q = st();
+  const size_t wood_bytes = sizeof(float) * MAX_PIECES * 12;
+  if (!d_rwood_) CFG_CUDA(cudaMalloc(&d_rwood_, wood_bytes));
+  const size_t bytes = sizeof(float) * 4 * (size_t)width * height;
+  if (bytes > image_bytes_) {
+    CFG_CUDA(cudaStreamSynchronize(q));
+    if (d_image_) CFG_CUDA(cudaFree(d_image_));
+    d_image_ = nullptr; image_bytes_ = 0;
+    CFG_CUDA(cudaMalloc(&d_image_, bytes));
+    image_bytes_ = bytes;
+  }
+  if (wood) CFG_CUDA(cudaMemcpyAsync(d_rwood_, wood, wood_bytes, cudaMemcpyHostToDevice, q));
+  else CFG_CUDA(cudaMemsetAsync(d_rwood_, 0, wood_bytes, q));
+  launch_render(d_scenes_, s, rp, d_rwood_, width, height, d_image_, q);
+  CFG_CUDA(cudaGetLastError());
+  CFG_CUDA(cudaMemcpyAsync(rgba, d_image_, bytes, cudaMemcpyDeviceToHost, q));
+  CFG_CUDA(cudaStreamSynchronize(q));
+  return CFG_OK;
+}
+
+// Renderer.writeParams as the app calls it (js/render.js:41-53, js/main.js:268-271)
+int Engine::render_defaults(int s, cfg_render_params* rp) {
+  if (!rp) return fail(CFG_ERR_INVAL, "rp is null");
+  const Scene& sc = scenes_[s];
+  const double ground = 0.03;   // GROUND, js/render.js:6
+  rp->view = 0;
+  rp->nPieces = std::min(std::max(sc.host.nPieces, 0), MAX_PIECES);
+  rp->exposure = 1.0f;          // Math.pow(2, 0)
+  rp->width = (float)(sc.nx * sc.dxd);
+  rp->height = (float)(sc.ny * sc.dxd);
+  rp->ground = (float)ground;
+  rp->time = (float)sc.time;
+  rp->tmax = 1800.0f;
+  rp->chemi = (float)3e-7;
+  rp->camX = 0.0f;
+  rp->camY = (float)(-ground);
+  rp->zoom = 1.0f;
+  return CFG_OK;
+}
+
 int Engine::field_ptr(int s, const std::string& nm, char** base, size_t* elem, int* w, int* h, size_t* pitch) {
   const Scene& sc = scenes_[s];
   const SceneDesc& d = sc.desc;
@@ -695,6 +746,7 @@ int Engine::field_ptr(int s, const std::string& nm, char** base, size_t* elem, i
   if (nm == "Y2") return set(d.Y2, 16, sc.nx, sc.ny, d.pc);
   if (nm == "SQ") return set(d.SQ, 8, sc.nx, sc.ny, d.pc);
   if (nm == "cellG") return set(d.cellG, 8, sc.nx, sc.ny, d.pc);
+  if (nm == "rad") return set(d.rad, 16, RAD_LEN, 1, RAD_LEN);   // encodeRadiation's output (vec4f per target)
   if (nm == "Uh" || nm == "Vh" || nm == "Th" || nm == "Yh")
     return fail(CFG_ERR_NOENT, "field " + nm + " is not kept: the first-order advection values live in shared memory only");
   std::string b = nm; int l = 0;

@@ -100,6 +100,9 @@ class Engine {
   int set_cfl(int s, double cfl, double dt_cap);
   int set_nray(int s, int nray);
   int readback(int s, int32_t* acc, float* rad, int32_t* faceW);
+  // render.wgsl's fragment stage into a host RGBA float image (wood: MAX_PIECES x 12 floats or null)
+  int render(int s, const cfg_render_params& rp, const float* wood, int width, int height, float* rgba);
+  int render_defaults(int s, cfg_render_params* rp);
   int field_size(int s, const char* name, size_t* count);
   int read_field(int s, const char* name, float* out, size_t count);
   int write_field(int s, const char* name, const float* in, size_t count);
@@ -182,6 +185,9 @@ class Engine {
   double* d_dxd_ = nullptr;
   double* d_alpha_ = nullptr;
   double* d_scratch_ = nullptr;   // small FP64 outputs (budgets, norms)
+  float* d_rwood_ = nullptr;      // the renderer's wood buffer (MAX_PIECES x 12 floats)
+  float* d_image_ = nullptr;      // the renderer's output image
+  size_t image_bytes_ = 0;
   Work* d_wl_[WL_COUNT] = {};
   int nwl_[WL_COUNT] = {};
   int mode_ = CFG_SOLVE_FIXED, ncycles_ = 1, max_cycles_ = 50;

@@ -109,5 +109,8 @@ void launch_radiation(const SceneDesc* scenes, int scene, int ntargets, int nray
 void launch_budgets(const SceneDesc* scenes, int scene, double* out, cudaStream_t st);
 // ||r||2 and ||rhs||2 of level 0 of one scene into out[2] (device, FP64)
 void launch_residual_norms(const SceneDesc* scenes, int scene, double* out, cudaStream_t st);
+// render.wgsl's fragment stage of one scene: W x H float4 pixels, row 0 at the top
+void launch_render(const SceneDesc* scenes, int scene, const cfg_render_params& rp, const float* wood, int width,
+                   int height, float* out, cudaStream_t st);
 
 }  // namespace cfg

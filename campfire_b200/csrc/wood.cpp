@@ -191,10 +191,21 @@ int WoodScene::remove(int slot) {
 
 int WoodScene::upload() {
   std::vector<float> data((size_t)MAX_PIECES * PIECE_FLOATS, 0.f);
+  std::fill(render_wood_.begin(), render_wood_.end(), 0.f);
   int n = 0;
   for (int s = 0; s < (int)slots_.size(); s++) {
     const WoodSlot& p = slots_[s];
     if (!p.used) continue;
+    // the renderer's wood buffer (main.js:200-203)
+    float* r = render_wood_.data() + (size_t)s * 12;
+    for (int f = 0; f < 4; f++) {
+      r[f] = (float)p.wood.Tp[f];
+      r[4 + f] = (float)p.wood.d[f];
+    }
+    r[8] = (float)p.wood.charFraction();
+    r[9] = (float)p.wood.Tc;
+    r[10] = (float)((p.vis[0] + p.vis[1] + p.vis[2] + p.vis[3]) / 4);
+    r[11] = p.wood.mv > 0 ? 1.f : 0.f;
     float* o = data.data() + (size_t)s * PIECE_FLOATS;
     const float body[8] = {(float)p.x, (float)p.y, (float)p.angle, (float)p.wood.half(), 0.f, 0.f, 0.f, 1.f};
     std::memcpy(o, body, sizeof body);

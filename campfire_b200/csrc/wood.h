@@ -57,6 +57,9 @@ class WoodScene {
   int frame(double sim_dt, int* nsteps);
   const WoodSlot* slot(int s) const { return (s >= 0 && s < (int)slots_.size() && slots_[s].used) ? &slots_[s] : nullptr; }
   double hrr = 0, rad = 0, tmax = 0;   // stats of the last readback (main.js:225-229, before smoothing)
+  // the renderer's wood buffer built with the last upload (main.js:188-207): 64 x {Tp[4], d[4],
+  // char fraction, Tcore, mean visible irradiance, has virgin wood}
+  const std::vector<float>& render_wood() const { return render_wood_; }
 
  private:
   int upload();
@@ -66,6 +69,7 @@ class WoodScene {
   WoodCtl ctl_;
   std::vector<WoodSlot> slots_ = std::vector<WoodSlot>(64);
   double sim_acc_ = 0;
+  std::vector<float> render_wood_ = std::vector<float>(64 * 12, 0.f);
 };
 
 }  // namespace cfg

@@ -5,6 +5,8 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
+
 from . import _lib
 from ._lib import CfgWoodPiece, check
 
@@ -90,6 +92,12 @@ class WoodScene:
         d = {k: (list(getattr(st, k)) if isinstance(getattr(st, k), ctypes.Array) else getattr(st, k))
              for k, _ in CfgWoodPiece._fields_ if k != "pad"}
         return d, list(qc), list(qi)
+
+    def render_data(self) -> np.ndarray:
+        """The renderer's wood buffer (64 x 12 float32) of the last upload (js/main.js:188-207)."""
+        out = np.zeros(64 * 12, np.float32)
+        check(_lib.lib().cfg_wood_render_data(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
 
     def stats(self):
         h, r, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

@@ -276,6 +276,27 @@ int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, dou
 /* heat release rate and radiative loss (W per m depth) and max T of the last frame (js/main.js:225-229) */
 int cfg_wood_stats(cfg_wood* w, double* hrr, double* rad, double* tmax);
 
+/* ---- headless renderer: the fragment stage of shaders/render.wgsl (fs :189-273) for one
+ * scene into an RGBA float image, in place of Renderer.encode's swapchain pass (js/render.js:
+ * 57-70). Pixel (x, y), row 0 at the top, is shaded at uv = ((x + 0.5) / W, 1 - (y + 0.5) / H);
+ * the values are the fragment output (sRGB-encoded in view 0) before 8-bit quantisation. */
+typedef struct cfg_render_params {    /* the uniform RP (render.wgsl:13-17, js/render.js:41-53) */
+  int32_t view;                       /* VIEWS (js/render.js:5): 0 photo, 1 temperature, 2 reaction,
+                                         3 oxygen, 4 fuel, 5 velocity, 6 soot */
+  int32_t nPieces;                    /* pieces scanned (0..64) */
+  float exposure, width, height, ground, time, tmax, chemi, camX, camY, zoom;
+} cfg_render_params;
+/* Renderer.writeParams's values for this scene (js/render.js:41-53, js/main.js:268-271): view 0,
+ * the scene's nPieces, exposure 1, width/height the domain, ground 0.03 m, time the scene's
+ * clock, tmax 1800 K, chemi 3e-7, camera (0, -ground), zoom 1 */
+int cfg_render_defaults(cfg_sim* sim, cfg_render_params* rp);
+/* Renders into rgba (width * height * 4 floats, host). wood: the renderer's wood buffer
+ * (64 pieces x 12 floats: Tp[4], d[4], char fraction, Tcore, mean visible irradiance,
+ * has virgin wood; js/main.js:200-203), or NULL for zeros. */
+int cfg_render(cfg_sim* sim, const cfg_render_params* rp, const float* wood, int width, int height, float* rgba);
+/* The wood buffer of a wood scene's pieces as uploadPieces builds it (js/main.js:188-207) */
+int cfg_wood_render_data(cfg_wood* w, float* wood);
+
 /* ---- serving: jobs of several grid sizes in resident batch slots (no counterpart in the
  * reference). One batch holds slots[c] scenes of size class c (nx[c] x ny[c]); a job is
  * admitted into a free slot of its class once it has arrived and the bytes of the slots in

@@ -60,6 +60,7 @@ def _declare(L, pfx):
                      ctypes.POINTER(ctypes.c_int32)],
         "budgets": [vp, dp], "info": [vp, dp], "level_dims": [vp, ci, ctypes.POINTER(ctypes.c_int)],
         "pressure_residual": [vp, dp], "set_coarse_solve": [vp, ci], "set_krylov": [vp, ci],
+        "render": [vp, vp, ctypes.POINTER(ctypes.c_float), ci, ci, ctypes.POINTER(ctypes.c_float)],
     }
     for name, args in sigs.items():
         fn = getattr(L, pfx + name, None)
@@ -176,6 +177,17 @@ class OracleSim:
     def clear_geometry(self): self._chk(self._f.clear_geometry(self._h))
     def geometry(self): self._chk(self._f.geometry(self._h))
     def radiation(self): self._chk(self._f.radiation(self._h))
+
+    def render(self, rp: bytes, wood, width: int, height: int) -> np.ndarray:
+        """render.wgsl's fragment stage (translated reference only): float32 [height, width, 4], row 0 at the top.
+        rp: the 48-byte RP uniform; wood: 64 x 12 float32 or None."""
+        out = np.zeros((height, width, 4), np.float32)
+        rb = ctypes.create_string_buffer(bytes(rp), 48)
+        w = None if wood is None else np.ascontiguousarray(np.asarray(wood, np.float32).ravel())
+        wp = None if w is None else w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        self._chk(self._f.render(self._h, ctypes.cast(rb, ctypes.c_void_p), wp, width, height,
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
     def step(self, n=1): self._chk(self._f.step(self._h, n))
     def vcycle(self, nu=2): self._chk(self._f.vcycle(self._h, nu))
     def stage(self, name): self._chk(self._f.stage(self._h, name.encode()))
@@ -194,6 +206,8 @@ class OracleSim:
             return 4 * nx * ny
         if name in ("SQ", "cellG"):
             return 2 * nx * ny
+        if name == "rad":
+            return 320 * 4
         d = (ctypes.c_int * 2)()
         self._chk(self._f.level_dims(self._h, lvl, d))
         lx, ly = d[0], d[1]

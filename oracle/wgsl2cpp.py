@@ -22,10 +22,10 @@ import os
 import re
 import sys
 
-SHADERS = ["advect", "diffuse", "sources", "forces", "pressure", "geometry", "radiation"]
+SHADERS = ["advect", "diffuse", "sources", "forces", "pressure", "geometry", "radiation", "render"]
 TYPE_MAP = {"f32": "float", "i32": "int32_t", "u32": "uint32_t", "bool": "bool",
-            "vec2f": "vec2f", "vec3u": "vec3u", "vec4f": "vec4f", "vec2i": "vec2i"}
-CPP_RESERVED = {"main": "main_", "near": "near_", "far": "far_", "union": "union_"}
+            "vec2f": "vec2f", "vec3f": "vec3f", "vec3u": "vec3u", "vec4f": "vec4f", "vec2i": "vec2i"}
+CPP_RESERVED = {"main": "main_", "near": "near_", "far": "far_", "union": "union_", "char": "char_"}
 
 
 # ----------------------------------------------------------------------------- js/gpu.js samplers
@@ -296,7 +296,14 @@ class Translator:
                 self.take("{")
                 fields = []
                 while self.peek()[1] != "}":
-                    fname = self.take()
+                    while self.peek()[1] == "@":   # @builtin(position), @location(n): interface attributes
+                        self.take("@")
+                        self.take()
+                        if self.peek()[1] == "(":
+                            self.take("(")
+                            self.expr_until({")"})
+                            self.take(")")
+                    fname = CPP_RESERVED.get(self.take(), None) or self.t[self.i - 1][1]
                     self.take(":")
                     fty = self.ctype(self.parse_type())
                     fields.append(f"  {fty} {fname};")
@@ -359,8 +366,26 @@ class Translator:
                 ret = "void"
                 if self.peek()[1] == "->":
                     self.take("->")
+                    while self.peek()[1] == "@":   # -> @location(0) vec4f
+                        self.take("@")
+                        self.take()
+                        self.take("(")
+                        self.expr_until({")"})
+                        self.take(")")
                     ret = self.ctype(self.parse_type())
                 cname = CPP_RESERVED.get(name, name)
+                if any(a[0] == "vertex" for a in attrs):
+                    # the full-screen triangle's vertex stage: the harness computes the
+                    # fragment's interpolated position itself, so the body is not needed
+                    depth = 0
+                    while True:
+                        v2 = self.take()
+                        depth += v2 == "{"
+                        depth -= v2 == "}"
+                        if depth == 0 and v2 == "}":
+                            break
+                    attrs = []
+                    continue
                 body = self.block("", cname)
                 self.protos.append(f"static {ret} {cname}({', '.join(params)});")
                 self.out += [f"static {ret} {cname}({', '.join(params)}) {{"] + body + ["}"]

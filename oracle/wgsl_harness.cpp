@@ -197,6 +197,24 @@ struct RefSim {
     bind("P", P); bind("T", T.data()); bind("Y", Y.data()); bind("pieces", pieces.data()); bind("rad", rad.data());
     dispatch_main_((uint32_t)(npieces() * 4 + 64), 1, 1);
   }
+  // Renderer.encode (js/render.js:57-70): the fragment stage at every pixel centre,
+  // row 0 at the top (uv.y = 1 - (y + 0.5) / H)
+  void render(const void* rp, const float* wood, int W, int H, float* out) {
+    using namespace wgsl_render;
+    std::vector<float> zero(64 * 12, 0.f);
+    bind("P", P); bind("R", const_cast<void*>(rp)); bind("T", T.data()); bind("Y", Y.data()); bind("SQ", SQ.data());
+    bind("pieces", pieces.data()); bind("U", U.data()); bind("V", V.data());
+    bind("wood", const_cast<float*>(wood ? wood : zero.data())); bind("rad", rad.data());
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        VSOut in;
+        in.pos = vec4f((float)x + 0.5f, (float)y + 0.5f, 0.f, 1.f);
+        in.uv = vec2f(((float)x + 0.5f) / (float)W, 1.0f - ((float)y + 0.5f) / (float)H);
+        const vec4f c = fs(in);
+        float* o = out + ((size_t)y * W + x) * 4;
+        o[0] = c.x; o[1] = c.y; o[2] = c.z; o[3] = c.w;
+      }
+  }
   std::vector<float>* field(const std::string& nm, int* lvl) {
     *lvl = -1;
     if (nm == "U") return &U; if (nm == "Uh") return &Uh; if (nm == "U2") return &U2;
@@ -204,6 +222,7 @@ struct RefSim {
     if (nm == "T") return &T; if (nm == "Th") return &Th; if (nm == "T2") return &T2;
     if (nm == "Y") return &Y; if (nm == "Yh") return &Yh; if (nm == "Y2") return &Y2;
     if (nm == "SQ") return &SQ; if (nm == "fx") return &fx; if (nm == "fy") return &fy;
+    if (nm == "rad") return &rad;
     std::string b = nm; int l = 0;
     const size_t dot = nm.find('.');
     if (dot != std::string::npos) { b = nm.substr(0, dot); l = std::atoi(nm.c_str() + dot + 1); }
@@ -245,6 +264,9 @@ int wref_upload_pieces(void* h, const float* data, int n) {
 int wref_clear_geometry(void* h) { std::fill(S(h)->faceW.begin(), S(h)->faceW.end(), 0); return 0; }
 int wref_geometry(void* h) { return guard([&] { S(h)->geometry(); return 0; }); }
 int wref_radiation(void* h) { return guard([&] { S(h)->radiation(); return 0; }); }
+int wref_render(void* h, const void* rp, const float* wood, int W, int H, float* out) {
+  return guard([&] { S(h)->render(rp, wood, W, H, out); return 0; });
+}
 int wref_step(void* h, int n) { return guard([&] { for (int i = 0; i < n; i++) S(h)->step(); return 0; }); }
 int wref_vcycle(void* h, int) { return guard([&] { S(h)->vcycle(); return 0; }); }
 int wref_stage(void* h, const char* st) { return guard([&] { S(h)->stage(st); return 0; }); }

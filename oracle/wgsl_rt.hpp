@@ -60,17 +60,33 @@ struct vec2f {
   template <class A> explicit vec2f(A a) : x(F(a)), y(F(a)) {}
   template <class A, class B> vec2f(A a, B b) : x(F(a)), y(F(b)) {}
 };
+struct vec3f {
+  float x, y, z;
+  vec3f() = default;
+  vec3f(const vec3f&) = default;
+  template <class A> explicit vec3f(A a) : x(F(a)), y(F(a)), z(F(a)) {}
+  template <class A, class B, class C> vec3f(A a, B b, C c) : x(F(a)), y(F(b)), z(F(c)) {}
+  float operator[](int32_t i) const { return i == 0 ? x : i == 1 ? y : z; }
+};
 struct vec4f {
   float x, y, z, w;
   vec4f() = default;
   vec4f(const vec4f&) = default;
   template <class A> explicit vec4f(A a) : x(F(a)), y(F(a)), z(F(a)), w(F(a)) {}
   template <class A, class B, class C, class D> vec4f(A a, B b, C c, D d) : x(F(a)), y(F(b)), z(F(c)), w(F(d)) {}
+  template <class A> vec4f(vec3f v, A a) : x(v.x), y(v.y), z(v.z), w(F(a)) {}
   float operator[](uint32_t i) const { return i == 0 ? x : i == 1 ? y : i == 2 ? z : w; }
   float operator[](int32_t i) const { return (*this)[(uint32_t)i]; }
 };
+struct vec2i {
+  int32_t x, y;
+  vec2i() = default;
+  vec2i(int32_t a, int32_t b) : x(a), y(b) {}
+  explicit vec2i(vec2f v);   // i32(f32) per component: truncating, saturating
+};
 struct vec3u { uint32_t x, y, z; };
 struct bvec2 { bool x, y; };
+struct bvec3 { bool x, y, z; };
 struct bvec4 { bool x, y, z, w; };
 
 inline vec2f operator+(vec2f a, vec2f b) { return {a.x + b.x, a.y + b.y}; }
@@ -89,6 +105,22 @@ template <class S> inline vec4f operator*(S s, vec4f a) { const float f = F(s); 
 template <class S> inline vec4f operator*(vec4f a, S s) { const float f = F(s); return {a.x * f, a.y * f, a.z * f, a.w * f}; }
 template <class S> inline vec4f operator/(vec4f a, S s) { const float f = F(s); return {a.x / f, a.y / f, a.z / f, a.w / f}; }
 inline vec4f& operator+=(vec4f& a, vec4f b) { a = a + b; return a; }
+inline vec4f operator-(vec4f a) { return {-a.x, -a.y, -a.z, -a.w}; }
+template <class S> inline vec2f operator-(S s, vec2f a) { const float f = F(s); return {f - a.x, f - a.y}; }
+// vec3f (the renderer's colours)
+inline vec3f operator+(vec3f a, vec3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline vec3f operator-(vec3f a, vec3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline vec3f operator*(vec3f a, vec3f b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline vec3f operator/(vec3f a, vec3f b) { return {a.x / b.x, a.y / b.y, a.z / b.z}; }
+template <class S> inline vec3f operator*(S s, vec3f a) { const float f = F(s); return {f * a.x, f * a.y, f * a.z}; }
+template <class S> inline vec3f operator*(vec3f a, S s) { const float f = F(s); return {a.x * f, a.y * f, a.z * f}; }
+template <class S> inline vec3f operator/(vec3f a, S s) { const float f = F(s); return {a.x / f, a.y / f, a.z / f}; }
+template <class S> inline vec3f operator+(vec3f a, S s) { const float f = F(s); return {a.x + f, a.y + f, a.z + f}; }
+template <class S> inline vec3f operator-(vec3f a, S s) { const float f = F(s); return {a.x - f, a.y - f, a.z - f}; }
+template <class S> inline vec3f operator+(S s, vec3f a) { const float f = F(s); return {f + a.x, f + a.y, f + a.z}; }
+inline vec3f operator-(vec3f a) { return {-a.x, -a.y, -a.z}; }
+inline vec3f& operator+=(vec3f& a, vec3f b) { a = a + b; return a; }
+inline bvec3 operator<=(vec3f a, vec3f b) { return {a.x <= b.x, a.y <= b.y, a.z <= b.z}; }
 inline vec2f& operator+=(vec2f& a, vec2f b) { a = a + b; return a; }
 inline bvec2 operator<(vec2f a, vec2f b) { return {a.x < b.x, a.y < b.y}; }
 inline bvec4 operator>=(vec4f a, vec4f b) { return {a.x >= b.x, a.y >= b.y, a.z >= b.z, a.w >= b.w}; }
@@ -117,6 +149,8 @@ inline float max(float a, AF b) { return max(a, (float)b.v); }
 inline vec2f min(vec2f a, vec2f b) { return {min(a.x, b.x), min(a.y, b.y)}; }
 inline vec2f max(vec2f a, vec2f b) { return {max(a.x, b.x), max(a.y, b.y)}; }
 inline vec4f min(vec4f a, vec4f b) { return {min(a.x, b.x), min(a.y, b.y), min(a.z, b.z), min(a.w, b.w)}; }
+inline vec3f min(vec3f a, vec3f b) { return {min(a.x, b.x), min(a.y, b.y), min(a.z, b.z)}; }
+inline vec3f max(vec3f a, vec3f b) { return {max(a.x, b.x), max(a.y, b.y), max(a.z, b.z)}; }
 inline vec4f max(vec4f a, vec4f b) { return {max(a.x, b.x), max(a.y, b.y), max(a.z, b.z), max(a.w, b.w)}; }
 template <class E, class L, class H> inline auto clamp(E e, L lo, H hi) { return min(max(e, lo), hi); }
 inline float clamp(float e, AF lo, AF hi) { return min(max(e, (float)lo.v), (float)hi.v); }
@@ -130,6 +164,7 @@ inline int select(int f, int t, bool c) { return c ? t : f; }
 inline uint32_t select(uint32_t f, uint32_t t, bool c) { return c ? t : f; }
 inline vec2f select(vec2f f, vec2f t, bvec2 c) { return {c.x ? t.x : f.x, c.y ? t.y : f.y}; }
 inline vec2f select(vec2f f, vec2f t, bool c) { return c ? t : f; }
+inline vec3f select(vec3f f, vec3f t, bvec3 c) { return {c.x ? t.x : f.x, c.y ? t.y : f.y, c.z ? t.z : f.z}; }
 
 inline float abs(float x) { return std::fabs(x); }
 inline vec2f abs(vec2f v) { return {std::fabs(v.x), std::fabs(v.y)}; }
@@ -146,10 +181,22 @@ inline float sin(float x) { return std::sin(x); }
 inline float atan2(float y, float x) { return std::atan2(y, x); }
 inline float sqrt(float x) { return std::sqrt(x); }
 inline float length(vec2f v) { return std::sqrt(v.x * v.x + v.y * v.y); }
+inline vec2f fract(vec2f v) { return {fract(v.x), fract(v.y)}; }
+inline vec3f exp(vec3f v) { return {exp(v.x), exp(v.y), exp(v.z)}; }
+inline vec4f exp(vec4f v) { return {exp(v.x), exp(v.y), exp(v.z), exp(v.w)}; }
+inline vec3f pow(vec3f a, vec3f b) { return {pow(a.x, b.x), pow(a.y, b.y), pow(a.z, b.z)}; }
+inline float dot(vec2f a, vec2f b) { return a.x * b.x + a.y * b.y; }
+inline float dot(vec3f a, vec3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// smoothstep(low, high, x) = t * t * (3 - 2 t), t = clamp((x - low) / (high - low), 0, 1)
+inline float smoothstep(float lo, float hi, float x) {
+  const float t = min(max((x - lo) / (hi - lo), 0.f), 1.f);
+  return t * t * (3.f - 2.f * t);
+}
 inline float round(float x) { return std::nearbyint(x); }
 // mix(a, b, t) = a * (1 - t) + b * t
 inline float mix(float a, float b, float t) { return a * (1.f - t) + b * t; }
 inline vec4f mix(vec4f a, vec4f b, float t) { return {mix(a.x, b.x, t), mix(a.y, b.y, t), mix(a.z, b.z, t), mix(a.w, b.w, t)}; }
+inline vec3f mix(vec3f a, vec3f b, float t) { return {mix(a.x, b.x, t), mix(a.y, b.y, t), mix(a.z, b.z, t)}; }
 
 // conversions: f32 -> i32/u32 truncate toward zero and saturate
 inline int32_t conv_i32(float v) {
@@ -171,6 +218,7 @@ inline float conv_f32(float v) { return v; }
 inline float conv_f32(int32_t v) { return (float)v; }
 inline float conv_f32(uint32_t v) { return (float)v; }
 inline float conv_f32(AF v) { return (float)v.v; }
+inline vec2i::vec2i(vec2f v) : x(conv_i32(v.x)), y(conv_i32(v.y)) {}
 template <class T, class V> inline T conv(V v) { return (T)cv(v); }
 inline uint32_t bitcast_uint32_t(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
 inline float bitcast_float(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }

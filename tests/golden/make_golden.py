@@ -16,6 +16,9 @@ Each fixture holds, for one seeded scene:
   st_<stage>_<field>
             the fields each stage writes, stage by stage, during one more step
   rad       encodeRadiation after that step
+  rnd_*     (cases in RENDER_CASES) render.wgsl's fragment stage on that final state:
+            per image k the 48-byte RP uniform rnd_rp_k and the RGB image rnd_img_k
+            (row 0 at the top; alpha is 1), with the seeded wood buffer rnd_wood
 
     python tests/golden/make_golden.py            # rewrite the fixtures
 """
@@ -24,6 +27,7 @@ from __future__ import annotations
 import glob
 import hashlib
 import os
+import struct
 import subprocess
 import sys
 
@@ -54,6 +58,8 @@ CASES = [
      {"diffMult": 200.0, "heaterX0": 0.1, "heaterX1": 0.2, "heaterY1": 0.03, "heaterT": 900.0,
       "burnerX0": 0.25, "burnerX1": 0.3, "burnerFlux": 0.02, "burnerT": 600.0}),
 ]
+RENDER_CASES = ("logs_32x48", "tepee_diff3_40x64")
+GROUND = 0.03   # js/render.js:6
 
 
 def shader_digest(ref: str) -> str:
@@ -123,8 +129,49 @@ def make_case(om, cb, name, kind, nx, ny, width, seed, steps, extra):
     d["st_acc"] = s.readback()["acc"].astype(np.int32)
     s.radiation()
     d["rad"] = s.readback()["rad"].astype(np.float32)
+    if name in RENDER_CASES:
+        add_renders(s, d, seed)
     s.close()
     return d
+
+
+def render_uniform(view, npieces, width, height, cam=None, exposure=1.0, time=0.0, tmax=1800.0, chemi=3e-7):
+    """The RP uniform as Renderer.writeParams packs it (js/render.js:41-53)."""
+    cx, cy, zoom = cam if cam else (0.0, -GROUND, 1.0)
+    return struct.pack("<ii10f", view, npieces, exposure, width, height, GROUND, time, tmax, chemi, cx, cy, zoom)
+
+
+def wood_buffer(npieces, seed):
+    """A seeded renderer wood buffer (Tp[4], d[4], char fraction, Tcore, visAvg, hasVirgin per piece)."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros((64, 12), np.float32)
+    for n in range(npieces):
+        w[n, 0:4] = rng.uniform(550.0, 900.0, 4)
+        w[n, 4:8] = rng.uniform(0.5e-3, 6e-3, 4)
+        w[n, 8:12] = [rng.uniform(0.05, 0.6), rng.uniform(350.0, 600.0), rng.uniform(1e3, 2e4), float(n % 3 != 2)]
+    return w.ravel()
+
+
+def add_renders(s, d, seed):
+    inf = s.info()
+    nx, ny, dx = int(inf["nx"]), int(inf["ny"]), float(inf["dx"])
+    W, H = nx * dx, ny * dx
+    npc = int(d["in_npieces"])
+    wood = wood_buffer(npc, seed)
+    d["rnd_wood"] = wood
+    # a camera zoomed 4x on the lowest piece (the app's ?zoom=4&cx=..&cy=.. inspection view, js/main.js:70-80)
+    pcs = d["in_pieces"].reshape(64, 20)
+    j = int(np.argmin(np.where(pcs[:npc, 7] > 0, pcs[:npc, 1], 1e9)))
+    zoom = 4.0
+    cam = (float(pcs[j, 0]) - W / 2 / zoom, float(pcs[j, 1]) - (H + GROUND) / 2 / zoom, zoom)
+    shots = [(f"v{v}", render_uniform(v, npc, W, H, time=float(inf["time"])), 40, 62) for v in range(7)]
+    shots += [("v0_zoom", render_uniform(0, npc, W, H, cam=cam, exposure=2.0), 48, 72),
+              ("v1_zoom", render_uniform(1, npc, W, H, cam=cam, tmax=1500.0), 48, 72)]
+    for k, rp, w, h in shots:
+        img = s.render(rp, wood, w, h)
+        assert np.all(img[..., 3] == 1.0)
+        d["rnd_rp_" + k] = np.frombuffer(rp, np.uint8).copy()
+        d["rnd_img_" + k] = img[..., :3].copy()
 
 
 def apply_inputs(sim, d):
