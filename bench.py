@@ -337,6 +337,64 @@ def run_served(dev, stream, lams, njobs: int, steps_lo: int, steps_hi: int, slot
             "runs": out}
 
 
+APP_MODE = (224, 320, 0.003)    # the app's "balanced" grid (js/config.js:8), width 0.7 m
+APP_IMAGE = (734, 1080)          # a canvas 1080 pixels high with the domain's aspect (ground strip included)
+
+
+def run_app_frames(dev, stream, frames: int, warmup: int):
+    """The campfire app's frame (js/main.js:247-283) on its default scene (defaultScene, :132-155):
+    wood model step on the host, piece upload, geometry, the frame's gas steps (reference solver: one
+    V-cycle per step), radiation, the synchronous readback and the wood coupling, then the photo view
+    rendered into device memory. Wall-clock per frame with a stream synchronisation at its end."""
+    import numpy as np
+    import torch
+    import campfire_b200 as cb
+    from campfire_b200.render import Renderer, render_device
+    from campfire_b200.wood import WoodScene, default_scene
+    nx, ny, dt = APP_MODE
+    W, H = APP_IMAGE
+    sim = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": dt}, width=0.7).init()
+    sim.set_stream(stream.cuda_stream)
+    sim.set_solver(cb.SOLVE_FIXED, 1)
+    sim.writeParams()
+    sim.reset()
+    ws = WoodScene(sim)
+    npieces = len(default_scene(ws))
+    ren = Renderer(sim)
+    img = torch.empty(H * W * 4, dtype=torch.float32, device=dev)
+    frame_dt = 1.0 / 60.0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
+    steps = 0
+    wall = 0.0
+    for k in range(warmup + frames):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        n = ws.frame(frame_dt)
+        ren.writeParams({"view": 0, "exposure": 1.0, "time": sim.info()["time"]})
+        ren.writeWood(ws)
+        if k >= warmup:
+            ev[k - warmup][0].record(stream)
+        render_device(sim, ren.rp, W, H, img.data_ptr(), ren.wood)
+        if k >= warmup:
+            ev[k - warmup][1].record(stream)
+        stream.synchronize()
+        if k >= warmup:
+            wall += time.perf_counter() - t0
+            steps += n
+    render_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    st = ws.stats()
+    ws.close()
+    sim.close()
+    px = W * H
+    return {"scene": f"the app's default fire ({npieces} pieces: 7 coals, 2 logs, 7 sticks), {nx}x{ny} "
+                     f"cells, dt {dt}, one V-cycle per step", "frame_sim_dt_s": frame_dt, "frames": frames,
+            "warmup_frames": warmup, "image": [W, H], "frames_per_s": frames / wall,
+            "ms_per_frame": 1e3 * wall / frames, "gas_steps_per_frame": steps / frames,
+            "sim_time_per_wall_time": steps * dt / wall,
+            "render_ms": float(np.median(render_ms)), "render_mpixel_per_s": px / (np.median(render_ms) / 1e3) / 1e6,
+            "last_frame_stats": {"hrr_w_per_m": st["hrr"], "rad_w_per_m": st["rad"], "tmax_k": st["tmax"]}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -353,6 +411,9 @@ def main():
     ap.add_argument("--served-steps", type=int, nargs=2, default=(20, 200), metavar=("LO", "HI"),
                     help="steps per served job, uniform in [LO, HI]")
     ap.add_argument("--served-rates", type=float, nargs="+", default=(10.0, 100.0, 1000.0))
+    ap.add_argument("--app-frames", type=int, default=120,
+                    help="timed frames of the app frame measurement (wood coupling + gas steps + render) "
+                         "added to the line (0: skip)")
     ap.add_argument("--fp64-error-every", type=int, default=0,
                     help="with --fp64-error-steps S: run the workload beside the FP64 oracle for S steps and "
                          "report the field errors every this many steps (0: skip)")
@@ -511,6 +572,10 @@ def main():
         served = run_served(dev, stream, a.served_rates, a.served_jobs, a.served_steps[0], a.served_steps[1],
                             slots=12, budget=150e9, tol=1e-10)
 
+    app = None
+    if a.app_frames > 0:
+        app = run_app_frames(dev, stream, a.app_frames, 30)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         th = cpu_threads()
@@ -532,7 +597,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 204 + 16,
                         "d2h_bytes_per_step": 528 * 4 + 320 * 16 + 256 * 4},
                 "gpu_launches": launches * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "batched": batched, "served": served, "fp64_oracle_error": fp64_error}
+                "batched": batched, "served": served, "app_frame": app, "fp64_oracle_error": fp64_error}
         print(json.dumps(line))
     sim.close()
     if world > 1:

@@ -137,6 +137,8 @@ def lib():
         "cfg_wood_stats": [vp, dp, dp, dp], "cfg_wood_render_data": [vp, fp],
         "cfg_render_defaults": [vp, ctypes.POINTER(CfgRenderParams)],
         "cfg_render": [vp, ctypes.POINTER(CfgRenderParams), fp, ci, ci, fp],
+        "cfg_render_device": [vp, ctypes.POINTER(CfgRenderParams), fp, ci, ci, vp],
+        "cfg_wood_set": [vp, ci, ctypes.POINTER(CfgWoodPiece)],
         "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
         "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci, ci],
         "cfg_set_krylov": [vp, ci], "cfg_batch_set_krylov": [vp, ci],

@@ -94,6 +94,12 @@ int cfg_render(cfg_sim* sim, const cfg_render_params* rp, const float* wood, int
   if (!rp) return cfg::fail(CFG_ERR_INVAL, "rp is null");
   return guarded([&] { return sim->eng->render(sim->scene, *rp, wood, width, height, rgba); });
 }
+int cfg_render_device(cfg_sim* sim, const cfg_render_params* rp, const float* wood, int width, int height,
+                      void* rgba_device) {
+  SIM_OK(sim);
+  if (!rp) return cfg::fail(CFG_ERR_INVAL, "rp is null");
+  return guarded([&] { return sim->eng->render_device(sim->scene, *rp, wood, width, height, (float*)rgba_device); });
+}
 int cfg_field_size(cfg_sim* sim, const char* name, size_t* count) { SCENE_CALL(sim, field_size(sim->scene, name, count)); }
 int cfg_read_field(cfg_sim* sim, const char* name, float* out, size_t count) { SCENE_CALL(sim, read_field(sim->scene, name, out, count)); }
 int cfg_write_field(cfg_sim* sim, const char* name, const float* in, size_t count) { SCENE_CALL(sim, write_field(sim->scene, name, in, count)); }
@@ -382,6 +388,10 @@ int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, dou
   if (qConv4) for (int f = 0; f < 4; f++) qConv4[f] = p->qConv[f];
   if (qInc4) for (int f = 0; f < 4; f++) qInc4[f] = p->qInc[f];
   return CFG_OK;
+}
+int cfg_wood_set(cfg_wood* w, int slot, const cfg_wood_piece* state) {
+  if (!w || !state) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  return w->scene->set(slot, from_c(state));
 }
 int cfg_wood_render_data(cfg_wood* w, float* wood) {
   if (!w || !wood) return cfg::fail(CFG_ERR_INVAL, "null argument");

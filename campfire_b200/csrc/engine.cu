@@ -684,15 +684,29 @@ int Engine::readback(int s, int32_t* acc, float* rad, int32_t* faceW) {
 // Renderer.encode (js/render.js:57-70) into a device image instead of the canvas:
 // the wood buffer (Renderer.writeWood, :55) is uploaded, one thread per pixel runs
 // the fragment stage, and the image is copied back.
-int Engine::render(int s, const cfg_render_params& rp, const float* wood, int width, int height, float* rgba) {
+int Engine::render_device(int s, const cfg_render_params& rp, const float* wood, int width, int height,
+                          float* rgba_dev) {
   if (width < 1 || height < 1 || width > 16384 || height > 16384)
     return fail(CFG_ERR_INVAL, "image size must be in [1, 16384] x [1, 16384]");
   if (rp.nPieces < 0 || rp.nPieces > MAX_PIECES) return fail(CFG_ERR_INVAL, "nPieces must be in [0, 64]");
-  if (!rgba) return fail(CFG_ERR_INVAL, "rgba is null");
+  if (!rgba_dev || ((uintptr_t)rgba_dev & 15)) return fail(CFG_ERR_INVAL, "rgba must be a 16-byte aligned device pointer");
   CFG_TRY(activate());
   cudaStream_t q = st();
   const size_t wood_bytes = sizeof(float) * MAX_PIECES * 12;
   if (!d_rwood_) CFG_CUDA(cudaMalloc(&d_rwood_, wood_bytes));
+  if (wood) CFG_CUDA(cudaMemcpyAsync(d_rwood_, wood, wood_bytes, cudaMemcpyHostToDevice, q));
+  else CFG_CUDA(cudaMemsetAsync(d_rwood_, 0, wood_bytes, q));
+  launch_render(d_scenes_, s, rp, d_rwood_, width, height, rgba_dev, q);
+  CFG_CUDA(cudaGetLastError());
+  return CFG_OK;
+}
+
+int Engine::render(int s, const cfg_render_params& rp, const float* wood, int width, int height, float* rgba) {
+  if (width < 1 || height < 1 || width > 16384 || height > 16384)
+    return fail(CFG_ERR_INVAL, "image size must be in [1, 16384] x [1, 16384]");
+  if (!rgba) return fail(CFG_ERR_INVAL, "rgba is null");
+  CFG_TRY(activate());
+  cudaStream_t q = st();
   const size_t bytes = sizeof(float) * 4 * (size_t)width * height;
   if (bytes > image_bytes_) {
     CFG_CUDA(cudaStreamSynchronize(q));
@@ -701,10 +715,7 @@ int Engine::render(int s, const cfg_render_params& rp, const float* wood, int wi
     CFG_CUDA(cudaMalloc(&d_image_, bytes));
     image_bytes_ = bytes;
   }
-  if (wood) CFG_CUDA(cudaMemcpyAsync(d_rwood_, wood, wood_bytes, cudaMemcpyHostToDevice, q));
-  else CFG_CUDA(cudaMemsetAsync(d_rwood_, 0, wood_bytes, q));
-  launch_render(d_scenes_, s, rp, d_rwood_, width, height, d_image_, q);
-  CFG_CUDA(cudaGetLastError());
+  CFG_TRY(render_device(s, rp, wood, width, height, d_image_));
   CFG_CUDA(cudaMemcpyAsync(rgba, d_image_, bytes, cudaMemcpyDeviceToHost, q));
   CFG_CUDA(cudaStreamSynchronize(q));
   return CFG_OK;

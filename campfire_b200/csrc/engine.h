@@ -103,6 +103,7 @@ class Engine {
   // render.wgsl's fragment stage into a host RGBA float image (wood: MAX_PIECES x 12 floats or null)
   int render(int s, const cfg_render_params& rp, const float* wood, int width, int height, float* rgba);
   int render_defaults(int s, cfg_render_params* rp);
+  int render_device(int s, const cfg_render_params& rp, const float* wood, int width, int height, float* rgba_dev);
   int field_size(int s, const char* name, size_t* count);
   int read_field(int s, const char* name, float* out, size_t count);
   int write_field(int s, const char* name, const float* in, size_t count);

@@ -183,6 +183,13 @@ int WoodScene::add(double x, double y, double angle, double side, double density
   return slot;
 }
 
+int WoodScene::set(int slot, const WoodPiece& w) {
+  if (slot < 0 || slot >= (int)slots_.size() || !slots_[slot].used) return fail(CFG_ERR_NOENT, "no piece in this slot");
+  if (!(w.side > 0) || !(w.rhoV > 0) || !(w.rhoC > 0)) return fail(CFG_ERR_INVAL, "piece side and densities must be positive");
+  slots_[slot].wood = w;
+  return CFG_OK;
+}
+
 int WoodScene::remove(int slot) {
   if (slot < 0 || slot >= (int)slots_.size() || !slots_[slot].used) return fail(CFG_ERR_NOENT, "no piece in this slot");
   slots_[slot] = WoodSlot{};

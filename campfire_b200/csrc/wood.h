@@ -51,6 +51,8 @@ class WoodScene {
   int add(double x, double y, double angle, double side, double density, const double* preheat3,
           const double* faceT4);
   int remove(int slot);
+  // replace a piece's wood state (the app's defaultScene sets coal state directly, main.js:135-142)
+  int set(int slot, const WoodPiece& w);
   // one frame of main.js frame() with `sim_dt` of gas time: the wood steps on the
   // last readback, pieces are uploaded, geometry rebuilt, floor(sim_dt/dt) gas steps
   // (at most ceil(0.034/dt)) and radiation run, and the readback applied

@@ -50,6 +50,18 @@ def render(sim, rp: CfgRenderParams, width: int, height: int, wood=None) -> np.n
     return out
 
 
+def render_device(sim, rp: CfgRenderParams, width: int, height: int, rgba_device_ptr: int, wood=None) -> None:
+    """Enqueue one frame into device memory (width * height * 4 float32 at rgba_device_ptr) on the
+    scene's stream, without waiting (cfg_render_device)."""
+    w = None
+    if wood is not None:
+        w = np.ascontiguousarray(np.asarray(wood, np.float32).ravel())
+        if w.size != _lib.MAX_PIECES * WOOD_FLOATS:
+            raise ValueError(f"wood must hold {_lib.MAX_PIECES * WOOD_FLOATS} floats")
+    check(_lib.lib().cfg_render_device(sim._h, ctypes.byref(rp), None if w is None else _fp(w), int(width),
+                                       int(height), ctypes.c_void_p(int(rgba_device_ptr))))
+
+
 class Renderer:
     """js/render.js:8-71 for a FluidSim (or a batch scene view)."""
 

@@ -4,6 +4,7 @@ frame loop of js/main.js for pieces frozen in place."""
 from __future__ import annotations
 
 import ctypes
+import math
 
 import numpy as np
 
@@ -93,6 +94,23 @@ class WoodScene:
              for k, _ in CfgWoodPiece._fields_ if k != "pad"}
         return d, list(qc), list(qi)
 
+    def set_piece(self, slot: int, state: dict):
+        """Replace a piece's wood state (keys of piece()'s state dict; missing keys keep their value)."""
+        cur = self.piece(slot)
+        if cur is None:
+            raise _lib.CampfireError(-2, "no piece in this slot")
+        st = dict(cur[0], **state)
+        c = CfgWoodPiece()
+        for k, _ in CfgWoodPiece._fields_:
+            if k == "pad":
+                continue
+            v = st[k]
+            if isinstance(getattr(c, k), ctypes.Array):
+                getattr(c, k)[:] = [float(x) for x in v]
+            else:
+                setattr(c, k, int(v) if k == "dead" else float(v))
+        check(_lib.lib().cfg_wood_set(self._h, slot, ctypes.byref(c)))
+
     def render_data(self) -> np.ndarray:
         """The renderer's wood buffer (64 x 12 float32) of the last upload (js/main.js:188-207)."""
         out = np.zeros(64 * 12, np.float32)
@@ -103,3 +121,40 @@ class WoodScene:
         h, r, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         check(_lib.lib().cfg_wood_stats(self._h, ctypes.byref(h), ctypes.byref(r), ctypes.byref(t)))
         return {"hrr": h.value, "rad": r.value, "tmax": t.value}
+
+
+SCENE_WIDTH = 0.7   # js/config.js:3
+
+
+def default_scene(ws: WoodScene, char_yield: float = 0.25, density: float = 500.0) -> list:
+    """The app's pre-lit fire (defaultScene, js/main.js:132-155): a bed of seven glowing coals,
+    two logs flanking it and seven sticks piled on it. Returns the slots."""
+    cx, S = SCENE_WIDTH / 2, 0.0125
+    slots = []
+
+    def coal(x, y, sz, T):
+        s = ws.add(x, y, 0.0, sz, density, preheat=(T, sz, T - 30))
+        st, _, _ = ws.piece(s)
+        mc = st["rhoC"] * sz * sz
+        side = math.sqrt(0.0 / st["rhoV"] + mc / st["rhoC"])     # WoodPiece.updateSide with mv = 0
+        ws.set_piece(s, {"mv": 0.0, "mc": mc, "side": side, "d": [sz / 2] * 4, "charCov": [1.0] * 4,
+                         "Tp": [T - 20] * 4})
+        slots.append(s)
+
+    def lit(x, y, sz):
+        s = ws.add(x, y, 0.0, sz, density, preheat=(880.0, 0.003 if sz > 0.03 else 0.002, 380.0))
+        ws.set_piece(s, {"Tp": [590.0] * 4})
+        slots.append(s)
+
+    x = cx - 0.06
+    for sz in (0.016, 0.02, 0.015, 0.018, 0.02, 0.016, 0.017):
+        coal(x + sz / 2, sz / 2, sz, 1050.0)
+        x += sz + 0.0015
+    lit(cx - 0.093, 0.025, 0.05)
+    lit(cx + 0.093, 0.025, 0.05)
+    y1 = 0.02 + S + 0.001
+    for dx in (-0.045, -0.016, 0.013, 0.042):
+        lit(cx + dx, y1, 0.025)
+    for dx in (-0.03, 0.0, 0.028):
+        lit(cx + dx, y1 + 2 * S + 0.002, 0.025)
+    return slots

@@ -294,6 +294,12 @@ int cfg_render_defaults(cfg_sim* sim, cfg_render_params* rp);
  * (64 pieces x 12 floats: Tp[4], d[4], char fraction, Tcore, mean visible irradiance,
  * has virgin wood; js/main.js:200-203), or NULL for zeros. */
 int cfg_render(cfg_sim* sim, const cfg_render_params* rp, const float* wood, int width, int height, float* rgba);
+/* The same into device memory of the scene's GPU (width * height * 4 floats, 16-byte aligned),
+ * enqueued on the handle's stream without waiting (the wood buffer is copied before return). */
+int cfg_render_device(cfg_sim* sim, const cfg_render_params* rp, const float* wood, int width, int height,
+                      void* rgba_device);
+/* Replace the wood state of a piece (js/main.js:135-142 sets a coal's state this way) */
+int cfg_wood_set(cfg_wood* w, int slot, const cfg_wood_piece* state);
 /* The wood buffer of a wood scene's pieces as uploadPieces builds it (js/main.js:188-207) */
 int cfg_wood_render_data(cfg_wood* w, float* wood);
 

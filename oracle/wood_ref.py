@@ -229,3 +229,33 @@ class WoodScene:
         self.rad = int(acc[ACC_GLOBAL + 1]) / G_SCALE / simDt
         self.tmax = float(acc[ACC_GLOBAL + 2])
         return n
+
+
+def default_scene(scene, charYield=0.25, density=500.0):
+    """defaultScene, js/main.js:132-155, on a WoodScene of this module (SCENE_WIDTH 0.7 m)."""
+    cx, S = 0.7 / 2, 0.0125
+
+    def coal(x, y, sz, T):
+        w = scene.slots[scene.add(x, y, 0.0, sz, density, preheat=(T, sz, T - 30))]["wood"]
+        w.mv = 0
+        w.mc = w.rhoC * sz * sz
+        w.updateSide()
+        w.d = [sz / 2, sz / 2, sz / 2, sz / 2]
+        w.charCov = [1, 1, 1, 1]
+        w.Tp = [T - 20, T - 20, T - 20, T - 20]
+
+    def lit(x, y, sz):
+        w = scene.slots[scene.add(x, y, 0.0, sz, density, preheat=(880, 0.003 if sz > 0.03 else 0.002, 380))]["wood"]
+        w.Tp = [590, 590, 590, 590]
+
+    x = cx - 0.06
+    for sz in (0.016, 0.02, 0.015, 0.018, 0.02, 0.016, 0.017):
+        coal(x + sz / 2, sz / 2, sz, 1050)
+        x += sz + 0.0015
+    lit(cx - 0.093, 0.025, 0.05)
+    lit(cx + 0.093, 0.025, 0.05)
+    y1 = 0.02 + S + 0.001
+    for dx in (-0.045, -0.016, 0.013, 0.042):
+        lit(cx + dx, y1, 0.025)
+    for dx in (-0.03, 0.0, 0.028):
+        lit(cx + dx, y1 + 2 * S + 0.002, 0.025)

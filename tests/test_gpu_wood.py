@@ -83,3 +83,37 @@ def test_slots_and_errors():
     with pytest.raises(cb.CampfireError):
         ws.add(0.2, 0.03, 0.0, -1.0)
     ws.close(); g.close()
+
+
+def test_default_scene_matches_oracle(oracle_mod):
+    """The app's default fire (js/main.js:132-155) set up through cfg_wood_add/cfg_wood_set is the
+    oracle's exactly, and its first frames agree as above."""
+    from campfire_b200.wood import default_scene
+    from oracle.wood_ref import default_scene as ref_default_scene
+    nx, ny, dt = 112, 160, 0.004
+    g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": dt}, width=0.7).init()
+    g.writeParams()
+    g.reset()
+    o = oracle_mod.OracleSim(nx, ny, 0.7, dt)
+    o.write_params()
+    o.reset()
+    ws, rs = WoodScene(g), RefScene(o)
+    slots = default_scene(ws)
+    ref_default_scene(rs)
+    assert slots == list(range(16))
+    for s in slots:
+        a = ws.piece(s)[0]
+        w = rs.slots[s]["wood"]
+        for k in ("side", "mv", "mc", "Tc", "rhoV", "rhoC"):
+            assert a[k] == getattr(w, k), (s, k)
+        for k in ("Ts", "Tp", "d", "charCov"):
+            assert a[k] == [float(v) for v in getattr(w, k)], (s, k)
+    for k in range(2):
+        assert ws.frame(1 / 60) == rs.frame(1 / 60)
+        for s in slots:
+            a = ws.piece(s)[0]
+            w = rs.slots[s]["wood"]
+            for f in range(4):
+                assert rel(a["Ts"][f], w.Ts[f], 1.0) <= 1e-4, (k, s, f)
+            assert rel(a["mc"], w.mc, 1e-12) <= 1e-5
+    ws.close(); g.close()
