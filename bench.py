@@ -343,14 +343,15 @@ APP_IMAGE = (734, 1080)          # a canvas 1080 pixels high with the domain's a
 
 def run_app_frames(dev, stream, frames: int, warmup: int):
     """The campfire app's frame (js/main.js:247-283) on its default scene (defaultScene, :132-155):
-    wood model step on the host, piece upload, geometry, the frame's gas steps (reference solver: one
-    V-cycle per step), radiation, the synchronous readback and the wood coupling, then the photo view
+    the rigid bodies advance and exchange heat at their contacts, the wood model steps on the host,
+    pieces are uploaded and rasterised, the frame's gas steps run (reference solver: one V-cycle per
+    step), then radiation, the synchronous readback and the wood coupling, and the photo view is
     rendered into device memory. Wall-clock per frame with a stream synchronisation at its end."""
     import numpy as np
     import torch
     import campfire_b200 as cb
     from campfire_b200.render import Renderer, render_device
-    from campfire_b200.wood import WoodScene, default_scene
+    from campfire_b200.wood import WoodScene, app_rigid_options, default_scene
     nx, ny, dt = APP_MODE
     W, H = APP_IMAGE
     sim = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": dt}, width=0.7).init()
@@ -358,7 +359,7 @@ def run_app_frames(dev, stream, frames: int, warmup: int):
     sim.set_solver(cb.SOLVE_FIXED, 1)
     sim.writeParams()
     sim.reset()
-    ws = WoodScene(sim)
+    ws = WoodScene(sim, rigid=app_rigid_options())
     npieces = len(default_scene(ws))
     ren = Renderer(sim)
     img = torch.empty(H * W * 4, dtype=torch.float32, device=dev)
@@ -386,7 +387,7 @@ def run_app_frames(dev, stream, frames: int, warmup: int):
     ws.close()
     sim.close()
     px = W * H
-    return {"scene": f"the app's default fire ({npieces} pieces: 7 coals, 2 logs, 7 sticks), {nx}x{ny} "
+    return {"scene": f"the app's default fire ({npieces} moving pieces: 7 coals, 2 logs, 7 sticks), {nx}x{ny} "
                      f"cells, dt {dt}, one V-cycle per step", "frame_sim_dt_s": frame_dt, "frames": frames,
             "warmup_frames": warmup, "image": [W, H], "frames_per_s": frames / wall,
             "ms_per_frame": 1e3 * wall / frames, "gas_steps_per_frame": steps / frames,

@@ -75,6 +75,20 @@ class CfgRenderParams(ctypes.Structure):
                                                "camX", "camY", "zoom")]
 
 
+class CfgRigidParams(ctypes.Structure):
+    """RIGID_DEFAULTS of js/rigid.js:12-27."""
+    _fields_ = [("gravity", ctypes.c_double * 2), ("width", ctypes.c_double), ("dt", ctypes.c_double),
+                ("substeps", ctypes.c_int32), ("pad", ctypes.c_int32)] + \
+               [(n, ctypes.c_double) for n in ("slop", "contact_hertz", "contact_damping", "max_pushout", "mu_static",
+                                               "mu_kinetic", "stick_speed", "max_speed", "drag_hertz",
+                                               "drag_strength")]
+
+
+class CfgRigidBody(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int32), ("dragging", ctypes.c_int32)] + \
+               [(n, ctypes.c_double) for n in ("x", "y", "a", "vx", "vy", "w", "half", "density", "mass")]
+
+
 class CampfireError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -139,6 +153,19 @@ def lib():
         "cfg_render": [vp, ctypes.POINTER(CfgRenderParams), fp, ci, ci, fp],
         "cfg_render_device": [vp, ctypes.POINTER(CfgRenderParams), fp, ci, ci, vp],
         "cfg_wood_set": [vp, ci, ctypes.POINTER(CfgWoodPiece)],
+        "cfg_wood_set_rigid": [vp, ctypes.POINTER(CfgRigidParams)], "cfg_wood_rigid": [vp, ctypes.POINTER(vp)],
+        "cfg_wood_body": [vp, ci, ip],
+        "cfg_rigid_defaults": [ctypes.POINTER(CfgRigidParams)],
+        "cfg_rigid_create": [ctypes.POINTER(CfgRigidParams), ctypes.POINTER(vp)], "cfg_rigid_destroy": [vp],
+        "cfg_rigid_get_params": [vp, ctypes.POINTER(CfgRigidParams)],
+        "cfg_rigid_set_params": [vp, ctypes.POINTER(CfgRigidParams)],
+        "cfg_rigid_add": [vp, cd, cd, cd, cd, cd, ip], "cfg_rigid_remove": [vp, ci],
+        "cfg_rigid_resize": [vp, ci, cd], "cfg_rigid_set_density": [vp, ci, cd],
+        "cfg_rigid_step": [vp, cd, ci], "cfg_rigid_advance": [vp, cd],
+        "cfg_rigid_bodies": [vp, ctypes.POINTER(CfgRigidBody), ci, ip],
+        "cfg_rigid_get": [vp, ci, ctypes.POINTER(CfgRigidBody)], "cfg_rigid_pick": [vp, cd, cd, ip, dp, dp],
+        "cfg_rigid_drag_start": [vp, ci, cd, cd, cd, cd], "cfg_rigid_drag_move": [vp, ci, cd, cd],
+        "cfg_rigid_drag_end": [vp, ci], "cfg_rigid_max_penetration": [vp, dp], "cfg_rigid_contacts": [vp, ip, ip],
         "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
         "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci, ci],
         "cfg_set_krylov": [vp, ci], "cfg_batch_set_krylov": [vp, ci],

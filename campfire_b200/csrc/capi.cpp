@@ -294,12 +294,35 @@ extern "C" int cfg_batch_set_krylov(cfg_batch* b, int on) {
 }
 
 // ------------------------------------------------------------------ wood
+struct cfg_rigid {
+  cfg::RigidWorld* world;                   // owned (cfg_rigid_create) or a wood scene's (cfg_wood_rigid)
+  std::unique_ptr<cfg::RigidWorld> own;
+};
 struct cfg_wood {
   cfg::Engine* eng;
   std::unique_ptr<cfg::WoodScene> scene;
+  cfg_rigid view{nullptr, nullptr};
 };
 
 namespace {
+void to_c(const cfg::RigidParams& r, cfg_rigid_params* o) {
+  o->gravity[0] = r.gx; o->gravity[1] = r.gy; o->width = r.width; o->dt = r.dt;
+  o->substeps = r.substeps; o->pad = 0;
+  o->slop = r.slop; o->contact_hertz = r.contactHertz; o->contact_damping = r.contactDamping;
+  o->max_pushout = r.maxPushout; o->mu_static = r.muStatic; o->mu_kinetic = r.muKinetic;
+  o->stick_speed = r.stickSpeed; o->max_speed = r.maxSpeed; o->drag_hertz = r.dragHertz;
+  o->drag_strength = r.dragStrength;
+}
+int from_c(const cfg_rigid_params* o, cfg::RigidParams* r) {
+  if (!(o->dt > 0) || o->substeps < 1 || o->substeps > 64 || !(o->width > 0))
+    return cfg::fail(CFG_ERR_INVAL, "rigid world: dt and width must be > 0, substeps in [1, 64]");
+  r->gx = o->gravity[0]; r->gy = o->gravity[1]; r->width = o->width; r->dt = o->dt; r->substeps = o->substeps;
+  r->slop = o->slop; r->contactHertz = o->contact_hertz; r->contactDamping = o->contact_damping;
+  r->maxPushout = o->max_pushout; r->muStatic = o->mu_static; r->muKinetic = o->mu_kinetic;
+  r->stickSpeed = o->stick_speed; r->maxSpeed = o->max_speed; r->dragHertz = o->drag_hertz;
+  r->dragStrength = o->drag_strength;
+  return CFG_OK;
+}
 void to_c(const cfg::WoodPiece& w, cfg_wood_piece* o) {
   o->side = w.side; o->rhoV = w.rhoV; o->rhoC = w.rhoC; o->mv = w.mv; o->mc = w.mc; o->Tc = w.Tc; o->gasRate = w.gasRate;
   for (int f = 0; f < 4; f++) {
@@ -389,6 +412,27 @@ int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, dou
   if (qInc4) for (int f = 0; f < 4; f++) qInc4[f] = p->qInc[f];
   return CFG_OK;
 }
+int cfg_wood_set_rigid(cfg_wood* w, const cfg_rigid_params* p) {
+  if (!w) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  if (!p) return w->scene->set_rigid(nullptr);
+  cfg::RigidParams rp;
+  CFG_TRY(from_c(p, &rp));
+  return w->scene->set_rigid(&rp);
+}
+int cfg_wood_rigid(cfg_wood* w, cfg_rigid** world) {
+  if (!w || !world) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  if (!w->scene->world()) return cfg::fail(CFG_ERR_NOENT, "the pieces of this scene are frozen (no rigid world)");
+  w->view.world = w->scene->world();
+  *world = &w->view;
+  return CFG_OK;
+}
+int cfg_wood_body(cfg_wood* w, int slot, int* body_id) {
+  if (!w || !body_id) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  const cfg::WoodSlot* p = w->scene->slot(slot);
+  if (!p) return cfg::fail(CFG_ERR_NOENT, "no piece in this slot");
+  *body_id = p->body;
+  return CFG_OK;
+}
 int cfg_wood_set(cfg_wood* w, int slot, const cfg_wood_piece* state) {
   if (!w || !state) return cfg::fail(CFG_ERR_INVAL, "null argument");
   return w->scene->set(slot, from_c(state));
@@ -404,6 +448,146 @@ int cfg_wood_stats(cfg_wood* w, double* hrr, double* rad, double* tmax) {
   if (hrr) *hrr = w->scene->hrr;
   if (rad) *rad = w->scene->rad;
   if (tmax) *tmax = w->scene->tmax;
+  return CFG_OK;
+}
+
+// ------------------------------------------------------------------ rigid bodies (js/rigid.js)
+#define RIGID_OK(w) do { if (!(w) || !(w)->world) return cfg::fail(CFG_ERR_INVAL, "null cfg_rigid handle"); } while (0)
+int cfg_rigid_defaults(cfg_rigid_params* p) {
+  if (!p) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  to_c(cfg::RigidParams{}, p);
+  return CFG_OK;
+}
+int cfg_rigid_create(const cfg_rigid_params* p, cfg_rigid** out) {
+  if (!out) return cfg::fail(CFG_ERR_INVAL, "null output");
+  cfg::RigidParams rp;
+  if (p) CFG_TRY(from_c(p, &rp));
+  return guarded([&] {
+    auto* r = new cfg_rigid{nullptr, std::make_unique<cfg::RigidWorld>(rp)};
+    r->world = r->own.get();
+    *out = r;
+    return CFG_OK;
+  });
+}
+int cfg_rigid_destroy(cfg_rigid* w) {
+  if (!w) return CFG_OK;
+  if (!w->own) return cfg::fail(CFG_ERR_INVAL, "a wood scene's rigid world is destroyed with the scene");
+  delete w;
+  return CFG_OK;
+}
+int cfg_rigid_get_params(cfg_rigid* w, cfg_rigid_params* p) {
+  RIGID_OK(w);
+  if (!p) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  to_c(w->world->p, p);
+  return CFG_OK;
+}
+int cfg_rigid_set_params(cfg_rigid* w, const cfg_rigid_params* p) {
+  RIGID_OK(w);
+  if (!p) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  return from_c(p, &w->world->p);
+}
+int cfg_rigid_add(cfg_rigid* w, double x, double y, double half, double density, double angle, int* id) {
+  RIGID_OK(w);
+  if (!(half > 0) || !(density > 0)) return cfg::fail(CFG_ERR_INVAL, "half side and density must be positive");
+  return guarded([&] {
+    cfg::Body* b = w->world->add(x, y, half, density, angle);
+    if (id) *id = b->id;
+    return CFG_OK;
+  });
+}
+int cfg_rigid_remove(cfg_rigid* w, int id) {
+  RIGID_OK(w);
+  if (w->world->remove(id) != CFG_OK) return cfg::fail(CFG_ERR_NOENT, "no body with this id");
+  return CFG_OK;
+}
+static cfg::Body* rigid_body(cfg_rigid* w, int id) { return w->world->find(id); }
+int cfg_rigid_resize(cfg_rigid* w, int id, double half) {
+  RIGID_OK(w);
+  cfg::Body* b = rigid_body(w, id);
+  if (!b) return cfg::fail(CFG_ERR_NOENT, "no body with this id");
+  if (!(half > 0)) return cfg::fail(CFG_ERR_INVAL, "half side must be positive");
+  w->world->resize(b, half);
+  return CFG_OK;
+}
+int cfg_rigid_set_density(cfg_rigid* w, int id, double density) {
+  RIGID_OK(w);
+  cfg::Body* b = rigid_body(w, id);
+  if (!b) return cfg::fail(CFG_ERR_NOENT, "no body with this id");
+  if (!(density > 0)) return cfg::fail(CFG_ERR_INVAL, "density must be positive");
+  b->density = density;
+  return CFG_OK;
+}
+int cfg_rigid_step(cfg_rigid* w, double dt, int nsteps) {
+  RIGID_OK(w);
+  if (!(dt > 0) || nsteps < 0) return cfg::fail(CFG_ERR_INVAL, "dt must be > 0 and nsteps >= 0");
+  return guarded([&] { for (int i = 0; i < nsteps; i++) w->world->step(dt); return CFG_OK; });
+}
+int cfg_rigid_advance(cfg_rigid* w, double dt) {
+  RIGID_OK(w);
+  if (!(dt >= 0)) return cfg::fail(CFG_ERR_INVAL, "dt must be >= 0");
+  return guarded([&] { w->world->advance(dt); return CFG_OK; });
+}
+static void body_to_c(const cfg::Body& b, cfg_rigid_body* o) {
+  o->id = b.id; o->dragging = b.dragging ? 1 : 0;
+  o->x = b.x; o->y = b.y; o->a = b.a; o->vx = b.vx; o->vy = b.vy; o->w = b.w;
+  o->half = b.half; o->density = b.density; o->mass = b.mass;
+}
+int cfg_rigid_bodies(cfg_rigid* w, cfg_rigid_body* out, int capacity, int* count) {
+  RIGID_OK(w);
+  if (!count || (capacity > 0 && !out)) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  const auto& bs = w->world->bodies();
+  *count = (int)bs.size();
+  for (int i = 0; i < capacity && i < (int)bs.size(); i++) body_to_c(*bs[i], &out[i]);
+  return CFG_OK;
+}
+int cfg_rigid_get(cfg_rigid* w, int id, cfg_rigid_body* out) {
+  RIGID_OK(w);
+  if (!out) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  const cfg::Body* b = rigid_body(w, id);
+  if (!b) return cfg::fail(CFG_ERR_NOENT, "no body with this id");
+  body_to_c(*b, out);
+  return CFG_OK;
+}
+int cfg_rigid_pick(cfg_rigid* w, double x, double y, int* id, double* lx, double* ly) {
+  RIGID_OK(w);
+  if (!id) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  const cfg::Body* b = w->world->pick(x, y, lx, ly);
+  *id = b ? b->id : 0;
+  return CFG_OK;
+}
+int cfg_rigid_drag_start(cfg_rigid* w, int id, double lx, double ly, double tx, double ty) {
+  RIGID_OK(w);
+  cfg::Body* b = rigid_body(w, id);
+  if (!b) return cfg::fail(CFG_ERR_NOENT, "no body with this id");
+  w->world->start_drag(b, lx, ly, tx, ty);
+  return CFG_OK;
+}
+int cfg_rigid_drag_move(cfg_rigid* w, int id, double tx, double ty) {
+  RIGID_OK(w);
+  cfg::Body* b = rigid_body(w, id);
+  if (!b) return cfg::fail(CFG_ERR_NOENT, "no body with this id");
+  w->world->move_drag(b, tx, ty);
+  return CFG_OK;
+}
+int cfg_rigid_drag_end(cfg_rigid* w, int id) {
+  RIGID_OK(w);
+  cfg::Body* b = rigid_body(w, id);
+  if (!b) return cfg::fail(CFG_ERR_NOENT, "no body with this id");
+  w->world->end_drag(b);
+  return CFG_OK;
+}
+int cfg_rigid_max_penetration(cfg_rigid* w, double* pen) {
+  RIGID_OK(w);
+  if (!pen) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  *pen = w->world->max_penetration();
+  return CFG_OK;
+}
+int cfg_rigid_contacts(cfg_rigid* w, int* manifolds, int* points) {
+  RIGID_OK(w);
+  int np = 0;
+  for (const auto& m : w->world->manifolds()) np += m.npts;
+  if (manifolds) *manifolds = (int)w->world->manifolds().size();
+  if (points) *points = np;
   return CFG_OK;
 }
 }  // extern "C"

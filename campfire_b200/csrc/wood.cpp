@@ -43,6 +43,13 @@ WoodPiece::WoodPiece(double side_, double rhoV_, double T0) {
 
 void WoodPiece::updateSide() { side = std::sqrt(mv / rhoV + mc / rhoC); }
 
+double WoodPiece::surfaceCap(int f) const {
+  const double s = side;
+  const double dS = std::min(WoodK::deltaS, s / 8);
+  const double phi = mv <= 1e-9 ? 1 : std::min(1.0, d[f] / dS);
+  return (rhoV * WoodK::cv * (1 - phi) + rhoC * WoodK::cc * phi) * dS * s;
+}
+
 double WoodPiece::charFraction() const { return mc / rhoC / (mv / rhoV + mc / rhoC + 1e-12); }
 
 void WoodPiece::preheat(double Tsurf, double charDepth, double Tcore, double charYield) {
@@ -180,8 +187,29 @@ int WoodScene::add(double x, double y, double angle, double side, double density
       }
   const double qa = kSigma * std::pow(kTamb, 4);
   p.qInc = {qa, qa, qa, qa};
+  if (world_) {   // new Body(x, y, half, (mv + mc) / side^2, angle) (main.js:109-110)
+    Body* b = world_->add(x, y, p.wood.half(), (p.wood.mv + p.wood.mc) / (p.wood.side * p.wood.side), angle);
+    b->user = slot;
+    p.body = b->id;
+  }
   return slot;
 }
+
+int WoodScene::set_rigid(const RigidParams* rp) {
+  for (const auto& p : slots_)
+    if (p.used) return fail(CFG_ERR_BUSY, "the rigid world can be switched only while the scene has no pieces");
+  if (rp) world_ = std::make_unique<RigidWorld>(*rp);
+  else world_.reset();
+  return CFG_OK;
+}
+
+// the wood side of js/contact.js: a slot's surface temperatures and capacities
+struct SlotWood : ContactWood {
+  std::vector<WoodSlot>& slots;
+  explicit SlotWood(std::vector<WoodSlot>& s) : slots(s) {}
+  double& Ts(int user, int f) override { return slots[user].wood.Ts[f]; }
+  double surface_cap(int user, int f) override { return slots[user].wood.surfaceCap(f); }
+};
 
 int WoodScene::set(int slot, const WoodPiece& w) {
   if (slot < 0 || slot >= (int)slots_.size() || !slots_[slot].used) return fail(CFG_ERR_NOENT, "no piece in this slot");
@@ -192,6 +220,7 @@ int WoodScene::set(int slot, const WoodPiece& w) {
 
 int WoodScene::remove(int slot) {
   if (slot < 0 || slot >= (int)slots_.size() || !slots_[slot].used) return fail(CFG_ERR_NOENT, "no piece in this slot");
+  if (world_ && slots_[slot].body) world_->remove(slots_[slot].body);
   slots_[slot] = WoodSlot{};
   return CFG_OK;
 }
@@ -214,7 +243,10 @@ int WoodScene::upload() {
     r[10] = (float)((p.vis[0] + p.vis[1] + p.vis[2] + p.vis[3]) / 4);
     r[11] = p.wood.mv > 0 ? 1.f : 0.f;
     float* o = data.data() + (size_t)s * PIECE_FLOATS;
-    const float body[8] = {(float)p.x, (float)p.y, (float)p.angle, (float)p.wood.half(), 0.f, 0.f, 0.f, 1.f};
+    const Body* b = world_ && p.body ? world_->find(p.body) : nullptr;
+    const float body[8] = {(float)(b ? b->x : p.x), (float)(b ? b->y : p.y), (float)(b ? b->a : p.angle),
+                           (float)(b ? b->half : p.wood.half()), (float)(b ? b->vx : 0.0), (float)(b ? b->vy : 0.0),
+                           (float)(b ? b->w : 0.0), 1.f};
     std::memcpy(o, body, sizeof body);
     for (int f = 0; f < 4; f++) {
       o[8 + f] = (float)p.wood.Ts[f];
@@ -261,13 +293,29 @@ int WoodScene::frame(double sim_dt, int* nsteps) {
   int n = (int)std::floor(sim_acc_ / dt);
   if (n > maxSteps) { n = maxSteps; sim_acc_ = 0; } else sim_acc_ -= n * dt;
   const double simDt = n * dt;
+  // the bodies move and touching pieces exchange heat (:262-263; the simulation runs, so
+  // the rigid world advances by the frame's gas time)
+  if (world_) {
+    world_->advance(simDt);
+    SlotWood sw(slots_);
+    exchange_contacts(*world_, simDt, sw);
+  }
   // stepWood (:232-243): the wood advances on the last readback's heat inputs
   if (simDt > 0)
     for (auto& p : slots_) {
       if (!p.used) continue;
       p.wood.step(simDt, p.qConv, p.qInc, p.charPending, ctl_);
       p.charPending = {0, 0, 0, 0};
-      if (p.wood.dead) p = WoodSlot{};
+      if (p.wood.dead) {
+        if (world_ && p.body) world_->remove(p.body);
+        p = WoodSlot{};
+        continue;
+      }
+      if (world_ && p.body) {
+        Body* b = world_->find(p.body);
+        b->density = (p.wood.mv + p.wood.mc) / (p.wood.side * p.wood.side);
+        world_->resize(b, p.wood.half());
+      }
     }
   CFG_TRY(upload());
   CFG_TRY(eng_->write_params(scene_));

@@ -10,7 +10,10 @@
 #pragma once
 #include <array>
 #include <cstdint>
+#include <memory>
 #include <vector>
+
+#include "rigid.h"
 
 namespace cfg {
 
@@ -29,6 +32,7 @@ struct WoodPiece {
   WoodPiece(double side, double rhoV, double T0 = 293.15);   // js/wood.js:34-49
   double half() const { return 0.5 * side; }
   void updateSide();                                          // :60
+  double surfaceCap(int f) const;                             // :53-58
   double charFraction() const;                                // :61
   void preheat(double Tsurf, double charDepth, double Tcore, double charYield);   // :64-76
   // :82-181: heat inputs per face (qConv W/m, qInc W/m^2, char burnt kg/m)
@@ -36,10 +40,12 @@ struct WoodPiece {
             const std::array<double, 4>& charBurnt, const WoodCtl& ctl);
 };
 
-// A piece of the scene: its body (frozen: position and angle fixed, size from the wood)
+// A piece of the scene: its body (frozen: position and angle fixed, size from the
+// wood; moving: a body of the scene's rigid world)
 struct WoodSlot {
   bool used = false;
   double x = 0, y = 0, angle = 0;
+  int body = 0;                     // rigid body id (moving pieces), 0 when frozen
   WoodPiece wood;
   std::array<double, 4> qConv{}, qInc{}, vis{}, charPending{};
 };
@@ -47,6 +53,10 @@ struct WoodSlot {
 class WoodScene {
  public:
   WoodScene(Engine* eng, int scene, WoodCtl ctl) : eng_(eng), scene_(scene), ctl_(ctl) {}
+  // moving pieces: a rigid world (js/main.js:61, friction from the controls :93-94) that
+  // the frame advances before the wood step; only while the scene has no pieces
+  int set_rigid(const RigidParams* p);
+  RigidWorld* world() { return world_.get(); }
   // :103-119 (returns the slot, or a negative status when all 64 are taken)
   int add(double x, double y, double angle, double side, double density, const double* preheat3,
           const double* faceT4);
@@ -72,6 +82,8 @@ class WoodScene {
   std::vector<WoodSlot> slots_ = std::vector<WoodSlot>(64);
   double sim_acc_ = 0;
   std::vector<float> render_wood_ = std::vector<float>(64 * 12, 0.f);
+  std::unique_ptr<RigidWorld> world_;
+  friend struct SlotWood;
 };
 
 }  // namespace cfg

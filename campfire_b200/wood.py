@@ -51,13 +51,39 @@ class WoodPiece:
 class WoodScene:
     """The pieces of a FluidSim and the per-frame coupling (cfg_wood_frame)."""
 
-    def __init__(self, sim, charYield: float = 0.25, pyroMult: float = 1.0):
+    def __init__(self, sim, charYield: float = 0.25, pyroMult: float = 1.0, rigid=None):
+        """rigid: None for pieces frozen in place, or the rigid world's options (app_rigid_options()
+        for the app's world) for moving pieces."""
         h = ctypes.c_void_p()
         check(_lib.lib().cfg_wood_create(sim._h, charYield, pyroMult, ctypes.byref(h)))
         self._h = h.value
+        self._world = None
+        if rigid is not None:
+            from .rigid import to_params
+            check(_lib.lib().cfg_wood_set_rigid(self._h, ctypes.byref(to_params(dict(rigid)))))
+
+    @property
+    def world(self):
+        """The scene's RigidWorld (moving pieces), or None."""
+        if self._world is None:
+            from .rigid import RigidWorld
+            h = ctypes.c_void_p()
+            rc = _lib.lib().cfg_wood_rigid(self._h, ctypes.byref(h))
+            if rc == -2:
+                return None
+            check(rc)
+            self._world = RigidWorld(_handle=h.value)
+        return self._world
+
+    def body(self, slot: int):
+        """The rigid body of a moving piece."""
+        i = ctypes.c_int()
+        check(_lib.lib().cfg_wood_body(self._h, slot, ctypes.byref(i)))
+        return self.world.body(i.value) if i.value else None
 
     def close(self):
         if self._h:
+            self._world = None
             _lib.lib().cfg_wood_destroy(self._h)
             self._h = None
 
@@ -126,6 +152,12 @@ class WoodScene:
 SCENE_WIDTH = 0.7   # js/config.js:3
 
 
+def app_rigid_options(friction: float = 0.7) -> dict:
+    """The app's rigid world: walls at the scene width (js/main.js:61) and the friction control
+    (applyControls, :93-94)."""
+    return {"width": SCENE_WIDTH, "muStatic": friction, "muKinetic": 0.75 * friction}
+
+
 def default_scene(ws: WoodScene, char_yield: float = 0.25, density: float = 500.0) -> list:
     """The app's pre-lit fire (defaultScene, js/main.js:132-155): a bed of seven glowing coals,
     two logs flanking it and seven sticks piled on it. Returns the slots."""
@@ -139,6 +171,10 @@ def default_scene(ws: WoodScene, char_yield: float = 0.25, density: float = 500.
         side = math.sqrt(0.0 / st["rhoV"] + mc / st["rhoC"])     # WoodPiece.updateSide with mv = 0
         ws.set_piece(s, {"mv": 0.0, "mc": mc, "side": side, "d": [sz / 2] * 4, "charCov": [1.0] * 4,
                          "Tp": [T - 20] * 4})
+        b = ws.body(s) if ws.world is not None else None
+        if b is not None:   # p.body.density = w.mc / (sz * sz); world.resize(p.body, w.half)
+            b.density = mc / (sz * sz)
+            ws.world.resize(b, 0.5 * side)
         slots.append(s)
 
     def lit(x, y, sz):

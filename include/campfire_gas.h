@@ -276,6 +276,57 @@ int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, dou
 /* heat release rate and radiative loss (W per m depth) and max T of the last frame (js/main.js:225-229) */
 int cfg_wood_stats(cfg_wood* w, double* hrr, double* rad, double* tmax);
 
+/* ---- rigid bodies: the campfire app's 2D rigid-body world (js/rigid.js) on the host in double
+ * precision: square pieces per unit depth on a floor between two side walls, soft contacts with
+ * warm starting, Coulomb friction with static anchors, and the hand grip. */
+typedef struct cfg_rigid cfg_rigid;
+typedef struct cfg_rigid_params {    /* RIGID_DEFAULTS, js/rigid.js:12-27 */
+  double gravity[2];                 /* m/s^2 */
+  double width;                      /* side walls at x = 0 and x = width */
+  double dt;                         /* collision step (s) */
+  int32_t substeps, pad;
+  double slop, contact_hertz, contact_damping, max_pushout;
+  double mu_static, mu_kinetic, stick_speed, max_speed;
+  double drag_hertz, drag_strength;
+} cfg_rigid_params;
+typedef struct cfg_rigid_body {
+  int32_t id, dragging;
+  double x, y, a, vx, vy, w;         /* centre (m), angle (rad), velocities */
+  double half, density, mass;        /* half side (m), kg/m^3, kg per m depth */
+} cfg_rigid_body;
+int cfg_rigid_defaults(cfg_rigid_params* p);
+/* new RigidWorld(opts) (js/rigid.js:160-166); p NULL: the defaults */
+int cfg_rigid_create(const cfg_rigid_params* p, cfg_rigid** out);
+int cfg_rigid_destroy(cfg_rigid* w);
+int cfg_rigid_get_params(cfg_rigid* w, cfg_rigid_params* p);
+/* world.p = ... (js/main.js:93-94 sets the friction coefficients) */
+int cfg_rigid_set_params(cfg_rigid* w, const cfg_rigid_params* p);
+/* add(new Body(x, y, half, density, angle)) (:40-49, :167); *id > 0 */
+int cfg_rigid_add(cfg_rigid* w, double x, double y, double half, double density, double angle, int* id);
+int cfg_rigid_remove(cfg_rigid* w, int id);                                   /* :168-172 */
+int cfg_rigid_resize(cfg_rigid* w, int id, double half);                      /* :176-184 */
+int cfg_rigid_set_density(cfg_rigid* w, int id, double density);             /* body.density = ... */
+int cfg_rigid_step(cfg_rigid* w, double dt, int nsteps);                      /* step(dt) x nsteps, :271-346 */
+int cfg_rigid_advance(cfg_rigid* w, double dt);                               /* fixed steps of p.dt, :187-193 */
+/* the bodies in world order; *count = all of them, at most `capacity` written */
+int cfg_rigid_bodies(cfg_rigid* w, cfg_rigid_body* out, int capacity, int* count);
+int cfg_rigid_get(cfg_rigid* w, int id, cfg_rigid_body* out);
+/* the topmost body under (x, y) and the point in its frame; *id = 0 if none (:419-428) */
+int cfg_rigid_pick(cfg_rigid* w, double x, double y, int* id, double* lx, double* ly);
+int cfg_rigid_drag_start(cfg_rigid* w, int id, double lx, double ly, double tx, double ty);   /* :431-439 */
+int cfg_rigid_drag_move(cfg_rigid* w, int id, double tx, double ty);                          /* :440-449 */
+int cfg_rigid_drag_end(cfg_rigid* w, int id);                                                 /* :451-455 */
+int cfg_rigid_max_penetration(cfg_rigid* w, double* pen);                     /* :458-462 */
+int cfg_rigid_contacts(cfg_rigid* w, int* manifolds, int* points);
+/* Moving pieces in a wood scene: a rigid world (p, or NULL for frozen pieces; only while the scene
+ * has no pieces). Each frame then advances the bodies by the frame's gas time and exchanges heat
+ * across wood-wood contacts (js/contact.js) before the wood step, the bodies follow the wood's
+ * size and density, and the geometry pass rasterises the moved pieces. */
+int cfg_wood_set_rigid(cfg_wood* w, const cfg_rigid_params* p);
+/* the scene's rigid world (owned by the scene: not for cfg_rigid_destroy), and a piece's body */
+int cfg_wood_rigid(cfg_wood* w, cfg_rigid** world);
+int cfg_wood_body(cfg_wood* w, int slot, int* body_id);
+
 /* ---- headless renderer: the fragment stage of shaders/render.wgsl (fs :189-273) for one
  * scene into an RGBA float image, in place of Renderer.encode's swapchain pass (js/render.js:
  * 57-70). Pixel (x, y), row 0 at the top, is shaded at uv = ((x + 0.5) / W, 1 - (y + 0.5) / H);

@@ -12,6 +12,8 @@ import math
 
 import numpy as np
 
+from .rigid_ref import exchange_contacts
+
 WOOD = dict(cv=1500, kv=0.15, cc=1000, kc=0.08, pore=0.001, charDensityRatio=0.3, eps=0.9, pyroA=2.0e7,
             pyroTa=12000, dHpyro=3.0e5, dHchar=32.8e6, cpGas=1150, deltaS=0.0015, deltaP=0.002, minDepth=0.0004,
             sigma=5.670374e-8, minHalf=0.0015)
@@ -147,8 +149,9 @@ class WoodPiece:
 class WoodScene:
     """The frame loop of js/main.js for frozen pieces, over an OracleSim."""
 
-    def __init__(self, sim, charYield=0.25, pyroMult=1.0):
-        self.sim, self.charYield, self.pyroMult = sim, charYield, pyroMult
+    def __init__(self, sim, charYield=0.25, pyroMult=1.0, world=None):
+        """world: an oracle.rigid_ref.RigidWorld for moving pieces (None: frozen)."""
+        self.sim, self.charYield, self.pyroMult, self.world = sim, charYield, pyroMult, world
         self.slots = [None] * 64
         self.simAcc = 0.0
         self.frame_no = 0
@@ -166,7 +169,11 @@ class WoodScene:
                     w.Tp[f] = max(w.Tp[f], 0.5 * (T + w.Tc))
         qa = SIGMA * TAMB ** 4
         self.slots[s] = dict(x=x, y=y, angle=angle, wood=w, qConv=[0.0] * 4, qInc=[qa] * 4, vis=[0.0] * 4,
-                             charPending=[0.0] * 4)
+                             charPending=[0.0] * 4, body=None)
+        if self.world is not None:   # new Body(x, y, half, (mv + mc) / side^2, angle), js/main.js:109-110
+            b = self.world.add(x, y, w.half, (w.mv + w.mc) / (w.side * w.side), angle)
+            b.user = w
+            self.slots[s]["body"] = b
         return s
 
     def upload(self):
@@ -175,8 +182,11 @@ class WoodScene:
         for s, p in enumerate(self.slots):
             if p is None:
                 continue
-            w = p["wood"]
-            data[s * 20:s * 20 + 8] = [p["x"], p["y"], p["angle"], w.half, 0, 0, 0, 1]
+            w, b = p["wood"], p["body"]
+            if b is not None:
+                data[s * 20:s * 20 + 8] = [b.x, b.y, b.a, b.half, b.vx, b.vy, b.w, 1]
+            else:
+                data[s * 20:s * 20 + 8] = [p["x"], p["y"], p["angle"], w.half, 0, 0, 0, 1]
             data[s * 20 + 8:s * 20 + 12] = w.Ts
             data[s * 20 + 12:s * 20 + 16] = w.mflux
             data[s * 20 + 16:s * 20 + 20] = w.charCov
@@ -193,14 +203,24 @@ class WoodScene:
         else:
             self.simAcc -= n * dt
         simDt = n * dt
+        if self.world is not None:   # js/main.js:262-263
+            self.world.advance(simDt)
+            exchange_contacts(self.world, simDt)
         if simDt > 0:
             for s, p in enumerate(self.slots):
                 if p is None:
                     continue
-                p["wood"].step(simDt, p["qConv"], p["qInc"], p["charPending"], self.charYield, self.pyroMult)
+                w = p["wood"]
+                w.step(simDt, p["qConv"], p["qInc"], p["charPending"], self.charYield, self.pyroMult)
                 p["charPending"] = [0.0] * 4
-                if p["wood"].dead:
+                if w.dead:
+                    if p["body"] is not None:
+                        self.world.remove(p["body"])
                     self.slots[s] = None
+                    continue
+                if p["body"] is not None:   # stepWood, js/main.js:239-241
+                    p["body"].density = (w.mv + w.mc) / (w.side * w.side)
+                    self.world.resize(p["body"], w.half)
         self.upload()
         self.sim.set_frame(self.frame_no)
         self.sim.write_params()
@@ -236,13 +256,17 @@ def default_scene(scene, charYield=0.25, density=500.0):
     cx, S = 0.7 / 2, 0.0125
 
     def coal(x, y, sz, T):
-        w = scene.slots[scene.add(x, y, 0.0, sz, density, preheat=(T, sz, T - 30))]["wood"]
+        p = scene.slots[scene.add(x, y, 0.0, sz, density, preheat=(T, sz, T - 30))]
+        w = p["wood"]
         w.mv = 0
         w.mc = w.rhoC * sz * sz
         w.updateSide()
         w.d = [sz / 2, sz / 2, sz / 2, sz / 2]
         w.charCov = [1, 1, 1, 1]
         w.Tp = [T - 20, T - 20, T - 20, T - 20]
+        if p["body"] is not None:
+            p["body"].density = w.mc / (sz * sz)
+            scene.world.resize(p["body"], w.half)
 
     def lit(x, y, sz):
         w = scene.slots[scene.add(x, y, 0.0, sz, density, preheat=(880, 0.003 if sz > 0.03 else 0.002, 380))]["wood"]

@@ -117,3 +117,41 @@ def test_default_scene_matches_oracle(oracle_mod):
                 assert rel(a["Ts"][f], w.Ts[f], 1.0) <= 1e-4, (k, s, f)
             assert rel(a["mc"], w.mc, 1e-12) <= 1e-5
     ws.close(); g.close()
+
+
+def test_moving_pieces_match_oracle(oracle_mod):
+    """Moving pieces (js/rigid.js world in the frame, js/contact.js heat exchange): a stick dropped
+    on two preheated logs. The bodies depend on the gas only through the wood's size and mass, so
+    they agree with the oracle's to 1e-9 m over these frames; the wood as in the frozen case."""
+    from campfire_b200.wood import app_rigid_options
+    from oracle.rigid_ref import RigidWorld as RefWorld
+    nx, ny, dt = 112, 160, 0.004
+    g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": dt}, width=0.7).init()
+    g.writeParams()
+    g.reset()
+    o = oracle_mod.OracleSim(nx, ny, 0.7, dt)
+    o.write_params()
+    o.reset()
+    opts = app_rigid_options()
+    ws = WoodScene(g, rigid=opts)
+    rs = RefScene(o, world=RefWorld(**opts))
+    for sc in (ws, rs):
+        sc.add(0.30, 0.025, 0.0, 0.05, 500.0, preheat=(950.0, 0.004, 450.0))
+        sc.add(0.40, 0.025, 0.0, 0.05, 500.0, preheat=(950.0, 0.004, 450.0))
+        sc.add(0.35, 0.09, 0.4, 0.025, 500.0)
+    y0 = ws.body(2).y
+    for k in range(15):
+        assert ws.frame(1 / 60) == rs.frame(1 / 60)
+        for s in range(3):
+            b, rb = ws.body(s), rs.slots[s]["body"]
+            for f in ("x", "y", "a"):
+                assert abs(getattr(b, f) - getattr(rb, f)) <= 1e-9, (k, s, f, getattr(b, f), getattr(rb, f))
+            a = ws.piece(s)[0]
+            w = rs.slots[s]["wood"]
+            for f in range(4):
+                assert rel(a["Ts"][f], w.Ts[f], 1.0) <= 1e-3, (k, s, f, a["Ts"][f], w.Ts[f])
+    stick = ws.body(2)
+    assert stick.y < y0 - 0.01                       # it fell
+    assert ws.world.contacts()[0] >= 4               # and rests on the logs (floor + log contacts)
+    assert abs(stick.vy) < 0.05
+    ws.close(); g.close()
