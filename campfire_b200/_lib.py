@@ -21,6 +21,7 @@ SOLVE_FIXED, SOLVE_TOL, SOLVE_FP64 = 0, 1, 2
 MAX_PIECES, PIECE_FLOATS, ACC_GLOBAL, ACC_LEN = 64, 20, 512, 528
 E_SCALE, M_SCALE, G_SCALE, N_FLOOR, RAD_LEN = 1e6, 1e12, 1e3, 64, 320
 MAX_LEVELS = 7
+CFG_JOB_KEEP_FIELDS = 1
 
 PARAM_FIELDS = [
     ("nx", "i"), ("ny", "i"), ("dx", "f"), ("dt", "f"),
@@ -52,7 +53,7 @@ class CfgInfo(ctypes.Structure):
 
 class CfgJob(ctypes.Structure):
     _fields_ = [("size_class", ctypes.c_int32), ("kind", ctypes.c_int32), ("seed", ctypes.c_uint64),
-                ("nsteps", ctypes.c_int32), ("pad", ctypes.c_int32), ("arrival_s", ctypes.c_double)]
+                ("nsteps", ctypes.c_int32), ("flags", ctypes.c_int32), ("arrival_s", ctypes.c_double)]
 
 
 class CfgJobResult(ctypes.Structure):
@@ -171,6 +172,11 @@ def lib():
         "cfg_set_krylov": [vp, ci], "cfg_batch_set_krylov": [vp, ci],
         "cfg_server_slot_bytes": [vp, ci, ctypes.POINTER(sz)],
         "cfg_server_run": [vp, ctypes.POINTER(CfgJob), ci, ctypes.POINTER(CfgJobResult), dp, dp],
+        "cfg_server_submit": [vp, ctypes.POINTER(CfgJob), ctypes.POINTER(ctypes.c_uint64)],
+        "cfg_server_poll": [vp, ctypes.c_uint64, ctypes.POINTER(CfgJobResult), ip],
+        "cfg_server_wait": [vp, ctypes.c_uint64, cd, ctypes.POINTER(CfgJobResult)],
+        "cfg_server_drain": [vp], "cfg_server_fetch": [vp, ctypes.c_uint64, cs, fp, sz],
+        "cfg_server_release": [vp, ctypes.c_uint64],
     }
     for name, args in sigs.items():
         f = getattr(L, name)

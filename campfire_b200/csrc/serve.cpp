@@ -14,12 +14,20 @@
 // once. A job's fields are read back after its last step, hashed, and its slot
 // disabled and freed. Every scene's solve decides for itself, so a job's result
 // does not depend on the other jobs in the batch.
+//
+// Two fronts share the loop: cfg_server_run takes a list of jobs with arrival
+// times and returns when all are done; cfg_server_submit hands jobs one at a
+// time to a service thread (started on the first submission) whose results are
+// collected with cfg_server_poll / cfg_server_wait.
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/campfire_gas.h"
@@ -28,17 +36,33 @@
 static_assert(sizeof(cfg_job) == 32, "cfg_job layout");
 static_assert(sizeof(cfg_job_result) == 64, "cfg_job_result layout");
 
+using Clock = std::chrono::steady_clock;
+
 struct cfg_server {
   cfg::Engine eng;
   std::vector<int> cls_nx, cls_ny;
   std::vector<int> slot_class;
   std::vector<size_t> slot_bytes;
   double budget = 0, width = 0.8;
+  // the service thread (cfg_server_submit)
+  struct Submitted { uint64_t ticket; cfg_job job; double arrival; };
+  struct Kept { std::vector<float> T, Y, U, V; };
+  std::mutex mu;
+  std::condition_variable work_cv, done_cv;
+  std::deque<Submitted> queue;                          // submitted, not yet taken by the loop
+  std::unordered_map<uint64_t, cfg_job_result> finished;
+  std::unordered_map<uint64_t, Kept> kept;              // CFG_JOB_KEEP_FIELDS
+  std::unordered_map<uint64_t, int> in_flight;          // tickets taken by the loop
+  uint64_t next_ticket = 1;
+  std::thread worker;
+  bool stopping = false, running = false, sync_busy = false;
+  int worker_rc = CFG_OK;
+  std::string worker_msg;
+  Clock::time_point t0;
+  ~cfg_server();
 };
 
 namespace {
-
-using Clock = std::chrono::steady_clock;
 
 // FNV-1a (64-bit) over the bytes of the dense fields T, Y, U, V: equal hashes mean
 // (with overwhelming likelihood) bit-identical states
@@ -50,23 +74,189 @@ struct Fnv {
   }
 };
 
-int field_hash(cfg::Engine& eng, int s, uint64_t* hash, double* tsum) {
+int read_dense(cfg::Engine& eng, int s, const char* name, std::vector<float>& buf) {
+  size_t n = 0;
+  CFG_TRY(eng.field_size(s, name, &n));
+  buf.resize(n);
+  return eng.read_field(s, name, buf.data(), n);
+}
+
+int field_hash(cfg::Engine& eng, int s, uint64_t* hash, double* tsum, cfg_server::Kept* keep) {
   Fnv f;
   double sum = 0;
-  for (const char* name : {"T", "Y", "U", "V"}) {
-    size_t n = 0;
-    CFG_TRY(eng.field_size(s, name, &n));
-    std::vector<float> buf(n);
-    CFG_TRY(eng.read_field(s, name, buf.data(), n));
-    f.add(buf.data(), n * sizeof(float));
-    if (name[0] == 'T') for (float v : buf) sum += v;
+  std::vector<float> local[4];
+  const char* names[4] = {"T", "Y", "U", "V"};
+  for (int k = 0; k < 4; k++) {
+    std::vector<float>& buf = keep ? (k == 0 ? keep->T : k == 1 ? keep->Y : k == 2 ? keep->U : keep->V) : local[k];
+    CFG_TRY(read_dense(eng, s, names[k], buf));
+    f.add(buf.data(), buf.size() * sizeof(float));
+    if (k == 0) for (float v : buf) sum += v;
   }
   *hash = f.h;
   *tsum = sum;
   return CFG_OK;
 }
 
+int check_job(const cfg_server* s, const cfg_job& j) {
+  const int ncls = (int)s->cls_nx.size(), nslot = (int)s->slot_class.size();
+  if (j.size_class < 0 || j.size_class >= ncls) return cfg::fail(CFG_ERR_INVAL, "job size class out of range");
+  if (j.nsteps < 1) return cfg::fail(CFG_ERR_INVAL, "job step count must be >= 1");
+  if (j.kind < 0 || j.kind > 2) return cfg::fail(CFG_ERR_INVAL, "job scene kind must be 0, 1 or 2");
+  for (int k = 0; k < nslot; k++)
+    if (s->slot_class[k] == j.size_class && s->slot_bytes[k] <= s->budget) return CFG_OK;
+  return cfg::fail(CFG_ERR_RANGE, "a job's size class has no slot within the budget");
+}
+
+// The admission / continuous-batching loop over the server's slots. Jobs are
+// identified by an index into `jobs` (the caller's list, or the service's
+// growing list of taken submissions).
+struct Loop {
+  cfg_server* s;
+  std::vector<std::deque<int>> waiting;
+  std::vector<int> slot_job, left;
+  size_t used = 0;
+  double cu = 0;
+  int active = 0;
+  long long nstep = 0;
+  cudaEvent_t ev[4] = {};
+  explicit Loop(cfg_server* srv)
+      : s(srv), waiting(srv->cls_nx.size()), slot_job(srv->slot_class.size(), -1), left(srv->slot_class.size(), 0) {}
+  ~Loop() { for (auto& e : ev) if (e) cudaEventDestroy(e); }
+  int init() {
+    for (auto& e : ev) CFG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return CFG_OK;
+  }
+  double now() const { return std::chrono::duration<double>(Clock::now() - s->t0).count(); }
+  // admission: per class in arrival order, while a slot is free and the budget allows
+  int admit(const std::vector<cfg_job>& jobs, std::vector<cfg_job_result>& res) {
+    cfg::Engine& eng = s->eng;
+    const int nslot = (int)s->slot_class.size();
+    for (size_t c = 0; c < waiting.size(); c++)
+      while (!waiting[c].empty()) {
+        int slot = -1;
+        for (int k = 0; k < nslot; k++)
+          if (s->slot_class[k] == (int)c && slot_job[k] < 0 && used + s->slot_bytes[k] <= s->budget) { slot = k; break; }
+        if (slot < 0) break;
+        const int j = waiting[c].front();
+        waiting[c].pop_front();
+        if (nstep > 0) CFG_TRY(eng.synchronize());
+        // enabled first: the geometry pass of the set-up skips disabled scenes
+        CFG_TRY(eng.set_active(slot, true));
+        CFG_TRY(cfg::load_generated_scene(eng, slot, jobs[j].kind, s->width, jobs[j].seed));
+        slot_job[slot] = j;
+        left[slot] = jobs[j].nsteps;
+        used += s->slot_bytes[slot];
+        active++;
+        res[j].slot = slot;
+        res[j].admit_s = now();
+      }
+    return CFG_OK;
+  }
+  // one batched step; the host runs at most two steps ahead of the device. on_done(j, slot)
+  // is called for each job that took its last step (the device is idle then).
+  template <class F>
+  int step(const std::vector<cfg_job>& jobs, std::vector<cfg_job_result>& res, F&& on_done) {
+    cfg::Engine& eng = s->eng;
+    if (nstep >= 2) CFG_CUDA(cudaEventSynchronize(ev[(nstep - 2) % 4]));
+    CFG_TRY(eng.step(1));
+    CFG_CUDA(cudaEventRecord(ev[nstep % 4], eng.stream()));
+    nstep++;
+    for (int k = 0; k < (int)slot_job.size(); k++) {
+      if (slot_job[k] < 0) continue;
+      cu += (double)s->cls_nx[s->slot_class[k]] * s->cls_ny[s->slot_class[k]];
+      if (--left[k] > 0) continue;
+      const int j = slot_job[k];
+      CFG_TRY(eng.synchronize());
+      cfg_info inf;
+      CFG_TRY(eng.info(k, &inf));
+      res[j].steps = jobs[j].nsteps;
+      res[j].last_cycles = inf.last_cycles;
+      res[j].last_rel = inf.last_rel;
+      CFG_TRY(on_done(j, k));
+      res[j].done_s = now();
+      CFG_TRY(eng.set_active(k, false));
+      slot_job[k] = -1;
+      used -= s->slot_bytes[k];
+      active--;
+    }
+    return CFG_OK;
+  }
+};
+
+// the service thread: takes submissions, runs the loop, files results
+void service(cfg_server* s) {
+  std::vector<cfg_job> jobs;
+  std::vector<cfg_job_result> res;
+  std::vector<uint64_t> ticket;
+  Loop loop(s);
+  int rc = loop.init();
+  auto fail_all = [&](int code) {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->worker_rc = code;
+    s->worker_msg = cfg::last_error();
+    s->running = false;
+    s->done_cv.notify_all();
+  };
+  if (rc != CFG_OK) { fail_all(rc); return; }
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> g(s->mu);
+      if (loop.active == 0 && s->queue.empty()) {
+        bool waiting = false;
+        for (auto& w : loop.waiting) waiting = waiting || !w.empty();
+        if (!waiting) {
+          if (s->stopping) { s->running = false; s->done_cv.notify_all(); return; }
+          s->work_cv.wait(g, [&] { return s->stopping || !s->queue.empty(); });
+        }
+      }
+      while (!s->queue.empty()) {
+        const cfg_server::Submitted sub = s->queue.front();
+        s->queue.pop_front();
+        const int j = (int)jobs.size();
+        jobs.push_back(sub.job);
+        cfg_job_result r;
+        std::memset(&r, 0, sizeof r);
+        r.slot = -1;
+        r.arrival_s = sub.arrival;
+        res.push_back(r);
+        ticket.push_back(sub.ticket);
+        s->in_flight[sub.ticket] = j;
+        loop.waiting[sub.job.size_class].push_back(j);
+      }
+    }
+    rc = loop.admit(jobs, res);
+    if (rc != CFG_OK) { fail_all(rc); return; }
+    if (loop.active == 0) continue;
+    rc = loop.step(jobs, res, [&](int j, int slot) {
+      cfg_server::Kept keep;
+      const bool want = (jobs[j].flags & CFG_JOB_KEEP_FIELDS) != 0;
+      CFG_TRY(field_hash(s->eng, slot, &res[j].hash, &res[j].t_sum, want ? &keep : nullptr));
+      res[j].done_s = loop.now();
+      std::lock_guard<std::mutex> g(s->mu);
+      s->finished[ticket[j]] = res[j];
+      if (want) s->kept[ticket[j]] = std::move(keep);
+      s->in_flight.erase(ticket[j]);
+      s->done_cv.notify_all();
+      return CFG_OK;
+    });
+    if (rc != CFG_OK) { fail_all(rc); return; }
+  }
+}
+
+void stop_service(cfg_server* s) {
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stopping = true;
+  }
+  s->work_cv.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  std::lock_guard<std::mutex> g(s->mu);
+  s->stopping = false;
+}
+
 }  // namespace
+
+cfg_server::~cfg_server() { stop_service(this); }
 
 extern "C" {
 
@@ -89,6 +279,7 @@ int cfg_server_create(int device, int nclasses, const int* nx, const int* ny, co
     s->slot_class = scls;
     s->budget = budget_bytes;
     s->width = width;
+    s->t0 = Clock::now();
     const int n = (int)snx.size();
     std::vector<double> w(n, width), dt(n, 0.002);
     int rc = s->eng.init(device, n, snx.data(), sny.data(), w.data(), dt.data());
@@ -107,9 +298,15 @@ int cfg_server_destroy(cfg_server* s) {
   return CFG_OK;
 }
 
+static bool server_busy(cfg_server* s) {
+  std::lock_guard<std::mutex> g(s->mu);
+  return s->running || s->sync_busy;
+}
+
 int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int max_cycles, int coarse_direct,
                           int coarse_cells, int krylov) {
   if (!s) return cfg::fail(CFG_ERR_INVAL, "null cfg_server handle");
+  if (server_busy(s)) return cfg::fail(CFG_ERR_BUSY, "the server is running jobs: drain it first");
   CFG_TRY(s->eng.set_solver(mode, ncycles, tol, max_cycles));
   CFG_TRY(s->eng.set_coarse_solve(coarse_direct ? 1 : 0));
   CFG_TRY(s->eng.set_krylov(krylov ? 1 : 0));
@@ -124,99 +321,141 @@ int cfg_server_slot_bytes(cfg_server* s, int size_class, size_t* bytes) {
   return cfg::fail(CFG_ERR_NOENT, "no slot of this size class");
 }
 
-int cfg_server_run(cfg_server* s, const cfg_job* jobs, int njobs, cfg_job_result* res, double* wall_s,
+int cfg_server_run(cfg_server* s, const cfg_job* jobs_in, int njobs, cfg_job_result* res_out, double* wall_s,
                    double* cell_updates) {
-  if (!s || (!jobs && njobs > 0) || (!res && njobs > 0) || njobs < 0 || !wall_s || !cell_updates)
+  if (!s || (!jobs_in && njobs > 0) || (!res_out && njobs > 0) || njobs < 0 || !wall_s || !cell_updates)
     return cfg::fail(CFG_ERR_INVAL, "bad argument");
-  const int ncls = (int)s->cls_nx.size(), nslot = (int)s->slot_class.size();
-  for (int j = 0; j < njobs; j++) {
-    if (jobs[j].size_class < 0 || jobs[j].size_class >= ncls) return cfg::fail(CFG_ERR_INVAL, "job size class out of range");
-    if (jobs[j].nsteps < 1) return cfg::fail(CFG_ERR_INVAL, "job step count must be >= 1");
-    if (jobs[j].kind < 0 || jobs[j].kind > 2) return cfg::fail(CFG_ERR_INVAL, "job scene kind must be 0, 1 or 2");
-    bool has_slot = false;
-    for (int k = 0; k < nslot; k++)
-      if (s->slot_class[k] == jobs[j].size_class && s->slot_bytes[k] <= s->budget) has_slot = true;
-    if (!has_slot) return cfg::fail(CFG_ERR_RANGE, "a job's size class has no slot within the budget");
-    std::memset(&res[j], 0, sizeof(cfg_job_result));
-    res[j].slot = -1;
+  for (int j = 0; j < njobs; j++) CFG_TRY(check_job(s, jobs_in[j]));
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->running || s->sync_busy) return cfg::fail(CFG_ERR_BUSY, "the server is running submitted jobs");
+    s->sync_busy = true;
   }
-  cfg::Engine& eng = s->eng;
+  struct Busy { cfg_server* s; ~Busy() { std::lock_guard<std::mutex> g(s->mu); s->sync_busy = false; } } busy{s};
+  std::vector<cfg_job> jobs(jobs_in, jobs_in + njobs);
+  std::vector<cfg_job_result> res(njobs);
+  for (auto& r : res) { std::memset(&r, 0, sizeof r); r.slot = -1; }
   std::vector<int> order(njobs);
   for (int j = 0; j < njobs; j++) order[j] = j;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a].arrival_s < jobs[b].arrival_s; });
-  std::vector<std::deque<int>> waiting(ncls);
-  std::vector<int> slot_job(nslot, -1), left(nslot, 0);
-  size_t used = 0;
-  double cu = 0;
-  int next = 0, done = 0, active = 0;
-  cudaEvent_t ev[4];
-  for (auto& e : ev) CFG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  struct EvGuard { cudaEvent_t* e; ~EvGuard() { for (int k = 0; k < 4; k++) cudaEventDestroy(e[k]); } } guard{ev};
-  long long nstep = 0;
-  const auto t0 = Clock::now();
-  auto now = [&] { return std::chrono::duration<double>(Clock::now() - t0).count(); };
-
+  Loop loop(s);
+  CFG_TRY(loop.init());
+  const Clock::time_point saved_t0 = s->t0;
+  s->t0 = Clock::now();
+  struct T0 { cfg_server* s; Clock::time_point t; ~T0() { s->t0 = t; } } restore{s, saved_t0};
+  int next = 0, done = 0;
   while (done < njobs) {
-    const double t = now();
+    const double t = loop.now();
     while (next < njobs && jobs[order[next]].arrival_s <= t) {
-      waiting[jobs[order[next]].size_class].push_back(order[next]);
+      res[order[next]].arrival_s = jobs[order[next]].arrival_s;
+      loop.waiting[jobs[order[next]].size_class].push_back(order[next]);
       next++;
     }
-    // admission: per class in arrival order, while a slot is free and the budget allows
-    for (int c = 0; c < ncls; c++)
-      while (!waiting[c].empty()) {
-        int slot = -1;
-        for (int k = 0; k < nslot; k++)
-          if (s->slot_class[k] == c && slot_job[k] < 0 && used + s->slot_bytes[k] <= s->budget) { slot = k; break; }
-        if (slot < 0) break;
-        const int j = waiting[c].front();
-        waiting[c].pop_front();
-        if (nstep > 0) CFG_TRY(eng.synchronize());
-        // enabled first: the geometry pass of the set-up skips disabled scenes
-        CFG_TRY(eng.set_active(slot, true));
-        CFG_TRY(cfg::load_generated_scene(eng, slot, jobs[j].kind, s->width, jobs[j].seed));
-        slot_job[slot] = j;
-        left[slot] = jobs[j].nsteps;
-        used += s->slot_bytes[slot];
-        active++;
-        res[j].slot = slot;
-        res[j].arrival_s = jobs[j].arrival_s;
-        res[j].admit_s = now();
-      }
-    if (active == 0) {
+    CFG_TRY(loop.admit(jobs, res));
+    if (loop.active == 0) {
       if (next >= njobs) return cfg::fail(CFG_ERR_RANGE, "waiting jobs can never be admitted");
-      const double dtw = jobs[order[next]].arrival_s - now();
+      const double dtw = jobs[order[next]].arrival_s - loop.now();
       if (dtw > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(dtw, 0.05)));
       continue;
     }
-    // one batched step; the host runs at most two steps ahead of the device
-    if (nstep >= 2) CFG_CUDA(cudaEventSynchronize(ev[(nstep - 2) % 4]));
-    CFG_TRY(eng.step(1));
-    CFG_CUDA(cudaEventRecord(ev[nstep % 4], eng.stream()));
-    nstep++;
-    for (int k = 0; k < nslot; k++) {
-      if (slot_job[k] < 0) continue;
-      cu += (double)s->cls_nx[s->slot_class[k]] * s->cls_ny[s->slot_class[k]];
-      if (--left[k] > 0) continue;
-      const int j = slot_job[k];
-      CFG_TRY(eng.synchronize());
-      cfg_info inf;
-      CFG_TRY(eng.info(k, &inf));
-      CFG_TRY(field_hash(eng, k, &res[j].hash, &res[j].t_sum));
-      res[j].done_s = now();
-      res[j].steps = jobs[j].nsteps;
-      res[j].last_cycles = inf.last_cycles;
-      res[j].last_rel = inf.last_rel;
-      CFG_TRY(eng.set_active(k, false));
-      slot_job[k] = -1;
-      used -= s->slot_bytes[k];
-      active--;
+    CFG_TRY(loop.step(jobs, res, [&](int j, int slot) {
       done++;
+      return field_hash(s->eng, slot, &res[j].hash, &res[j].t_sum, nullptr);
+    }));
+  }
+  CFG_TRY(s->eng.synchronize());
+  *wall_s = loop.now();
+  *cell_updates = loop.cu;
+  std::copy(res.begin(), res.end(), res_out);
+  return CFG_OK;
+}
+
+int cfg_server_submit(cfg_server* s, const cfg_job* job, uint64_t* ticket) {
+  if (!s || !job || !ticket) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  CFG_TRY(check_job(s, *job));
+  std::lock_guard<std::mutex> g(s->mu);
+  if (s->sync_busy) return cfg::fail(CFG_ERR_BUSY, "cfg_server_run is in progress");
+  if (s->worker_rc != CFG_OK) return cfg::fail(s->worker_rc, "the service stopped: " + s->worker_msg);
+  if (!s->running) {
+    if (s->worker.joinable()) s->worker.join();   // a service that drained and exited
+    s->running = true;
+    s->worker = std::thread(service, s);
+  }
+  const uint64_t t = s->next_ticket++;
+  s->queue.push_back({t, *job, std::chrono::duration<double>(Clock::now() - s->t0).count()});
+  *ticket = t;
+  s->work_cv.notify_all();
+  return CFG_OK;
+}
+
+static int take_result(cfg_server* s, uint64_t ticket, cfg_job_result* out, bool* done) {
+  auto it = s->finished.find(ticket);
+  if (it != s->finished.end()) {
+    if (out) *out = it->second;
+    s->finished.erase(it);
+    *done = true;
+    return CFG_OK;
+  }
+  *done = false;
+  if (s->worker_rc != CFG_OK) return cfg::fail(s->worker_rc, "the service stopped: " + s->worker_msg);
+  bool queued = s->in_flight.count(ticket) != 0;
+  for (const auto& q : s->queue) queued = queued || q.ticket == ticket;
+  if (!queued) return cfg::fail(CFG_ERR_NOENT, "unknown ticket (or its result was already taken)");
+  return CFG_OK;
+}
+
+int cfg_server_poll(cfg_server* s, uint64_t ticket, cfg_job_result* out, int* done) {
+  if (!s || !done) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> g(s->mu);
+  bool d = false;
+  const int rc = take_result(s, ticket, out, &d);
+  *done = d ? 1 : 0;
+  return rc;
+}
+
+int cfg_server_wait(cfg_server* s, uint64_t ticket, double timeout_s, cfg_job_result* out) {
+  if (!s || !(timeout_s >= 0)) return cfg::fail(CFG_ERR_INVAL, "bad argument");
+  const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(timeout_s));
+  std::unique_lock<std::mutex> g(s->mu);
+  for (;;) {
+    bool d = false;
+    CFG_TRY(take_result(s, ticket, out, &d));
+    if (d) return CFG_OK;
+    if (s->done_cv.wait_until(g, deadline) == std::cv_status::timeout) {
+      CFG_TRY(take_result(s, ticket, out, &d));
+      if (d) return CFG_OK;
+      return cfg::fail(CFG_ERR_TIMEDOUT, "the job has not finished");
     }
   }
-  CFG_TRY(eng.synchronize());
-  *wall_s = now();
-  *cell_updates = cu;
+}
+
+int cfg_server_drain(cfg_server* s) {
+  if (!s) return cfg::fail(CFG_ERR_INVAL, "null cfg_server handle");
+  stop_service(s);
+  std::lock_guard<std::mutex> g(s->mu);
+  if (s->worker_rc != CFG_OK) return cfg::fail(s->worker_rc, "the service stopped: " + s->worker_msg);
+  return CFG_OK;
+}
+
+int cfg_server_fetch(cfg_server* s, uint64_t ticket, const char* name, float* out, size_t count) {
+  if (!s || !name) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> g(s->mu);
+  auto it = s->kept.find(ticket);
+  if (it == s->kept.end()) return cfg::fail(CFG_ERR_NOENT, "no kept fields for this ticket (submit with CFG_JOB_KEEP_FIELDS)");
+  const std::string n(name);
+  const std::vector<float>* f = n == "T" ? &it->second.T : n == "Y" ? &it->second.Y : n == "U" ? &it->second.U
+                              : n == "V" ? &it->second.V : nullptr;
+  if (!f) return cfg::fail(CFG_ERR_NOENT, "kept fields are T, Y, U and V");
+  if (!out) return cfg::fail(CFG_ERR_INVAL, "null output");
+  if (count != f->size()) return cfg::fail(CFG_ERR_INVAL, "count must be " + std::to_string(f->size()));
+  std::copy(f->begin(), f->end(), out);
+  return CFG_OK;
+}
+
+int cfg_server_release(cfg_server* s, uint64_t ticket) {
+  if (!s) return cfg::fail(CFG_ERR_INVAL, "null cfg_server handle");
+  std::lock_guard<std::mutex> g(s->mu);
+  if (!s->kept.erase(ticket)) return cfg::fail(CFG_ERR_NOENT, "no kept fields for this ticket");
   return CFG_OK;
 }
 

@@ -367,6 +367,41 @@ class Server:
         out = [{k: getattr(res[i], k) for k, _ in _lib.CfgJobResult._fields_ if k != "pad"} for i in range(n)]
         return out, wall.value, cu.value
 
+    # -- the asynchronous service (a host thread runs the loop on submitted jobs)
+    def submit(self, size_class: int, kind: int, seed: int, nsteps: int, keep_fields: bool = False) -> int:
+        """Hand a job to the service; returns its ticket."""
+        job = _lib.CfgJob(size_class, kind, seed, nsteps, _lib.CFG_JOB_KEEP_FIELDS if keep_fields else 0, 0.0)
+        t = ctypes.c_uint64()
+        check(_lib.lib().cfg_server_submit(self._h, ctypes.byref(job), ctypes.byref(t)))
+        return t.value
+
+    @staticmethod
+    def _result(r) -> dict:
+        return {k: getattr(r, k) for k, _ in _lib.CfgJobResult._fields_ if k != "pad"}
+
+    def poll(self, ticket: int):
+        """The job's result once it has finished (then released), else None."""
+        r, done = _lib.CfgJobResult(), ctypes.c_int()
+        check(_lib.lib().cfg_server_poll(self._h, ticket, ctypes.byref(r), ctypes.byref(done)))
+        return self._result(r) if done.value else None
+
+    def wait(self, ticket: int, timeout_s: float = 60.0) -> dict:
+        r = _lib.CfgJobResult()
+        check(_lib.lib().cfg_server_wait(self._h, ticket, float(timeout_s), ctypes.byref(r)))
+        return self._result(r)
+
+    def drain(self):
+        check(_lib.lib().cfg_server_drain(self._h))
+
+    def fetch(self, ticket: int, name: str, count: int) -> np.ndarray:
+        """A finished keep_fields job's final field (dense float32)."""
+        out = np.empty(count, np.float32)
+        check(_lib.lib().cfg_server_fetch(self._h, ticket, name.encode(), _fp(out), count))
+        return out
+
+    def release(self, ticket: int):
+        check(_lib.lib().cfg_server_release(self._h, ticket))
+
 
 def field_hash(sim) -> int:
     """FNV-1a 64 of the dense T, Y, U, V float32 bytes (the hash cfg_server_run reports)."""

@@ -365,9 +365,10 @@ typedef struct cfg_job {
   int32_t kind;             /* scene generator kind (cfg_scene_generate) */
   uint64_t seed;            /* scene seed */
   int32_t nsteps;           /* gas steps to run */
-  int32_t pad;
-  double arrival_s;         /* arrival time, seconds after cfg_server_run starts */
+  int32_t flags;            /* CFG_JOB_KEEP_FIELDS (cfg_server_submit) */
+  double arrival_s;         /* arrival time, seconds after cfg_server_run starts (cfg_server_run only) */
 } cfg_job;
+#define CFG_JOB_KEEP_FIELDS 1   /* keep the final T, Y, U, V on the host for cfg_server_fetch */
 typedef struct cfg_job_result {
   double arrival_s, admit_s, done_s;   /* seconds after cfg_server_run starts */
   int32_t slot, steps, last_cycles, pad;
@@ -388,6 +389,20 @@ int cfg_server_slot_bytes(cfg_server* s, int size_class, size_t* bytes);
  * results[j] for jobs[j]; *wall_s the run's duration, *cell_updates the cells stepped */
 int cfg_server_run(cfg_server* s, const cfg_job* jobs, int njobs, cfg_job_result* results, double* wall_s,
                    double* cell_updates);
+/* Asynchronous service: a host thread (started by the first submission) runs the same loop on
+ * jobs handed over one at a time; a job arrives when it is submitted. Times in the results are
+ * seconds after cfg_server_create. */
+int cfg_server_submit(cfg_server* s, const cfg_job* job, uint64_t* ticket);
+/* *done = 1 and *out filled (the result is then released) once the job has finished, else 0 */
+int cfg_server_poll(cfg_server* s, uint64_t ticket, cfg_job_result* out, int* done);
+/* waits up to timeout_s for the job; CFG_ERR_TIMEDOUT if it has not finished */
+int cfg_server_wait(cfg_server* s, uint64_t ticket, double timeout_s, cfg_job_result* out);
+/* runs every submitted job to completion and stops the service thread (destroy does the same) */
+int cfg_server_drain(cfg_server* s);
+/* a finished CFG_JOB_KEEP_FIELDS job's final field ("T", "Y", "U", "V"; dense, count floats) */
+int cfg_server_fetch(cfg_server* s, uint64_t ticket, const char* name, float* out, size_t count);
+/* frees a job's kept fields */
+int cfg_server_release(cfg_server* s, uint64_t ticket);
 
 #ifdef __cplusplus
 }

@@ -88,3 +88,65 @@ def test_bad_jobs_are_rejected():
         small.run([{"size_class": 0, "seed": 1, "nsteps": 2, "arrival_s": 0.0}])
     assert e.value.code == -34
     small.close()
+
+
+def fnv(arrays):
+    h = 1469598103934665603
+    for a in arrays:
+        for b in np.ascontiguousarray(a, np.float32).tobytes():
+            h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def test_submitted_jobs_match_the_batch_run():
+    """The service thread (cfg_server_submit / poll / wait / fetch): jobs handed over one at a
+    time while others run give the same results as the list run, and kept fields hash to the
+    reported hash."""
+    import threading
+    import time
+    js = jobs()
+    ref, _, _ = serve(js)
+    s = cb.Server(CLASSES, [2, 2], 64e9)
+    s.set_solver(**SOLVER)
+    tickets = [None] * len(js)
+
+    def client():   # a second host thread submits while the first polls
+        for k, j in enumerate(js):
+            tickets[k] = s.submit(j["size_class"], j["kind"], j["seed"], j["nsteps"], keep_fields=(k == 0))
+            time.sleep(0.005)
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    got = {}
+    deadline = time.time() + 120
+    while len(got) < len(js) and time.time() < deadline:
+        for k, t in enumerate(tickets):
+            if k not in got:
+                r = s.poll(t)
+                if r is not None:
+                    got[k] = r
+        time.sleep(0.002)
+    assert len(got) == len(js)
+    for k, j in enumerate(js):
+        assert got[k]["hash"] == ref[k]["hash"], j
+        assert got[k]["steps"] == j["nsteps"] and got[k]["done_s"] >= got[k]["admit_s"] >= got[k]["arrival_s"]
+    nx, ny = CLASSES[js[0]["size_class"]]
+    fields = [s.fetch(tickets[0], "T", nx * ny), s.fetch(tickets[0], "Y", 4 * nx * ny),
+              s.fetch(tickets[0], "U", (nx + 1) * ny), s.fetch(tickets[0], "V", nx * (ny + 1))]
+    assert fnv(fields) == got[0]["hash"]
+    s.release(tickets[0])
+    with pytest.raises(cb.CampfireError, match="NOENT"):
+        s.fetch(tickets[0], "T", nx * ny)
+    with pytest.raises(cb.CampfireError, match="NOENT"):
+        s.poll(tickets[1])               # already taken
+    # wait() on a fresh job, then drain; a new submission restarts the service
+    t = s.submit(0, 1, 4242, 3)
+    r = s.wait(t, 60.0)
+    assert r["steps"] == 3
+    s.drain()
+    t = s.submit(1, 2, 4243, 2)
+    assert s.wait(t, 60.0)["steps"] == 2
+    with pytest.raises(cb.CampfireError, match="BUSY"):
+        s.submit(0, 1, 1, 400)
+        s.set_solver(**SOLVER)
+    s.close()
