@@ -98,6 +98,9 @@ Engine::~Engine() {
   if (h_ctl_pinned_) cudaFreeHost(h_ctl_pinned_);
   if (stream_) cudaStreamDestroy(stream_);
   if (body_stream_) cudaStreamDestroy(body_stream_);
+  if (side_stream_) { cudaStreamSynchronize(side_stream_); cudaStreamDestroy(side_stream_); }
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
 }
 
 int Engine::activate() const {
@@ -134,6 +137,8 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
     if (sc.lnx[L - 1] * sc.lny[L - 1] > 256) return fail(CFG_ERR_RANGE, "coarsest level too large");
     sc.lc = choose_lc(sc, coarse_cells_);
     coarse_smem_ = std::max(coarse_smem_, coarse_smem_bytes(sc.lnx, sc.lny, sc.lc, sc.nlev));
+    const int cn = sc.lnx[L - 1] * sc.lny[L - 1], cbw = sc.lnx[L - 1];
+    if (cbw <= 32) { cf_smem_ = std::max(cf_smem_, coarse_factor_smem(cn, cbw)); cf_bw_ = std::max(cf_bw_, cbw); }
   }
   int ndev = 0;
   const cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -144,8 +149,12 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   // CAMPFIRE_PDL=0 launches the pressure-loop kernels without programmatic dependent launch
   if (const char* v = std::getenv("CAMPFIRE_PDL")) set_pdl(v[0] != '0');
   CFG_CUDA(prepare_mg_coarse(coarse_smem_));
+  CFG_CUDA(prepare_coarse_factor(cf_smem_));
   CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
+  CFG_CUDA(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking));
+  CFG_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+  CFG_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
   CFG_CUDA(cudaMalloc(&d_scenes_, sizeof(SceneDesc) * n));
   CFG_CUDA(cudaMalloc(&d_solve_, sizeof(SolveState) * n));
   CFG_CUDA(cudaMemset(d_solve_, 0, sizeof(SolveState) * n));
@@ -246,7 +255,7 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.r64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.dA, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.dB, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.q64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.tmap, (size_t)MAX_LEVELS * TM_PER_LEVEL * TMAP_BYTES},
-    {(void**)&d.cinv, (size_t)sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * 4},
+    {(void**)&d.cinv, (size_t)2 * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * 4},
   };
   double h = sc.dxd;
   for (int l = 0; l < sc.nlev; l++) {
@@ -274,7 +283,9 @@ int Engine::alloc_scene(Scene& sc) {
   for (auto& it : items) {
     *it.ptr = (char*)arena + off;
     off += (it.bytes + 255) / 256 * 256;
-    const bool scratch = it.ptr == (void**)&d.tmap || it.ptr == (void**)&d.part || it.ptr == (void**)&d.cinv;
+    // the coarsest inverses are state: with the pipelined coarse solve the next step uses the
+    // one factored during the last step
+    const bool scratch = it.ptr == (void**)&d.tmap || it.ptr == (void**)&d.part;
     sc.items.push_back({*it.ptr, it.bytes, !scratch});
   }
   return build_tmaps(sc);
@@ -541,6 +552,8 @@ int Engine::reset(int s) {
     CFG_CUDA(cudaMemsetAsync(d.lev[l].pb, 0, (size_t)d.lev[l].ny * d.lev[l].pc * 4, q));
   }
   CFG_CUDA(cudaMemsetAsync(d.p64, 0, (size_t)sc.nx * sc.ny * 8, q));
+  // no coarsest inverse of an earlier state survives a reset (direct_ok, cinv_cur, direct_ok_next)
+  CFG_CUDA(cudaMemsetAsync(&d_solve_[s].direct_ok, 0, 3 * sizeof(int), q));
   CFG_CUDA(cudaGetLastError());
   sc.time = 0;
   return CFG_OK;
@@ -874,7 +887,7 @@ void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_con
   launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); launches_++;
   for (int l = FR_KMAX; l + 1 < max_levels(); l++)
     if (nwl_[WL_MGC0 + l] > 0) { launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s); launches_++; }
-  if (direct_coarse()) { launch_coarse_factor(d_scenes_, nscenes(), s); launches_++; }
+  enqueue_factor(s);
   if (fp64) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s); launches_++; }
   // the loop's cycle counter starts at zero in every step
   cudaMemsetAsync(&d_ctl_->iter, 0, sizeof(int), s);
@@ -899,7 +912,8 @@ int Engine::set_krylov(int on) {
 }
 
 int Engine::set_coarse_solve(int direct) {
-  if (direct != 0 && direct != 1) return fail(CFG_ERR_INVAL, "coarse solve must be 0 (sweeps) or 1 (direct)");
+  if (direct < 0 || direct > 2)
+    return fail(CFG_ERR_INVAL, "coarse solve must be 0 (sweeps), 1 (direct) or 2 (direct, pipelined)");
   CFG_TRY(activate());
   coarse_direct_ = direct;
   graph_dirty_ = true;
@@ -982,7 +996,30 @@ void Engine::enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_co
   vcycle_launches_++;
 }
 
+// The coarsest inverse of the step's operator: before the loop on the step's stream
+// (direct), or on a side branch that runs beside the whole pressure loop (pipelined)
+void Engine::enqueue_factor(cudaStream_t s) {
+  if (!direct_coarse()) return;
+  if (!pipelined_coarse()) {
+    launch_coarse_factor(d_scenes_, nscenes(), cf_smem_, cf_bw_, 0, s);
+    launches_++;
+    return;
+  }
+  cudaEventRecord(ev_fork_, s);
+  cudaStreamWaitEvent(side_stream_, ev_fork_, 0);
+  launch_coarse_factor(d_scenes_, nscenes(), cf_smem_, cf_bw_, 1, side_stream_);
+  cudaEventRecord(ev_join_, side_stream_);
+  launches_++;
+}
+void Engine::enqueue_factor_join(cudaStream_t s) {
+  if (!pipelined_coarse()) return;
+  cudaStreamWaitEvent(s, ev_join_, 0);
+  launch_cinv_swap(d_scenes_, nscenes(), s);
+  launches_++;
+}
+
 void Engine::enqueue_post_solve(cudaStream_t s) {
+  enqueue_factor_join(s);
   launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], any_fp64(), s); launches_++;
   bool cfl = false;
   for (auto& sc : scenes_) cfl = cfl || sc.cfl > 0;
@@ -1153,7 +1190,7 @@ int Engine::step_profiled(float* ms) {
     launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   CFG_CUDA(cudaEventRecord(ev[5], s));
   CFG_TRY(set_cond_mode(false));
-  if (direct_coarse()) launch_coarse_factor(d_scenes_, nscenes(), s);
+  enqueue_factor(s);
   CFG_TRY(host_pressure_loop());
   CFG_CUDA(cudaEventRecord(ev[6], s));
   enqueue_post_solve(s);
@@ -1182,9 +1219,10 @@ int Engine::run_stage(const char* stage) {
       launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   } else if (st_ == "pressure") {
     CFG_TRY(set_cond_mode(false));
-    if (direct_coarse()) launch_coarse_factor(d_scenes_, nscenes(), s);
+    enqueue_factor(s);
     enqueue_bnorm(s);
     CFG_TRY(host_pressure_loop());
+    enqueue_factor_join(s);
   } else if (st_ == "project") launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s);
   else if (st_ == "update_dt") launch_cfl_update(d_scenes_, nscenes(), d_dxd_, d_alpha_, s);
   else return fail(CFG_ERR_NOENT, "unknown stage " + st_);
@@ -1255,6 +1293,25 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   } else if (n == "project") {
     go = [&](int) { launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s); };
     b = 32 * cells;
+  } else if (n == "coarse_factor") {
+    go = [&](int) { launch_coarse_factor(d_scenes_, nscenes(), cf_smem_, cf_bw_, pipelined_coarse() ? 1 : 0, s); };
+    b = 0; cnt = direct_coarse() ? 1 : 0;
+  } else if (n == "pcg_dir") {
+    go = [&](int) { launch_pcg_dir(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
+    b = 40 * cells; cnt = krylov() ? cyc : 0;   // d, z, p64 (f64) read, d and q written
+  } else if (n == "pcg_update") {
+    go = [&](int) { launch_pcg_update(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
+    b = 40 * cells; cnt = krylov() ? cyc : 0;   // p64, r, d, q read, p64 and r written (f64)
+  } else if (n.size() == 8 && (n.compare(0, 7, "mg_down") == 0) && n[7] >= '1' && n[7] <= '6') {
+    const int l = n[7] - '0';
+    if (l >= sc.lc) return fail(CFG_ERR_NOENT, "level " + n.substr(7) + " is in the coarse block");
+    go = [&, l](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, 0, s); };
+    b = (4 * 16 + 18) * (double)sc.lnx[l] * sc.lny[l]; cnt = cyc;
+  } else if (n.size() == 6 && (n.compare(0, 5, "mg_up") == 0) && n[5] >= '1' && n[5] <= '6') {
+    const int l = n[5] - '0';
+    if (l >= sc.lc) return fail(CFG_ERR_NOENT, "level " + n.substr(5) + " is in the coarse block");
+    go = [&, l](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, 0, d_ctl_, s); };
+    b = (17 + 4 * 16) * (double)sc.lnx[l] * sc.lny[l]; cnt = cyc;
   } else return fail(CFG_ERR_NOENT, "unknown kernel " + n);
   CFG_TRY(set_cond_mode(false));
   launch_bnorm(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, false, s);   // arm the multigrid kernels

@@ -133,7 +133,8 @@ class Engine {
   // most `cells` cells (levels above it run as tiled down/up kernels)
   int set_coarse_cells(int cells);
   int coarse_cells() const { return coarse_cells_; }
-  // coarsest level of the TOL/FP64 modes: 0 the reference's 120 sweeps, 1 its inverse
+  // coarsest level of the TOL/FP64 modes: 0 the reference's 120 sweeps, 1 its inverse,
+  // 2 its inverse factored beside the pressure loop and used from the next step on
   int set_coarse_solve(int direct);
   // FP64 mode: flexible preconditioned CG around the V-cycle (1) or plain defect correction (0)
   int set_krylov(int on);
@@ -168,6 +169,9 @@ class Engine {
   void enqueue_vcycle_ref(cudaStream_t s);   // one kernel per reference dispatch (cfg_vcycle)
   int max_lc() const;
   bool direct_coarse() const { return mode_ != CFG_SOLVE_FIXED && coarse_direct_ != 0; }
+  bool pipelined_coarse() const { return direct_coarse() && coarse_direct_ == 2; }
+  void enqueue_factor(cudaStream_t s);
+  void enqueue_factor_join(cudaStream_t s);
   bool krylov() const { return mode_ == CFG_SOLVE_FP64 && krylov_ != 0; }
   int cycle_tail() const { return any_fp64() ? (krylov() ? 3 : 2) : 1; }
   void enqueue_fp64_tail(cudaStream_t s);
@@ -178,6 +182,8 @@ class Engine {
 
   int device_ = 0;
   cudaStream_t stream_ = nullptr, user_stream_ = nullptr, body_stream_ = nullptr;
+  cudaStream_t side_stream_ = nullptr;           // the pipelined coarse factorisation's branch
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   std::vector<Scene> scenes_;
   SceneDesc* d_scenes_ = nullptr;
   SolveState* d_solve_ = nullptr;
@@ -201,6 +207,8 @@ class Engine {
   int last_cycles_ = 1;        // V-cycles of scene 0's last step, recorded by synchronize()
   int vcycle_launches_ = 0;
   size_t coarse_smem_ = 0;
+  size_t cf_smem_ = 0;          // k_coarse_factor's dynamic shared memory (largest coarsest level)
+  int cf_bw_ = 0;               // the widest coarsest level (k_coarse_factor's register window)
   int coarse_cells_ = COARSE_CELLS;
   int coarse_direct_ = 0;
   int krylov_ = 0;

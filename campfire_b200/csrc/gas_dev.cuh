@@ -43,7 +43,9 @@ struct SolveState {
   int active;               // 1 while this scene keeps cycling
   unsigned int counter;     // CTAs finished in the current reduction
   unsigned int maxu;        // max |u| over faces after projection (f32 bits; CFL step)
-  int direct_ok;            // the coarsest operator's inverse of this step is valid (direct coarse solve)
+  int direct_ok;            // the coarsest inverse in half cinv_cur of SceneDesc::cinv is valid (direct coarse solve)
+  int cinv_cur;             // the half of the double-buffered inverse the cycles use
+  int direct_ok_next;       // pipelined coarse solve: the other half, factored from this step's operator, is valid
   int pad;
   double delta, alpha, beta;   // Krylov FP64 mode: r.z of this cycle, the step length, the direction update
 };
@@ -70,7 +72,7 @@ struct SceneDesc {
   double *r64, *dA, *dB, *q64;  // Krylov FP64 mode: residual, search directions (ping-pong), L d
   SolveState* solve;
   const char* tmap;         // TMA tensor maps of the levels (TM_PER_LEVEL per level, 128 bytes each)
-  float* cinv;              // inverse of the coarsest operator (n x n, n = its cells), direct coarse solve
+  float* cinv;              // inverses of the coarsest operator, two halves of n x n (n = its cells), direct coarse solve
   LevelDesc lev[MAX_LEVELS];
 };
 

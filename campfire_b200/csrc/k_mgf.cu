@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       sres[k] = diag > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
     }
     __syncthreads();
-    const float* A = S.cinv;
+    const float* A = S.cinv + (size_t)S.solve->cinv_cur * n * n;
     const int q = lane & 7;
     for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
       const int k = base + (lane >> 3);
@@ -560,21 +560,49 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
 namespace {
 constexpr int CF_THREADS = 256;   // the coarsest level has at most 256 cells
 constexpr int CF_MAXBW = 32;
+constexpr size_t CF_SMEM_BUDGET = 200 * 1024;
 }
 
-__global__ void __launch_bounds__(CF_THREADS) k_coarse_factor(const SceneDesc* __restrict__ scenes) {
-  __shared__ float band[CF_THREADS * (CF_MAXBW + 1)];
-  __shared__ float rinv[CF_THREADS];
+// Columns of the inverse solved per pass: all n when the working columns fit the
+// shared-memory budget beside the band, else 128 per pass.
+__host__ __device__ inline int coarse_factor_cols(int n) {
+  const size_t W = CF_MAXBW + 1;   // the widest band
+  return ((size_t)n * n + (size_t)n * W + n) * sizeof(float) <= CF_SMEM_BUDGET ? n : 128;
+}
+size_t coarse_factor_smem(int n, int bw) {
+  const int C = coarse_factor_cols(n);
+  return ((size_t)n * (bw + 1) + n + (size_t)n * C) * sizeof(float);
+}
+
+// The inverse of the coarsest operator of each scene: the banded matrix is
+// factored L L^T by one warp (right-looking; lane l owns row jc + 1 + l of the
+// trailing band, takes the new column's l_kj from the lanes that computed them
+// by shuffle and updates its row from registers), then each thread solves
+// L L^T x = e_c for its column c with the band's sliding window in registers
+// (BWM = the band width bound, a compile-time size so the window stays in
+// registers); the forward result is kept in shared memory (Y[i * C + t]).
+// pipelined = 0: the inverse of this step's operator into the half the cycles use (direct_ok);
+// pipelined = 1: into the other half for the next step (direct_ok_next), while this step's
+// cycles use the current half.
+template <int BWM>
+__global__ void __launch_bounds__(CF_THREADS) k_coarse_factor(const SceneDesc* __restrict__ scenes, int pipelined) {
+  extern __shared__ float cf_smem[];
   __shared__ float s_dmax;
   __shared__ int s_ok;
   const SceneDesc& S = scenes[blockIdx.x];
   if (!S.enabled) return;
   const LevelDesc L = S.lev[S.nlev - 1];
   const int n = L.nx * L.ny, bw = L.nx, W = bw + 1;
-  if (n > CF_THREADS || bw > CF_MAXBW) {
-    if (threadIdx.x == 0) S.solve->direct_ok = 0;
+  int* ok_flag = pipelined ? &S.solve->direct_ok_next : &S.solve->direct_ok;
+  float* cinv = S.cinv + (size_t)(pipelined ? 1 - S.solve->cinv_cur : S.solve->cinv_cur) * n * n;
+  if (n > CF_THREADS || bw > BWM) {
+    if (threadIdx.x == 0) *ok_flag = 0;
     return;
   }
+  float* band = cf_smem;                 // n * W
+  float* rinv = band + (size_t)n * W;    // n
+  float* Y = rinv + n;                   // n * C
+  const int C = coarse_factor_cols(n);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int e = tid; e < n * W; e += CF_THREADS) band[e] = 0.f;
   __syncthreads();
@@ -619,40 +647,81 @@ __global__ void __launch_bounds__(CF_THREADS) k_coarse_factor(const SceneDesc* _
       const bool mine = lane < bw && i < n;
       float lij = 0.f;
       if (mine) lij = band[i * W + (i - jc)] / ljj;
+      // A[i][k] -= l_ij l_kj for k = jc + 1 + m <= i: l_kj from lane m, A[i][k] at band[i*W + lane - m]
+      float lk[BWM], tg[BWM];
+#pragma unroll
+      for (int m = 0; m < BWM; m++) lk[m] = __shfl_sync(0xffffffffu, lij, m);
+#pragma unroll
+      for (int m = 0; m < BWM; m++) tg[m] = (mine && m <= lane) ? band[i * W + (lane - m)] : 0.f;
       __syncwarp();
       if (lane == 0) band[jc * W] = ljj;
       if (mine) band[i * W + (i - jc)] = lij;
-      __syncwarp();
-      if (mine)
-        for (int k = jc + 1; k <= i; k++) band[i * W + (i - k)] = __fmaf_rn(-lij, band[k * W + (k - jc)], band[i * W + (i - k)]);
+#pragma unroll
+      for (int m = 0; m < BWM; m++)
+        if (mine && m <= lane) band[i * W + (lane - m)] = __fmaf_rn(-lij, lk[m], tg[m]);
       __syncwarp();
     }
   }
   __syncthreads();
   if (!s_ok) {
-    if (tid == 0) S.solve->direct_ok = 0;
+    if (tid == 0) *ok_flag = 0;
     return;
   }
   for (int k = tid; k < n; k += CF_THREADS) rinv[k] = 1.0f / band[k * W];
   __syncthreads();
-  const int c = tid;
-  if (c < n) {
-    float y[CF_THREADS];
-    for (int i = 0; i < c; i++) y[i] = 0.f;
-    for (int i = c; i < n; i++) {
-      float sum = i == c ? 1.f : 0.f;
-      for (int k = max(c, i - bw); k < i; k++) sum = __fmaf_rn(-band[i * W + (i - k)], y[k], sum);
-      y[i] = sum * rinv[i];
+  for (int c0 = 0; c0 < n; c0 += C) {
+    const int t = tid, c = c0 + tid;
+    if (t < C && c < n) {
+      float* y = Y + t;   // y[i * C]
+      for (int i = 0; i < c; i++) y[i * C] = 0.f;
+      // forward: y_i = (e_c[i] - sum_{k = max(c, i-bw)}^{i-1} L[i][k] y_k) / L[i][i], k ascending;
+      // win[m] = y_{i-1-m}
+      float win[BWM];
+#pragma unroll
+      for (int m = 0; m < BWM; m++) win[m] = 0.f;
+      for (int i = c; i < n; i++) {
+        float sum = i == c ? 1.f : 0.f;
+#pragma unroll
+        for (int m = BWM - 1; m >= 0; m--)
+          if (m < bw && i - 1 - m >= c) sum = __fmaf_rn(-band[i * W + (m + 1)], win[m], sum);
+        const float yi = sum * rinv[i];
+        y[i * C] = yi;
+#pragma unroll
+        for (int m = BWM - 1; m > 0; m--) win[m] = win[m - 1];
+        win[0] = yi;
+      }
+      // backward: x_i = (y_i - sum_{k = i+1}^{min(n-1, i+bw)} L[k][i] x_k) / L[i][i], k ascending;
+      // win[m] = x_{i+1+m}
+#pragma unroll
+      for (int m = 0; m < BWM; m++) win[m] = 0.f;
+      for (int i = n - 1; i >= 0; i--) {
+        float sum = y[i * C];
+#pragma unroll
+        for (int m = 0; m < BWM; m++)
+          if (m < bw && i + 1 + m <= n - 1) sum = __fmaf_rn(-band[(i + 1 + m) * W + (m + 1)], win[m], sum);
+        const float xi = sum * rinv[i];
+        cinv[(size_t)i * n + c] = xi;
+#pragma unroll
+        for (int m = BWM - 1; m > 0; m--) win[m] = win[m - 1];
+        win[0] = xi;
+      }
     }
-    for (int i = n - 1; i >= 0; i--) {
-      float sum = y[i];
-      const int kend = min(n - 1, i + bw);
-      for (int k = i + 1; k <= kend; k++) sum = __fmaf_rn(-band[k * W + (k - i)], y[k], sum);
-      y[i] = sum * rinv[i];
-    }
-    for (int i = 0; i < n; i++) S.cinv[(size_t)i * n + c] = y[i];
+    __syncthreads();
   }
-  if (tid == 0) S.solve->direct_ok = 1;
+  if (tid == 0) *ok_flag = 1;
+}
+
+// Pipelined coarse solve, after the step's pressure loop and the factorisation have both
+// finished: the next step's cycles use the inverse just factored.
+__global__ void k_cinv_swap(const SceneDesc* __restrict__ scenes, int nscenes) {
+  for (int s = threadIdx.x; s < nscenes; s += blockDim.x) {
+    const SceneDesc& S = scenes[s];
+    if (!S.enabled) continue;
+    SolveState* ss = S.solve;
+    ss->cinv_cur ^= 1;
+    ss->direct_ok = ss->direct_ok_next;
+    ss->direct_ok_next = 0;
+  }
 }
 
 // shared bytes of the coarse block for one scene (the layout built by k_mg_coarse)
@@ -684,11 +753,29 @@ void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int t
     launch_pdl(pdl_enabled(), k_mg_coarse, dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail,
                count_iter);
 }
-void launch_coarse_factor(const SceneDesc* scenes, int nscenes, cudaStream_t st) {
-  if (nscenes > 0) k_coarse_factor<<<nscenes, CF_THREADS, 0, st>>>(scenes);
+// bw: the widest coarsest level of the batch (the register window's bound)
+void launch_coarse_factor(const SceneDesc* scenes, int nscenes, size_t smem, int bw, int pipelined, cudaStream_t st) {
+  if (nscenes <= 0) return;
+  if (bw <= 8) k_coarse_factor<8><<<nscenes, CF_THREADS, smem, st>>>(scenes, pipelined);
+  else if (bw <= 16) k_coarse_factor<16><<<nscenes, CF_THREADS, smem, st>>>(scenes, pipelined);
+  else k_coarse_factor<32><<<nscenes, CF_THREADS, smem, st>>>(scenes, pipelined);
+}
+void launch_cinv_swap(const SceneDesc* scenes, int nscenes, cudaStream_t st) {
+  if (nscenes > 0) k_cinv_swap<<<1, 128, 0, st>>>(scenes, nscenes);
+}
+// The attribute belongs to the kernel, not to an engine: it is set to the largest size any
+// coarsest level can ask for, so engines of different sizes never lower it under each other.
+cudaError_t prepare_coarse_factor(size_t smem) {
+  const int cap = (int)std::max(smem, CF_SMEM_BUDGET);   // every level that fits: the columns' budget bounds it
+  cudaError_t e = cudaFuncSetAttribute(k_coarse_factor<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_coarse_factor<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_coarse_factor<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+  return e;
 }
 cudaError_t prepare_mg_coarse(size_t smem) {
-  return cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the kernel's attribute, shared by every engine: the largest size any schedule can ask for
+  return cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)std::max(smem, kCoarseSmemMax));
 }
 
 }  // namespace cfg

@@ -95,7 +95,13 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);
 cudaError_t prepare_mg_coarse(size_t smem);
 // direct coarse solve: the inverse of each scene's coarsest operator (scenes whose
 // coarsest level is wider than 32 cells keep the sweeps)
-void launch_coarse_factor(const SceneDesc* scenes, int nscenes, cudaStream_t st);
+// pipelined: factor this step's operator into the half the next step uses (see k_cinv_swap)
+void launch_coarse_factor(const SceneDesc* scenes, int nscenes, size_t smem, int bw, int pipelined, cudaStream_t st);
+// pipelined coarse solve: switch every enabled scene to the inverse factored during the step
+void launch_cinv_swap(const SceneDesc* scenes, int nscenes, cudaStream_t st);
+// dynamic shared memory of k_coarse_factor for a coarsest level of n cells and band width bw
+size_t coarse_factor_smem(int n, int bw);
+cudaError_t prepare_coarse_factor(size_t smem);
 // ||rhs||^2 (FP64 mode: ||rhs64||^2) of level 0; arms the pressure loop
 void launch_bnorm(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool fp64, cudaStream_t st);
 // FP64: p64 += p0

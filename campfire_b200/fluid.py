@@ -37,6 +37,12 @@ def _fp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
+def _coarse_mode(direct) -> int:
+    if direct == "pipelined" or (not isinstance(direct, bool) and direct == 2):
+        return 2
+    return 1 if direct else 0
+
+
 class _SceneOps:
     """Per-scene FluidSim surface shared by FluidSim and batch scene views."""
 
@@ -220,9 +226,10 @@ class FluidSim(_SceneOps):
         """Smoother schedule: the one-CTA coarse block starts at the first level with <= cells cells."""
         check(_lib.lib().cfg_set_coarse_cells(self._h, int(cells)))
 
-    def set_coarse_solve(self, direct: bool):
-        """TOL/FP64 modes: solve the coarsest level with its inverse (True) or 120 sweeps (False)."""
-        check(_lib.lib().cfg_set_coarse_solve(self._h, 1 if direct else 0))
+    def set_coarse_solve(self, direct):
+        """TOL/FP64 modes: the coarsest level by its inverse (True), by 120 sweeps (False), or by the
+        inverse factored beside the previous step's solve ("pipelined")."""
+        check(_lib.lib().cfg_set_coarse_solve(self._h, _coarse_mode(direct)))
 
     def set_krylov(self, on: bool):
         """FP64 mode: preconditioned CG around the V-cycle (True) or plain defect correction (False)."""
@@ -293,8 +300,8 @@ class Batch:
     def set_coarse_cells(self, cells: int):
         check(_lib.lib().cfg_batch_set_coarse_cells(self._h, int(cells)))
 
-    def set_coarse_solve(self, direct: bool):
-        check(_lib.lib().cfg_batch_set_coarse_solve(self._h, 1 if direct else 0))
+    def set_coarse_solve(self, direct):
+        check(_lib.lib().cfg_batch_set_coarse_solve(self._h, _coarse_mode(direct)))
 
     def set_krylov(self, on: bool):
         check(_lib.lib().cfg_batch_set_krylov(self._h, 1 if on else 0))
@@ -347,7 +354,7 @@ class Server:
 
     def set_solver(self, mode=_lib.SOLVE_FP64, ncycles=1, tol=1e-10, max_cycles=300, coarse_direct=True,
                    coarse_cells=0, krylov=False):
-        check(_lib.lib().cfg_server_set_solver(self._h, mode, ncycles, tol, max_cycles, 1 if coarse_direct else 0,
+        check(_lib.lib().cfg_server_set_solver(self._h, mode, ncycles, tol, max_cycles, _coarse_mode(coarse_direct),
                                                coarse_cells, 1 if krylov else 0))
 
     def slot_bytes(self, size_class: int) -> int:

@@ -188,8 +188,11 @@ int cfg_set_coarse_cells(cfg_sim* sim, int cells);
 /* Coarsest-level solve of the TOL and FP64 modes (no counterpart in the reference, which runs
  * one fixed cycle): 0 (default) the reference's 120 red-black sweeps; 1 the level's operator
  * inverted once per step (f32 banded Cholesky and column solves, after the coefficients are
- * built) and applied in every cycle. Scenes whose coarsest level is wider than 32 cells, or
- * has a sealed gas pocket (no open boundary in reach: singular operator), keep the sweeps.
+ * built) and applied in every cycle; 2 (pipelined) the same inverse factored beside the step's
+ * pressure loop and applied from the next step on, so the factorisation leaves the critical
+ * path (each step's cycles use the previous step's coarsest operator inverse; the first step
+ * after a reset or load keeps the sweeps). Scenes whose coarsest level is wider than 32 cells,
+ * or has a sealed gas pocket (no open boundary in reach: singular operator), keep the sweeps.
  * FIXED mode ignores it. */
 int cfg_set_coarse_solve(cfg_sim* sim, int direct);
 int cfg_batch_set_coarse_solve(cfg_batch* b, int direct);

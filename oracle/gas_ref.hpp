@@ -206,6 +206,7 @@ struct Sim {
 
   // js/fluid.js:162-176
   void reset() {
+    cinv_ok = false;
     std::fill(T.begin(), T.end(), R((float)Phys::Tamb));
     T2 = T; Th = T;
     const Vec4<R> y0{R(0), R(host.YOamb), R(0), R(0)};
@@ -1010,14 +1011,20 @@ struct Sim {
         }
       }
   }
+  // coarse_direct 2 (pipelined): the cycles use the inverse factored during the previous
+  // step; this step's operator is factored after its solve for the next step
   void pressure_solve() {
+    pressure_solve_inner();
+    if (coarse_direct == 2 && mode != SOLVE_FIXED) coarse_factor();
+  }
+  void pressure_solve_inner() {
     if (mode == SOLVE_FIXED) {
       for (int c = 0; c < ncycles; c++) vcycle();
       last_cycles = ncycles;
       const double b = rhs_norm(); last_rel = b > 0 ? res_norm() / b : 0.0;
       return;
     }
-    if (coarse_direct) coarse_factor();
+    if (coarse_direct == 1) coarse_factor();
     const bool direct = coarse_direct && cinv_ok;
     if (mode == SOLVE_TOL) {
       const double b = rhs_norm();

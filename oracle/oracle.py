@@ -163,7 +163,7 @@ class OracleSim:
         self._chk(self._f.set_solver(self._h, mode, ncycles, tol, max_cycles))
 
     def set_coarse_solve(self, direct):
-        self._chk(self._f.set_coarse_solve(self._h, 1 if direct else 0))
+        self._chk(self._f.set_coarse_solve(self._h, 2 if (direct == "pipelined" or (not isinstance(direct, bool) and direct == 2)) else (1 if direct else 0)))
 
     def set_krylov(self, on):
         self._chk(self._f.set_krylov(self._h, 1 if on else 0))

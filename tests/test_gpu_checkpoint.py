@@ -15,10 +15,10 @@ from campfire_b200.fluid import load_scene
 pytestmark = pytest.mark.gpu
 
 
-def make(nx, ny, sc, dt=None):
+def make(nx, ny, sc, dt=None, coarse=True):
     g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": dt or sc["dt"]}, width=0.8).init()
     g.set_solver(cb.SOLVE_FP64, 1, 1e-9, 100)
-    g.set_coarse_solve(True)
+    g.set_coarse_solve(coarse)
     return g
 
 
@@ -26,17 +26,18 @@ def state(g):
     return cb.field_hash(g), g.read_p64().tobytes()
 
 
-@pytest.mark.parametrize("cfl", [0.0, 0.5])
-def test_resume_is_bit_exact(tmp_path, cfl):
+@pytest.mark.parametrize("cfl,coarse", [(0.0, True), (0.5, True), (0.0, "pipelined")])
+def test_resume_is_bit_exact(tmp_path, cfl, coarse):
+    # pipelined: the inverse factored during the last saved step is part of the state
     nx, ny = 96, 144
     sc = cb.generate_scene(1, nx, ny, 0.8, 4321)
-    a = make(nx, ny, sc)
+    a = make(nx, ny, sc, coarse=coarse)
     load_scene(a, sc)
     if cfl:
         a.set_cfl(cfl, sc["dt"])
     a.step(6)
     ref = state(a)
-    b = make(nx, ny, sc)
+    b = make(nx, ny, sc, coarse=coarse)
     load_scene(b, sc)
     if cfl:
         b.set_cfl(cfl, sc["dt"])
@@ -44,7 +45,7 @@ def test_resume_is_bit_exact(tmp_path, cfl):
     path = str(tmp_path / "scene.ckpt")
     b.save_checkpoint(path)
     b.close()
-    c = make(nx, ny, sc, dt=0.001)   # another dt and an empty state: all of it comes from the file
+    c = make(nx, ny, sc, dt=0.001, coarse=coarse)   # another dt and an empty state: all of it comes from the file
     if cfl:
         c.set_cfl(cfl, sc["dt"])
     c.load_checkpoint(path)

@@ -79,3 +79,55 @@ def test_singular_coarsest_keeps_the_sweeps(oracle_mod):
     a, b = g.readBuffer("p").astype(np.float64), o.read("p")
     assert np.array_equal(a, b), norm_err(a, b)
     g.close()
+
+
+def test_pipelined_stages_are_bit_exact(oracle_mod):
+    """Pipelined coarse solve: the first solve after a reset has no inverse (sweeps) and factors
+    its operator for the next; the second solve applies that inverse. Both bit-exact."""
+    g, o, _ = make_pair(oracle_mod, 128, 192, kind=0, seed=1234, warm_steps=6, mode=cb.SOLVE_TOL, tol=1e-30,
+                        max_cycles=3)
+    g.set_coarse_solve("pipelined"); o.set_coarse_solve("pipelined")
+    g.run_stage("coef_rhs"); o.stage("coef_rhs")
+    sync(o, g)
+    for k in range(2):
+        g.run_stage("pressure"); o.stage("pressure")
+        a, b = g.readBuffer("p").astype(np.float64), o.read("p")
+        assert np.array_equal(a, b), (k, norm_err(a, b))
+    g.close()
+
+
+def test_pipelined_fp64_steps_match_oracle(oracle_mod):
+    g, o, _ = make_pair(oracle_mod, 128, 192, kind=0, seed=1400, warm_steps=4, mode=cb.SOLVE_FP64, tol=1e-10,
+                        max_cycles=200)
+    g.set_krylov(True); o.set_krylov(True)
+    g.set_coarse_solve("pipelined"); o.set_coarse_solve("pipelined")
+    for k in range(3):
+        g.step(1); o.step(1)
+        gi, oi = g.info(), o.info()
+        assert abs(gi["last_cycles"] - oi["last_cycles"]) <= 1, (k, gi, oi)
+        assert gi["last_rel"] <= 1e-10
+        e = norm_err(g.read_p64(), o.read("p64"))
+        assert e <= 1e-5 * (k + 1), (k, e)
+    g.close()
+
+
+def test_pipelined_and_direct_take_the_same_cycles():
+    """On the benchmark scene the previous step's coarsest inverse costs no cycles in the
+    Krylov mode (the oracle: 121 cycles over 14 steps either way at 256x384, 1e-6)."""
+    sc = cb.generate_scene(0, 128, 192, 0.8, 1234)
+    from campfire_b200.fluid import load_scene
+    cyc = {}
+    for mode in (True, "pipelined"):
+        g = cb.FluidSim(0, {"nx": 128, "ny": 192, "dt": sc["dt"]}, width=0.8).init()
+        load_scene(g, sc)
+        g.set_solver(cb.SOLVE_FP64, 1, 1e-6, 100)
+        g.set_krylov(True)
+        g.set_coarse_solve(mode)
+        c = 0
+        for k in range(8):
+            g.step(1)
+            g.synchronize()
+            c += g.info()["last_cycles"]
+        cyc[mode] = c
+        g.close()
+    assert abs(cyc["pipelined"] - cyc[True]) <= 2, cyc

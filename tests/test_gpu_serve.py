@@ -150,3 +150,18 @@ def test_submitted_jobs_match_the_batch_run():
         s.submit(0, 1, 1, 400)
         s.set_solver(**SOLVER)
     s.close()
+
+
+def test_pipelined_coarse_solve_keeps_results_independent_of_the_mix():
+    """With the pipelined coarsest inverse a slot's inverse belongs to its own scene: a job
+    admitted into a used slot starts without one (reset), so mixes and reuse change nothing."""
+    js = jobs()[:4]
+    s = cb.Server(CLASSES, [1, 1], 64e9)
+    s.set_solver(**dict(SOLVER, coarse_direct="pipelined"))
+    mixed, _, _ = s.run(js)
+    alone = []
+    for j in js:
+        r, _, _ = s.run([dict(j, arrival_s=0.0)])
+        alone.append(r[0]["hash"])
+    s.close()
+    assert [r["hash"] for r in mixed] == alone
