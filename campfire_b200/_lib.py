@@ -140,6 +140,7 @@ def lib():
         "cfg_time_kernel": [vp, cs, ci, dp, dp, dp],
         "cfg_pressure_residual_noalloc": [vp, vp, vp, vp, ci, ci, cd, vp, dp],
         "cfg_set_coarse_cells": [vp, ci], "cfg_batch_set_coarse_cells": [vp, ci],
+        "cfg_set_coarse_cluster": [vp, ci], "cfg_batch_set_coarse_cluster": [vp, ci],
         "cfg_autotune": [ci, ci, ip, ip, ci, ci, ip, ip, dp, ip],
         "cfg_set_coarse_solve": [vp, ci], "cfg_batch_set_coarse_solve": [vp, ci],
         "cfg_checkpoint_save": [vp, cs], "cfg_checkpoint_load": [vp, cs],

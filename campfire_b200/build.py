@@ -23,9 +23,9 @@ LIB = os.path.join(HERE, "libcampfire_gas.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2",
                      "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
-SOURCES = ["k_advect.cu", "k_diffsrc.cu", "k_forces.cu", "k_mg.cu", "k_mgf.cu", "k_misc.cu", "k_render.cu", "noalloc.cu", "engine.cu",
+SOURCES = ["k_advect.cu", "k_diffsrc.cu", "k_forces.cu", "k_mg.cu", "k_mgf.cu", "k_mgc.cu", "k_misc.cu", "k_render.cu", "noalloc.cu", "engine.cu",
            "capi.cpp", "scene.cpp", "serve.cpp", "wood.cpp", "rigid.cpp"]
-HEADERS = ["gas_dev.cuh", "kernels.h", "reduce.cuh", "engine.h", "tma.cuh", "wood.h", "rigid.h"]
+HEADERS = ["gas_dev.cuh", "kernels.h", "reduce.cuh", "engine.h", "tma.cuh", "wood.h", "rigid.h", "mg_common.cuh"]
 
 
 def nvcc() -> str:

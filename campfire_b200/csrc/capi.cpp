@@ -191,6 +191,14 @@ extern "C" int cfg_batch_set_coarse_cells(cfg_batch* b, int cells) {
   if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
   return guarded([&] { return b->eng->set_coarse_cells(cells); });
 }
+extern "C" int cfg_set_coarse_cluster(cfg_sim* sim, int cs) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->set_coarse_cluster(cs); });
+}
+extern "C" int cfg_batch_set_coarse_cluster(cfg_batch* b, int cs) {
+  if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
+  return guarded([&] { return b->eng->set_coarse_cluster(cs); });
+}
 
 int cfg::load_generated_scene(cfg::Engine& eng, int s, int kind, double width, uint64_t seed) {
   const int nx = eng.scene_nx(s), ny = eng.scene_ny(s);

@@ -110,7 +110,15 @@ int Engine::activate() const {
 
 // The coarse block starts at the first level with at most `cells` cells whose
 // arrays fit in one CTA's shared memory (else at the coarsest level).
-int Engine::choose_lc(const Scene& sc, int cells) {
+// cs > 0: the cluster coarse phase, which starts at level 1 at the earliest (level 0
+// always runs as tiled kernels) and fits each CTA's share of the levels
+int Engine::choose_lc(const Scene& sc, int cells, int cs) {
+  if (cs > 0) {
+    for (int l = std::min(1, sc.nlev - 1); l < sc.nlev; l++)
+      if (sc.lnx[l] * sc.lny[l] <= cells && cluster_smem_bytes(sc.lnx, sc.lny, l, sc.nlev, cs) <= kClusterSmemMax)
+        return l;
+    return sc.nlev - 1;
+  }
   for (int l = 0; l < sc.nlev; l++)
     if (sc.lnx[l] * sc.lny[l] <= cells && coarse_smem_bytes(sc.lnx, sc.lny, l, sc.nlev) <= kCoarseSmemMax) return l;
   return sc.nlev - 1;
@@ -135,7 +143,7 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
     }
     sc.nlev = L;
     if (sc.lnx[L - 1] * sc.lny[L - 1] > 256) return fail(CFG_ERR_RANGE, "coarsest level too large");
-    sc.lc = choose_lc(sc, coarse_cells_);
+    sc.lc = choose_lc(sc, coarse_cells_, 0);
     coarse_smem_ = std::max(coarse_smem_, coarse_smem_bytes(sc.lnx, sc.lny, sc.lc, sc.nlev));
     const int cn = sc.lnx[L - 1] * sc.lny[L - 1], cbw = sc.lnx[L - 1];
     if (cbw <= 32) { cf_smem_ = std::max(cf_smem_, coarse_factor_smem(cn, cbw)); cf_bw_ = std::max(cf_bw_, cbw); }
@@ -458,21 +466,41 @@ int Engine::build_worklists() {
   return CFG_OK;
 }
 
+int Engine::set_coarse_cluster(int cs) {
+  if (cs != 0 && cs != 2 && cs != 4 && cs != 8 && cs != 16)
+    return fail(CFG_ERR_INVAL, "the coarse cluster size must be 0 (one CTA), 2, 4, 8 or 16");
+  for (const auto& sc : scenes_)
+    if (cs > 0 && sc.nlev < 2) return fail(CFG_ERR_INVAL, "the cluster coarse phase needs two levels or more in every scene");
+  const int prev = coarse_cluster_;
+  coarse_cluster_ = cs;
+  const int rc = set_coarse_cells(coarse_cells_);
+  if (rc != CFG_OK) coarse_cluster_ = prev;
+  return rc;
+}
+
 int Engine::set_coarse_cells(int cells) {
   if (cells < 1) return fail(CFG_ERR_INVAL, "coarse cells must be >= 1");
   CFG_TRY(activate());
   CFG_CUDA(cudaStreamSynchronize(st()));
+  const int cs = coarse_cluster_;
   size_t smem = 0;
   std::vector<int> lcs(scenes_.size());
   for (size_t s = 0; s < scenes_.size(); s++) {
     const Scene& sc = scenes_[s];
-    lcs[s] = choose_lc(sc, cells);
-    smem = std::max(smem, coarse_smem_bytes(sc.lnx, sc.lny, lcs[s], sc.nlev));
+    lcs[s] = choose_lc(sc, cells, cs);
+    smem = std::max(smem, cs > 0 ? cluster_smem_bytes(sc.lnx, sc.lny, lcs[s], sc.nlev, cs)
+                                 : coarse_smem_bytes(sc.lnx, sc.lny, lcs[s], sc.nlev));
   }
-  if (smem > kCoarseSmemMax) return fail(CFG_ERR_RANGE, "the coarsest level does not fit in one CTA's shared memory");
-  CFG_CUDA(prepare_mg_coarse(smem));
+  if (cs > 0) {
+    if (smem > kClusterSmemMax) return fail(CFG_ERR_RANGE, "the coarse levels do not fit in the cluster's shared memory");
+    CFG_CUDA(prepare_mg_cluster());
+    cluster_smem_ = smem;
+  } else {
+    if (smem > kCoarseSmemMax) return fail(CFG_ERR_RANGE, "the coarsest level does not fit in one CTA's shared memory");
+    CFG_CUDA(prepare_mg_coarse(smem));
+    coarse_smem_ = smem;
+  }
   coarse_cells_ = cells;
-  coarse_smem_ = smem;
   for (size_t s = 0; s < scenes_.size(); s++) {
     scenes_[s].lc = lcs[s];
     scenes_[s].desc.lc = lcs[s];
@@ -937,7 +965,10 @@ void Engine::enqueue_vcycle(cudaStream_t s, int tail, int count_iter) {
     count_iter = 0;
     vcycle_launches_++;
   }
-  launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, count_iter, coarse_smem_, s);
+  if (coarse_cluster_ > 0)
+    launch_mg_cluster(d_scenes_, nscenes(), d_ctl_, coarse_cluster_, count_iter, cluster_smem_, s);
+  else
+    launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, count_iter, coarse_smem_, s);
   vcycle_launches_++;
   for (int l = LD - 1; l >= 0; l--) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
@@ -1273,7 +1304,10 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 0, d_ctl_, s); };
     b = (17 + 4 * 16) * cells; cnt = cyc;   // prolongation + 4 colour passes
   } else if (n == "mg_coarse") {
-    go = [&](int) { launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, 0, coarse_smem_, s); };
+    go = [&](int) {
+      if (coarse_cluster_ > 0) launch_mg_cluster(d_scenes_, nscenes(), d_ctl_, coarse_cluster_, 0, cluster_smem_, s);
+      else launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, 0, coarse_smem_, s);
+    };
     // the reference schedule's V-cycle bytes of the levels the block covers (163 B per level cell)
     b = 0;
     for (int l = sc.lc; l < sc.nlev; l++) b += 163.0 * sc.lnx[l] * sc.lny[l];

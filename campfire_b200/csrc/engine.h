@@ -133,6 +133,9 @@ class Engine {
   // most `cells` cells (levels above it run as tiled down/up kernels)
   int set_coarse_cells(int cells);
   int coarse_cells() const { return coarse_cells_; }
+  // the coarse phase on one CTA (0) or on a cluster of cs CTAs per scene (2..16, from level 1)
+  int set_coarse_cluster(int cs);
+  int coarse_cluster() const { return coarse_cluster_; }
   // coarsest level of the TOL/FP64 modes: 0 the reference's 120 sweeps, 1 its inverse,
   // 2 its inverse factored beside the pressure loop and used from the next step on
   int set_coarse_solve(int direct);
@@ -146,7 +149,7 @@ class Engine {
   int nscenes() const { return (int)scenes_.size(); }
 
  private:
-  static int choose_lc(const Scene& sc, int cells);
+  static int choose_lc(const Scene& sc, int cells, int cs);
   int alloc_scene(Scene& sc);
   int build_tmaps(Scene& sc);
   int upload_desc(int s);
@@ -208,6 +211,8 @@ class Engine {
   int vcycle_launches_ = 0;
   size_t coarse_smem_ = 0;
   size_t cf_smem_ = 0;          // k_coarse_factor's dynamic shared memory (largest coarsest level)
+  int coarse_cluster_ = 0;      // 0: one-CTA coarse block; cs: the cluster coarse phase
+  size_t cluster_smem_ = 0;
   int cf_bw_ = 0;               // the widest coarsest level (k_coarse_factor's register window)
   int coarse_cells_ = COARSE_CELLS;
   int coarse_direct_ = 0;

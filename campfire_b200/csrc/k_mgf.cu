@@ -21,6 +21,7 @@
 #include "gas_dev.cuh"
 #include "kernels.h"
 #include "reduce.cuh"
+#include "mg_common.cuh"
 #include "tma.cuh"
 
 #include <algorithm>
@@ -285,31 +286,34 @@ namespace {
 constexpr int CB_THREADS = 1024;
 constexpr int CB_WARPS = CB_THREADS / 32;
 constexpr int COARSEST_SCRATCH = 0;     // the coarsest keeps its stencils in registers
+using namespace mgc;
 
-struct LvS { float *p, *rhs, *ax, *ay; int nx, ny, pc, pu; float h2; int pad; };
 
-__device__ __forceinline__ void stencil_d(const LvS& L, int i, int j, float& off, float& diag) {
-  off = 0.f; diag = 0.f;
-  const float w = L.ax[j * L.pu + i], e = L.ax[j * L.pu + i + 1];
-  const float s = L.ay[j * L.pc + i], n = L.ay[(j + 1) * L.pc + i];
-  const float* p = L.p;
-  if (i > 0) { off += w * p[j * L.pc + i - 1]; diag += w; } else { diag += 2.f * w; }
-  if (i < L.nx - 1) { off += e * p[j * L.pc + i + 1]; diag += e; } else { diag += 2.f * e; }
-  if (j > 0) { off += s * p[(j - 1) * L.pc + i]; diag += s; }
-  if (j < L.ny - 1) { off += n * p[(j + 1) * L.pc + i]; diag += n; } else { diag += 2.f * n; }
-}
-// one colour pass: warps take rows, lanes take every other cell of the row
-// A pass reads only cells of the other colour: up to 4 rows of a thread are computed
-// before any is stored, so their shared-memory loads overlap.
-__device__ __forceinline__ void pass_d(const LvS& L, int color) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i0 = 0; i0 < L.nx; i0 += 64)
-    for (int j0 = warp; j0 < L.ny; j0 += 4 * CB_WARPS) {
+// Cells of a level mapped linearly onto the block: thread t takes column t % w of rows
+// t / w, t / w + R, ... (R = rows per round of the block), so every lane works whatever the
+// level's width and warps beyond the level's cells skip at once. w > CB_THREADS: the block
+// strides along each row instead.
+struct LinMap {
+  int i0, j0, R;   // first column and row of this thread, rows per round (0: the thread idles)
+  __device__ __forceinline__ LinMap(int w) {
+    if (w >= CB_THREADS) { i0 = threadIdx.x; j0 = 0; R = 1; }
+    else { R = CB_THREADS / w; i0 = threadIdx.x % w; j0 = threadIdx.x / w; if (j0 >= R) R = 0; }
+  }
+  __device__ __forceinline__ int di(int w) const { return w >= CB_THREADS ? CB_THREADS : w; }   // column stride
+};
+// one colour pass over the cells of one colour: slot q of row j is cell i = 2q + ((j + color) & 1).
+// A pass reads only cells of the other colour: up to 4 rows of a thread are computed before
+// any is stored, so their shared-memory loads overlap.
+__device__ __forceinline__ void pass_d(const LvS& L, int color, const LinMap& mp) {
+  const int half = (L.nx + 1) >> 1;
+  if (!mp.R) return;
+  for (int q = mp.i0; q < half; q += mp.di(half))
+    for (int jb = mp.j0; jb < L.ny; jb += 4 * mp.R) {
       float v[4];
       int kk[4];
       #pragma unroll
       for (int m = 0; m < 4; m++) {
-        const int j = j0 + m * CB_WARPS, i = i0 + 2 * lane + ((j + color) & 1);
+        const int j = jb + m * mp.R, i = 2 * q + ((j + color) & 1);
         kk[m] = -1;
         if (j < L.ny && i < L.nx) {
           float off, diag; stencil_d(L, i, j, off, diag);
@@ -323,51 +327,64 @@ __device__ __forceinline__ void pass_d(const LvS& L, int color) {
         if (kk[m] >= 0) L.p[kk[m]] = v[m];
     }
 }
-__device__ __forceinline__ void bar_coarsest(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
-
-// x / d rounded to nearest from r = RN(1/d): q0 = RN(x r), q = RN(q0 + r (x - d q0)),
-// the residual x - d q0 exact by FMA (Markstein, IBM J. Res. Dev. 34(1), 1990). Equal
-// to the IEEE quotient for quotients in the normal range; it replaces the division
-// subroutine on the coarsest level, whose diagonals stay fixed for all its sweeps.
-__device__ __forceinline__ float div_by_rcp(float x, float d, float r) {
-  const float q0 = __fmul_rn(x, r);
-  const float e = __fmaf_rn(-q0, d, x);
-  return __fmaf_rn(e, r, q0);
-}
-
-// One coarsest-level cell with its fixed stencil (pressure.wgsl:132-156).
-struct CCell {
-  float w, e, s, n, rh, diag, rcp;
-  int kp;
-  bool act, hw, he, hs, hn;
-};
-__device__ __forceinline__ CCell coarsest_cell(const LvS& L, int k) {
-  CCell c{};
-  c.act = k < L.nx * L.ny;
-  if (!c.act) return c;
-  const int i = k % L.nx, j = k / L.nx;
-  c.kp = j * L.pc + i;
-  c.w = L.ax[j * L.pu + i]; c.e = L.ax[j * L.pu + i + 1];
-  c.s = L.ay[j * L.pc + i]; c.n = L.ay[(j + 1) * L.pc + i];
-  float diag = 0.f;
-  if (i > 0) diag += c.w; else diag += 2.f * c.w;
-  if (i < L.nx - 1) diag += c.e; else diag += 2.f * c.e;
-  if (j > 0) diag += c.s;
-  if (j < L.ny - 1) diag += c.n; else diag += 2.f * c.n;
-  c.diag = diag;
-  c.rcp = diag > 0.f ? __frcp_rn(diag) : 0.f;
-  c.rh = L.rhs[c.kp] * L.h2;
-  c.hw = i > 0; c.he = i < L.nx - 1; c.hs = j > 0; c.hn = j < L.ny - 1;
+// A level visit's smoothing with every cell's stencil in registers: thread t owns colour
+// slots t, t + CB_THREADS, ... (slot -> row slot / half, cell 2 (slot % half) + parity) of
+// each colour, and builds their stencils once (coefficients, neighbour flags, rhs h2, the
+// diagonal and its correctly rounded reciprocal) for the visit's two sweeps. The update is
+// pass_d's, with the division by the diagonal as div_by_rcp: the same quotient.
+// one cell's stencil in 9 registers: fl bit 0..3 = west, east, south, north neighbour present
+struct RCell { float w, e, s, n, rh, diag, rcp; int kp, fl; };
+__device__ __forceinline__ RCell rcell_of(const LvS& L, int i, int j) {
+  const CCell q = coarsest_cell(L, j * L.nx + i);
+  RCell c;
+  c.w = q.w; c.e = q.e; c.s = q.s; c.n = q.n; c.rh = q.rh; c.diag = q.diag; c.rcp = q.rcp; c.kp = q.kp;
+  c.fl = (q.hw ? 1 : 0) | (q.he ? 2 : 0) | (q.hs ? 4 : 0) | (q.hn ? 8 : 0);
   return c;
 }
-__device__ __forceinline__ void coarsest_update(float* p, int pc, const CCell& c) {
-  if (!c.act) return;
-  float off = 0.f;
-  if (c.hw) off += c.w * p[c.kp - 1];
-  if (c.he) off += c.e * p[c.kp + 1];
-  if (c.hs) off += c.s * p[c.kp - pc];
-  if (c.hn) off += c.n * p[c.kp + pc];
-  p[c.kp] = c.diag > 0.f ? div_by_rcp(off - c.rh, c.diag, c.rcp) : 0.f;
+template <int NPER>
+__device__ __forceinline__ void smooth_regs(const LvS& L, int first) {
+  const int half = (L.nx + 1) >> 1;
+  RCell c[2][NPER];
+  bool act[2][NPER];
+  #pragma unroll
+  for (int col = 0; col < 2; col++)
+    #pragma unroll
+    for (int m = 0; m < NPER; m++) {
+      const int t = threadIdx.x + m * CB_THREADS;
+      const int j = t / half, i = 2 * (t - j * half) + ((j + col) & 1);
+      act[col][m] = j < L.ny && i < L.nx;
+      if (act[col][m]) c[col][m] = rcell_of(L, i, j);
+    }
+  #pragma unroll 1
+  for (int k = 0; k < 2; k++)
+    #pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int col = h == 0 ? first : 1 - first;
+      float v[NPER];
+      #pragma unroll
+      for (int m = 0; m < NPER; m++) {
+        if (!act[col][m]) continue;
+        const RCell& q = c[col][m];
+        float off = 0.f;
+        if (q.fl & 1) off += q.w * L.p[q.kp - 1];
+        if (q.fl & 2) off += q.e * L.p[q.kp + 1];
+        if (q.fl & 4) off += q.s * L.p[q.kp - L.pc];
+        if (q.fl & 8) off += q.n * L.p[q.kp + L.pc];
+        v[m] = q.diag > 0.f ? div_by_rcp(off - q.rh, q.diag, q.rcp) : 0.f;
+      }
+      #pragma unroll
+      for (int m = 0; m < NPER; m++)
+        if (act[col][m]) L.p[c[col][m].kp] = v[m];
+      __syncthreads();
+    }
+}
+// both sweeps of a level visit (colour `first` first in each sweep, a block barrier after
+// every pass): in registers when each thread owns at most one cell of a colour
+__device__ __forceinline__ void smooth_visit(const LvS& L, int first) {
+  const int half = (L.nx + 1) >> 1, nslot = half * L.ny;
+  if (nslot <= CB_THREADS) { smooth_regs<1>(L, first); return; }
+  const LinMap mh(half);
+  for (int k = 0; k < 2; k++) { pass_d(L, first, mh); __syncthreads(); pass_d(L, 1 - first, mh); __syncthreads(); }
 }
 }  // namespace
 
@@ -432,16 +449,22 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // ---- down
   for (int l = lc; l < nl - 1; l++) {
     const LvS F = lv[l], Cc = lv[l + 1];
-    for (int k = 0; k < 2; k++) { pass_d(F, 0); __syncthreads(); pass_d(F, 1); __syncthreads(); }
-    for (int j = warp; j < F.ny; j += CB_WARPS)
-      for (int i = lane; i < F.nx; i += 32) {
-        float off, diag; stencil_d(F, i, j, off, diag);
-        const int e = j * F.pc + i;
-        sres[j * F.nx + i] = diag <= 0.f ? 0.f : F.rhs[e] - (off - diag * F.p[e]) / F.h2;
-      }
+    smooth_visit(F, 0);
+    {
+      const LinMap mp(F.nx);
+      if (mp.R)
+        for (int j = mp.j0; j < F.ny; j += mp.R)
+          for (int i = mp.i0; i < F.nx; i += mp.di(F.nx)) {
+            float off, diag; stencil_d(F, i, j, off, diag);
+            const int e = j * F.pc + i;
+            sres[j * F.nx + i] = diag <= 0.f ? 0.f : F.rhs[e] - (off - diag * F.p[e]) / F.h2;
+          }
+    }
     __syncthreads();
-    for (int J = warp; J < Cc.ny; J += CB_WARPS)
-      for (int I = lane; I < Cc.nx; I += 32) {
+    const LinMap mc(Cc.nx);
+    if (mc.R)
+    for (int J = mc.j0; J < Cc.ny; J += mc.R)
+      for (int I = mc.i0; I < Cc.nx; I += mc.di(Cc.nx)) {
         const float r = sres[(2 * J) * F.nx + 2 * I] + sres[(2 * J) * F.nx + 2 * I + 1] + sres[(2 * J + 1) * F.nx + 2 * I] +
                         sres[(2 * J + 1) * F.nx + 2 * I + 1];
         Cc.rhs[J * Cc.pc + I] = 0.25f * r;
@@ -505,8 +528,10 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // ---- up
   for (int l = nl - 2; l >= lc; l--) {
     const LvS F = lv[l], Cc = lv[l + 1];
-    for (int j = warp; j < F.ny; j += CB_WARPS)
-      for (int i = lane; i < F.nx; i += 32) {
+    const LinMap mp(F.nx);
+    if (mp.R)
+    for (int j = mp.j0; j < F.ny; j += mp.R)
+      for (int i = mp.i0; i < F.nx; i += mp.di(F.nx)) {
         const int I = i / 2, J = j / 2;
         const int I2 = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), Cc.nx - 1);
         const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), Cc.ny - 1);
@@ -516,13 +541,15 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
         F.p[j * F.pc + i] += diag > 0.f ? c : 0.f;
       }
     __syncthreads();
-    for (int k = 0; k < 2; k++) { pass_d(F, 1); __syncthreads(); pass_d(F, 0); __syncthreads(); }
+    smooth_visit(F, 1);
   }
   // ---- write level lc back; when the block covers level 0, finish the cycle here
   const LevelDesc& G = S.lev[lc];
   double part = 0.0, part2 = 0.0;
-  for (int j = warp; j < G.ny; j += CB_WARPS)
-    for (int i = lane; i < G.nx; i += 32) {
+  const LinMap mw(G.nx);
+  if (mw.R)
+  for (int j = mw.j0; j < G.ny; j += mw.R)
+    for (int i = mw.i0; i < G.nx; i += mw.di(G.nx)) {
       const int e = j * V0.pc + i;
       G.p[j * G.pc + i] = V0.p[e];
       if (lc == 0 && tail == 1) {

@@ -92,6 +92,12 @@ void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int nt
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
                       cudaStream_t st);
 size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);
+// the cluster coarse phase (k_mgc.cu): levels lc..coarsest of each scene on a cluster of cs CTAs
+constexpr size_t kClusterSmemMax = 232448 - 2048;
+size_t cluster_smem_bytes(const int* lnx, const int* lny, int lc, int nlev, int cs);
+cudaError_t prepare_mg_cluster();
+void launch_mg_cluster(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int cs, int count_iter, size_t smem,
+                       cudaStream_t st);
 cudaError_t prepare_mg_coarse(size_t smem);
 // direct coarse solve: the inverse of each scene's coarsest operator (scenes whose
 // coarsest level is wider than 32 cells keep the sweeps)

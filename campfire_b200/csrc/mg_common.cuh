@@ -1,0 +1,71 @@
+// Pieces of the multigrid level solves shared by the one-CTA coarse block (k_mgf.cu)
+// and the cluster coarse phase (k_mgc.cu): a level held in shared memory with the
+// global row pitches, its 5-point stencil (pressure.wgsl:77-86), and the coarsest
+// level's red-black sweeps with fixed stencils (pressure.wgsl:132-156).
+#pragma once
+#include "gas_dev.cuh"
+
+namespace cfg {
+namespace mgc {
+
+struct LvS { float *p, *rhs, *ax, *ay; int nx, ny, pc, pu; float h2; int pad; };
+
+__device__ __forceinline__ void stencil_d(const LvS& L, int i, int j, float& off, float& diag) {
+  off = 0.f; diag = 0.f;
+  const float w = L.ax[j * L.pu + i], e = L.ax[j * L.pu + i + 1];
+  const float s = L.ay[j * L.pc + i], n = L.ay[(j + 1) * L.pc + i];
+  const float* p = L.p;
+  if (i > 0) { off += w * p[j * L.pc + i - 1]; diag += w; } else { diag += 2.f * w; }
+  if (i < L.nx - 1) { off += e * p[j * L.pc + i + 1]; diag += e; } else { diag += 2.f * e; }
+  if (j > 0) { off += s * p[(j - 1) * L.pc + i]; diag += s; }
+  if (j < L.ny - 1) { off += n * p[(j + 1) * L.pc + i]; diag += n; } else { diag += 2.f * n; }
+}
+__device__ __forceinline__ void bar_coarsest(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
+
+// x / d rounded to nearest from r = RN(1/d): q0 = RN(x r), q = RN(q0 + r (x - d q0)),
+// the residual x - d q0 exact by FMA (Markstein, IBM J. Res. Dev. 34(1), 1990). Equal
+// to the IEEE quotient for quotients in the normal range; it replaces the division
+// subroutine on the coarsest level, whose diagonals stay fixed for all its sweeps.
+__device__ __forceinline__ float div_by_rcp(float x, float d, float r) {
+  const float q0 = __fmul_rn(x, r);
+  const float e = __fmaf_rn(-q0, d, x);
+  return __fmaf_rn(e, r, q0);
+}
+
+// One coarsest-level cell with its fixed stencil (pressure.wgsl:132-156).
+struct CCell {
+  float w, e, s, n, rh, diag, rcp;
+  int kp;
+  bool act, hw, he, hs, hn;
+};
+__device__ __forceinline__ CCell coarsest_cell(const LvS& L, int k) {
+  CCell c{};
+  c.act = k < L.nx * L.ny;
+  if (!c.act) return c;
+  const int i = k % L.nx, j = k / L.nx;
+  c.kp = j * L.pc + i;
+  c.w = L.ax[j * L.pu + i]; c.e = L.ax[j * L.pu + i + 1];
+  c.s = L.ay[j * L.pc + i]; c.n = L.ay[(j + 1) * L.pc + i];
+  float diag = 0.f;
+  if (i > 0) diag += c.w; else diag += 2.f * c.w;
+  if (i < L.nx - 1) diag += c.e; else diag += 2.f * c.e;
+  if (j > 0) diag += c.s;
+  if (j < L.ny - 1) diag += c.n; else diag += 2.f * c.n;
+  c.diag = diag;
+  c.rcp = diag > 0.f ? __frcp_rn(diag) : 0.f;
+  c.rh = L.rhs[c.kp] * L.h2;
+  c.hw = i > 0; c.he = i < L.nx - 1; c.hs = j > 0; c.hn = j < L.ny - 1;
+  return c;
+}
+__device__ __forceinline__ void coarsest_update(float* p, int pc, const CCell& c) {
+  if (!c.act) return;
+  float off = 0.f;
+  if (c.hw) off += c.w * p[c.kp - 1];
+  if (c.he) off += c.e * p[c.kp + 1];
+  if (c.hs) off += c.s * p[c.kp - pc];
+  if (c.hn) off += c.n * p[c.kp + pc];
+  p[c.kp] = c.diag > 0.f ? div_by_rcp(off - c.rh, c.diag, c.rcp) : 0.f;
+}
+
+}  // namespace mgc
+}  // namespace cfg

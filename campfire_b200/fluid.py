@@ -226,6 +226,10 @@ class FluidSim(_SceneOps):
         """Smoother schedule: the one-CTA coarse block starts at the first level with <= cells cells."""
         check(_lib.lib().cfg_set_coarse_cells(self._h, int(cells)))
 
+    def set_coarse_cluster(self, cs: int):
+        """The coarse phase on one CTA (0) or on a cluster of cs CTAs (2, 4, 8, 16); bit-identical."""
+        check(_lib.lib().cfg_set_coarse_cluster(self._h, int(cs)))
+
     def set_coarse_solve(self, direct):
         """TOL/FP64 modes: the coarsest level by its inverse (True), by 120 sweeps (False), or by the
         inverse factored beside the previous step's solve ("pipelined")."""
@@ -302,6 +306,9 @@ class Batch:
 
     def set_coarse_solve(self, direct):
         check(_lib.lib().cfg_batch_set_coarse_solve(self._h, _coarse_mode(direct)))
+
+    def set_coarse_cluster(self, cs: int):
+        check(_lib.lib().cfg_batch_set_coarse_cluster(self._h, int(cs)))
 
     def set_krylov(self, on: bool):
         check(_lib.lib().cfg_batch_set_krylov(self._h, 1 if on else 0))

@@ -185,6 +185,11 @@ int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, double* mean_ms
  * scene, the levels above as tiled down/up kernels. Results are bit-identical for every
  * choice; only the time changes. Default 6144. Batch views: use cfg_batch_set_coarse_cells. */
 int cfg_set_coarse_cells(cfg_sim* sim, int cells);
+/* Where that coarse phase runs: 0 (default) one CTA per scene; 2, 4, 8 or 16: a thread-block
+ * cluster of that many CTAs per scene, each owning a share of every level's rows (from level 1
+ * at the earliest; level 0 stays tiled). Results are bit-identical for every choice. */
+int cfg_set_coarse_cluster(cfg_sim* sim, int cs);
+int cfg_batch_set_coarse_cluster(cfg_batch* b, int cs);
 /* Coarsest-level solve of the TOL and FP64 modes (no counterpart in the reference, which runs
  * one fixed cycle): 0 (default) the reference's 120 red-black sweeps; 1 the level's operator
  * inverted once per step (f32 banded Cholesky and column solves, after the coefficients are
