@@ -91,31 +91,69 @@ __device__ __forceinline__ bool stage_tile(const SceneDesc& S, int level, int pk
   return true;
 }
 
-// one red-black colour pass (pressure.wgsl:87-94) over cells [xa,xb) x [ya,yb) of colour
-// `color`: warps take rows, lanes every other cell (the region is at most 64 cells wide).
-// A pass reads only cells of the other colour, so each thread computes all its cells
-// before it stores any (their shared-memory loads overlap).
-template <int NW, int RH>
-__device__ __forceinline__ void colour_pass(const Tile& t, const LevelDesc& L, int xa, int xb, int ya, int yb, int color) {
-  constexpr int M = (RH + NW - 1) / NW;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float v[M];
-  int kk[M];
+
+// The four colour passes of a fused kernel with every cell's stencil in registers. Pass k
+// (1..4) covers [x0-H+k, x0+TX+H-k) x [y0-H+k, y0+TY+H-k) clipped to the level, with colour
+// (first + k - 1) & 1; thread t owns slots t and t + 256 of each colour in pass 1's region
+// (the largest; 20 cells of a colour per row), builds their stencils once (coefficients,
+// neighbour flags, rhs h2, diagonal, its correctly rounded reciprocal, and the passes that
+// include the cell) and updates them as colour_pass does, dividing by div_by_rcp.
+struct TCell { float w, e, s, n, rh, diag, rcp; int kp, fl; };   // fl: 1 w, 2 e, 4 s, 8 n; 16 << k: pass k
+__device__ __forceinline__ void smooth_tile(const Tile& t, const LevelDesc& L, int x0, int y0, int first) {
+  constexpr int W1 = MGF_TX + 2 * MGF_H - 2, H1 = MGF_TY + 2 * MGF_H - 2, HALF = W1 / 2;
+  static_assert(W1 % 2 == 0 && HALF * H1 <= 2 * 256, "two slots of a colour per thread");
+  const int ib = x0 - MGF_H + 1, jb = y0 - MGF_H + 1;
+  TCell c[2][2];
   #pragma unroll
-  for (int m = 0; m < M; m++) {
-    const int j = ya + warp + NW * m;
-    const int i = xa + ((xa + j + color) & 1) + 2 * lane;
-    kk[m] = -1;
-    if (j < yb && i < xb) {
-      float off, diag; stencil_s(t, L.nx, L.ny, i, j, off, diag);
+  for (int col = 0; col < 2; col++)
+    #pragma unroll
+    for (int m = 0; m < 2; m++) {
+      TCell& q = c[col][m];
+      q.fl = 0;
+      const int sl = threadIdx.x + 256 * m;
+      if (sl >= HALF * H1) continue;
+      const int r = sl / HALF, j = jb + r, i = ib + ((ib + j + col) & 1) + 2 * (sl - r * HALF);
+      if (i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
+      int pm = 0;
+      #pragma unroll
+      for (int k = 1; k <= 4; k++)
+        if (((first + k - 1) & 1) == col && i >= x0 - MGF_H + k && i < x0 + MGF_TX + MGF_H - k &&
+            j >= y0 - MGF_H + k && j < y0 + MGF_TY + MGF_H - k)
+          pm |= 16 << k;
+      if (!pm) continue;
       const int k = t.c(i, j);
-      v[m] = diag > 0.f ? (off - t.rhs[k] * L.h2) / diag : 0.f;
-      kk[m] = k;
+      q.kp = k;
+      q.w = t.ax[k]; q.e = t.ax[k + 1]; q.s = t.ay[k]; q.n = t.ay[k + MGF_BW];
+      float diag = 0.f;
+      if (i > 0) diag += q.w; else diag += 2.f * q.w;
+      if (i < L.nx - 1) diag += q.e; else diag += 2.f * q.e;
+      if (j > 0) diag += q.s;
+      if (j < L.ny - 1) diag += q.n; else diag += 2.f * q.n;
+      q.diag = diag;
+      q.rcp = diag > 0.f ? __frcp_rn(diag) : 0.f;
+      q.rh = t.rhs[k] * L.h2;
+      q.fl = pm | (i > 0 ? 1 : 0) | (i < L.nx - 1 ? 2 : 0) | (j > 0 ? 4 : 0) | (j < L.ny - 1 ? 8 : 0);
     }
-  }
   #pragma unroll
-  for (int m = 0; m < M; m++)
-    if (kk[m] >= 0) t.p[kk[m]] = v[m];
+  for (int k = 1; k <= 4; k++) {
+    const int col = (first + k - 1) & 1;
+    float v[2];
+    #pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const TCell& q = c[col][m];
+      if (!(q.fl & (16 << k))) continue;
+      float off = 0.f;
+      if (q.fl & 1) off += q.w * t.p[q.kp - 1];
+      if (q.fl & 2) off += q.e * t.p[q.kp + 1];
+      if (q.fl & 4) off += q.s * t.p[q.kp - MGF_BW];
+      if (q.fl & 8) off += q.n * t.p[q.kp + MGF_BW];
+      v[m] = q.diag > 0.f ? mgc::div_by_rcp(off - q.rh, q.diag, q.rcp) : 0.f;
+    }
+    #pragma unroll
+    for (int m = 0; m < 2; m++)
+      if (c[col][m].fl & (16 << k)) t.p[c[col][m].kp] = v[m];
+    __syncthreads();
+  }
 }
 
 __device__ __forceinline__ bool scene_live(const SceneDesc& S) { return S.enabled && S.solve->active; }
@@ -143,12 +181,7 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!scene_live(S)) return;
   if (!stage_tile(S, level, TM_P, t, nullptr, 0, 0, &bar, ctl)) return;
-  #pragma unroll 1
-  for (int k = 1; k <= 4; k++) {   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
-    colour_pass<8, MGF_BH>(t, L, max(x0 - MGF_H + k, 0), min(x0 + TX + MGF_H - k, L.nx), max(y0 - MGF_H + k, 0),
-                           min(y0 + TY + MGF_H - k, L.ny), (k - 1) & 1);
-    __syncthreads();
-  }
+  smooth_tile(t, L, x0, y0, 0);   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
   // residual of the tile cells (pressure.wgsl:96-101) and the smoothed p
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
@@ -239,12 +272,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
     t.p[t.c(i, j)] += diag_s(t, L.nx, L.ny, i, j) > 0.f ? c : 0.f;
   }
   __syncthreads();
-  #pragma unroll 1
-  for (int k = 1; k <= 4; k++) {   // colours 1, 0, 1, 0 (js/fluid.js:307-310)
-    colour_pass<8, MGF_BH>(t, L, max(x0 - MGF_H + k, 0), min(x0 + TX + MGF_H - k, L.nx), max(y0 - MGF_H + k, 0),
-                           min(y0 + TY + MGF_H - k, L.ny), k & 1);
-    __syncthreads();
-  }
+  smooth_tile(t, L, x0, y0, 1);   // colours 1, 0, 1, 0 (js/fluid.js:307-310)
   double part = 0.0, part2 = 0.0;
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
