@@ -97,7 +97,7 @@ __device__ __forceinline__ bool stage_tile(const SceneDesc& S, int level, int pk
 // (first + k - 1) & 1; thread t owns slots t and t + 256 of each colour in pass 1's region
 // (the largest; 20 cells of a colour per row), builds their stencils once (coefficients,
 // neighbour flags, rhs h2, diagonal, its correctly rounded reciprocal, and the passes that
-// include the cell) and updates them as colour_pass does, dividing by div_by_rcp.
+// include the cell) and updates them by pressure.wgsl:87-94, dividing by div_by_rcp.
 struct TCell { float w, e, s, n, rh, diag, rcp; int kp, fl; };   // fl: 1 w, 2 e, 4 s, 8 n; 16 << k: pass k
 __device__ __forceinline__ void smooth_tile(const Tile& t, const LevelDesc& L, int x0, int y0, int first) {
   constexpr int W1 = MGF_TX + 2 * MGF_H - 2, H1 = MGF_TY + 2 * MGF_H - 2, HALF = W1 / 2;
@@ -439,28 +439,41 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       v.ay = q; q += (G.ny + 1) * G.pc;
       lv[l] = v;
     }
-    mbar_init(&bar, 1);
+    mbar_init(&bar, 2);
   }
   __syncthreads();
-  pdl_wait();
-  if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
-  if (!scene_live(S)) return;
-  const LvS V0 = lv[lc];
-  float* sres = lv[nl - 1].ay + (lv[nl - 1].ny + 1) * lv[nl - 1].pc;   // residual scratch (level lc size)
-  // ---- stage the arrays with TMA bulk copies (one per array; sizes are multiples of 128 bytes)
-  if (threadIdx.x == 0) {
+  // ---- stage the arrays with TMA bulk copies (one per array; sizes are multiples of 128 bytes).
+  // The coefficients are built before the pressure loop and no loop kernel writes them: their
+  // copies start before the wait on the previous kernel (first arrival on the barrier); the
+  // rhs (and level 0's p) follow after it (second arrival, no bytes if the scene has stopped).
+  const bool on = S.enabled;   // host-written, constant during the step
+  if (threadIdx.x == 0 && on) {
     uint32_t bytes = 0;
-    const LevelDesc& G0 = S.lev[lc];
-    bytes += G0.ny * G0.pc * 4 * (lc == 0 ? 2 : 1);
     for (int l = lc; l < nl; l++) bytes += (S.lev[l].ny * S.lev[l].pu + (S.lev[l].ny + 1) * S.lev[l].pc) * 4;
     mbar_arrive_expect_tx(&bar, bytes);
-    bulk_g2s(V0.rhs, G0.rhs, G0.ny * G0.pc * 4, &bar);
-    if (lc == 0) bulk_g2s(V0.p, G0.p, G0.ny * G0.pc * 4, &bar);   // warm start
     for (int l = lc; l < nl; l++) {
       const LevelDesc& G = S.lev[l];
       bulk_g2s(lv[l].ax, G.ax, G.ny * G.pu * 4, &bar);
       bulk_g2s(lv[l].ay, G.ay, (G.ny + 1) * G.pc * 4, &bar);
     }
+  }
+  pdl_wait();
+  if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
+  if (!on) return;
+  const bool live = S.solve->active != 0;
+  const LvS V0 = lv[lc];
+  float* sres = lv[nl - 1].ay + (lv[nl - 1].ny + 1) * lv[nl - 1].pc;   // residual scratch (level lc size)
+  if (threadIdx.x == 0) {
+    const LevelDesc& G0 = S.lev[lc];
+    mbar_arrive_expect_tx(&bar, live ? G0.ny * G0.pc * 4 * (lc == 0 ? 2 : 1) : 0u);
+    if (live) {
+      bulk_g2s(V0.rhs, G0.rhs, G0.ny * G0.pc * 4, &bar);
+      if (lc == 0) bulk_g2s(V0.p, G0.p, G0.ny * G0.pc * 4, &bar);   // warm start
+    }
+  }
+  if (!live) {   // the coefficient copies land before the block leaves (bounded)
+    mbar_wait(&bar, 0);
+    return;
   }
   // level lc's p is zero after the restriction into it (pressure.wgsl:112)
   if (lc > 0)
@@ -522,8 +535,10 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
       const int k = base + (lane >> 3);
       float sum = 0.f;
-      if (k < n)
+      if (k < n) {
+        #pragma unroll 4
         for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(A + (size_t)k * n + m), sres[m], sum);
+      }
       sum += __shfl_xor_sync(0xffffffffu, sum, 1);
       sum += __shfl_xor_sync(0xffffffffu, sum, 2);
       sum += __shfl_xor_sync(0xffffffffu, sum, 4);
