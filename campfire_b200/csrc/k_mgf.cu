@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
 // rhs, ay; pu for ax), so each array arrives by one TMA bulk copy; then a
 // residual scratch of level lc's size.
 namespace {
-constexpr int CB_THREADS = 1024;
+constexpr int CB_THREADS = 512;
 constexpr int CB_WARPS = CB_THREADS / 32;
 constexpr int COARSEST_SCRATCH = 0;     // the coarsest keeps its stencils in registers
 using namespace mgc;
@@ -407,10 +407,11 @@ __device__ __forceinline__ void smooth_regs(const LvS& L, int first) {
     }
 }
 // both sweeps of a level visit (colour `first` first in each sweep, a block barrier after
-// every pass): in registers when each thread owns at most one cell of a colour
+// every pass): in registers when each thread owns at most two cells of a colour
 __device__ __forceinline__ void smooth_visit(const LvS& L, int first) {
   const int half = (L.nx + 1) >> 1, nslot = half * L.ny;
   if (nslot <= CB_THREADS) { smooth_regs<1>(L, first); return; }
+  if (nslot <= 2 * CB_THREADS) { smooth_regs<2>(L, first); return; }
   const LinMap mh(half);
   for (int k = 0; k < 2; k++) { pass_d(L, first, mh); __syncthreads(); pass_d(L, 1 - first, mh); __syncthreads(); }
 }
