@@ -544,7 +544,8 @@ def main():
     # ---- roofline of the dominant kernel (device time per step share), measured after the timed region
     hbm, peak_kind = peaks()
     kern = {}
-    for name in ("advect", "diffuse_sources", "forces", "mg_down0", "mg_up0", "mg_coarse", "defect64", "project"):
+    for name in ("advect", "diffuse_sources", "forces", "mg_down0", "mg_up0", "mg_coarse", "pcg_step", "defect64",
+                 "project"):
         m, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         cb._lib.check(L.cfg_time_kernel(sim._h, name.encode(), 50, ctypes.byref(m), ctypes.byref(b), ctypes.byref(n)))
         kern[name] = {"ms": m.value, "bytes": b.value, "per_step": n.value, "share_ms": m.value * n.value}

@@ -259,7 +259,7 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.acc, ACC_LEN * 4}, {(void**)&d.faceW, MAX_PIECES * 4 * 4},
     {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4}, {(void**)&d.rad, RAD_LEN * 16},
     {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
-    {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 16},
+    {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 24},
     {(void**)&d.r64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.dA, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.dB, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.q64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.tmap, (size_t)MAX_LEVELS * TM_PER_LEVEL * TMAP_BYTES},
@@ -1011,9 +1011,8 @@ void Engine::enqueue_vcycle_ref(cudaStream_t s) {
 void Engine::enqueue_fp64_tail(cudaStream_t s) {
   if (!any_fp64()) return;
   if (krylov()) {
-    launch_pcg_dir(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
-    launch_pcg_update(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
-    vcycle_launches_ += 2;
+    launch_pcg_step(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
+    vcycle_launches_++;
   } else {
     launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, s);
     vcycle_launches_++;
@@ -1320,7 +1319,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     cnt = cyc;
   } else if (n == "defect64") {
     go = [&](int) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 0, s); };
-    b = 32 * cells; cnt = fp64 ? cyc : 0;
+    b = 32 * cells; cnt = fp64 ? (krylov() ? 1 : cyc) : 0;   // the Krylov loop runs it once, to start
   } else if (n == "resnorm") {
     go = [&](int) { launch_resnorm(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
     b = (fp64 ? 32 : 16) * cells; cnt = cyc;
@@ -1330,12 +1329,9 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   } else if (n == "coarse_factor") {
     go = [&](int) { launch_coarse_factor(d_scenes_, nscenes(), cf_smem_, cf_bw_, pipelined_coarse() ? 1 : 0, s); };
     b = 0; cnt = direct_coarse() ? 1 : 0;
-  } else if (n == "pcg_dir") {
-    go = [&](int) { launch_pcg_dir(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
-    b = 40 * cells; cnt = krylov() ? cyc : 0;   // d, z, p64 (f64) read, d and q written
-  } else if (n == "pcg_update") {
-    go = [&](int) { launch_pcg_update(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
-    b = 40 * cells; cnt = krylov() ? cyc : 0;   // p64, r, d, q read, p64 and r written (f64)
+  } else if (n == "pcg_step") {
+    go = [&](int) { launch_pcg_step(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
+    b = 84 * cells; cnt = krylov() ? cyc : 0;   // z, Lz, d, q, p64, r read; d, q, p64, r, rhs0, p0 written
   } else if (n.size() == 8 && (n.compare(0, 7, "mg_down") == 0) && n[7] >= '1' && n[7] <= '6') {
     const int l = n[7] - '0';
     if (l >= sc.lc) return fail(CFG_ERR_NOENT, "level " + n.substr(7) + " is in the coarse block");

@@ -48,6 +48,7 @@ struct SolveState {
   int direct_ok_next;       // pipelined coarse solve: the other half, factored from this step's operator, is valid
   int pad;
   double delta, alpha, beta;   // Krylov FP64 mode: r.z of this cycle, the step length, the direction update
+  double pi;                // Krylov FP64 mode: d.q of this cycle
 };
 
 struct SceneDesc {
@@ -68,8 +69,8 @@ struct SceneDesc {
   int32_t *acc, *faceW;
   float *pieces;
   float4 *rad;
-  double *p64, *rhs64, *part;   // FP64 pressure, FP64 rhs, per-CTA partial sums (2 per tile)
-  double *r64, *dA, *dB, *q64;  // Krylov FP64 mode: residual, search directions (ping-pong), L d
+  double *p64, *rhs64, *part;   // FP64 pressure, FP64 rhs, per-CTA partial sums (3 per tile)
+  double *r64, *dA, *dB, *q64;  // Krylov FP64 mode: residual, search direction d, L z of the cycle, q = L d
   SolveState* solve;
   const char* tmap;         // TMA tensor maps of the levels (TM_PER_LEVEL per level, 128 bytes each)
   float* cinv;              // inverses of the coarsest operator, two halves of n x n (n = its cells), direct coarse solve

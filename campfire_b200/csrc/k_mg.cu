@@ -243,10 +243,11 @@ __global__ void __launch_bounds__(256) k_defect64(const SceneDesc* __restrict__ 
 
 // Krylov FP64 mode (flexible preconditioned CG on the level-0 operator L, the V-cycle's
 // z ~ L^-1 r as preconditioner), after the V-cycle and the direction update beta:
-// d = z + beta d_prev on the tile and its neighbours (z = the cycle's level-0 p),
-// q = L d, and d.q -> alpha = delta / (d.q). Cycle c writes d into dB (c even) or dA.
-__global__ void __launch_bounds__(256) k_pcg_dir(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work,
-                                                 SolveCtl* ctl) {
+// Krylov FP64 mode after the V-cycle (beta, alpha from the level-0 up kernel): d = z + beta d,
+// q = Lz + beta q (= L d, L symmetric; z the cycle's level-0 p, Lz from the up kernel),
+// p64 += alpha d, r -= alpha q, rhs0 = f32(r), p0 = 0, ||r|| -> the loop decision
+__global__ void __launch_bounds__(256) k_pcg_step(const SceneDesc* __restrict__ scenes, int nscenes,
+                                                  const Work* __restrict__ work, SolveCtl* ctl) {
   __shared__ double red[32];
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
@@ -255,53 +256,19 @@ __global__ void __launch_bounds__(256) k_pcg_dir(const SceneDesc* __restrict__ s
   pdl_wait();
   if (!scene_live(S)) return;
   const int nx = L.nx;
-  const int c = S.solve->cycles;
-  const double beta = S.solve->beta;
-  const double* dold = (c & 1) ? S.dB : S.dA;
-  double* dnew = (c & 1) ? S.dA : S.dB;
+  const bool first = S.solve->cycles == 0;
+  const double alpha = S.solve->alpha, beta = S.solve->beta;
   const int i = w.tx * MG_TX + (threadIdx.x % MG_TX), j = w.ty * MG_TY + (threadIdx.x / MG_TX);
   double v = 0.0;
   if (i < L.nx && j < L.ny) {
-    auto dn = [&](int ii, int jj) { return (double)L.p[jj * L.pc + ii] + beta * dold[jj * nx + ii]; };
-    const double wv = __ldg(L.ax + j * L.pu + i), e = __ldg(L.ax + j * L.pu + i + 1);
-    const double so = __ldg(L.ay + j * L.pc + i), n = __ldg(L.ay + (j + 1) * L.pc + i);
-    double off = 0.0, diag = 0.0;
-    if (i > 0) { off += wv * dn(i - 1, j); diag += wv; } else diag += 2.0 * wv;
-    if (i < L.nx - 1) { off += e * dn(i + 1, j); diag += e; } else diag += 2.0 * e;
-    if (j > 0) { off += so * dn(i, j - 1); diag += so; }
-    if (j < L.ny - 1) { off += n * dn(i, j + 1); diag += n; } else diag += 2.0 * n;
     const int k = j * nx + i;
-    const double dc = dn(i, j);
-    const double q = diag > 0.0 ? (off - diag * dc) / (double)L.h2 : 0.0;
-    dnew[k] = dc;
+    const double z = (double)L.p[j * L.pc + i], lz = S.dB[k];
+    const double d = first ? z : z + beta * S.dA[k];
+    const double q = first ? lz : lz + beta * S.q64[k];
+    S.dA[k] = d;
     S.q64[k] = q;
-    v = dc * q;
-  }
-  const double bp = block_sum(v, red);
-  double total = 0.0;
-  if (scene_reduce(S, w.tile, S.nt_mg0, bp, red, &total) && threadIdx.x == 0)
-    S.solve->alpha = total != 0.0 ? S.solve->delta / total : 0.0;
-}
-
-// Krylov FP64 mode: p64 += alpha d, r -= alpha q, rhs0 = f32(r), p0 = 0, ||r|| -> decision
-__global__ void __launch_bounds__(256) k_pcg_update(const SceneDesc* __restrict__ scenes, int nscenes,
-                                                    const Work* __restrict__ work, SolveCtl* ctl) {
-  __shared__ double red[32];
-  const Work w = work[blockIdx.x];
-  const SceneDesc& S = scenes[w.scene];
-  pdl_trigger();
-  const LevelDesc L = S.lev[0];
-  pdl_wait();
-  if (!scene_live(S)) return;
-  const int nx = L.nx;
-  const double alpha = S.solve->alpha;
-  const double* d = (S.solve->cycles & 1) ? S.dA : S.dB;
-  const int i = w.tx * MG_TX + (threadIdx.x % MG_TX), j = w.ty * MG_TY + (threadIdx.x / MG_TX);
-  double v = 0.0;
-  if (i < L.nx && j < L.ny) {
-    const int k = j * nx + i;
-    S.p64[k] += alpha * d[k];
-    const double r = S.r64[k] - alpha * S.q64[k];
+    S.p64[k] += alpha * d;
+    const double r = S.r64[k] - alpha * q;
     S.r64[k] = r;
     L.rhs[j * L.pc + i] = (float)r;
     L.p[j * L.pc + i] = 0.f;
@@ -391,13 +358,10 @@ void launch_defect64(const SceneDesc* scenes, int nscenes, const Work* work, int
   if (ntiles > 0)
     launch_pdl(pdl_enabled(), k_defect64, dim3(ntiles), dim3(MG_TX * MG_TY), 0, st, scenes, nscenes, work, ctl, first);
 }
-void launch_pcg_dir(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, cudaStream_t st) {
-  if (ntiles > 0) launch_pdl(pdl_enabled(), k_pcg_dir, dim3(ntiles), dim3(MG_TX * MG_TY), 0, st, scenes, work, ctl);
-}
-void launch_pcg_update(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
-                       cudaStream_t st) {
+void launch_pcg_step(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
+                     cudaStream_t st) {
   if (ntiles > 0)
-    launch_pdl(pdl_enabled(), k_pcg_update, dim3(ntiles), dim3(MG_TX * MG_TY), 0, st, scenes, nscenes, work, ctl);
+    launch_pdl(pdl_enabled(), k_pcg_step, dim3(ntiles), dim3(MG_TX * MG_TY), 0, st, scenes, nscenes, work, ctl);
 }
 void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_cond, cudaStream_t st) {
   launch_pdl(pdl_enabled(), k_loop_guard, dim3(1), dim3(32), 0, st, ctl, cond_handle, use_cond);

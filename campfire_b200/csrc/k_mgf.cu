@@ -49,6 +49,18 @@ __device__ __forceinline__ void stencil_s(const Tile& t, int nx, int ny, int i, 
   if (j > 0) { off += s * t.p[k - MGF_BW]; diag += s; }
   if (j < ny - 1) { off += n * t.p[k + MGF_BW]; diag += n; } else { diag += 2.f * n; }
 }
+// (L z)_ij in FP64 from the tile's f32 z and coefficients (pressure.wgsl:77-85 promoted,
+// as the FP64 defect: (off - diag z) / h2, 0 in closed cells)
+__device__ __forceinline__ double lap_tile64(const Tile& t, const LevelDesc& L, int i, int j) {
+  const int k = t.c(i, j);
+  const double w = t.ax[k], e = t.ax[k + 1], s = t.ay[k], n = t.ay[k + MGF_BW];
+  double off = 0.0, diag = 0.0;
+  if (i > 0) { off += w * (double)t.p[k - 1]; diag += w; } else diag += 2.0 * w;
+  if (i < L.nx - 1) { off += e * (double)t.p[k + 1]; diag += e; } else diag += 2.0 * e;
+  if (j > 0) { off += s * (double)t.p[k - MGF_BW]; diag += s; }
+  if (j < L.ny - 1) { off += n * (double)t.p[k + MGF_BW]; diag += n; } else diag += 2.0 * n;
+  return diag > 0.0 ? (off - diag * (double)t.p[k]) / (double)L.h2 : 0.0;
+}
 __device__ __forceinline__ float diag_s(const Tile& t, int nx, int ny, int i, int j) {
   const int k = t.c(i, j);
   const float w = t.ax[k], e = t.ax[k + 1], s = t.ay[k], n = t.ay[k + MGF_BW];
@@ -273,7 +285,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   }
   __syncthreads();
   smooth_tile(t, L, x0, y0, 1);   // colours 1, 0, 1, 0 (js/fluid.js:307-310)
-  double part = 0.0, part2 = 0.0;
+  double part = 0.0, part2 = 0.0, part3 = 0.0;
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
     if (i >= L.nx || j >= L.ny) continue;
@@ -286,17 +298,22 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
     } else if (tail == 2) {
       S.p64[j * L.nx + i] += (double)t.p[k];
     } else if (tail == 3) {
+      // z = the cycle's p; Lz from the tile (its ring is exact after the fourth pass), in FP64
       const int kk = j * L.nx + i;
       const double z = (double)t.p[k];
+      const double lz = lap_tile64(t, L, i, j);
+      S.dB[kk] = lz;
       part += S.r64[kk] * z;
       part2 += S.q64[kk] * z;
+      part3 += z * lz;
     }
   }
   if (tail == 3) {
     const double pa = block_sum(part, red);
     const double pb = block_sum(part2, red);
-    double ta = 0.0, tb = 0.0;
-    if (scene_reduce2(S, w.tile, S.nt_up0, pa, pb, red, &ta, &tb) && threadIdx.x == 0) pcg_beta(S, ta, tb);
+    const double pz = block_sum(part3, red);
+    double ta = 0.0, tb = 0.0, tz = 0.0;
+    if (scene_reduce3(S, w.tile, S.nt_up0, pa, pb, pz, red, &ta, &tb, &tz) && threadIdx.x == 0) pcg_coef(S, ta, tb, tz);
     return;
   }
   if (tail != 1) return;
@@ -589,7 +606,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   }
   // ---- write level lc back; when the block covers level 0, finish the cycle here
   const LevelDesc& G = S.lev[lc];
-  double part = 0.0, part2 = 0.0;
+  double part = 0.0, part2 = 0.0, part3 = 0.0;
   const LinMap mw(G.nx);
   if (mw.R)
   for (int j = mw.j0; j < G.ny; j += mw.R)
@@ -604,8 +621,11 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
         S.p64[j * G.nx + i] += (double)V0.p[e];
       } else if (lc == 0 && tail == 3) {
         const double z = (double)V0.p[e];
+        const double lz = lap_block64(V0, i, j);
+        S.dB[j * G.nx + i] = lz;
         part += S.r64[j * G.nx + i] * z;
         part2 += S.q64[j * G.nx + i] * z;
+        part3 += z * lz;
       }
     }
   if (lc == 0 && tail == 1) {
@@ -614,7 +634,8 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   } else if (lc == 0 && tail == 3) {
     const double ta = block_sum(part, red);
     const double tb = block_sum(part2, red);
-    if (threadIdx.x == 0) pcg_beta(S, ta, tb);
+    const double tz = block_sum(part3, red);
+    if (threadIdx.x == 0) pcg_coef(S, ta, tb, tz);
   }
 }
 

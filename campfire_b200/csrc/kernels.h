@@ -76,9 +76,8 @@ void launch_resnorm(const SceneDesc* scenes, int nscenes, const Work* work, int 
 void launch_defect64(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
                      int first, cudaStream_t st);
 // Krylov FP64 mode: direction + L d + alpha; then p64/r update + ||r|| + loop decision
-void launch_pcg_dir(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, cudaStream_t st);
-void launch_pcg_update(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
-                       cudaStream_t st);
+void launch_pcg_step(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
+                     cudaStream_t st);
 // end of a loop iteration: count it and set the WHILE node's condition (bounded by SolveCtl::hard_cap)
 void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_cond, cudaStream_t st);
 // fused V(2,2) cycle: per fine level a down kernel (4 passes + restriction) and an

@@ -20,6 +20,18 @@ __device__ __forceinline__ void stencil_d(const LvS& L, int i, int j, float& off
   if (j > 0) { off += s * p[(j - 1) * L.pc + i]; diag += s; }
   if (j < L.ny - 1) { off += n * p[(j + 1) * L.pc + i]; diag += n; } else { diag += 2.f * n; }
 }
+// (L z)_ij in FP64 from a level in shared memory (the FP64 defect's form)
+__device__ __forceinline__ double lap_block64(const LvS& L, int i, int j) {
+  const int k = j * L.pc + i;
+  const double w = L.ax[j * L.pu + i], e = L.ax[j * L.pu + i + 1];
+  const double s = L.ay[j * L.pc + i], n = L.ay[(j + 1) * L.pc + i];
+  double off = 0.0, diag = 0.0;
+  if (i > 0) { off += w * (double)L.p[k - 1]; diag += w; } else diag += 2.0 * w;
+  if (i < L.nx - 1) { off += e * (double)L.p[k + 1]; diag += e; } else diag += 2.0 * e;
+  if (j > 0) { off += s * (double)L.p[k - L.pc]; diag += s; }
+  if (j < L.ny - 1) { off += n * (double)L.p[k + L.pc]; diag += n; } else diag += 2.0 * n;
+  return diag > 0.0 ? (off - diag * (double)L.p[k]) / (double)L.h2 : 0.0;
+}
 __device__ __forceinline__ void bar_coarsest(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
 
 // x / d rounded to nearest from r = RN(1/d): q0 = RN(x r), q = RN(q0 + r (x - d q0)),

@@ -91,13 +91,49 @@ __device__ __forceinline__ bool scene_reduce2(const SceneDesc& S, int tile, int 
   return true;
 }
 
-// Krylov FP64 mode, after the V-cycle: delta = r.z and eta = q_prev.z give the
-// direction update beta = -alpha_prev eta / delta_prev (0 in the first cycle)
-__device__ __forceinline__ void pcg_beta(const SceneDesc& S, double delta, double eta) {
+// Three sums at once (partials at part[3 tile + 0..2]); same protocol.
+__device__ __forceinline__ bool scene_reduce3(const SceneDesc& S, int tile, int ntiles, double a, double b, double c,
+                                              double* sh, double* ta, double* tb, double* tc) {
+  __shared__ int s_last3;
+  if (threadIdx.x == 0) {
+    S.part[3 * tile] = a;
+    S.part[3 * tile + 1] = b;
+    S.part[3 * tile + 2] = c;
+    __threadfence();
+    const unsigned prev = atomicAdd(&S.solve->counter, 1u);
+    s_last3 = (prev == (unsigned)ntiles - 1u) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last3) return false;
+  __threadfence();
+  double va = 0.0, vb = 0.0, vc = 0.0;
+  for (int k = threadIdx.x; k < ntiles; k += blockDim.x) {
+    va += __ldcg(S.part + 3 * k);
+    vb += __ldcg(S.part + 3 * k + 1);
+    vc += __ldcg(S.part + 3 * k + 2);
+  }
+  const double sa = block_sum(va, sh);
+  const double sb = block_sum(vb, sh);
+  const double sc = block_sum(vc, sh);
+  if (threadIdx.x == 0) { *ta = sa; *tb = sb; *tc = sc; S.solve->counter = 0u; }
+  return true;
+}
+
+// Krylov FP64 mode, after the V-cycle, from delta = r.z, eta = q_prev.z and zeta = z.Lz:
+// the direction update beta = -alpha_prev eta / delta_prev (0 in the first cycle), the
+// direction's d.q = zeta + 2 beta eta + beta^2 (d.q)_prev (d = z + beta d_prev and
+// q = L d = Lz + beta q_prev, L symmetric), and the step length alpha = delta / d.q.
+__device__ __forceinline__ void pcg_coef(const SceneDesc& S, double delta, double eta, double zeta) {
   SolveState* ss = S.solve;
   const double prev = ss->delta;
-  ss->beta = (ss->cycles > 0 && prev != 0.0) ? -ss->alpha * eta / prev : 0.0;
+  const bool more = ss->cycles > 0 && prev != 0.0;
+  const double beta = more ? -ss->alpha * eta / prev : 0.0;
+  const double pi = more ? zeta + 2.0 * beta * eta + beta * beta * ss->pi : zeta;
+  ss->beta = beta;
   ss->delta = delta;
+  ss->pi = pi;
+  ss->alpha = pi != 0.0 ? delta / pi : 0.0;
 }
+
 
 }  // namespace cfg

@@ -944,34 +944,43 @@ struct Sim {
   }
   // FP64 mode, Krylov variant: flexible (Polak-Ribiere) preconditioned CG on the level-0
   // operator, one FP32 V-cycle on f32(r) per iteration as the preconditioner z ~ L^-1 r:
-  // delta = r.z; beta = -alpha_prev (q_prev.z) / delta_prev; d = z + beta d; q = L d;
+  // delta = r.z; beta = -alpha_prev (q_prev.z) / delta_prev; d = z + beta d; q = L d kept
+  // as Lz + beta q (L symmetric), with d.q = z.Lz + 2 beta (q_prev.z) + beta^2 (d.q)_prev;
   // alpha = delta / (d.q); p64 += alpha d; r -= alpha q; stop on ||r|| / ||rhs64||.
   void pressure_pcg(bool direct) {
     rhs0_64();
     double b = 0; for (double v : rhs64) b += v * v; b = std::sqrt(b);
-    std::vector<double> r, z, d, q;
+    std::vector<double> r, z, d, q, lz;
     double rn = res64(r);
     last_rel0 = b > 0 ? rn / b : 0.0;
     Level& L0 = lv[0];
     const size_t n = r.size();
     d.assign(n, 0.0); q.assign(n, 0.0); z.assign(n, 0.0);
-    double alpha = 0, delta_prev = 0;
+    double alpha = 0, delta_prev = 0, pi_prev = 0;
     int c = 0;
     while (b > 0 && rn / b > tol && c < max_cycles) {
       for (size_t k = 0; k < n; k++) { L0.rhs[k] = R((float)r[k]); L0.p[k] = R(0); }
-      vcycle(2, direct); c++;
+      vcycle(2, direct);
       for (size_t k = 0; k < n; k++) z[k] = (double)L0.p[k];
-      double delta = 0, eta = 0;
-      for (size_t k = 0; k < n; k++) { delta += r[k] * z[k]; eta += q[k] * z[k]; }
-      const double beta = c > 1 && delta_prev != 0 ? -alpha * eta / delta_prev : 0.0;
-      for (size_t k = 0; k < n; k++) d[k] = z[k] + beta * d[k];
-      lap64(d, q);
-      double pi = 0;
-      for (size_t k = 0; k < n; k++) pi += d[k] * q[k];
+      lap64(z, lz);
+      // delta = r.z, eta = q.z, zeta = z.Lz; beta (Polak-Ribiere); d.q = zeta + 2 beta eta +
+      // beta^2 (d.q)_prev with d = z + beta d and q = Lz + beta q (L symmetric); alpha = delta / d.q
+      double delta = 0, eta = 0, zeta = 0;
+      for (size_t k = 0; k < n; k++) { delta += r[k] * z[k]; eta += q[k] * z[k]; zeta += z[k] * lz[k]; }
+      const bool more = c > 0 && delta_prev != 0;
+      const double beta = more ? -alpha * eta / delta_prev : 0.0;
+      const double pi = more ? zeta + 2.0 * beta * eta + beta * beta * pi_prev : zeta;
       alpha = pi != 0 ? delta / pi : 0.0;
-      delta_prev = delta;
+      delta_prev = delta; pi_prev = pi;
       double s2 = 0;
-      for (size_t k = 0; k < n; k++) { p64[k] += alpha * d[k]; r[k] -= alpha * q[k]; s2 += r[k] * r[k]; }
+      for (size_t k = 0; k < n; k++) {
+        d[k] = c == 0 ? z[k] : z[k] + beta * d[k];
+        q[k] = c == 0 ? lz[k] : lz[k] + beta * q[k];
+        p64[k] += alpha * d[k];
+        r[k] -= alpha * q[k];
+        s2 += r[k] * r[k];
+      }
+      c++;
       rn = std::sqrt(s2);
     }
     last_cycles = c; last_rel = b > 0 ? rn / b : 0.0;
