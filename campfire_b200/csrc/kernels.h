@@ -9,10 +9,10 @@ namespace cfg {
 // Tile shapes (cells) of the level-0 kernels. Tiles are aligned to multiples of
 // 8 cells so the 8x8 blocks of the heat-release reduction match the WGSL
 // workgroups of sources.wgsl:34 exactly.
-constexpr int ADV_TX = 32, ADV_TY = 16, ADV_H = 2;   // advection (halo for |displacement| < 2 cells)
+constexpr int ADV_TX = 32, ADV_TY = 8, ADV_H = 2;    // advection (halo for |displacement| < 2 cells)
 constexpr int DS_TX = 32, DS_TY = 8;                 // diffusion + sources
-constexpr int FR_TX = 32, FR_TY = 16;                // forces + coef + rhs0 (+ coefficient hierarchy)
-constexpr int FR_KMAX = 4;                           // coarse coefficient levels built inside FR tiles
+constexpr int FR_TX = 32, FR_TY = 8;                 // forces + coef + rhs0 (+ coefficient hierarchy)
+constexpr int FR_KMAX = 3;                           // coarse coefficient levels built inside FR tiles
 constexpr int MG_TX = 32, MG_TY = 8;                 // single-pass multigrid kernels
 constexpr int MGF_TX = 32, MGF_TY = 16;              // fused (temporally blocked) multigrid kernels
 constexpr int MGF_H = 5;                             // their halo: 4 colour passes + the residual's neighbours
