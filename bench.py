@@ -39,6 +39,7 @@ WORKLOADS = {
     "fine": (512, 768, 1, 1236, 2, 1e-10, 300),
 }
 METRIC = "cell-updates/s"
+PLAIN_CFL, PLAIN_DT_CAP = 0.5, 2e-3   # the plain workload's time step: CFL 0.5, at most 2 ms
 # algorithmic bytes per cell-update (reference schedule, one read + one write per element at storage width):
 # advect 156, diffuse 48 per sub-step, sources 68, forces 28, coef 20, rhs0 28, coefRestrict 13.3, project 32,
 # V(2,2) cycle 216.8, FP64 defect-correction iteration 40, FP64 rhs assembly 12
@@ -131,6 +132,7 @@ def run_cpu(workload: str, steps: int, warmup: int, threads: int):
     o = oracle.OracleSim(nx, ny, 0.8, sc["dt"])
     load_scene(o, sc)
     o.set_solver(mode, 1, tol, maxc)
+    o.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)
     o.step(warmup)
     cyc = 0.0
     t0 = time.perf_counter()
@@ -251,9 +253,11 @@ def run_fp64_error(dev, workload: str, steps: int, every: int, threads: int):
     g.set_solver(mode, 1, tol, maxc)
     g.set_coarse_solve("pipelined")
     g.set_krylov(True)
+    g.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)
     o = oracle.OracleSim(nx, ny, 0.8, sc["dt"], fp64=True)
     load_scene(o, sc)
     o.set_solver(mode, 1, tol, maxc)
+    o.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)
     rows = []
     for k in range(1, steps + 1):
         g.step(1)
@@ -419,6 +423,10 @@ def main():
                     help="with --fp64-error-steps S: run the workload beside the FP64 oracle for S steps and "
                          "report the field errors every this many steps (0: skip)")
     ap.add_argument("--fp64-error-steps", type=int, default=2000)
+    ap.add_argument("--coarse-cells", type=int, default=0,
+                    help="start the coarse block at the first level with at most this many cells instead of "
+                         "autotuning (0: autotune); for profiling runs whose launch indices must not depend on "
+                         "the autotuner")
     ap.add_argument("--launch", default="graph", choices=["graph", "stream"],
                     help="graph: one CUDA graph per step (pressure loop as a device-side WHILE node); "
                          "stream: kernel by kernel, the host polling the loop decision (for profilers that "
@@ -471,13 +479,19 @@ def main():
     sim.set_solver(mode, 1, tol, maxc)
     sim.set_coarse_solve("pipelined")
     sim.set_krylov(True)
+    sim.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)   # dt set by CFL 0.5 each step, capped at 2 ms
+    config["dt"] = {"cfl": PLAIN_CFL, "cap_s": PLAIN_DT_CAP}
     config["pressure"]["coarsest"] = "direct: inverse factored beside the pressure loop, applied from the next step (pipelined)"
     config["pressure"]["outer"] = "flexible preconditioned CG in FP64, FP32 V(2,2) as preconditioner"
     # smoother schedule picked by the autotuner (fused V-cycles timed on a scratch scene of this size)
-    tune = cb.autotune([(nx, ny)], iters=20, device=local, coarse_direct=True)
-    sim.set_coarse_cells(tune["best"])
-    config["schedule"] = {"coarse_cells": tune["best"],
-                          "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}}
+    if a.coarse_cells > 0:
+        sim.set_coarse_cells(a.coarse_cells)
+        config["schedule"] = {"coarse_cells": a.coarse_cells, "autotune": "skipped"}
+    else:
+        tune = cb.autotune([(nx, ny)], iters=20, device=local, coarse_direct=True)
+        sim.set_coarse_cells(tune["best"])
+        config["schedule"] = {"coarse_cells": tune["best"],
+                              "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}}
     sim.set_stream(stream.cuda_stream)
     sim.set_graphs(a.launch == "graph")
     config["launch"] = a.launch
