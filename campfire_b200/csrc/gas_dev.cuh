@@ -81,7 +81,7 @@ struct SceneDesc {
 struct SolveCtl {
   int mode, ncycles, max_cycles, min_cycles;
   double tol;
-  unsigned int scenes_done;   // scenes that finished the current reduction
+  unsigned int scenes_done;   // arrivals of the current reduction (decisions: arrivals << 16 | scenes cycling on)
   int nscenes;                // enabled scenes taking part in this solve
   int nactive;                // scenes cycling in the current V-cycle
   int any_active;             // the loop decision of the last cycle
@@ -108,6 +108,16 @@ __host__ __device__ inline int round_up(int x, int m) { return (x + m - 1) / m *
 // successor begin launching. Both are no-ops for an ordinary launch.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Arrival on a gpu-scope counter (atomic add of v with acquire-release semantics): the
+// calling thread's earlier writes are visible to any thread that later observes the
+// count, and the thread that makes the last arrival sees every earlier arriver's writes
+// (the counter's release sequence). Returns the count before this arrival.
+__device__ __forceinline__ unsigned arrive_acq_rel(unsigned* counter, unsigned v = 1u) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(counter), "r"(v) : "memory");
+  return old;
+}
 
 // Pressure loop as a graph WHILE node: the first kernel of each iteration counts it
 // (one thread; at the hard cap the loop ends after this iteration even if no

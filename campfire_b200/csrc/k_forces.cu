@@ -191,8 +191,7 @@ __global__ void __launch_bounds__(256) k_forces(const SceneDesc* __restrict__ sc
     ss->bnorm2 = total;
     ss->cycles = 0;
     ss->active = 1;
-    __threadfence();
-    const unsigned d = atomicAdd(&ctl->scenes_done, 1u);
+    const unsigned d = arrive_acq_rel(&ctl->scenes_done);
     if (d == (unsigned)ctl->nscenes - 1u) {
       ctl->scenes_done = 0u;
       ctl->nactive = ctl->nscenes;

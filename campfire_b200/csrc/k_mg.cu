@@ -42,34 +42,6 @@ __device__ __forceinline__ float residual(const LevelDesc& L, int i, int j) {
 
 __device__ __forceinline__ bool scene_live(const SceneDesc& S) { return S.enabled && S.solve->active; }
 
-// Per-scene loop decision after a norm reduction (thread 0 of the finishing CTA);
-// the last scene of this round records whether any scene cycles again and, in a
-// graph, sets the loop's condition (loop_decide).
-__device__ void solve_decide(const SceneDesc* scenes, int nscenes, const SceneDesc& S, SolveCtl* ctl, double r2,
-                             bool count_cycle) {
-  SolveState* ss = S.solve;
-  if (count_cycle) ss->cycles += 1;
-  ss->rnorm2 = r2;
-  const double b2 = ss->bnorm2;
-  const double rel = b2 > 0.0 ? sqrt(r2 / b2) : 0.0;
-  ss->rel = rel;
-  int act;
-  if (ctl->mode == CFG_SOLVE_FIXED) act = ss->cycles < ctl->ncycles;
-  else act = (rel > ctl->tol) && (ss->cycles < ctl->max_cycles);
-  ss->active = act;
-  __threadfence();
-  const unsigned d = atomicAdd(&ctl->scenes_done, 1u);
-  if (d == (unsigned)ctl->nactive - 1u) {
-    __threadfence();
-    int na = 0;
-    for (int s = 0; s < nscenes; s++)
-      if (scenes[s].enabled && *((volatile int*)&scenes[s].solve->active)) na++;
-    ctl->scenes_done = 0u;
-    ctl->nactive = na;
-    loop_decide(ctl, na);
-  }
-}
-
 }  // namespace
 
 // Last kernel of each iteration of the host-driven loop (launches outside a graph):
@@ -195,7 +167,7 @@ __global__ void __launch_bounds__(256) k_resnorm(const SceneDesc* __restrict__ s
   const double bp = block_sum(v, red);
   double total = 0.0;
   if (scene_reduce(S, w.tile, S.nt_mg0, bp, red, &total) && threadIdx.x == 0)
-    solve_decide(scenes, nscenes, S, ctl, total, true);
+    solve_decide(ctl, S.solve, total, true);
 }
 
 // FP64 defect: r64 = rhs64 - A p64 (f32 coefficients promoted), rhs0 = f32(r64), p0 = 0
@@ -237,15 +209,15 @@ __global__ void __launch_bounds__(256) k_defect64(const SceneDesc* __restrict__ 
       S.solve->rel0 = S.solve->bnorm2 > 0.0 ? sqrt(total / S.solve->bnorm2) : 0.0;
       S.solve->alpha = 0.0; S.solve->beta = 0.0; S.solve->delta = 0.0;
     }
-    solve_decide(scenes, nscenes, S, ctl, total, !first);
+    solve_decide(ctl, S.solve, total, !first);
   }
 }
 
 // Krylov FP64 mode (flexible preconditioned CG on the level-0 operator L, the V-cycle's
-// z ~ L^-1 r as preconditioner), after the V-cycle and the direction update beta:
-// Krylov FP64 mode after the V-cycle (beta, alpha from the level-0 up kernel): d = z + beta d,
-// q = Lz + beta q (= L d, L symmetric; z the cycle's level-0 p, Lz from the up kernel),
-// p64 += alpha d, r -= alpha q, rhs0 = f32(r), p0 = 0, ||r|| -> the loop decision
+// z ~ L^-1 r as preconditioner), after the V-cycle (beta, alpha from the level-0 up
+// kernel): d = z + beta d, q = Lz + beta q (= L d, L symmetric; z the cycle's level-0 p,
+// Lz from the up kernel), p64 += alpha d, r -= alpha q, rhs0 = f32(r), p0 = 0, ||r|| ->
+// the loop decision. The scene's solve state is read in one round after the wait.
 __global__ void __launch_bounds__(256) k_pcg_step(const SceneDesc* __restrict__ scenes, int nscenes,
                                                   const Work* __restrict__ work, SolveCtl* ctl) {
   __shared__ double red[32];
@@ -253,11 +225,15 @@ __global__ void __launch_bounds__(256) k_pcg_step(const SceneDesc* __restrict__ 
   const SceneDesc& S = scenes[w.scene];
   pdl_trigger();
   const LevelDesc L = S.lev[0];
+  const bool on = S.enabled;   // host-written, constant during the step
+  SolveState* ss = S.solve;
   pdl_wait();
-  if (!scene_live(S)) return;
+  if (!on) return;
+  const int live = ss->active, cyc = ss->cycles;
+  const double alpha = ss->alpha, beta = ss->beta;
+  if (!live) return;
   const int nx = L.nx;
-  const bool first = S.solve->cycles == 0;
-  const double alpha = S.solve->alpha, beta = S.solve->beta;
+  const bool first = cyc == 0;
   const int i = w.tx * MG_TX + (threadIdx.x % MG_TX), j = w.ty * MG_TY + (threadIdx.x / MG_TX);
   double v = 0.0;
   if (i < L.nx && j < L.ny) {
@@ -276,8 +252,7 @@ __global__ void __launch_bounds__(256) k_pcg_step(const SceneDesc* __restrict__ 
   }
   const double bp = block_sum(v, red);
   double total = 0.0;
-  if (scene_reduce(S, w.tile, S.nt_mg0, bp, red, &total) && threadIdx.x == 0)
-    solve_decide(scenes, nscenes, S, ctl, total, true);
+  if (scene_reduce(S, w.tile, S.nt_mg0, bp, red, &total) && threadIdx.x == 0) solve_decide(ctl, ss, total, true);
 }
 
 // FP64: p64 += p0 after a V-cycle on the defect
@@ -325,8 +300,7 @@ __global__ void __launch_bounds__(256) k_bnorm(const SceneDesc* __restrict__ sce
   double total = 0.0;
   if (scene_reduce(S, w.tile, S.nt_mg0, bp, red, &total) && threadIdx.x == 0) {
     S.solve->bnorm2 = total; S.solve->cycles = 0; S.solve->active = 1;
-    __threadfence();
-    const unsigned d = atomicAdd(&ctl->scenes_done, 1u);
+    const unsigned d = arrive_acq_rel(&ctl->scenes_done);
     if (d == (unsigned)ctl->nscenes - 1u) { ctl->scenes_done = 0u; ctl->nactive = ctl->nscenes; ctl->any_active = 1; }
   }
 }

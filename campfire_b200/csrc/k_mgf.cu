@@ -79,20 +79,31 @@ __device__ __forceinline__ const void* tmap_of(const SceneDesc& S, int level, in
   return S.tmap + (size_t)(level * TM_PER_LEVEL + kind) * TMAP_BYTES;
 }
 
-// one thread issues the tile's tensor copies (p from map `pkind`), all threads wait
-// (bounded); false if the copies did not land, after recording the error and
-// waiting once more for the copies still in flight
-__device__ __forceinline__ bool stage_tile(const SceneDesc& S, int level, int pkind, const Tile& t, float* cp, int cx,
-                                           int cy, uint64_t* bar, SolveCtl* ctl) {
+// Tile staging in two parts around the wait on the previous kernel. stage_coef (before
+// the wait): one thread arms the barrier for every byte of the tile and requests the
+// coefficients ax, ay, which are built before the pressure loop and written by no loop
+// kernel (the loop is entered through a full dependency: a graph node or a memset).
+// stage_state (after the wait): p from map `pkind`, rhs and the coarse p under the tile;
+// the copies are issued whether or not the scene is still cycling, so the read of its
+// `active` flag overlaps them. stage_wait: all threads wait (bounded); false if the
+// copies did not land, after recording the error and waiting once more.
+__device__ __forceinline__ void stage_coef(const SceneDesc& S, int level, const Tile& t, bool cp, uint64_t* bar) {
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_arrive_expect_tx(bar, 3 * BOX_BYTES + BOX_AY_BYTES + (cp ? CBOX_BYTES : 0u));
-    tma_load_2d(t.p, tmap_of(S, level, pkind), t.sx, t.sy, bar);
-    tma_load_2d(t.rhs, tmap_of(S, level, TM_RHS), t.sx, t.sy, bar);
     tma_load_2d(t.ax, tmap_of(S, level, TM_AX), t.sx, t.sy, bar);
     tma_load_2d(t.ay, tmap_of(S, level, TM_AY), t.sx, t.sy, bar);
+  }
+}
+__device__ __forceinline__ void stage_state(const SceneDesc& S, int level, int pkind, const Tile& t, float* cp, int cx,
+                                            int cy, uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    tma_load_2d(t.p, tmap_of(S, level, pkind), t.sx, t.sy, bar);
+    tma_load_2d(t.rhs, tmap_of(S, level, TM_RHS), t.sx, t.sy, bar);
     if (cp) tma_load_2d(cp, tmap_of(S, level + 1, TM_PC), cx, cy, bar);
   }
+}
+__device__ __forceinline__ bool stage_wait(uint64_t* bar, SolveCtl* ctl) {
   __syncthreads();
   const bool ok = mbar_wait(bar, 0);
   if (__syncthreads_or(!ok)) {
@@ -168,8 +179,6 @@ __device__ __forceinline__ void smooth_tile(const Tile& t, const LevelDesc& L, i
   }
 }
 
-__device__ __forceinline__ bool scene_live(const SceneDesc& S) { return S.enabled && S.solve->active; }
-
 }  // namespace
 
 // ------------------------------------------------------------------ down: 4 passes + restrict
@@ -189,10 +198,15 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
   const LevelDesc L = S.lev[level], C = S.lev[level + 1];
   const int x0 = w.tx * TX, y0 = w.ty * TY;
   const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
+  const bool on = S.enabled;   // host-written, constant during the step
+  const volatile int* act = &S.solve->active;
+  if (on) stage_coef(S, level, t, false, &bar);
   pdl_wait();
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
-  if (!scene_live(S)) return;
-  if (!stage_tile(S, level, TM_P, t, nullptr, 0, 0, &bar, ctl)) return;
+  if (!on) return;
+  stage_state(S, level, TM_P, t, nullptr, 0, 0, &bar);
+  const bool live = *act != 0;
+  if (!stage_wait(&bar, ctl) || !live) return;
   smooth_tile(t, L, x0, y0, 0);   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
   // residual of the tile cells (pressure.wgsl:96-101) and the smoothed p
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
@@ -223,31 +237,6 @@ template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, int tail, SolveCtl* ctl);
 
-namespace {
-__device__ void solve_decide_f(const SceneDesc* scenes, int nscenes, const SceneDesc& S, SolveCtl* ctl, double r2) {
-  SolveState* ss = S.solve;
-  ss->cycles += 1;
-  ss->rnorm2 = r2;
-  const double b2 = ss->bnorm2;
-  const double rel = b2 > 0.0 ? sqrt(r2 / b2) : 0.0;
-  ss->rel = rel;
-  const int act = ctl->mode == CFG_SOLVE_FIXED ? (ss->cycles < ctl->ncycles)
-                                               : ((rel > ctl->tol) && (ss->cycles < ctl->max_cycles));
-  ss->active = act;
-  __threadfence();
-  const unsigned d = atomicAdd(&ctl->scenes_done, 1u);
-  if (d == (unsigned)ctl->nactive - 1u) {
-    __threadfence();
-    int na = 0;
-    for (int s = 0; s < nscenes; s++)
-      if (scenes[s].enabled && *((volatile int*)&scenes[s].solve->active)) na++;
-    ctl->scenes_done = 0u;
-    ctl->nactive = na;
-    loop_decide(ctl, na);
-  }
-}
-}  // namespace
-
 template <int TX, int TY>
 __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, int tail, SolveCtl* ctl) {
@@ -268,9 +257,14 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
   // coarse p under the region: columns x0/2-4 .. x0/2+TX/2+3, rows y0/2-4 .. y0/2+TY/2+3
   const int cx = x0 / 2 - 8, cy = y0 / 2 - 4;
+  const bool on = S.enabled;   // host-written, constant during the step
+  const volatile int* act = &S.solve->active;
+  if (on) stage_coef(S, level, t, true, &bar);
   pdl_wait();
-  if (!scene_live(S)) return;
-  if (!stage_tile(S, level, TM_PB, t, scp, cx, cy, &bar, ctl)) return;
+  if (!on) return;
+  stage_state(S, level, TM_PB, t, scp, cx, cy, &bar);
+  const bool live = *act != 0;
+  if (!stage_wait(&bar, ctl) || !live) return;
   // prolongation (pressure.wgsl:116-129) on the whole region
   for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
     const int i = x0 - MGF_H + e % RW, j = y0 - MGF_H + e / RW;
@@ -320,7 +314,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   const double bp = block_sum(part, red);
   double total = 0.0;
   if (scene_reduce(S, w.tile, S.nt_up0, bp, red, &total) && threadIdx.x == 0)
-    solve_decide_f(scenes, nscenes, S, ctl, total);
+    solve_decide(ctl, S.solve, total, true);
 }
 
 // ------------------------------------------------------------------ coarse block: levels lc..coarsest in one CTA
@@ -465,6 +459,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // copies start before the wait on the previous kernel (first arrival on the barrier); the
   // rhs (and level 0's p) follow after it (second arrival, no bytes if the scene has stopped).
   const bool on = S.enabled;   // host-written, constant during the step
+  const volatile int* act = &S.solve->active;
   if (threadIdx.x == 0 && on) {
     uint32_t bytes = 0;
     for (int l = lc; l < nl; l++) bytes += (S.lev[l].ny * S.lev[l].pu + (S.lev[l].ny + 1) * S.lev[l].pc) * 4;
@@ -478,7 +473,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   pdl_wait();
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!on) return;
-  const bool live = S.solve->active != 0;
+  const bool live = *act != 0;
   const LvS V0 = lv[lc];
   float* sres = lv[nl - 1].ay + (lv[nl - 1].ny + 1) * lv[nl - 1].pc;   // residual scratch (level lc size)
   if (threadIdx.x == 0) {
@@ -630,7 +625,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     }
   if (lc == 0 && tail == 1) {
     const double t = block_sum(part, red);
-    if (threadIdx.x == 0) solve_decide_f(scenes, nscenes, S, ctl, t);
+    if (threadIdx.x == 0) solve_decide(ctl, S.solve, t, true);
   } else if (lc == 0 && tail == 3) {
     const double ta = block_sum(part, red);
     const double tb = block_sum(part2, red);

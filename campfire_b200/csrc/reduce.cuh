@@ -2,9 +2,10 @@
 // protocol used by the norm reductions of the pressure solve.
 //
 // A reduction over the tiles of one scene: every CTA writes its partial to
-// scene.part[tile], fences, and bumps scene.solve->counter; the CTA that sees
-// the count reach the scene's tile count sums the partials in tile order (so
-// the total does not depend on CTA scheduling) and resets the counter.
+// scene.part[tile] and arrives on scene.solve->counter (release); the CTA that
+// makes the last arrival (acquire) sums the partials in tile order (so the total
+// does not depend on CTA scheduling) and resets the counter. Its other threads read
+// the partials after the block barrier that follows thread 0's acquire, from L2.
 #pragma once
 #include "gas_dev.cuh"
 
@@ -51,13 +52,11 @@ __device__ __forceinline__ bool scene_reduce(const SceneDesc& S, int tile, int n
   __shared__ int s_last;
   if (threadIdx.x == 0) {
     S.part[tile] = partial;
-    __threadfence();
-    const unsigned prev = atomicAdd(&S.solve->counter, 1u);
+    const unsigned prev = arrive_acq_rel(&S.solve->counter);
     s_last = (prev == (unsigned)ntiles - 1u) ? 1 : 0;
   }
   __syncthreads();
   if (!s_last) return false;
-  __threadfence();
   double v = 0.0;
   // each thread sums a fixed strided subset in order, then the fixed block tree
   for (int k = threadIdx.x; k < ntiles; k += blockDim.x) v += __ldcg(S.part + k);
@@ -73,13 +72,11 @@ __device__ __forceinline__ bool scene_reduce2(const SceneDesc& S, int tile, int 
   if (threadIdx.x == 0) {
     S.part[2 * tile] = a;
     S.part[2 * tile + 1] = b;
-    __threadfence();
-    const unsigned prev = atomicAdd(&S.solve->counter, 1u);
+    const unsigned prev = arrive_acq_rel(&S.solve->counter);
     s_last2 = (prev == (unsigned)ntiles - 1u) ? 1 : 0;
   }
   __syncthreads();
   if (!s_last2) return false;
-  __threadfence();
   double va = 0.0, vb = 0.0;
   for (int k = threadIdx.x; k < ntiles; k += blockDim.x) {
     va += __ldcg(S.part + 2 * k);
@@ -99,13 +96,11 @@ __device__ __forceinline__ bool scene_reduce3(const SceneDesc& S, int tile, int 
     S.part[3 * tile] = a;
     S.part[3 * tile + 1] = b;
     S.part[3 * tile + 2] = c;
-    __threadfence();
-    const unsigned prev = atomicAdd(&S.solve->counter, 1u);
+    const unsigned prev = arrive_acq_rel(&S.solve->counter);
     s_last3 = (prev == (unsigned)ntiles - 1u) ? 1 : 0;
   }
   __syncthreads();
   if (!s_last3) return false;
-  __threadfence();
   double va = 0.0, vb = 0.0, vc = 0.0;
   for (int k = threadIdx.x; k < ntiles; k += blockDim.x) {
     va += __ldcg(S.part + 3 * k);
@@ -133,6 +128,33 @@ __device__ __forceinline__ void pcg_coef(const SceneDesc& S, double delta, doubl
   ss->delta = delta;
   ss->pi = pi;
   ss->alpha = pi != 0.0 ? delta / pi : 0.0;
+}
+
+// The loop decision of one scene after a norm reduction (thread 0 of the CTA that
+// finished it): count the cycle, record ||r|| / ||rhs||, keep cycling while rel > tol
+// (TOL/FP64) or cycles < n (FIXED), and cycles < max. Every scene deciding in this
+// cycle arrives on ctl->scenes_done with 1 << 16 | (cycles on), so the last one knows
+// how many scenes cycle on without reading them; it records that and, in a graph, sets
+// the loop's condition (loop_decide). The control values are read together up front.
+__device__ __forceinline__ void solve_decide(SolveCtl* ctl, SolveState* ss, double r2, bool count_cycle) {
+  const int cyc0 = ss->cycles;
+  const double b2 = ss->bnorm2;
+  const int mode = ctl->mode, ncyc = ctl->ncycles, maxc = ctl->max_cycles, nact = ctl->nactive;
+  const double tol = ctl->tol;
+  const int cyc = cyc0 + (count_cycle ? 1 : 0);
+  const double rel = b2 > 0.0 ? sqrt(r2 / b2) : 0.0;
+  const int act = mode == CFG_SOLVE_FIXED ? (cyc < ncyc) : ((rel > tol) && (cyc < maxc));
+  ss->cycles = cyc;
+  ss->rnorm2 = r2;
+  ss->rel = rel;
+  ss->active = act;
+  const unsigned old = arrive_acq_rel(&ctl->scenes_done, (1u << 16) | (unsigned)act);
+  if ((int)(old >> 16) + 1 == nact) {
+    const int na = (int)(old & 0xffffu) + act;
+    ctl->scenes_done = 0u;
+    ctl->nactive = na;
+    loop_decide(ctl, na);
+  }
 }
 
 
