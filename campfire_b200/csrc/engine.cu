@@ -259,7 +259,7 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.acc, ACC_LEN * 4}, {(void**)&d.faceW, MAX_PIECES * 4 * 4},
     {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4}, {(void**)&d.rad, RAD_LEN * 16},
     {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
-    {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 24},
+    {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 72},   // up to 9 sums per tile
     {(void**)&d.r64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.dA, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.dB, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.q64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.tmap, (size_t)MAX_LEVELS * TM_PER_LEVEL * TMAP_BYTES},
@@ -954,6 +954,20 @@ int Engine::max_lc() const {
   return m;
 }
 
+bool Engine::pcg_fused() const {
+  if (!krylov() || scenes_.empty()) return false;
+  for (auto& sc : scenes_)
+    if (sc.lc < 1) return false;
+  return true;
+}
+
+// after the pressure loop: the fused Krylov mode's last update
+void Engine::enqueue_loop_end(cudaStream_t s) {
+  if (!pcg_fused()) return;
+  launch_pcg_finish(d_scenes_, d_wl_[WL_MG0], nwl_[WL_MG0], s);
+  launches_++;
+}
+
 // The step's V(2,2) cycle with the fused kernels (k_mgf.cu); the level-0 up
 // kernel (or the coarse block of scenes whose block starts at level 0) ends
 // the cycle with the residual norm (FP32 modes) or p64 += p (FP64 mode).
@@ -961,7 +975,7 @@ void Engine::enqueue_vcycle(cudaStream_t s, int tail, int count_iter) {
   const int LD = max_lc();
   for (int l = 0; l < LD; l++) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
-    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, count_iter, s);
+    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, count_iter, tail == 4 && l == 0, s);
     count_iter = 0;
     vcycle_launches_++;
   }
@@ -1011,6 +1025,7 @@ void Engine::enqueue_vcycle_ref(cudaStream_t s) {
 void Engine::enqueue_fp64_tail(cudaStream_t s) {
   if (!any_fp64()) return;
   if (krylov()) {
+    if (pcg_fused()) return;   // the level-0 smoother kernels carry the update
     launch_pcg_step(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s);
     vcycle_launches_++;
   } else {
@@ -1080,6 +1095,7 @@ int Engine::host_pressure_loop() {
     any = h_ctl_pinned_->any_active;
     if (++guard > std::max(ncycles_, max_cycles_) + 2) return fail(CFG_ERR_TIMEDOUT, "pressure loop did not terminate");
   }
+  enqueue_loop_end(s);
   return CFG_OK;
 }
 
@@ -1127,11 +1143,12 @@ int Engine::ensure_graph() {
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamBeginCaptureToGraph");
   vcycle_launches_ = 0;
   // the first kernel of the body counts the iteration and the cycle's decision sets the
-  // condition (loop_count / loop_decide): no guard kernel in the body
+  // condition (loop_count / solve_decide): no guard kernel in the body
   enqueue_vcycle(body_stream_, cycle_tail(), 1);
   enqueue_fp64_tail(body_stream_);
   e = cudaStreamEndCapture(body_stream_, &body);
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamEndCapture(body)");
+  enqueue_loop_end(s);
   enqueue_post_solve(s);
   e = cudaStreamEndCapture(s, &g);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
@@ -1297,7 +1314,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     go = [&](int) { launch_coarsest(d_scenes_, nscenes(), s); };
     b = 0; cnt = cyc;
   } else if (n == "mg_down0") {
-    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, 0, s); };
+    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, 0, 0, s); };
     b = (4 * 16 + 18) * cells; cnt = cyc;   // 4 colour passes + residual restriction
   } else if (n == "mg_up0") {
     go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 0, d_ctl_, s); };
@@ -1331,11 +1348,11 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     b = 0; cnt = direct_coarse() ? 1 : 0;
   } else if (n == "pcg_step") {
     go = [&](int) { launch_pcg_step(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, s); };
-    b = 84 * cells; cnt = krylov() ? cyc : 0;   // z, Lz, d, q, p64, r read; d, q, p64, r, rhs0, p0 written
+    b = 84 * cells; cnt = krylov() && !pcg_fused() ? cyc : 0;   // z, Lz, d, q, p64, r read; d, q, p64, r, rhs0, p0 written
   } else if (n.size() == 8 && (n.compare(0, 7, "mg_down") == 0) && n[7] >= '1' && n[7] <= '6') {
     const int l = n[7] - '0';
     if (l >= sc.lc) return fail(CFG_ERR_NOENT, "level " + n.substr(7) + " is in the coarse block");
-    go = [&, l](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, 0, s); };
+    go = [&, l](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, 0, 0, s); };
     b = (4 * 16 + 18) * (double)sc.lnx[l] * sc.lny[l]; cnt = cyc;
   } else if (n.size() == 6 && (n.compare(0, 5, "mg_up") == 0) && n[5] >= '1' && n[5] <= '6') {
     const int l = n[5] - '0';

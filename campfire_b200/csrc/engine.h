@@ -176,7 +176,11 @@ class Engine {
   void enqueue_factor(cudaStream_t s);
   void enqueue_factor_join(cudaStream_t s);
   bool krylov() const { return mode_ == CFG_SOLVE_FP64 && krylov_ != 0; }
-  int cycle_tail() const { return any_fp64() ? (krylov() ? 3 : 2) : 1; }
+  // Krylov mode with the update folded into the level-0 smoother kernels: every scene's
+  // coarse block starts below level 0
+  bool pcg_fused() const;
+  int cycle_tail() const { return any_fp64() ? (krylov() ? (pcg_fused() ? 4 : 3) : 2) : 1; }
+  void enqueue_loop_end(cudaStream_t s);
   void enqueue_fp64_tail(cudaStream_t s);
   void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
   void enqueue_post_solve(cudaStream_t s);

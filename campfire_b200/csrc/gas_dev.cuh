@@ -128,11 +128,6 @@ __device__ __forceinline__ void loop_count(SolveCtl* ctl) {
   ctl->iter = it;
   if (it >= ctl->hard_cap && ctl->use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond, 0u);
 }
-__device__ __forceinline__ void loop_decide(SolveCtl* ctl, int nactive) {
-  const int go = (nactive > 0 && ctl->iter < ctl->hard_cap) ? 1 : 0;
-  ctl->any_active = go;
-  if (ctl->use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ctl->cond, (unsigned)go);
-}
 
 
 // ------------------------------------------------------------- common.wgsl

@@ -229,9 +229,11 @@ __global__ void __launch_bounds__(256) k_pcg_step(const SceneDesc* __restrict__ 
   SolveState* ss = S.solve;
   pdl_wait();
   if (!on) return;
-  const int live = ss->active, cyc = ss->cycles;
+  const int live = ss->active;
   const double alpha = ss->alpha, beta = ss->beta;
+  const DecideIn din = decide_load(ctl, ss);
   if (!live) return;
+  const int cyc = din.cycles;
   const int nx = L.nx;
   const bool first = cyc == 0;
   const int i = w.tx * MG_TX + (threadIdx.x % MG_TX), j = w.ty * MG_TY + (threadIdx.x / MG_TX);
@@ -252,7 +254,30 @@ __global__ void __launch_bounds__(256) k_pcg_step(const SceneDesc* __restrict__ 
   }
   const double bp = block_sum(v, red);
   double total = 0.0;
-  if (scene_reduce(S, w.tile, S.nt_mg0, bp, red, &total) && threadIdx.x == 0) solve_decide(ctl, ss, total, true);
+  if (scene_reduce(S, w.tile, S.nt_mg0, bp, red, &total) && threadIdx.x == 0) solve_decide(ctl, ss, din, total, true);
+}
+
+// Fused Krylov mode, after the loop: the update of each scene's last cycle (cycles >= 1),
+// d = z + beta d (z on the first cycle), p64 += alpha d; r and q are not needed again
+__global__ void __launch_bounds__(256) k_pcg_finish(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work) {
+  const Work w = work[blockIdx.x];
+  const SceneDesc& S = scenes[w.scene];
+  pdl_trigger();
+  const LevelDesc L = S.lev[0];
+  const bool on = S.enabled;   // host-written, constant during the step
+  SolveState* ss = S.solve;
+  pdl_wait();
+  if (!on) return;
+  const int cyc = ss->cycles;
+  const double alpha = ss->alpha, beta = ss->beta;
+  if (cyc < 1) return;
+  const int i = w.tx * MG_TX + (threadIdx.x % MG_TX), j = w.ty * MG_TY + (threadIdx.x / MG_TX);
+  if (i >= L.nx || j >= L.ny) return;
+  const int k = j * L.nx + i;
+  const double z = (double)L.p[j * L.pc + i];
+  const double d = cyc == 1 ? z : z + beta * S.dA[k];
+  S.dA[k] = d;
+  S.p64[k] += alpha * d;
 }
 
 // FP64: p64 += p0 after a V-cycle on the defect
@@ -331,6 +356,10 @@ void launch_defect64(const SceneDesc* scenes, int nscenes, const Work* work, int
                      int first, cudaStream_t st) {
   if (ntiles > 0)
     launch_pdl(pdl_enabled(), k_defect64, dim3(ntiles), dim3(MG_TX * MG_TY), 0, st, scenes, nscenes, work, ctl, first);
+}
+void launch_pcg_finish(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st) {
+  // after the loop node (or the host loop's copy-back): an ordinary launch
+  if (ntiles > 0) k_pcg_finish<<<ntiles, MG_TX * MG_TY, 0, st>>>(scenes, work);
 }
 void launch_pcg_step(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
                      cudaStream_t st) {

@@ -79,32 +79,36 @@ __device__ __forceinline__ const void* tmap_of(const SceneDesc& S, int level, in
   return S.tmap + (size_t)(level * TM_PER_LEVEL + kind) * TMAP_BYTES;
 }
 
-// Tile staging in two parts around the wait on the previous kernel. stage_coef (before
-// the wait): one thread arms the barrier for every byte of the tile and requests the
-// coefficients ax, ay, which are built before the pressure loop and written by no loop
-// kernel (the loop is entered through a full dependency: a graph node or a memset).
-// stage_state (after the wait): p from map `pkind`, rhs and the coarse p under the tile;
-// the copies are issued whether or not the scene is still cycling, so the read of its
-// `active` flag overlaps them. stage_wait: all threads wait (bounded); false if the
-// copies did not land, after recording the error and waiting once more.
-__device__ __forceinline__ void stage_coef(const SceneDesc& S, int level, const Tile& t, bool cp, uint64_t* bar) {
+// Tile staging on two barriers around the wait on the previous kernel. stage_coef
+// (before the wait): one thread initialises both barriers and requests the coefficients
+// ax, ay on bar[0]; they are built before the pressure loop and written by no loop kernel
+// (the loop is entered through a full dependency: a graph node or a memset). stage_state
+// (after the wait): p from map `pkind`, rhs and the coarse p under the tile on bar[1]; with
+// `copy` false nothing is requested and bar[1] completes on its arrival. The copies are
+// issued whether or not the scene still cycles, so the read of its `active` flag overlaps
+// them. tile_wait: all threads wait for one barrier (bounded); false in every thread if a
+// wait ran out, after recording the error and waiting once more for the copies in flight.
+__device__ __forceinline__ void stage_coef(const SceneDesc& S, int level, const Tile& t, uint64_t* bar) {
   if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_arrive_expect_tx(bar, 3 * BOX_BYTES + BOX_AY_BYTES + (cp ? CBOX_BYTES : 0u));
-    tma_load_2d(t.ax, tmap_of(S, level, TM_AX), t.sx, t.sy, bar);
-    tma_load_2d(t.ay, tmap_of(S, level, TM_AY), t.sx, t.sy, bar);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_arrive_expect_tx(&bar[0], BOX_BYTES + BOX_AY_BYTES);
+    tma_load_2d(t.ax, tmap_of(S, level, TM_AX), t.sx, t.sy, &bar[0]);
+    tma_load_2d(t.ay, tmap_of(S, level, TM_AY), t.sx, t.sy, &bar[0]);
   }
 }
-__device__ __forceinline__ void stage_state(const SceneDesc& S, int level, int pkind, const Tile& t, float* cp, int cx,
-                                            int cy, uint64_t* bar) {
+__device__ __forceinline__ void stage_state(const SceneDesc& S, int level, int pkind, const Tile& t, bool copy,
+                                            float* cp, int cx, int cy, uint64_t* bar) {
   if (threadIdx.x == 0) {
-    tma_load_2d(t.p, tmap_of(S, level, pkind), t.sx, t.sy, bar);
-    tma_load_2d(t.rhs, tmap_of(S, level, TM_RHS), t.sx, t.sy, bar);
-    if (cp) tma_load_2d(cp, tmap_of(S, level + 1, TM_PC), cx, cy, bar);
+    mbar_arrive_expect_tx(&bar[1], copy ? 2 * BOX_BYTES + (cp ? CBOX_BYTES : 0u) : 0u);
+    if (copy) {
+      tma_load_2d(t.p, tmap_of(S, level, pkind), t.sx, t.sy, &bar[1]);
+      tma_load_2d(t.rhs, tmap_of(S, level, TM_RHS), t.sx, t.sy, &bar[1]);
+      if (cp) tma_load_2d(cp, tmap_of(S, level + 1, TM_PC), cx, cy, &bar[1]);
+    }
   }
 }
-__device__ __forceinline__ bool stage_wait(uint64_t* bar, SolveCtl* ctl) {
-  __syncthreads();
+__device__ __forceinline__ bool tile_wait(uint64_t* bar, SolveCtl* ctl) {
   const bool ok = mbar_wait(bar, 0);
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) atomicExch(&ctl->err, 1);
@@ -113,20 +117,32 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, SolveCtl* ctl) {
   }
   return true;
 }
+// both barriers of a tile: the coefficients (then `between`, e.g. the stencils), the state
+template <class F>
+__device__ __forceinline__ bool tile_wait2(uint64_t* bar, SolveCtl* ctl, F&& between) {
+  if (!tile_wait(&bar[0], ctl)) {
+    mbar_wait(&bar[1], 0);
+    return false;
+  }
+  between();
+  return tile_wait(&bar[1], ctl);
+}
 
 
 // The four colour passes of a fused kernel with every cell's stencil in registers. Pass k
 // (1..4) covers [x0-H+k, x0+TX+H-k) x [y0-H+k, y0+TY+H-k) clipped to the level, with colour
 // (first + k - 1) & 1; thread t owns slots t and t + 256 of each colour in pass 1's region
-// (the largest; 20 cells of a colour per row), builds their stencils once (coefficients,
-// neighbour flags, rhs h2, diagonal, its correctly rounded reciprocal, and the passes that
-// include the cell) and updates them by pressure.wgsl:87-94, dividing by div_by_rcp.
+// (the largest; 20 cells of a colour per row). tile_stencils builds their stencils from the
+// coefficients alone (coefficients, neighbour flags, diagonal, its correctly rounded
+// reciprocal, the passes that include the cell); tile_passes adds rhs h2 once the state
+// has landed and updates the cells by pressure.wgsl:87-94, dividing by div_by_rcp.
 struct TCell { float w, e, s, n, rh, diag, rcp; int kp, fl; };   // fl: 1 w, 2 e, 4 s, 8 n; 16 << k: pass k
-__device__ __forceinline__ void smooth_tile(const Tile& t, const LevelDesc& L, int x0, int y0, int first) {
-  constexpr int W1 = MGF_TX + 2 * MGF_H - 2, H1 = MGF_TY + 2 * MGF_H - 2, HALF = W1 / 2;
-  static_assert(W1 % 2 == 0 && HALF * H1 <= 2 * 256, "two slots of a colour per thread");
+constexpr int SM_W1 = MGF_TX + 2 * MGF_H - 2, SM_H1 = MGF_TY + 2 * MGF_H - 2;   // pass 1's region
+__device__ __forceinline__ void tile_stencils(const Tile& t, const LevelDesc& L, int x0, int y0, int first,
+                                              TCell (&c)[2][2]) {
+  constexpr int HALF = SM_W1 / 2;
+  static_assert(SM_W1 % 2 == 0 && HALF * SM_H1 <= 2 * 256, "two slots of a colour per thread");
   const int ib = x0 - MGF_H + 1, jb = y0 - MGF_H + 1;
-  TCell c[2][2];
   #pragma unroll
   for (int col = 0; col < 2; col++)
     #pragma unroll
@@ -134,7 +150,7 @@ __device__ __forceinline__ void smooth_tile(const Tile& t, const LevelDesc& L, i
       TCell& q = c[col][m];
       q.fl = 0;
       const int sl = threadIdx.x + 256 * m;
-      if (sl >= HALF * H1) continue;
+      if (sl >= HALF * SM_H1) continue;
       const int r = sl / HALF, j = jb + r, i = ib + ((ib + j + col) & 1) + 2 * (sl - r * HALF);
       if (i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
       int pm = 0;
@@ -154,9 +170,15 @@ __device__ __forceinline__ void smooth_tile(const Tile& t, const LevelDesc& L, i
       if (j < L.ny - 1) diag += q.n; else diag += 2.f * q.n;
       q.diag = diag;
       q.rcp = diag > 0.f ? __frcp_rn(diag) : 0.f;
-      q.rh = t.rhs[k] * L.h2;
       q.fl = pm | (i > 0 ? 1 : 0) | (i < L.nx - 1 ? 2 : 0) | (j > 0 ? 4 : 0) | (j < L.ny - 1 ? 8 : 0);
     }
+}
+__device__ __forceinline__ void tile_passes(const Tile& t, const LevelDesc& L, int first, TCell (&c)[2][2]) {
+  #pragma unroll
+  for (int col = 0; col < 2; col++)
+    #pragma unroll
+    for (int m = 0; m < 2; m++)
+      if (c[col][m].fl) c[col][m].rh = t.rhs[c[col][m].kp] * L.h2;
   #pragma unroll
   for (int k = 1; k <= 4; k++) {
     const int col = (first + k - 1) & 1;
@@ -179,10 +201,76 @@ __device__ __forceinline__ void smooth_tile(const Tile& t, const LevelDesc& L, i
   }
 }
 
+// Fused Krylov mode on level 0 (all scenes' coarse blocks start below it). The update of
+// cycle c (d = z + beta d, q = Lz + beta q, p64 += alpha d, r -= alpha q with cycle c's
+// alpha, beta) is split: the next cycle's down kernel forms d and p64 on its tile and the
+// new rhs0 = f32(r - alpha q) on pass 1's region from the stored r, q, Lz (read only
+// there, so no CTA reads a value another rewrites); the next up kernel rewrites r and q on
+// its tile before its dot products; the update of the last cycle is applied by
+// k_pcg_finish after the loop. The up kernel also returns ||r_c||^2 = r.r - 2 alpha r.q_c +
+// alpha^2 q_c.q_c (q_c = Lz + beta q) from its dot products, for the loop decision.
+// This thread's share of the down kernel's update: up to 4 cells of pass 1's region and
+// 2 tile cells, with their stored values loaded right after the wait.
+struct PcgDown {
+  double r[4], q[4], lz[4], dA[2], p64[2];
+  float z[2];
+};
+__device__ __forceinline__ void pcg_down_load(const SceneDesc& S, const LevelDesc& L, int x0, int y0, PcgDown& u) {
+  constexpr int N1 = SM_W1 * SM_H1;
+  #pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const int e = threadIdx.x + 256 * m;
+    const int i = x0 - MGF_H + 1 + e % SM_W1, j = y0 - MGF_H + 1 + e / SM_W1;
+    if (e < N1 && i >= 0 && i < L.nx && j >= 0 && j < L.ny) {
+      const int k = j * L.nx + i;
+      u.r[m] = __ldcg(S.r64 + k); u.q[m] = __ldcg(S.q64 + k); u.lz[m] = __ldcg(S.dB + k);
+    }
+  }
+  #pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const int e = threadIdx.x + 256 * m;
+    const int i = x0 + e % MGF_TX, j = y0 + e / MGF_TX;
+    if (i < L.nx && j < L.ny) {
+      u.dA[m] = __ldcg(S.dA + j * L.nx + i); u.p64[m] = __ldcg(S.p64 + j * L.nx + i);
+      u.z[m] = __ldcg(L.p + j * L.pc + i);
+    }
+  }
+}
+// after the state barrier: p = 0 on the whole box, rhs0 on pass 1's region, d and p64 on the
+// tile (rhs0 of the tile to global for the up kernel's staging once the block has synced)
+__device__ __forceinline__ void pcg_down_apply(const SceneDesc& S, const LevelDesc& L, const Tile& t, int x0, int y0,
+                                               const PcgPrev& pv, const PcgDown& u) {
+  constexpr int N1 = SM_W1 * SM_H1;
+  const bool first = pv.cycles == 1;
+  for (int e = threadIdx.x; e < MGF_BW * MGF_BH; e += 256) t.p[e] = 0.f;
+  #pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const int e = threadIdx.x + 256 * m;
+    const int i = x0 - MGF_H + 1 + e % SM_W1, j = y0 - MGF_H + 1 + e / SM_W1;
+    if (e < N1 && i >= 0 && i < L.nx && j >= 0 && j < L.ny) {
+      const double q = first ? u.lz[m] : u.lz[m] + pv.beta * u.q[m];
+      const double r = u.r[m] - pv.alpha * q;
+      t.rhs[t.c(i, j)] = (float)r;
+    }
+  }
+  #pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const int e = threadIdx.x + 256 * m;
+    const int i = x0 + e % MGF_TX, j = y0 + e / MGF_TX;
+    if (i < L.nx && j < L.ny) {
+      const double z = (double)u.z[m];
+      const double d = first ? z : z + pv.beta * u.dA[m];
+      S.dA[j * L.nx + i] = d;
+      S.p64[j * L.nx + i] = u.p64[m] + pv.alpha * d;
+    }
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ down: 4 passes + restrict
-template <int TX, int TY>
+// PCG: the fused Krylov update on level 0 (above)
+template <int TX, int TY, bool PCG>
 __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work, int level,
                                                  SolveCtl* ctl, int count_iter) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
@@ -191,7 +279,7 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
   __shared__ __align__(128) float sax[MGF_BH * MGF_BW];
   __shared__ __align__(128) float say[(MGF_BH + 1) * MGF_BW];
   __shared__ float sr[TY * TX];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[2];
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
   pdl_trigger();
@@ -199,15 +287,32 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
   const int x0 = w.tx * TX, y0 = w.ty * TY;
   const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
   const bool on = S.enabled;   // host-written, constant during the step
-  const volatile int* act = &S.solve->active;
-  if (on) stage_coef(S, level, t, false, &bar);
+  SolveState* ss = S.solve;
+  if (on) stage_coef(S, level, t, bar);
+  __syncthreads();
   pdl_wait();
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!on) return;
-  stage_state(S, level, TM_P, t, nullptr, 0, 0, &bar);
-  const bool live = *act != 0;
-  if (!stage_wait(&bar, ctl) || !live) return;
-  smooth_tile(t, L, x0, y0, 0);   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
+  PcgPrev pv{};
+  PcgDown u;
+  if (PCG) {
+    pv = pcg_load(ss);
+    pcg_down_load(S, L, x0, y0, u);
+  }
+  const bool live = *(volatile int*)&ss->active != 0;
+  const bool upd = PCG && pv.cycles >= 1;   // an update of the previous cycle is pending
+  stage_state(S, level, TM_P, t, !upd, nullptr, 0, 0, bar);
+  TCell c[2][2];
+  if (!tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 0, c); }) || !live) return;
+  if (upd) {
+    pcg_down_apply(S, L, t, x0, y0, pv, u);
+    __syncthreads();
+    for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
+      const int i = x0 + e % TX, j = y0 + e / TX;
+      if (i < L.nx && j < L.ny) L.rhs[j * L.pc + i] = t.rhs[t.c(i, j)];
+    }
+  }
+  tile_passes(t, L, 0, c);   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
   // residual of the tile cells (pressure.wgsl:96-101) and the smoothed p
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
@@ -232,12 +337,10 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
 
 // ------------------------------------------------------------------ up: prolong + 4 passes (+ level-0 tail)
 // tail: 0 none, 1 residual norm + loop decision (FP32 modes), 2 p64 += p (FP64 defect correction),
-// 3 r.z and q.z -> the direction update (Krylov FP64 mode)
-template <int TX, int TY>
-__global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
-                                               int level, int tail, SolveCtl* ctl);
-
-template <int TX, int TY>
+// 3 r.z, q.z, z.Lz -> the direction update (Krylov FP64 mode), 4 the same in the fused Krylov
+// mode (the pending r, q update first; the loop decision from the recurrence for ||r||),
+// compiled into the KRY instance only
+template <int TX, int TY, bool KRY>
 __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, int tail, SolveCtl* ctl) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
@@ -247,8 +350,8 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   __shared__ __align__(128) float sax[MGF_BH * MGF_BW];
   __shared__ __align__(128) float say[(MGF_BH + 1) * MGF_BW];
   __shared__ __align__(128) float scp[MGF_CBH * MGF_CBW];
-  __shared__ double red[32];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ double red[9 * 32];
+  __shared__ __align__(8) uint64_t bar[2];
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
   pdl_trigger();
@@ -258,13 +361,32 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   // coarse p under the region: columns x0/2-4 .. x0/2+TX/2+3, rows y0/2-4 .. y0/2+TY/2+3
   const int cx = x0 / 2 - 8, cy = y0 / 2 - 4;
   const bool on = S.enabled;   // host-written, constant during the step
-  const volatile int* act = &S.solve->active;
-  if (on) stage_coef(S, level, t, true, &bar);
+  SolveState* ss = S.solve;
+  if (on) stage_coef(S, level, t, bar);
+  __syncthreads();
   pdl_wait();
   if (!on) return;
-  stage_state(S, level, TM_PB, t, scp, cx, cy, &bar);
-  const bool live = *act != 0;
-  if (!stage_wait(&bar, ctl) || !live) return;
+  stage_state(S, level, TM_PB, t, true, scp, cx, cy, bar);
+  const bool live = *(volatile int*)&ss->active != 0;
+  // fused Krylov mode: the solve state and this thread's stored r, q, Lz, read beside the copies
+  PcgPrev pv{};
+  DecideIn din{};
+  double r0[2] = {0.0, 0.0}, q0[2] = {0.0, 0.0}, lz0[2] = {0.0, 0.0};
+  if (KRY) {
+    pv = pcg_load(ss);
+    din = decide_load(ctl, ss);
+    #pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const int e = threadIdx.x + 256 * m;
+      const int i = x0 + e % TX, j = y0 + e / TX;
+      if (i < L.nx && j < L.ny) {
+        const int kk = j * L.nx + i;
+        r0[m] = __ldcg(S.r64 + kk); q0[m] = __ldcg(S.q64 + kk); lz0[m] = __ldcg(S.dB + kk);
+      }
+    }
+  }
+  TCell c[2][2];
+  if (!tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 1, c); }) || !live) return;
   // prolongation (pressure.wgsl:116-129) on the whole region
   for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
     const int i = x0 - MGF_H + e % RW, j = y0 - MGF_H + e / RW;
@@ -272,13 +394,50 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
     const int I = i / 2, J = j / 2;
     const int I2 = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), C.nx - 1);
     const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), C.ny - 1);
-    const int r0 = (J - cy) * MGF_CBW, r1 = (J2 - cy) * MGF_CBW;
-    const float c = 0.5625f * scp[r0 + I - cx] + 0.1875f * (scp[r0 + I2 - cx] + scp[r1 + I - cx]) +
-                    0.0625f * scp[r1 + I2 - cx];
-    t.p[t.c(i, j)] += diag_s(t, L.nx, L.ny, i, j) > 0.f ? c : 0.f;
+    const int r0_ = (J - cy) * MGF_CBW, r1 = (J2 - cy) * MGF_CBW;
+    const float c_ = 0.5625f * scp[r0_ + I - cx] + 0.1875f * (scp[r0_ + I2 - cx] + scp[r1 + I - cx]) +
+                     0.0625f * scp[r1 + I2 - cx];
+    t.p[t.c(i, j)] += diag_s(t, L.nx, L.ny, i, j) > 0.f ? c_ : 0.f;
   }
   __syncthreads();
-  smooth_tile(t, L, x0, y0, 1);   // colours 1, 0, 1, 0 (js/fluid.js:307-310)
+  tile_passes(t, L, 1, c);   // colours 1, 0, 1, 0 (js/fluid.js:307-310)
+  if (KRY) {
+    // the pending r, q update (cycles >= 1), then r.z, q.z, z.Lz and the recurrence's r.r,
+    // r.Lz, r.q, Lz.Lz, Lz.q, q.q on the tile
+    const bool upd = pv.cycles >= 1, first = pv.cycles == 1;
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    #pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const int e = threadIdx.x + 256 * m;
+      const int i = x0 + e % TX, j = y0 + e / TX;
+      if (i >= L.nx || j >= L.ny) continue;
+      const int k = t.c(i, j), kk = j * L.nx + i;
+      L.p[j * L.pc + i] = t.p[k];
+      double r = r0[m], q = q0[m];
+      if (upd) {
+        q = first ? lz0[m] : lz0[m] + pv.beta * q;
+        r = r - pv.alpha * q;
+        S.q64[kk] = q;
+        S.r64[kk] = r;
+      }
+      const double z = (double)t.p[k];
+      const double lz = lap_tile64(t, L, i, j);
+      S.dB[kk] = lz;
+      v[0] += r * z; v[1] += q * z; v[2] += z * lz;
+      v[3] += r * r; v[4] += r * lz; v[5] += r * q; v[6] += lz * lz; v[7] += lz * q; v[8] += q * q;
+    }
+    block_sum_n<9>(v, red);
+    if (scene_reduce_n<9>(S, w.tile, S.nt_up0, v, red) && threadIdx.x == 0) {
+      double alpha, beta;
+      pcg_coef(ss, pv, v[0], v[1], v[2], &alpha, &beta);
+      // ||r - alpha (Lz + beta q)||^2 from the dot products
+      const double rq = v[4] + beta * v[5];
+      const double qq = v[6] + 2.0 * beta * v[7] + beta * beta * v[8];
+      const double r2 = v[3] - 2.0 * alpha * rq + alpha * alpha * qq;
+      solve_decide(ctl, ss, din, r2 > 0.0 ? r2 : 0.0, true);
+    }
+    return;
+  }
   double part = 0.0, part2 = 0.0, part3 = 0.0;
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
@@ -313,8 +472,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   if (tail != 1) return;
   const double bp = block_sum(part, red);
   double total = 0.0;
-  if (scene_reduce(S, w.tile, S.nt_up0, bp, red, &total) && threadIdx.x == 0)
-    solve_decide(ctl, S.solve, total, true);
+  if (scene_reduce(S, w.tile, S.nt_up0, bp, red, &total) && threadIdx.x == 0) solve_decide(ctl, ss, total, true);
 }
 
 // ------------------------------------------------------------------ coarse block: levels lc..coarsest in one CTA
@@ -823,16 +981,16 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
 }
 
 void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, int count_iter,
-                    cudaStream_t st) {
+                    int pcg, cudaStream_t st) {
   if (ntiles > 0)
-    launch_pdl(pdl_enabled(), k_mg_down<MGF_TX, MGF_TY>, dim3(ntiles), dim3(256), 0, st, scenes, work, level, ctl,
-               count_iter);
+    launch_pdl(pdl_enabled(), pcg ? k_mg_down<MGF_TX, MGF_TY, true> : k_mg_down<MGF_TX, MGF_TY, false>, dim3(ntiles),
+               dim3(256), 0, st, scenes, work, level, ctl, count_iter);
 }
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {
   if (ntiles > 0)
-    launch_pdl(pdl_enabled(), k_mg_up<MGF_TX, MGF_TY>, dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, tail,
-               ctl);
+    launch_pdl(pdl_enabled(), tail == 4 ? k_mg_up<MGF_TX, MGF_TY, true> : k_mg_up<MGF_TX, MGF_TY, false>, dim3(ntiles),
+               dim3(256), 0, st, scenes, nscenes, work, level, tail, ctl);
 }
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
                       cudaStream_t st) {

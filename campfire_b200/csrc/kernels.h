@@ -78,14 +78,18 @@ void launch_defect64(const SceneDesc* scenes, int nscenes, const Work* work, int
 // Krylov FP64 mode: direction + L d + alpha; then p64/r update + ||r|| + loop decision
 void launch_pcg_step(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, SolveCtl* ctl,
                      cudaStream_t st);
+// fused Krylov mode, after the loop: the last cycle's d and p64 update
+void launch_pcg_finish(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
 // end of a loop iteration: count it and set the WHILE node's condition (bounded by SolveCtl::hard_cap)
 void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_cond, cudaStream_t st);
 // fused V(2,2) cycle: per fine level a down kernel (4 passes + restriction) and an
 // up kernel (prolongation + 4 passes; level 0 tail: 1 residual norm + decision,
-// 2 p64 += p), and one CTA per scene for levels lc..coarsest
-// count_iter: the kernel opens a graph loop iteration (loop_count)
+// 2 p64 += p, 3 the Krylov dot products, 4 the fused Krylov mode's), and one CTA per
+// scene for levels lc..coarsest
+// count_iter: the kernel opens a graph loop iteration (loop_count); pcg: level 0 of the
+// fused Krylov mode (applies the previous cycle's update)
 void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, int count_iter,
-                    cudaStream_t st);
+                    int pcg, cudaStream_t st);
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st);
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,

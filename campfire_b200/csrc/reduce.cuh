@@ -114,20 +114,102 @@ __device__ __forceinline__ bool scene_reduce3(const SceneDesc& S, int tile, int 
   return true;
 }
 
+// N sums over the block at once (each in the fixed order of block_sum); the results are
+// valid in thread 0. sh holds at least 32 N doubles.
+template <int N>
+__device__ __forceinline__ void block_sum_n(double (&v)[N], double* sh) {
+  #pragma unroll
+  for (int m = 0; m < N; m++)
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[m] += __shfl_down_sync(0xffffffffu, v[m], o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+    #pragma unroll
+    for (int m = 0; m < N; m++) sh[m * 32 + warp] = v[m];
+  __syncthreads();
+  if (warp == 0)
+    #pragma unroll
+    for (int m = 0; m < N; m++) {
+      double t = lane < nw ? sh[m * 32 + lane] : 0.0;
+      #pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      v[m] = t;
+    }
+}
+
+// N sums of one scene at once (partials at part[N tile + m]); the scene_reduce protocol.
+// On return true (the CTA that completed the scene), v holds the totals in thread 0.
+template <int N>
+__device__ __forceinline__ bool scene_reduce_n(const SceneDesc& S, int tile, int ntiles, double (&v)[N], double* sh) {
+  __shared__ int s_lastn;
+  if (threadIdx.x == 0) {
+    #pragma unroll
+    for (int m = 0; m < N; m++) S.part[N * tile + m] = v[m];
+    const unsigned prev = arrive_acq_rel(&S.solve->counter);
+    s_lastn = (prev == (unsigned)ntiles - 1u) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_lastn) return false;
+  #pragma unroll
+  for (int m = 0; m < N; m++) v[m] = 0.0;
+  for (int k = threadIdx.x; k < ntiles; k += blockDim.x)
+    #pragma unroll
+    for (int m = 0; m < N; m++) v[m] += __ldcg(S.part + N * k + m);
+  block_sum_n<N>(v, sh);
+  if (threadIdx.x == 0) S.solve->counter = 0u;
+  return true;
+}
+
+// The Krylov state a cycle's coefficients start from (read after the wait on the previous kernel)
+struct PcgPrev {
+  double alpha, beta, delta, pi;
+  int cycles;
+};
+__device__ __forceinline__ PcgPrev pcg_load(const SolveState* ss) {
+  PcgPrev p;
+  p.alpha = ss->alpha; p.beta = ss->beta; p.delta = ss->delta; p.pi = ss->pi; p.cycles = ss->cycles;
+  return p;
+}
+
 // Krylov FP64 mode, after the V-cycle, from delta = r.z, eta = q_prev.z and zeta = z.Lz:
 // the direction update beta = -alpha_prev eta / delta_prev (0 in the first cycle), the
 // direction's d.q = zeta + 2 beta eta + beta^2 (d.q)_prev (d = z + beta d_prev and
 // q = L d = Lz + beta q_prev, L symmetric), and the step length alpha = delta / d.q.
-__device__ __forceinline__ void pcg_coef(const SceneDesc& S, double delta, double eta, double zeta) {
-  SolveState* ss = S.solve;
-  const double prev = ss->delta;
-  const bool more = ss->cycles > 0 && prev != 0.0;
-  const double beta = more ? -ss->alpha * eta / prev : 0.0;
-  const double pi = more ? zeta + 2.0 * beta * eta + beta * beta * ss->pi : zeta;
+__device__ __forceinline__ void pcg_coef(SolveState* ss, const PcgPrev& pv, double delta, double eta, double zeta,
+                                         double* alpha_out, double* beta_out) {
+  const double prev = pv.delta;
+  const bool more = pv.cycles > 0 && prev != 0.0;
+  const double beta = more ? -pv.alpha * eta / prev : 0.0;
+  const double pi = more ? zeta + 2.0 * beta * eta + beta * beta * pv.pi : zeta;
+  const double alpha = pi != 0.0 ? delta / pi : 0.0;
   ss->beta = beta;
   ss->delta = delta;
   ss->pi = pi;
-  ss->alpha = pi != 0.0 ? delta / pi : 0.0;
+  ss->alpha = alpha;
+  *alpha_out = alpha;
+  *beta_out = beta;
+}
+__device__ __forceinline__ void pcg_coef(const SceneDesc& S, double delta, double eta, double zeta) {
+  double a, b;
+  pcg_coef(S.solve, pcg_load(S.solve), delta, eta, zeta, &a, &b);
+}
+
+// What a scene's loop decision reads: its cycle count and ||rhs||^2, and the loop's
+// control values. Kernels that decide load it after their wait on the previous kernel,
+// beside their other reads, so the decision itself waits on no load.
+struct DecideIn {
+  double b2, tol;
+  unsigned long long cond;
+  int cycles, mode, ncycles, max_cycles, nactive, iter, hard_cap, use_cond;
+};
+__device__ __forceinline__ DecideIn decide_load(const SolveCtl* ctl, const SolveState* ss) {
+  DecideIn d;
+  d.b2 = ss->bnorm2; d.tol = ctl->tol;
+  d.cycles = ss->cycles; d.mode = ctl->mode; d.ncycles = ctl->ncycles; d.max_cycles = ctl->max_cycles;
+  d.nactive = ctl->nactive; d.iter = ctl->iter; d.hard_cap = ctl->hard_cap; d.use_cond = ctl->use_cond;
+  d.cond = ctl->cond;
+  return d;
 }
 
 // The loop decision of one scene after a norm reduction (thread 0 of the CTA that
@@ -135,26 +217,28 @@ __device__ __forceinline__ void pcg_coef(const SceneDesc& S, double delta, doubl
 // (TOL/FP64) or cycles < n (FIXED), and cycles < max. Every scene deciding in this
 // cycle arrives on ctl->scenes_done with 1 << 16 | (cycles on), so the last one knows
 // how many scenes cycle on without reading them; it records that and, in a graph, sets
-// the loop's condition (loop_decide). The control values are read together up front.
-__device__ __forceinline__ void solve_decide(SolveCtl* ctl, SolveState* ss, double r2, bool count_cycle) {
-  const int cyc0 = ss->cycles;
-  const double b2 = ss->bnorm2;
-  const int mode = ctl->mode, ncyc = ctl->ncycles, maxc = ctl->max_cycles, nact = ctl->nactive;
-  const double tol = ctl->tol;
-  const int cyc = cyc0 + (count_cycle ? 1 : 0);
-  const double rel = b2 > 0.0 ? sqrt(r2 / b2) : 0.0;
-  const int act = mode == CFG_SOLVE_FIXED ? (cyc < ncyc) : ((rel > tol) && (cyc < maxc));
+// the loop's condition.
+__device__ __forceinline__ void solve_decide(SolveCtl* ctl, SolveState* ss, const DecideIn& in, double r2,
+                                             bool count_cycle) {
+  const int cyc = in.cycles + (count_cycle ? 1 : 0);
+  const double rel = in.b2 > 0.0 ? sqrt(r2 / in.b2) : 0.0;
+  const int act = in.mode == CFG_SOLVE_FIXED ? (cyc < in.ncycles) : ((rel > in.tol) && (cyc < in.max_cycles));
   ss->cycles = cyc;
   ss->rnorm2 = r2;
   ss->rel = rel;
   ss->active = act;
   const unsigned old = arrive_acq_rel(&ctl->scenes_done, (1u << 16) | (unsigned)act);
-  if ((int)(old >> 16) + 1 == nact) {
+  if ((int)(old >> 16) + 1 == in.nactive) {
     const int na = (int)(old & 0xffffu) + act;
     ctl->scenes_done = 0u;
     ctl->nactive = na;
-    loop_decide(ctl, na);
+    const int go = (na > 0 && in.iter < in.hard_cap) ? 1 : 0;
+    ctl->any_active = go;
+    if (in.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)in.cond, (unsigned)go);
   }
+}
+__device__ __forceinline__ void solve_decide(SolveCtl* ctl, SolveState* ss, double r2, bool count_cycle) {
+  solve_decide(ctl, ss, decide_load(ctl, ss), r2, count_cycle);
 }
 
 

@@ -946,7 +946,10 @@ struct Sim {
   // operator, one FP32 V-cycle on f32(r) per iteration as the preconditioner z ~ L^-1 r:
   // delta = r.z; beta = -alpha_prev (q_prev.z) / delta_prev; d = z + beta d; q = L d kept
   // as Lz + beta q (L symmetric), with d.q = z.Lz + 2 beta (q_prev.z) + beta^2 (d.q)_prev;
-  // alpha = delta / (d.q); p64 += alpha d; r -= alpha q; stop on ||r|| / ||rhs64||.
+  // alpha = delta / (d.q); p64 += alpha d; r -= alpha q; stop on ||r|| / ||rhs64|| with
+  // ||r - alpha q||^2 = r.r - 2 alpha (r.Lz + beta r.q_prev) + alpha^2 (Lz.Lz + 2 beta
+  // Lz.q_prev + beta^2 q_prev.q_prev) from the dot products taken before the update (the
+  // GPU's fused Krylov mode decides from these before it updates r).
   void pressure_pcg(bool direct) {
     rhs0_64();
     double b = 0; for (double v : rhs64) b += v * v; b = std::sqrt(b);
@@ -965,23 +968,26 @@ struct Sim {
       lap64(z, lz);
       // delta = r.z, eta = q.z, zeta = z.Lz; beta (Polak-Ribiere); d.q = zeta + 2 beta eta +
       // beta^2 (d.q)_prev with d = z + beta d and q = Lz + beta q (L symmetric); alpha = delta / d.q
-      double delta = 0, eta = 0, zeta = 0;
-      for (size_t k = 0; k < n; k++) { delta += r[k] * z[k]; eta += q[k] * z[k]; zeta += z[k] * lz[k]; }
+      double delta = 0, eta = 0, zeta = 0, rr = 0, rl = 0, rq = 0, ll = 0, lq = 0, qq = 0;
+      for (size_t k = 0; k < n; k++) {
+        delta += r[k] * z[k]; eta += q[k] * z[k]; zeta += z[k] * lz[k];
+        rr += r[k] * r[k]; rl += r[k] * lz[k]; rq += r[k] * q[k]; ll += lz[k] * lz[k]; lq += lz[k] * q[k]; qq += q[k] * q[k];
+      }
       const bool more = c > 0 && delta_prev != 0;
       const double beta = more ? -alpha * eta / delta_prev : 0.0;
       const double pi = more ? zeta + 2.0 * beta * eta + beta * beta * pi_prev : zeta;
       alpha = pi != 0 ? delta / pi : 0.0;
       delta_prev = delta; pi_prev = pi;
-      double s2 = 0;
+      const double rqc = rl + beta * rq, qqc = ll + 2.0 * beta * lq + beta * beta * qq;
+      const double s2 = rr - 2.0 * alpha * rqc + alpha * alpha * qqc;
       for (size_t k = 0; k < n; k++) {
         d[k] = c == 0 ? z[k] : z[k] + beta * d[k];
         q[k] = c == 0 ? lz[k] : lz[k] + beta * q[k];
         p64[k] += alpha * d[k];
         r[k] -= alpha * q[k];
-        s2 += r[k] * r[k];
       }
       c++;
-      rn = std::sqrt(s2);
+      rn = std::sqrt(s2 > 0 ? s2 : 0.0);
     }
     last_cycles = c; last_rel = b > 0 ? rn / b : 0.0;
   }
