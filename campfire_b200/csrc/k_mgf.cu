@@ -492,9 +492,14 @@ using namespace mgc;
 // strides along each row instead.
 struct LinMap {
   int i0, j0, R;   // first column and row of this thread, rows per round (0: the thread idles)
-  __device__ __forceinline__ LinMap(int w) {
+  __device__ __forceinline__ LinMap(int w, unsigned long long mw) {   // mw = fdiv_magic(w)
     if (w >= CB_THREADS) { i0 = threadIdx.x; j0 = 0; R = 1; }
-    else { R = CB_THREADS / w; i0 = threadIdx.x % w; j0 = threadIdx.x / w; if (j0 >= R) R = 0; }
+    else {
+      R = fdiv(CB_THREADS, mw);
+      j0 = fdiv(threadIdx.x, mw);
+      i0 = threadIdx.x - j0 * w;
+      if (j0 >= R) R = 0;
+    }
   }
   __device__ __forceinline__ int di(int w) const { return w >= CB_THREADS ? CB_THREADS : w; }   // column stride
 };
@@ -548,7 +553,7 @@ __device__ __forceinline__ void smooth_regs(const LvS& L, int first) {
     #pragma unroll
     for (int m = 0; m < NPER; m++) {
       const int t = threadIdx.x + m * CB_THREADS;
-      const int j = t / half, i = 2 * (t - j * half) + ((j + col) & 1);
+      const int j = fdiv(t, L.mhalf), i = 2 * (t - j * half) + ((j + col) & 1);
       act[col][m] = j < L.ny && i < L.nx;
       if (act[col][m]) c[col][m] = rcell_of(L, i, j);
     }
@@ -581,7 +586,7 @@ __device__ __forceinline__ void smooth_visit(const LvS& L, int first) {
   const int half = (L.nx + 1) >> 1, nslot = half * L.ny;
   if (nslot <= CB_THREADS) { smooth_regs<1>(L, first); return; }
   if (nslot <= 2 * CB_THREADS) { smooth_regs<2>(L, first); return; }
-  const LinMap mh(half);
+  const LinMap mh(half, L.mhalf);
   for (int k = 0; k < 2; k++) { pass_d(L, first, mh); __syncthreads(); pass_d(L, 1 - first, mh); __syncthreads(); }
 }
 }  // namespace
@@ -602,7 +607,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     for (int l = lc; l < nl; l++) {
       const LevelDesc& G = S.lev[l];
       LvS v;
-      v.nx = G.nx; v.ny = G.ny; v.pc = G.pc; v.pu = G.pu; v.h2 = G.h2; v.pad = 0;
+      v.nx = G.nx; v.ny = G.ny; v.pc = G.pc; v.pu = G.pu; v.h2 = G.h2; lvs_derive(v);
       v.p = q; q += G.ny * G.pc;
       v.rhs = q; q += G.ny * G.pc;
       v.ax = q; q += G.ny * G.pu;
@@ -663,17 +668,17 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     const LvS F = lv[l], Cc = lv[l + 1];
     smooth_visit(F, 0);
     {
-      const LinMap mp(F.nx);
+      const LinMap mp(F.nx, F.mnx);
       if (mp.R)
         for (int j = mp.j0; j < F.ny; j += mp.R)
           for (int i = mp.i0; i < F.nx; i += mp.di(F.nx)) {
             float off, diag; stencil_d(F, i, j, off, diag);
             const int e = j * F.pc + i;
-            sres[j * F.nx + i] = diag <= 0.f ? 0.f : F.rhs[e] - (off - diag * F.p[e]) / F.h2;
+            sres[j * F.nx + i] = diag <= 0.f ? 0.f : F.rhs[e] - div_by_rcp(off - diag * F.p[e], F.h2, F.rh2);
           }
     }
     __syncthreads();
-    const LinMap mc(Cc.nx);
+    const LinMap mc(Cc.nx, Cc.mnx);
     if (mc.R)
     for (int J = mc.j0; J < Cc.ny; J += mc.R)
       for (int I = mc.i0; I < Cc.nx; I += mc.di(Cc.nx)) {
@@ -696,9 +701,8 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     const LvS L = lv[nl - 1];
     const int n = L.nx * L.ny;
     for (int k = threadIdx.x; k < n; k += CB_THREADS) {
-      const int i = k % L.nx, j = k / L.nx;
-      float off, diag; stencil_d(L, i, j, off, diag);
-      sres[k] = diag > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
+      const int j = fdiv(k, L.mnx), i = k - j * L.nx;
+      sres[k] = diag_d(L, i, j) > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
     }
     __syncthreads();
     const float* A = S.cinv + (size_t)S.solve->cinv_cur * n * n;
@@ -713,7 +717,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       sum += __shfl_xor_sync(0xffffffffu, sum, 1);
       sum += __shfl_xor_sync(0xffffffffu, sum, 2);
       sum += __shfl_xor_sync(0xffffffffu, sum, 4);
-      if (k < n && q == 0) L.p[(k / L.nx) * L.pc + k % L.nx] = sum;
+      if (k < n && q == 0) { const int j = fdiv(k, L.mnx); L.p[j * L.pc + k - j * L.nx] = sum; }
     }
   } else {
     const LvS L = lv[nl - 1];
@@ -725,7 +729,8 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       if (b.act) L.p[b.kp] = 0.f;
       // colour of cell 2t: (i + j) & 1
       const int k0 = 2 * threadIdx.x;
-      const bool a_red = ((k0 % L.nx + k0 / L.nx) & 1) == 0;
+      const int j0 = fdiv(k0, L.mnx);
+      const bool a_red = ((k0 - j0 * L.nx + j0) & 1) == 0;
       const CCell c0 = a_red ? a : b, c1 = a_red ? b : a;
       float* p = L.p;
       bar_coarsest(nthr);
@@ -742,7 +747,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // ---- up
   for (int l = nl - 2; l >= lc; l--) {
     const LvS F = lv[l], Cc = lv[l + 1];
-    const LinMap mp(F.nx);
+    const LinMap mp(F.nx, F.mnx);
     if (mp.R)
     for (int j = mp.j0; j < F.ny; j += mp.R)
       for (int i = mp.i0; i < F.nx; i += mp.di(F.nx)) {
@@ -751,8 +756,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
         const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), Cc.ny - 1);
         const float c = 0.5625f * Cc.p[J * Cc.pc + I] + 0.1875f * (Cc.p[J * Cc.pc + I2] + Cc.p[J2 * Cc.pc + I]) +
                         0.0625f * Cc.p[J2 * Cc.pc + I2];
-        float off, diag; stencil_d(F, i, j, off, diag);
-        F.p[j * F.pc + i] += diag > 0.f ? c : 0.f;
+        F.p[j * F.pc + i] += diag_d(F, i, j) > 0.f ? c : 0.f;
       }
     __syncthreads();
     smooth_visit(F, 1);
@@ -760,7 +764,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // ---- write level lc back; when the block covers level 0, finish the cycle here
   const LevelDesc& G = S.lev[lc];
   double part = 0.0, part2 = 0.0, part3 = 0.0;
-  const LinMap mw(G.nx);
+  const LinMap mw(V0.nx, V0.mnx);
   if (mw.R)
   for (int j = mw.j0; j < G.ny; j += mw.R)
     for (int i = mw.i0; i < G.nx; i += mw.di(G.nx)) {

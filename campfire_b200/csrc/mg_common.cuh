@@ -8,7 +8,28 @@
 namespace cfg {
 namespace mgc {
 
-struct LvS { float *p, *rhs, *ax, *ay; int nx, ny, pc, pu; float h2; int pad; };
+struct LvS {
+  float *p, *rhs, *ax, *ay;
+  int nx, ny, pc, pu;
+  float h2, rh2;                      // rh2 = RN(1 / h2)
+  unsigned long long mnx, mhalf;      // fdiv multipliers of nx and (nx + 1) / 2
+};
+
+// t / d without a division instruction for 0 <= t < 2^16 and 1 <= d < 2^16, from
+// m = floor(2^32 / d) + 1 = (2^32 + e) / d with 0 < e <= d: t m / 2^32 = t / d + t e / (d 2^32)
+// and t e < 2^32, so the excess stays below 1/d and the floor is t / d (the invariant-divisor
+// multiplication of Granlund & Montgomery, PLDI 1994). The coarse levels in shared memory
+// and the block's thread indices are far below 2^16.
+__device__ __forceinline__ unsigned long long fdiv_magic(int d) { return 0x100000000ull / (unsigned)d + 1ull; }
+__device__ __forceinline__ int fdiv(int t, unsigned long long m) {
+  return (int)(((unsigned long long)(unsigned)t * m) >> 32);
+}
+// the derived constants of a level (one thread, once per kernel)
+__device__ __forceinline__ void lvs_derive(LvS& v) {
+  v.rh2 = __frcp_rn(v.h2);
+  v.mnx = fdiv_magic(v.nx);
+  v.mhalf = fdiv_magic((v.nx + 1) >> 1);
+}
 
 __device__ __forceinline__ void stencil_d(const LvS& L, int i, int j, float& off, float& diag) {
   off = 0.f; diag = 0.f;
@@ -19,6 +40,17 @@ __device__ __forceinline__ void stencil_d(const LvS& L, int i, int j, float& off
   if (i < L.nx - 1) { off += e * p[j * L.pc + i + 1]; diag += e; } else { diag += 2.f * e; }
   if (j > 0) { off += s * p[(j - 1) * L.pc + i]; diag += s; }
   if (j < L.ny - 1) { off += n * p[(j + 1) * L.pc + i]; diag += n; } else { diag += 2.f * n; }
+}
+// the diagonal of stencil_d alone (the same sums in the same order)
+__device__ __forceinline__ float diag_d(const LvS& L, int i, int j) {
+  const float w = L.ax[j * L.pu + i], e = L.ax[j * L.pu + i + 1];
+  const float s = L.ay[j * L.pc + i], n = L.ay[(j + 1) * L.pc + i];
+  float diag = 0.f;
+  if (i > 0) diag += w; else diag += 2.f * w;
+  if (i < L.nx - 1) diag += e; else diag += 2.f * e;
+  if (j > 0) diag += s;
+  if (j < L.ny - 1) diag += n; else diag += 2.f * n;
+  return diag;
 }
 // (L z)_ij in FP64 from a level in shared memory (the FP64 defect's form)
 __device__ __forceinline__ double lap_block64(const LvS& L, int i, int j) {
@@ -54,7 +86,7 @@ __device__ __forceinline__ CCell coarsest_cell(const LvS& L, int k) {
   CCell c{};
   c.act = k < L.nx * L.ny;
   if (!c.act) return c;
-  const int i = k % L.nx, j = k / L.nx;
+  const int j = fdiv(k, L.mnx), i = k - j * L.nx;
   c.kp = j * L.pc + i;
   c.w = L.ax[j * L.pu + i]; c.e = L.ax[j * L.pu + i + 1];
   c.s = L.ay[j * L.pc + i]; c.n = L.ay[(j + 1) * L.pc + i];
