@@ -591,29 +591,37 @@ __device__ __forceinline__ void smooth_visit(const LvS& L, int first) {
 }
 }  // namespace
 
+// smem_floats: the launch's dynamic shared memory in floats; past the levels and the residual
+// scratch, the coarsest inverse of the direct solve is staged there when it fits
 __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __restrict__ scenes, int nscenes, SolveCtl* ctl, int tail,
-                                                         int count_iter) {
+                                                         int count_iter, int smem_floats) {
   extern __shared__ __align__(128) float smem[];
   __shared__ double red[32];
-  __shared__ LvS lv[MAX_LEVELS];
+  __shared__ LvO lvo[MAX_LEVELS];
   __shared__ __align__(8) uint64_t bar;
-  __shared__ int s_ok;
+  __shared__ int s_ok, s_inv, s_res, s_A;   // s_res, s_A: offsets of the residual scratch and the inverse
   const SceneDesc& S = scenes[blockIdx.x];
   pdl_trigger();
   const int lc = S.lc, nl = S.nlev;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    float* q = smem;
+    int q = 0;
     for (int l = lc; l < nl; l++) {
       const LevelDesc& G = S.lev[l];
       LvS v;
-      v.nx = G.nx; v.ny = G.ny; v.pc = G.pc; v.pu = G.pu; v.h2 = G.h2; lvs_derive(v);
-      v.p = q; q += G.ny * G.pc;
-      v.rhs = q; q += G.ny * G.pc;
-      v.ax = q; q += G.ny * G.pu;
-      v.ay = q; q += (G.ny + 1) * G.pc;
-      lv[l] = v;
+      v.nx = G.nx; v.h2 = G.h2; lvs_derive(v);
+      LvO o;
+      o.nx = G.nx; o.ny = G.ny; o.pc = G.pc; o.pu = G.pu; o.h2 = G.h2; o.rh2 = v.rh2; o.mnx = v.mnx; o.mhalf = v.mhalf;
+      o.po = q; q += G.ny * G.pc;
+      o.ro = q; q += G.ny * G.pc;
+      o.ao = q; q += G.ny * G.pu;
+      o.yo = q; q += (G.ny + 1) * G.pc;
+      lvo[l] = o;
     }
+    s_res = q;
+    const int nres = S.lev[lc].nx * S.lev[lc].ny;
+    q += round_up(nres > COARSEST_SCRATCH ? nres : COARSEST_SCRATCH, 32);   // residual scratch
+    s_A = q;
     mbar_init(&bar, 2);
   }
   __syncthreads();
@@ -621,24 +629,38 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // The coefficients are built before the pressure loop and no loop kernel writes them: their
   // copies start before the wait on the previous kernel (first arrival on the barrier); the
   // rhs (and level 0's p) follow after it (second arrival, no bytes if the scene has stopped).
+  // The direct solve's inverse (the half cinv_cur of S.cinv) is also fixed for the loop: it is
+  // factored before the loop or, pipelined, during the previous step (the side branch of this
+  // step writes the other half), so it is staged here too when it fits (n even: 16-byte size).
   const bool on = S.enabled;   // host-written, constant during the step
   const volatile int* act = &S.solve->active;
-  if (threadIdx.x == 0 && on) {
-    uint32_t bytes = 0;
-    for (int l = lc; l < nl; l++) bytes += (S.lev[l].ny * S.lev[l].pu + (S.lev[l].ny + 1) * S.lev[l].pc) * 4;
-    mbar_arrive_expect_tx(&bar, bytes);
-    for (int l = lc; l < nl; l++) {
-      const LevelDesc& G = S.lev[l];
-      bulk_g2s(lv[l].ax, G.ax, G.ny * G.pu * 4, &bar);
-      bulk_g2s(lv[l].ay, G.ay, (G.ny + 1) * G.pc * 4, &bar);
+  if (threadIdx.x == 0) {
+    s_inv = 0;
+    if (on) {
+      uint32_t bytes = 0;
+      for (int l = lc; l < nl; l++) bytes += (S.lev[l].ny * S.lev[l].pu + (S.lev[l].ny + 1) * S.lev[l].pc) * 4;
+      const int n = S.lev[nl - 1].nx * S.lev[nl - 1].ny;
+      const bool inv = ctl->coarse_direct && S.solve->direct_ok && (n % 2) == 0 &&
+                       s_A + n * n <= smem_floats;
+      if (inv) bytes += (uint32_t)(n * n * 4);
+      mbar_arrive_expect_tx(&bar, bytes);
+      for (int l = lc; l < nl; l++) {
+        const LevelDesc& G = S.lev[l];
+        bulk_g2s(smem + lvo[l].ao, G.ax, G.ny * G.pu * 4, &bar);
+        bulk_g2s(smem + lvo[l].yo, G.ay, (G.ny + 1) * G.pc * 4, &bar);
+      }
+      if (inv) {
+        bulk_g2s(smem + s_A, S.cinv + (size_t)S.solve->cinv_cur * n * n, (uint32_t)(n * n * 4), &bar);
+        s_inv = 1;
+      }
     }
   }
   pdl_wait();
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!on) return;
   const bool live = *act != 0;
-  const LvS V0 = lv[lc];
-  float* sres = lv[nl - 1].ay + (lv[nl - 1].ny + 1) * lv[nl - 1].pc;   // residual scratch (level lc size)
+  const LvS V0 = lvs_at(smem, lvo[lc]);
+  float* sres = smem + s_res;   // residual scratch (level lc size)
   if (threadIdx.x == 0) {
     const LevelDesc& G0 = S.lev[lc];
     mbar_arrive_expect_tx(&bar, live ? G0.ny * G0.pc * 4 * (lc == 0 ? 2 : 1) : 0u);
@@ -663,27 +685,21 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     mbar_wait(&bar, 0);
     return;
   }
-  // ---- down
+  // ---- down: smoothing, then per coarse cell the residuals of its four fine cells
+  // (pressure.wgsl:96-101) summed in the restriction's order (pressure.wgsl:104-113)
   for (int l = lc; l < nl - 1; l++) {
-    const LvS F = lv[l], Cc = lv[l + 1];
+    const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
     smooth_visit(F, 0);
-    {
-      const LinMap mp(F.nx, F.mnx);
-      if (mp.R)
-        for (int j = mp.j0; j < F.ny; j += mp.R)
-          for (int i = mp.i0; i < F.nx; i += mp.di(F.nx)) {
-            float off, diag; stencil_d(F, i, j, off, diag);
-            const int e = j * F.pc + i;
-            sres[j * F.nx + i] = diag <= 0.f ? 0.f : F.rhs[e] - div_by_rcp(off - diag * F.p[e], F.h2, F.rh2);
-          }
-    }
-    __syncthreads();
+    auto res = [&](int i, int j) {
+      float off, diag; stencil_d(F, i, j, off, diag);
+      const int e = j * F.pc + i;
+      return diag <= 0.f ? 0.f : F.rhs[e] - div_by_rcp(off - diag * F.p[e], F.h2, F.rh2);
+    };
     const LinMap mc(Cc.nx, Cc.mnx);
     if (mc.R)
     for (int J = mc.j0; J < Cc.ny; J += mc.R)
       for (int I = mc.i0; I < Cc.nx; I += mc.di(Cc.nx)) {
-        const float r = sres[(2 * J) * F.nx + 2 * I] + sres[(2 * J) * F.nx + 2 * I + 1] + sres[(2 * J + 1) * F.nx + 2 * I] +
-                        sres[(2 * J + 1) * F.nx + 2 * I + 1];
+        const float r = res(2 * I, 2 * J) + res(2 * I + 1, 2 * J) + res(2 * I, 2 * J + 1) + res(2 * I + 1, 2 * J + 1);
         Cc.rhs[J * Cc.pc + I] = 0.25f * r;
         Cc.p[J * Cc.pc + I] = 0.f;
       }
@@ -698,21 +714,27 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   if (ctl->coarse_direct && S.solve->direct_ok) {
     // direct coarse solve (TOL/FP64 modes): p = A^-1 b with b = -rhs h2 (0 in closed cells),
     // each row's dot product as 8 strided partial sums combined pairwise (the oracle's order)
-    const LvS L = lv[nl - 1];
+    const LvS L = lvs_at(smem, lvo[nl - 1]);
     const int n = L.nx * L.ny;
     for (int k = threadIdx.x; k < n; k += CB_THREADS) {
       const int j = fdiv(k, L.mnx), i = k - j * L.nx;
       sres[k] = diag_d(L, i, j) > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
     }
     __syncthreads();
-    const float* A = S.cinv + (size_t)S.solve->cinv_cur * n * n;
     const int q = lane & 7;
+    const bool staged = s_inv != 0;
+    const float* A = staged ? smem + s_A : S.cinv + (size_t)S.solve->cinv_cur * n * n;
     for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
       const int k = base + (lane >> 3);
       float sum = 0.f;
       if (k < n) {
-        #pragma unroll 4
-        for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(A + (size_t)k * n + m), sres[m], sum);
+        if (staged) {
+          #pragma unroll 4
+          for (int m = q; m < n; m += 8) sum = __fmaf_rn(A[k * n + m], sres[m], sum);
+        } else {
+          #pragma unroll 4
+          for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(A + (size_t)k * n + m), sres[m], sum);
+        }
       }
       sum += __shfl_xor_sync(0xffffffffu, sum, 1);
       sum += __shfl_xor_sync(0xffffffffu, sum, 2);
@@ -720,7 +742,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       if (k < n && q == 0) { const int j = fdiv(k, L.mnx); L.p[j * L.pc + k - j * L.nx] = sum; }
     }
   } else {
-    const LvS L = lv[nl - 1];
+    const LvS L = lvs_at(smem, lvo[nl - 1]);
     const int npair = (L.nx * L.ny + 1) >> 1;
     const int nthr = (npair + 31) & ~31;
     if ((int)threadIdx.x < nthr) {
@@ -746,7 +768,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   __syncthreads();
   // ---- up
   for (int l = nl - 2; l >= lc; l--) {
-    const LvS F = lv[l], Cc = lv[l + 1];
+    const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
     const LinMap mp(F.nx, F.mnx);
     if (mp.R)
     for (int j = mp.j0; j < F.ny; j += mp.R)
@@ -980,7 +1002,10 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
     const size_t pc = (size_t)round_up(lnx[l], 32), pu = (size_t)round_up(lnx[l] + 1, 32);
     f += 2 * lny[l] * pc + lny[l] * pu + (lny[l] + 1) * pc;
   }
-  f += std::max((size_t)lnx[lc] * lny[lc], (size_t)COARSEST_SCRATCH);
+  f += (size_t)round_up(std::max(lnx[lc] * lny[lc], COARSEST_SCRATCH), 32);
+  // room for the coarsest inverse of the direct solve when it fits
+  const size_t n = (size_t)lnx[nlev - 1] * lny[nlev - 1];
+  if (n % 2 == 0 && (f + n * n) * 4 <= kCoarseSmemMax) f += n * n;
   return f * 4;
 }
 
@@ -1000,7 +1025,7 @@ void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int t
                       cudaStream_t st) {
   if (nscenes > 0)
     launch_pdl(pdl_enabled(), k_mg_coarse, dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail,
-               count_iter);
+               count_iter, (int)(smem / 4));
 }
 // bw: the widest coarsest level of the batch (the register window's bound)
 void launch_coarse_factor(const SceneDesc* scenes, int nscenes, size_t smem, int bw, int pipelined, cudaStream_t st) {

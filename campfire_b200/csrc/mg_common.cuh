@@ -24,6 +24,21 @@ __device__ __forceinline__ unsigned long long fdiv_magic(int d) { return 0x10000
 __device__ __forceinline__ int fdiv(int t, unsigned long long m) {
   return (int)(((unsigned long long)(unsigned)t * m) >> 32);
 }
+// A level of a block's shared-memory layout as offsets from the block's dynamic shared
+// array; lvs_at rebuilds the pointers from that array inside the kernel, so the compiler
+// sees shared-memory addresses (shared loads and stores, 32-bit addresses).
+struct LvO {
+  int po, ro, ao, yo;
+  int nx, ny, pc, pu;
+  float h2, rh2;
+  unsigned long long mnx, mhalf;
+};
+__device__ __forceinline__ LvS lvs_at(float* base, const LvO& o) {
+  LvS v;
+  v.p = base + o.po; v.rhs = base + o.ro; v.ax = base + o.ao; v.ay = base + o.yo;
+  v.nx = o.nx; v.ny = o.ny; v.pc = o.pc; v.pu = o.pu; v.h2 = o.h2; v.rh2 = o.rh2; v.mnx = o.mnx; v.mhalf = o.mhalf;
+  return v;
+}
 // the derived constants of a level (one thread, once per kernel)
 __device__ __forceinline__ void lvs_derive(LvS& v) {
   v.rh2 = __frcp_rn(v.h2);
