@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(CC_THREADS) k_mg_cluster(const SceneDesc* __re
     } else {
       // the reference's 120 sweeps from zero on rank 0 over a gathered copy of the level
       LvS D;
-      D.nx = L.nx; D.ny = L.ny; D.pc = L.pc; D.pu = L.pu; D.h2 = L.h2; lvs_derive(D);
+      D.nx = L.nx; D.ny = L.ny; D.pc = L.pc; D.pu = L.pu; D.h2 = L.h2; D.rc = nullptr; lvs_derive(D);
       D.p = dense; D.rhs = D.p + L.ny * L.pc; D.ax = D.rhs + L.ny * L.pc; D.ay = D.ax + L.ny * L.pu;
       cl.sync();   // the owners' coarsest rhs is complete
       if (rank == 0) {

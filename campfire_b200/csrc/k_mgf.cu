@@ -536,11 +536,21 @@ __device__ __forceinline__ void pass_d(const LvS& L, int color, const LinMap& mp
 // pass_d's, with the division by the diagonal as div_by_rcp: the same quotient.
 // one cell's stencil in 9 registers: fl bit 0..3 = west, east, south, north neighbour present
 struct RCell { float w, e, s, n, rh, diag, rcp; int kp, fl; };
+// the diagonal's reciprocal comes from the block's table (L.rc, built once per kernel)
 __device__ __forceinline__ RCell rcell_of(const LvS& L, int i, int j) {
-  const CCell q = coarsest_cell(L, j * L.nx + i);
   RCell c;
-  c.w = q.w; c.e = q.e; c.s = q.s; c.n = q.n; c.rh = q.rh; c.diag = q.diag; c.rcp = q.rcp; c.kp = q.kp;
-  c.fl = (q.hw ? 1 : 0) | (q.he ? 2 : 0) | (q.hs ? 4 : 0) | (q.hn ? 8 : 0);
+  c.kp = j * L.pc + i;
+  c.w = L.ax[j * L.pu + i]; c.e = L.ax[j * L.pu + i + 1];
+  c.s = L.ay[c.kp]; c.n = L.ay[c.kp + L.pc];
+  float diag = 0.f;
+  if (i > 0) diag += c.w; else diag += 2.f * c.w;
+  if (i < L.nx - 1) diag += c.e; else diag += 2.f * c.e;
+  if (j > 0) diag += c.s;
+  if (j < L.ny - 1) diag += c.n; else diag += 2.f * c.n;
+  c.diag = diag;
+  c.rcp = L.rc[j * L.nx + i];
+  c.rh = L.rhs[c.kp] * L.h2;
+  c.fl = (i > 0 ? 1 : 0) | (i < L.nx - 1 ? 2 : 0) | (j > 0 ? 4 : 0) | (j < L.ny - 1 ? 8 : 0);
   return c;
 }
 template <int NPER>
@@ -598,8 +608,9 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   extern __shared__ __align__(128) float smem[];
   __shared__ double red[32];
   __shared__ LvO lvo[MAX_LEVELS];
-  __shared__ __align__(8) uint64_t bar;
-  __shared__ int s_ok, s_inv, s_res, s_A;   // s_res, s_A: offsets of the residual scratch and the inverse
+  __shared__ __align__(8) uint64_t bar;    // the coefficients (+ inverse)
+  __shared__ int s_inv, s_res, s_A, s_dir, s_gpc;   // offsets: residual scratch, inverse
+  __shared__ float* s_gp;                         // level lc's p in global memory
   const SceneDesc& S = scenes[blockIdx.x];
   pdl_trigger();
   const int lc = S.lc, nl = S.nlev;
@@ -621,27 +632,32 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     s_res = q;
     const int nres = S.lev[lc].nx * S.lev[lc].ny;
     q += round_up(nres > COARSEST_SCRATCH ? nres : COARSEST_SCRATCH, 32);   // residual scratch
+    for (int l = lc; l < nl; l++) { lvo[l].to = q; q += S.lev[l].nx * S.lev[l].ny; }
+    q = round_up(q, 32);
     s_A = q;
-    mbar_init(&bar, 2);
+    s_gp = S.lev[lc].p; s_gpc = S.lev[lc].pc;
+    mbar_init(&bar, 1);
   }
   __syncthreads();
-  // ---- stage the arrays with TMA bulk copies (one per array; sizes are multiples of 128 bytes).
-  // The coefficients are built before the pressure loop and no loop kernel writes them: their
-  // copies start before the wait on the previous kernel (first arrival on the barrier); the
-  // rhs (and level 0's p) follow after it (second arrival, no bytes if the scene has stopped).
-  // The direct solve's inverse (the half cinv_cur of S.cinv) is also fixed for the loop: it is
-  // factored before the loop or, pipelined, during the previous step (the side branch of this
-  // step writes the other half), so it is staged here too when it fits (n even: 16-byte size).
+  // ---- stage the arrays. The coefficients are built before the pressure loop and no loop
+  // kernel writes them; the direct solve's inverse (the half cinv_cur of S.cinv) is factored
+  // before the loop or, pipelined, during the previous step (this step's side branch writes
+  // the other half). Both arrive by TMA bulk copies (sizes multiples of 16 bytes; the
+  // inverse when it fits, n even) before the wait on the previous kernel, and the reciprocal
+  // of each cell's diagonal (pressure.wgsl:77-86; 0 marks a closed cell) is tabled then too,
+  // beside the previous kernel. After the wait only level lc's rhs (and p when lc = 0) is
+  // read, with plain loads from L2.
   const bool on = S.enabled;   // host-written, constant during the step
   const volatile int* act = &S.solve->active;
   if (threadIdx.x == 0) {
     s_inv = 0;
+    s_dir = 0;
     if (on) {
       uint32_t bytes = 0;
       for (int l = lc; l < nl; l++) bytes += (S.lev[l].ny * S.lev[l].pu + (S.lev[l].ny + 1) * S.lev[l].pc) * 4;
       const int n = S.lev[nl - 1].nx * S.lev[nl - 1].ny;
-      const bool inv = ctl->coarse_direct && S.solve->direct_ok && (n % 2) == 0 &&
-                       s_A + n * n <= smem_floats;
+      s_dir = ctl->coarse_direct && S.solve->direct_ok;   // both fixed for the loop
+      const bool inv = s_dir && (n % 2) == 0 && s_A + n * n <= smem_floats;
       if (inv) bytes += (uint32_t)(n * n * 4);
       mbar_arrive_expect_tx(&bar, bytes);
       for (int l = lc; l < nl; l++) {
@@ -655,36 +671,40 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       }
     }
   }
+  const LvS V0 = lvs_at(smem, lvo[lc]);
+  const float* grhs = S.lev[lc].rhs;
+  bool okc = true;
+  if (on) {
+    okc = mbar_wait(&bar, 0);
+    if (okc)
+      for (int l = lc; l < nl; l++) {
+        const LvS L = lvs_at(smem, lvo[l]);
+        float* rc = smem + lvo[l].to;
+        for (int e = threadIdx.x; e < L.nx * L.ny; e += CB_THREADS) {
+          const int j = fdiv(e, L.mnx), i = e - j * L.nx;
+          const float d = diag_d(L, i, j);
+          rc[e] = d > 0.f ? __frcp_rn(d) : 0.f;
+        }
+      }
+    // level lc's p is zero after the restriction into it (pressure.wgsl:112)
+    if (lc > 0)
+      for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.p[e] = 0.f;
+  }
   pdl_wait();
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!on) return;
-  const bool live = *act != 0;
-  const LvS V0 = lvs_at(smem, lvo[lc]);
-  float* sres = smem + s_res;   // residual scratch (level lc size)
-  if (threadIdx.x == 0) {
-    const LevelDesc& G0 = S.lev[lc];
-    mbar_arrive_expect_tx(&bar, live ? G0.ny * G0.pc * 4 * (lc == 0 ? 2 : 1) : 0u);
-    if (live) {
-      bulk_g2s(V0.rhs, G0.rhs, G0.ny * G0.pc * 4, &bar);
-      if (lc == 0) bulk_g2s(V0.p, G0.p, G0.ny * G0.pc * 4, &bar);   // warm start
-    }
-  }
-  if (!live) {   // the coefficient copies land before the block leaves (bounded)
-    mbar_wait(&bar, 0);
-    return;
-  }
-  // level lc's p is zero after the restriction into it (pressure.wgsl:112)
-  if (lc > 0)
-    for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.p[e] = 0.f;
-  const bool ok = mbar_wait(&bar, 0);
-  if (threadIdx.x == 0) s_ok = ok ? 1 : 0;
-  __syncthreads();
-  if (!s_ok) {
+  if (__syncthreads_or(!okc)) {
     // the copies did not land in time: record it and leave once they have (bounded)
     if (threadIdx.x == 0) atomicExch(&ctl->err, 1);
     mbar_wait(&bar, 0);
     return;
   }
+  if (*act == 0) return;
+  float* sres = smem + s_res;   // residual scratch (level lc size)
+  for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.rhs[e] = __ldcg(grhs + e);
+  if (lc == 0)   // warm start
+    for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.p[e] = __ldcg(s_gp + e);
+  __syncthreads();
   // ---- down: smoothing, then per coarse cell the residuals of its four fine cells
   // (pressure.wgsl:96-101) summed in the restriction's order (pressure.wgsl:104-113)
   for (int l = lc; l < nl - 1; l++) {
@@ -711,14 +731,14 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // thread works in every pass; the ceil(n/2) threads (<= 128, rounded up to warps)
   // sync on a named barrier while the other warps wait at the block barrier below.
   // Stencils, diagonals and their reciprocals stay in registers for all sweeps.
-  if (ctl->coarse_direct && S.solve->direct_ok) {
+  if (s_dir) {
     // direct coarse solve (TOL/FP64 modes): p = A^-1 b with b = -rhs h2 (0 in closed cells),
     // each row's dot product as 8 strided partial sums combined pairwise (the oracle's order)
     const LvS L = lvs_at(smem, lvo[nl - 1]);
     const int n = L.nx * L.ny;
     for (int k = threadIdx.x; k < n; k += CB_THREADS) {
       const int j = fdiv(k, L.mnx), i = k - j * L.nx;
-      sres[k] = diag_d(L, i, j) > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
+      sres[k] = L.rc[k] > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
     }
     __syncthreads();
     const int q = lane & 7;
@@ -778,32 +798,33 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
         const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), Cc.ny - 1);
         const float c = 0.5625f * Cc.p[J * Cc.pc + I] + 0.1875f * (Cc.p[J * Cc.pc + I2] + Cc.p[J2 * Cc.pc + I]) +
                         0.0625f * Cc.p[J2 * Cc.pc + I2];
-        F.p[j * F.pc + i] += diag_d(F, i, j) > 0.f ? c : 0.f;
+        F.p[j * F.pc + i] += F.rc[j * F.nx + i] > 0.f ? c : 0.f;
       }
     __syncthreads();
     smooth_visit(F, 1);
   }
   // ---- write level lc back; when the block covers level 0, finish the cycle here
-  const LevelDesc& G = S.lev[lc];
+  float* const gp = s_gp;
+  const int gpc = s_gpc, gnx = V0.nx;
   double part = 0.0, part2 = 0.0, part3 = 0.0;
   const LinMap mw(V0.nx, V0.mnx);
   if (mw.R)
-  for (int j = mw.j0; j < G.ny; j += mw.R)
-    for (int i = mw.i0; i < G.nx; i += mw.di(G.nx)) {
+  for (int j = mw.j0; j < V0.ny; j += mw.R)
+    for (int i = mw.i0; i < V0.nx; i += mw.di(V0.nx)) {
       const int e = j * V0.pc + i;
-      G.p[j * G.pc + i] = V0.p[e];
+      gp[j * gpc + i] = V0.p[e];
       if (lc == 0 && tail == 1) {
         float off, diag; stencil_d(V0, i, j, off, diag);
         const double r = diag <= 0.f ? 0.0 : (double)(V0.rhs[e] - (off - diag * V0.p[e]) / V0.h2);
         part += r * r;
       } else if (lc == 0 && tail == 2) {
-        S.p64[j * G.nx + i] += (double)V0.p[e];
+        S.p64[j * gnx + i] += (double)V0.p[e];
       } else if (lc == 0 && tail == 3) {
         const double z = (double)V0.p[e];
         const double lz = lap_block64(V0, i, j);
-        S.dB[j * G.nx + i] = lz;
-        part += S.r64[j * G.nx + i] * z;
-        part2 += S.q64[j * G.nx + i] * z;
+        S.dB[j * gnx + i] = lz;
+        part += S.r64[j * gnx + i] * z;
+        part2 += S.q64[j * gnx + i] * z;
         part3 += z * lz;
       }
     }
@@ -1003,6 +1024,9 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
     f += 2 * lny[l] * pc + lny[l] * pu + (lny[l] + 1) * pc;
   }
   f += (size_t)round_up(std::max(lnx[lc] * lny[lc], COARSEST_SCRATCH), 32);
+  size_t cells = 0;   // the 1/diag table of every level
+  for (int l = lc; l < nlev; l++) cells += (size_t)lnx[l] * lny[l];
+  f += (size_t)round_up((int)cells, 32);
   // room for the coarsest inverse of the direct solve when it fits
   const size_t n = (size_t)lnx[nlev - 1] * lny[nlev - 1];
   if (n % 2 == 0 && (f + n * n) * 4 <= kCoarseSmemMax) f += n * n;

@@ -10,6 +10,7 @@ namespace mgc {
 
 struct LvS {
   float *p, *rhs, *ax, *ay;
+  const float* rc;                    // the coarse block's RN(1/diag) per cell (0: closed), row-major
   int nx, ny, pc, pu;
   float h2, rh2;                      // rh2 = RN(1 / h2)
   unsigned long long mnx, mhalf;      // fdiv multipliers of nx and (nx + 1) / 2
@@ -28,7 +29,7 @@ __device__ __forceinline__ int fdiv(int t, unsigned long long m) {
 // array; lvs_at rebuilds the pointers from that array inside the kernel, so the compiler
 // sees shared-memory addresses (shared loads and stores, 32-bit addresses).
 struct LvO {
-  int po, ro, ao, yo;
+  int po, ro, ao, yo, to;             // p, rhs, ax, ay; to: the 1/diag table
   int nx, ny, pc, pu;
   float h2, rh2;
   unsigned long long mnx, mhalf;
@@ -36,6 +37,7 @@ struct LvO {
 __device__ __forceinline__ LvS lvs_at(float* base, const LvO& o) {
   LvS v;
   v.p = base + o.po; v.rhs = base + o.ro; v.ax = base + o.ao; v.ay = base + o.yo;
+  v.rc = base + o.to;
   v.nx = o.nx; v.ny = o.ny; v.pc = o.pc; v.pu = o.pu; v.h2 = o.h2; v.rh2 = o.rh2; v.mnx = o.mnx; v.mhalf = o.mhalf;
   return v;
 }
