@@ -234,7 +234,9 @@ __device__ __forceinline__ void solve_decide(SolveCtl* ctl, SolveState* ss, cons
     ctl->nactive = na;
     const int go = (na > 0 && in.iter < in.hard_cap) ? 1 : 0;
     ctl->any_active = go;
-    if (in.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)in.cond, (unsigned)go);
+    // the condition starts every launch of the step graph at 1 (cudaGraphCondAssignDefault)
+    // and only this decision or the hard cap clears it, so it is written only to stop
+    if (in.use_cond && !go) cudaGraphSetConditional((cudaGraphConditionalHandle)in.cond, 0u);
   }
 }
 __device__ __forceinline__ void solve_decide(SolveCtl* ctl, SolveState* ss, double r2, bool count_cycle) {
