@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   __shared__ __align__(128) float sax[MGF_BH * MGF_BW];
   __shared__ __align__(128) float say[(MGF_BH + 1) * MGF_BW];
   __shared__ __align__(128) float scp[MGF_CBH * MGF_CBW];
-  __shared__ double red[9 * 32];
+  __shared__ double red[32];
   __shared__ __align__(8) uint64_t bar[2];
   const Work w = work[blockIdx.x];
   const SceneDesc& S = scenes[w.scene];
@@ -426,8 +426,9 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
       v[0] += r * z; v[1] += q * z; v[2] += z * lz;
       v[3] += r * r; v[4] += r * lz; v[5] += r * q; v[6] += lz * lz; v[7] += lz * q; v[8] += q * q;
     }
-    block_sum_n<9>(v, red);
-    if (scene_reduce_n<9>(S, w.tile, S.nt_up0, v, red) && threadIdx.x == 0) {
+    __shared__ double redt[9 * 256 + 9];
+    block_sum_t<9>(v, redt);
+    if (scene_reduce_n<9>(S, w.tile, S.nt_up0, v, redt) && threadIdx.x == 0) {
       double alpha, beta;
       pcg_coef(ss, pv, v[0], v[1], v[2], &alpha, &beta);
       // ||r - alpha (Lz + beta q)||^2 from the dot products

@@ -114,32 +114,33 @@ __device__ __forceinline__ bool scene_reduce3(const SceneDesc& S, int tile, int 
   return true;
 }
 
-// N sums over the block at once (each in the fixed order of block_sum); the results are
-// valid in thread 0. sh holds at least 32 N doubles.
+// N sums over a block of 256 threads at once, in a fixed order: every thread's values go to
+// shared memory; warp w sums quantities w, w + 8, ...: lane l adds threads l, l + 32, ...,
+// l + 224 in that order, then the warp's shuffle tree. The totals are valid in thread 0.
+// sh holds at least 256 N + N doubles.
 template <int N>
-__device__ __forceinline__ void block_sum_n(double (&v)[N], double* sh) {
+__device__ __forceinline__ void block_sum_t(double (&v)[N], double* sh) {
   #pragma unroll
-  for (int m = 0; m < N; m++)
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[m] += __shfl_down_sync(0xffffffffu, v[m], o);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int m = 0; m < N; m++) sh[m * 256 + threadIdx.x] = v[m];
   __syncthreads();
-  if (lane == 0)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int m = warp; m < N; m += 8) {
+    double t = 0.0;
     #pragma unroll
-    for (int m = 0; m < N; m++) sh[m * 32 + warp] = v[m];
+    for (int k = 0; k < 8; k++) t += sh[m * 256 + lane + 32 * k];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) sh[N * 256 + m] = t;
+  }
   __syncthreads();
-  if (warp == 0)
+  if (threadIdx.x == 0)
     #pragma unroll
-    for (int m = 0; m < N; m++) {
-      double t = lane < nw ? sh[m * 32 + lane] : 0.0;
-      #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-      v[m] = t;
-    }
+    for (int m = 0; m < N; m++) v[m] = sh[N * 256 + m];
 }
 
 // N sums of one scene at once (partials at part[N tile + m]); the scene_reduce protocol.
 // On return true (the CTA that completed the scene), v holds the totals in thread 0.
+// 256 threads; sh as for block_sum_t.
 template <int N>
 __device__ __forceinline__ bool scene_reduce_n(const SceneDesc& S, int tile, int ntiles, double (&v)[N], double* sh) {
   __shared__ int s_lastn;
@@ -156,7 +157,7 @@ __device__ __forceinline__ bool scene_reduce_n(const SceneDesc& S, int tile, int
   for (int k = threadIdx.x; k < ntiles; k += blockDim.x)
     #pragma unroll
     for (int m = 0; m < N; m++) v[m] += __ldcg(S.part + N * k + m);
-  block_sum_n<N>(v, sh);
+  block_sum_t<N>(v, sh);
   if (threadIdx.x == 0) S.solve->counter = 0u;
   return true;
 }
@@ -227,7 +228,8 @@ __device__ __forceinline__ void solve_decide(SolveCtl* ctl, SolveState* ss, cons
   ss->rnorm2 = r2;
   ss->rel = rel;
   ss->active = act;
-  const unsigned old = arrive_acq_rel(&ctl->scenes_done, (1u << 16) | (unsigned)act);
+  // one scene cycling: it is the last to decide, with no arrival to count
+  const unsigned old = in.nactive == 1 ? 0u : arrive_acq_rel(&ctl->scenes_done, (1u << 16) | (unsigned)act);
   if ((int)(old >> 16) + 1 == in.nactive) {
     const int na = (int)(old & 0xffffu) + act;
     ctl->scenes_done = 0u;
