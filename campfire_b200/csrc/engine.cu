@@ -955,7 +955,9 @@ int Engine::max_lc() const {
 }
 
 bool Engine::pcg_fused() const {
-  if (!krylov() || scenes_.empty()) return false;
+  // one scene: the folded update shortens the cycle's kernel chain; a batch is bound by
+  // bandwidth instead, and the separate update kernel moves fewer bytes than the fold
+  if (!krylov() || scenes_.size() != 1) return false;
   for (auto& sc : scenes_)
     if (sc.lc < 1) return false;
   return true;
@@ -975,7 +977,7 @@ void Engine::enqueue_vcycle(cudaStream_t s, int tail, int count_iter) {
   const int LD = max_lc();
   for (int l = 0; l < LD; l++) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
-    launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, count_iter, tail == 4 && l == 0, s);
+    launch_mg_down(d_scenes_, nscenes(), d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, count_iter, tail == 4 && l == 0, s);
     count_iter = 0;
     vcycle_launches_++;
   }
@@ -1314,7 +1316,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
     go = [&](int) { launch_coarsest(d_scenes_, nscenes(), s); };
     b = 0; cnt = cyc;
   } else if (n == "mg_down0") {
-    go = [&](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, 0, 0, s); };
+    go = [&](int) { launch_mg_down(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, 0, 0, s); };
     b = (4 * 16 + 18) * cells; cnt = cyc;   // 4 colour passes + residual restriction
   } else if (n == "mg_up0") {
     go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 0, d_ctl_, s); };
@@ -1352,7 +1354,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   } else if (n.size() == 8 && (n.compare(0, 7, "mg_down") == 0) && n[7] >= '1' && n[7] <= '6') {
     const int l = n[7] - '0';
     if (l >= sc.lc) return fail(CFG_ERR_NOENT, "level " + n.substr(7) + " is in the coarse block");
-    go = [&, l](int) { launch_mg_down(d_scenes_, d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, 0, 0, s); };
+    go = [&, l](int) { launch_mg_down(d_scenes_, nscenes(), d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, d_ctl_, 0, 0, s); };
     b = (4 * 16 + 18) * (double)sc.lnx[l] * sc.lny[l]; cnt = cyc;
   } else if (n.size() == 6 && (n.compare(0, 5, "mg_up") == 0) && n[5] >= '1' && n[5] <= '6') {
     const int l = n[5] - '0';

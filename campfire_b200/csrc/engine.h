@@ -176,8 +176,8 @@ class Engine {
   void enqueue_factor(cudaStream_t s);
   void enqueue_factor_join(cudaStream_t s);
   bool krylov() const { return mode_ == CFG_SOLVE_FP64 && krylov_ != 0; }
-  // Krylov mode with the update folded into the level-0 smoother kernels: every scene's
-  // coarse block starts below level 0
+  // Krylov mode with the update folded into the level-0 smoother kernels: an engine of one
+  // scene whose coarse block starts below level 0
   bool pcg_fused() const;
   int cycle_tail() const { return any_fp64() ? (krylov() ? (pcg_fused() ? 4 : 3) : 2) : 1; }
   void enqueue_loop_end(cudaStream_t s);

@@ -80,7 +80,8 @@ __device__ __forceinline__ const void* tmap_of(const SceneDesc& S, int level, in
 }
 
 // Tile staging on two barriers around the wait on the previous kernel. stage_coef
-// (before the wait): one thread initialises both barriers and requests the coefficients
+// (before the wait in a one-scene engine, else once the scene's flag says it still cycles):
+// one thread initialises both barriers and requests the coefficients
 // ax, ay on bar[0]; they are built before the pressure loop and written by no loop kernel
 // (the loop is entered through a full dependency: a graph node or a memset). stage_state
 // (after the wait): p from map `pkind`, rhs and the coarse p under the tile on bar[1]; with
@@ -271,8 +272,8 @@ __device__ __forceinline__ void pcg_down_apply(const SceneDesc& S, const LevelDe
 // ------------------------------------------------------------------ down: 4 passes + restrict
 // PCG: the fused Krylov update on level 0 (above)
 template <int TX, int TY, bool PCG>
-__global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work, int level,
-                                                 SolveCtl* ctl, int count_iter) {
+__global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
+                                                 int level, SolveCtl* ctl, int count_iter) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
   __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
   __shared__ __align__(128) float srhs[MGF_BH * MGF_BW];
@@ -288,11 +289,19 @@ __global__ void __launch_bounds__(256) k_mg_down(const SceneDesc* __restrict__ s
   const Tile t{sp, srhs, sax, say, x0 - MGF_SX, y0 - MGF_H};
   const bool on = S.enabled;   // host-written, constant during the step
   SolveState* ss = S.solve;
-  if (on) stage_coef(S, level, t, bar);
+  // one scene: its flag only ends the loop, so the tile is requested before it is read;
+  // several: a scene that stopped loads nothing
+  const bool spec = nscenes == 1;
+  if (on && spec) stage_coef(S, level, t, bar);
   __syncthreads();
   pdl_wait();
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
   if (!on) return;
+  if (!spec) {
+    if (*(volatile int*)&ss->active == 0) return;
+    stage_coef(S, level, t, bar);
+    __syncthreads();
+  }
   PcgPrev pv{};
   PcgDown u;
   if (PCG) {
@@ -362,10 +371,16 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
   const int cx = x0 / 2 - 8, cy = y0 / 2 - 4;
   const bool on = S.enabled;   // host-written, constant during the step
   SolveState* ss = S.solve;
-  if (on) stage_coef(S, level, t, bar);
+  const bool spec = nscenes == 1;   // as in k_mg_down
+  if (on && spec) stage_coef(S, level, t, bar);
   __syncthreads();
   pdl_wait();
   if (!on) return;
+  if (!spec) {
+    if (*(volatile int*)&ss->active == 0) return;
+    stage_coef(S, level, t, bar);
+    __syncthreads();
+  }
   stage_state(S, level, TM_PB, t, true, scp, cx, cy, bar);
   const bool live = *(volatile int*)&ss->active != 0;
   // fused Krylov mode: the solve state and this thread's stored r, q, Lz, read beside the copies
@@ -482,6 +497,7 @@ __global__ void __launch_bounds__(256) k_mg_up(const SceneDesc* __restrict__ sce
 // residual scratch of level lc's size.
 namespace {
 constexpr int CB_THREADS = 512;
+constexpr int kStagedInverseMax = 128;   // coarsest unknowns whose inverse (<= 64 KB) is staged in shared memory
 constexpr int CB_WARPS = CB_THREADS / 32;
 constexpr int COARSEST_SCRATCH = 0;     // the coarsest keeps its stencils in registers
 using namespace mgc;
@@ -658,7 +674,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       for (int l = lc; l < nl; l++) bytes += (S.lev[l].ny * S.lev[l].pu + (S.lev[l].ny + 1) * S.lev[l].pc) * 4;
       const int n = S.lev[nl - 1].nx * S.lev[nl - 1].ny;
       s_dir = ctl->coarse_direct && S.solve->direct_ok;   // both fixed for the loop
-      const bool inv = s_dir && (n % 2) == 0 && s_A + n * n <= smem_floats;
+      const bool inv = s_dir && (n % 2) == 0 && n <= kStagedInverseMax && s_A + n * n <= smem_floats;
       if (inv) bytes += (uint32_t)(n * n * 4);
       mbar_arrive_expect_tx(&bar, bytes);
       for (int l = lc; l < nl; l++) {
@@ -1030,15 +1046,15 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
   f += (size_t)round_up((int)cells, 32);
   // room for the coarsest inverse of the direct solve when it fits
   const size_t n = (size_t)lnx[nlev - 1] * lny[nlev - 1];
-  if (n % 2 == 0 && (f + n * n) * 4 <= kCoarseSmemMax) f += n * n;
+  if (n % 2 == 0 && n <= (size_t)kStagedInverseMax && (f + n * n) * 4 <= kCoarseSmemMax) f += n * n;
   return f * 4;
 }
 
-void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, int count_iter,
-                    int pcg, cudaStream_t st) {
+void launch_mg_down(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, SolveCtl* ctl,
+                    int count_iter, int pcg, cudaStream_t st) {
   if (ntiles > 0)
     launch_pdl(pdl_enabled(), pcg ? k_mg_down<MGF_TX, MGF_TY, true> : k_mg_down<MGF_TX, MGF_TY, false>, dim3(ntiles),
-               dim3(256), 0, st, scenes, work, level, ctl, count_iter);
+               dim3(256), 0, st, scenes, nscenes, work, level, ctl, count_iter);
 }
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {

@@ -87,9 +87,10 @@ void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_co
 // 2 p64 += p, 3 the Krylov dot products, 4 the fused Krylov mode's), and one CTA per
 // scene for levels lc..coarsest
 // count_iter: the kernel opens a graph loop iteration (loop_count); pcg: level 0 of the
-// fused Krylov mode (applies the previous cycle's update)
-void launch_mg_down(const SceneDesc* scenes, const Work* work, int ntiles, int level, SolveCtl* ctl, int count_iter,
-                    int pcg, cudaStream_t st);
+// fused Krylov mode (applies the previous cycle's update); nscenes: the engine's scenes
+// (with one, tiles are requested before the scene's active flag is read: it only stops the loop)
+void launch_mg_down(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, SolveCtl* ctl,
+                    int count_iter, int pcg, cudaStream_t st);
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st);
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
