@@ -47,7 +47,7 @@ B_FIXED = 156 + 68 + 28 + 20 + 28 + 13.3 + 32
 
 
 # DRAM bytes (read + write) per launch of a kernel, from one ncu capture of the workload
-NCU_TRAFFIC = {("plain", "mg_coarse"): 122624, ("plain", "mg_up0"): 3352064, ("plain", "pcg_step"): 4347904}
+NCU_TRAFFIC = {("plain", "mg_coarse"): 123904, ("plain", "advect"): 2967808}
 
 
 def bytes_per_cell(diff_sub: int, cycles: float, fp64: bool) -> float:

@@ -760,17 +760,19 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     __syncthreads();
     const int q = lane & 7;
     const bool staged = s_inv != 0;
-    const float* A = staged ? smem + s_A : S.cinv + (size_t)S.solve->cinv_cur * n * n;
+    // the global copy is addressed only when the inverse is not staged
+    const float* Ag = staged ? nullptr : S.cinv + (size_t)S.solve->cinv_cur * n * n;
+    const float* As = smem + s_A;
     for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
       const int k = base + (lane >> 3);
       float sum = 0.f;
       if (k < n) {
         if (staged) {
           #pragma unroll 4
-          for (int m = q; m < n; m += 8) sum = __fmaf_rn(A[k * n + m], sres[m], sum);
+          for (int m = q; m < n; m += 8) sum = __fmaf_rn(As[k * n + m], sres[m], sum);
         } else {
           #pragma unroll 4
-          for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(A + (size_t)k * n + m), sres[m], sum);
+          for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(Ag + (size_t)k * n + m), sres[m], sum);
         }
       }
       sum += __shfl_xor_sync(0xffffffffu, sum, 1);
