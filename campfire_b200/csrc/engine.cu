@@ -637,11 +637,12 @@ int Engine::write_params(int s) {
   SceneDesc& d = sc.desc;
   d.P = sc.P; d.diff_sub = n; d.diff_dt = sc.diff_dt;
   d.cfl = (float)sc.cfl; d.dt_cap = (float)sc.dt_cap; d.nray = sc.nray; d.enabled = sc.enabled ? 1 : 0;
-  // only the leading scalar block changes here (the uniform and the step controls)
+  // only the leading scalar block changes here (the uniform and the step controls). The
+  // sources are pageable host memory, which a copy has staged by the time it returns, so
+  // the copies stay in stream order without a wait here.
   CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &d, kDescParamBytes, cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaMemcpyAsync(d_dxd_ + s, &sc.dxd, 8, cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaMemcpyAsync(d_alpha_ + s, &sc.alpha, 8, cudaMemcpyHostToDevice, st()));
-  CFG_CUDA(cudaStreamSynchronize(st()));
   if (graph_sub_ >= 0 && max_sub() > graph_sub_) graph_dirty_ = true;
   return CFG_OK;
 }
@@ -659,8 +660,8 @@ int Engine::upload_pieces(int s, const float* data, int n) {
   sc.host.nPieces = n;
   std::memset(sc.pieces, 0, sizeof sc.pieces);
   if (data) std::memcpy(sc.pieces, data, sizeof sc.pieces);
+  // pageable source: staged by the time the copy returns (no wait needed)
   CFG_CUDA(cudaMemcpyAsync(sc.desc.pieces, sc.pieces, sizeof sc.pieces, cudaMemcpyHostToDevice, st()));
-  CFG_CUDA(cudaStreamSynchronize(st()));
   return CFG_OK;
 }
 
