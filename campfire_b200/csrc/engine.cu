@@ -1066,12 +1066,16 @@ void Engine::enqueue_factor_join(cudaStream_t s) {
   launches_++;
 }
 
+// The step's tail: the projection, which also swaps the pipelined coarsest inverse
+// (after the factorisation's branch has joined) and sets the next CFL dt
 void Engine::enqueue_post_solve(cudaStream_t s) {
-  enqueue_factor_join(s);
-  launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], any_fp64(), s); launches_++;
+  const bool pipe = pipelined_coarse();
+  if (pipe) cudaStreamWaitEvent(s, ev_join_, 0);
   bool cfl = false;
   for (auto& sc : scenes_) cfl = cfl || sc.cfl > 0;
-  if (cfl) { launch_cfl_update(d_scenes_, nscenes(), d_dxd_, d_alpha_, s); launches_++; }
+  launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], any_fp64(), s, nscenes(), (pipe ? 1 : 0) | (cfl ? 2 : 0),
+                 d_dxd_, d_alpha_);
+  launches_++;
 }
 
 void Engine::enqueue_bnorm(cudaStream_t s) {

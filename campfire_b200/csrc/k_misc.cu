@@ -9,11 +9,39 @@ namespace cfg {
 
 // u -= dt (1/rho_f) grad p; ghost -p at the open sides/top, closed faces 0.
 // FP64: the FP64 pressure of the defect-correction loop, rounded once to f32.
+// CFL step for the next step: dt = min(dt_cap, cfl*dx/max|u|) and the diffusion
+// sub-step count of js/fluid.js:190-198 for that dt (one thread, after max|u| is complete)
+__device__ __forceinline__ void cfl_next_dt(SceneDesc& S, double h, double alpha) {
+  const float m = __uint_as_float(S.solve->maxu);
+  const float cand = m > 0.f ? S.cfl * S.P.dx / m : S.dt_cap;
+  const float dt = fminf(S.dt_cap, cand);
+  S.P.dt = dt;
+  int n = (int)ceil((double)dt / (h * h / (4.5 * alpha)));
+  n = min(5, n % 2 ? n : n + 1);
+  S.diff_sub = n;
+  S.diff_dt = (float)((double)dt / n);
+  S.solve->maxu = 0u;
+}
+
+// post (the step's tail folded into the projection): bit 0 swaps every scene's coarsest
+// inverse halves (after the factorisation's branch has joined), bit 1 sets each CFL scene's
+// next dt in the scene's last CTA (arrival on the scene's counter after its max|u|).
 template <bool FP64>
-__global__ void __launch_bounds__(256) k_project(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work) {
+__global__ void __launch_bounds__(256) k_project(SceneDesc* __restrict__ scenes, const Work* __restrict__ work, int nscenes,
+                                                 int post, const double* dxd, const double* alpha) {
   __shared__ float redm[32];
+  __shared__ int s_last;
   const Work w = work[blockIdx.x];
-  const SceneDesc& S = scenes[w.scene];
+  if ((post & 1) && blockIdx.x == 0)
+    for (int s = threadIdx.x; s < nscenes; s += blockDim.x) {
+      const SceneDesc& Q = scenes[s];
+      if (!Q.enabled) continue;
+      SolveState* ss = Q.solve;
+      ss->cinv_cur ^= 1;
+      ss->direct_ok = ss->direct_ok_next;
+      ss->direct_ok_next = 0;
+    }
+  SceneDesc& S = scenes[w.scene];
   if (!S.enabled) return;
   const cfg_params& P = S.P;
   const int nx = S.nx, ny = S.ny, pc = S.pc, pu = S.pu;
@@ -72,25 +100,23 @@ __global__ void __launch_bounds__(256) k_project(const SceneDesc* __restrict__ s
   }
   const float bm = block_max(m, redm);
   if (threadIdx.x == 0 && S.cfl > 0.f) atomicMax(&S.solve->maxu, __float_as_uint(bm));
+  if (!(post & 2) || !(S.cfl > 0.f)) return;
+  // every CTA of the scene has read P.dt and added its max|u| before it arrives
+  if (threadIdx.x == 0) s_last = arrive_acq_rel(&S.solve->counter) == (unsigned)S.nt_mg0 - 1u;
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    S.solve->counter = 0u;
+    cfl_next_dt(S, dxd[w.scene], alpha[w.scene]);
+  }
 }
 
-// CFL step for the next step: dt = min(dt_cap, cfl*dx/max|u|) and the diffusion
-// sub-step count of js/fluid.js:190-198 for that dt (one thread per scene)
+// the CFL update on its own (one thread per scene)
 __global__ void k_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, const double* alpha) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nscenes) return;
   SceneDesc& S = scenes[s];
   if (!S.enabled || !(S.cfl > 0.f)) return;
-  const float m = __uint_as_float(S.solve->maxu);
-  const float cand = m > 0.f ? S.cfl * S.P.dx / m : S.dt_cap;
-  const float dt = fminf(S.dt_cap, cand);
-  S.P.dt = dt;
-  const double h = dxd[s];
-  int n = (int)ceil((double)dt / (h * h / (4.5 * alpha[s])));
-  n = min(5, n % 2 ? n : n + 1);
-  S.diff_sub = n;
-  S.diff_dt = (float)((double)dt / n);
-  S.solve->maxu = 0u;
+  cfl_next_dt(S, dxd[s], alpha[s]);
 }
 
 // geometry.wgsl:121-153: per cell the nearest piece (sdf, piece*4+face) and the
@@ -308,10 +334,11 @@ __global__ void __launch_bounds__(1024) k_budgets(const SceneDesc* __restrict__ 
   if (threadIdx.x == 0) out[7] = (double)tm;
 }
 
-void launch_project(const SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st) {
+void launch_project(SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st, int nscenes, int post,
+                    const double* dxd, const double* alpha) {
   if (ntiles <= 0) return;
-  if (fp64) k_project<true><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work);
-  else k_project<false><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work);
+  if (fp64) k_project<true><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work, nscenes, post, dxd, alpha);
+  else k_project<false><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work, nscenes, post, dxd, alpha);
 }
 void launch_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, const double* alpha, cudaStream_t st) {
   if (nscenes > 0) k_cfl_update<<<(nscenes + 127) / 128, 128, 0, st>>>(scenes, nscenes, dxd, alpha);

@@ -28,6 +28,7 @@ constexpr int TMAP_BYTES = 128;
 constexpr int COARSE_CELLS = 6144;                   // default: largest level handled by the one-CTA coarse block
 constexpr size_t kCoarseSmemMax = 232448 - 2048;     // dynamic shared memory of the coarse block (227 KB less static)
 constexpr int PR_TX = 32, PR_TY = 8;                 // projection
+static_assert(PR_TX == MG_TX && PR_TY == MG_TY, "the projection's tiles are counted as the level-0 multigrid tiles");
 constexpr int GEO_TX = 32, GEO_TY = 8;               // geometry
 
 // Launch with programmatic stream serialization (the kernel must call pdl_wait()
@@ -117,7 +118,10 @@ void launch_bnorm(const SceneDesc* scenes, const Work* work, int ntiles, SolveCt
 // FP64: p64 += p0
 void launch_accum64(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
 // projection (+ max|u| and the CFL step for the next step)
-void launch_project(const SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st);
+// post: bit 0 swaps the scenes' coarsest inverse halves, bit 1 sets the CFL scenes' next dt
+// (what k_cinv_swap and k_cfl_update do on their own), both after the projection's work
+void launch_project(SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st, int nscenes = 0,
+                    int post = 0, const double* dxd = nullptr, const double* alpha = nullptr);
 void launch_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, const double* alpha, cudaStream_t st);
 void launch_geometry(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
 void launch_radiation(const SceneDesc* scenes, int scene, int ntargets, int nray, cudaStream_t st);
