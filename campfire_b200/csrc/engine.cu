@@ -914,8 +914,8 @@ void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_con
   launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s); launches_++;
   launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, s); launches_++;
   launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); launches_++;
-  for (int l = FR_KMAX; l + 1 < max_levels(); l++)
-    if (nwl_[WL_MGC0 + l] > 0) { launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s); launches_++; }
+  // the levels below the forces kernel's in-tile restriction, one block per scene
+  if (FR_KMAX + 1 < max_levels()) { launch_coef_restrict_tail(d_scenes_, nscenes(), FR_KMAX, s); launches_++; }
   enqueue_factor(s);
   if (fp64) { launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s); launches_++; }
   // the loop's cycle counter starts at zero in every step

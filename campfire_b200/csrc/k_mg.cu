@@ -153,6 +153,26 @@ __global__ void __launch_bounds__(256) k_coef_restrict(const SceneDesc* __restri
   if (J == nyc - 1 && I < nxc) ay(I, nyc);
 }
 
+// pressure.wgsl:57-67 for every level from `level` down, one CTA per scene (the levels
+// below the forces kernel's in-tile restriction are small): level by level, a block
+// barrier between them (each level reads the one just written by the same block)
+__global__ void __launch_bounds__(512) k_coef_restrict_tail(const SceneDesc* __restrict__ scenes, int level) {
+  const SceneDesc& S = scenes[blockIdx.x];
+  if (!S.enabled) return;
+  for (int l = level; l + 1 < S.nlev; l++) {
+    const LevelDesc F = S.lev[l], C = S.lev[l + 1];
+    const int nxc = C.nx, nyc = C.ny;
+    for (int e = threadIdx.x; e < nxc * nyc; e += blockDim.x) {
+      const int J = e / nxc, I = e - J * nxc;
+      C.ax[J * C.pu + I] = 0.5f * (F.ax[(2 * J) * F.pu + 2 * I] + F.ax[(2 * J + 1) * F.pu + 2 * I]);
+      C.ay[J * C.pc + I] = 0.5f * (F.ay[(2 * J) * F.pc + 2 * I] + F.ay[(2 * J) * F.pc + 2 * I + 1]);
+      if (I == nxc - 1) C.ax[J * C.pu + nxc] = 0.5f * (F.ax[(2 * J) * F.pu + 2 * nxc] + F.ax[(2 * J + 1) * F.pu + 2 * nxc]);
+      if (J == nyc - 1) C.ay[nyc * C.pc + I] = 0.5f * (F.ay[(2 * nyc) * F.pc + 2 * I] + F.ay[(2 * nyc) * F.pc + 2 * I + 1]);
+    }
+    __syncthreads();
+  }
+}
+
 // ||r||^2 of level 0 after a V-cycle -> per-scene decision -> loop condition
 __global__ void __launch_bounds__(256) k_resnorm(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                  SolveCtl* ctl) {
@@ -330,6 +350,9 @@ __global__ void __launch_bounds__(256) k_bnorm(const SceneDesc* __restrict__ sce
   }
 }
 
+void launch_coef_restrict_tail(const SceneDesc* scenes, int nscenes, int level, cudaStream_t st) {
+  if (nscenes > 0) k_coef_restrict_tail<<<nscenes, 512, 0, st>>>(scenes, level);
+}
 void launch_bnorm(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool fp64, cudaStream_t st) {
   if (ntiles > 0) k_bnorm<<<ntiles, MG_TX * MG_TY, 0, st>>>(scenes, work, ctl, fp64 ? 1 : 0);
 }

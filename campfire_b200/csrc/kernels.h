@@ -120,6 +120,8 @@ void launch_accum64(const SceneDesc* scenes, const Work* work, int ntiles, cudaS
 // projection (+ max|u| and the CFL step for the next step)
 // post: bit 0 swaps the scenes' coarsest inverse halves, bit 1 sets the CFL scenes' next dt
 // (what k_cinv_swap and k_cfl_update do on their own), both after the projection's work
+// the coefficient restriction of every level from `level` down, one CTA per scene
+void launch_coef_restrict_tail(const SceneDesc* scenes, int nscenes, int level, cudaStream_t st);
 void launch_project(SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st, int nscenes = 0,
                     int post = 0, const double* dxd = nullptr, const double* alpha = nullptr);
 void launch_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, const double* alpha, cudaStream_t st);
