@@ -104,9 +104,11 @@ int cfg_set_param(cfg_sim* sim, const char* name, double value);
 int cfg_get_param(cfg_sim* sim, const char* name, double* value);
 /* sim.dt = dt (public field; applied by the next cfg_write_params) */
 int cfg_set_dt(cfg_sim* sim, double dt);
-/* writeParams(): upload the 40-field uniform, recompute the diffusion sub-steps  (js/fluid.js:180-199) */
+/* writeParams(): upload the 40-field uniform, recompute the diffusion sub-steps  (js/fluid.js:180-199);
+   ordered on the stream (with a CFL step it first reads the device's dt back) */
 int cfg_write_params(cfg_sim* sim);
-/* uploadPieces(Float32Array(64*20), n)  (js/fluid.js:201-204; packing js/main.js:190-199) */
+/* uploadPieces(Float32Array(64*20), n)  (js/fluid.js:201-204; packing js/main.js:190-199);
+   ordered on the stream, `data` may be reused as soon as the call returns */
 int cfg_upload_pieces(cfg_sim* sim, const float* data, int n);
 /* clearGeometry(enc)  (js/fluid.js:213): zero the per-face band weights */
 int cfg_clear_geometry(cfg_sim* sim);
