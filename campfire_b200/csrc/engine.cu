@@ -96,6 +96,9 @@ Engine::~Engine() {
   if (d_rwood_) cudaFree(d_rwood_);
   if (d_image_) cudaFree(d_image_);
   if (h_ctl_pinned_) cudaFreeHost(h_ctl_pinned_);
+  if (h_dt_pinned_) cudaFreeHost(h_dt_pinned_);
+  if (d_dtv_) cudaFree(d_dtv_);
+  if (ev_dt_) cudaEventDestroy(ev_dt_);
   if (stream_) cudaStreamDestroy(stream_);
   if (body_stream_) cudaStreamDestroy(body_stream_);
   if (side_stream_) { cudaStreamSynchronize(side_stream_); cudaStreamDestroy(side_stream_); }
@@ -163,11 +166,14 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   CFG_CUDA(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
   CFG_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+  CFG_CUDA(cudaEventCreateWithFlags(&ev_dt_, cudaEventDisableTiming));
   CFG_CUDA(cudaMalloc(&d_scenes_, sizeof(SceneDesc) * n));
   CFG_CUDA(cudaMalloc(&d_solve_, sizeof(SolveState) * n));
   CFG_CUDA(cudaMemset(d_solve_, 0, sizeof(SolveState) * n));
   CFG_CUDA(cudaMalloc(&d_ctl_, sizeof(SolveCtl)));
   CFG_CUDA(cudaMallocHost(&h_ctl_pinned_, sizeof(SolveCtl)));
+  CFG_CUDA(cudaMallocHost(&h_dt_pinned_, sizeof(float) * n));
+  CFG_CUDA(cudaMalloc(&d_dtv_, sizeof(float) * n));
   CFG_CUDA(cudaMalloc(&d_dxd_, sizeof(double) * n));
   CFG_CUDA(cudaMalloc(&d_alpha_, sizeof(double) * n));
   CFG_CUDA(cudaMalloc(&d_scratch_, sizeof(double) * 64));
@@ -429,6 +435,7 @@ int Engine::checkpoint_load(int s, const char* path) {
   sc.P = sc.desc.P;
   sc.diff_sub = sc.desc.diff_sub;
   sc.diff_dt = sc.desc.diff_dt;
+  dt_from_step_ = false;
   CFG_CUDA(cudaMemcpy(d_scenes_ + s, &sc.desc, kDescParamBytes, cudaMemcpyHostToDevice));
   CFG_CUDA(cudaMemcpy(sc.desc.solve, &ss, sizeof ss, cudaMemcpyHostToDevice));
   graph_dirty_ = true;
@@ -518,6 +525,7 @@ int Engine::set_coarse_cells(int cells) {
 }
 
 int Engine::upload_desc(int s) {
+  dt_from_step_ = false;
   CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &scenes_[s].desc, sizeof(SceneDesc), cudaMemcpyHostToDevice, st()));
   return CFG_OK;
 }
@@ -617,11 +625,17 @@ int Engine::write_params(int s) {
   CFG_TRY(activate());
   Scene& sc = scenes_[s];
   if (sc.cfl > 0 && sc.desc.solve) {
-    // keep the device's CFL step: read it back before the upload overwrites it
+    // keep the device's CFL step: take the copy the last step made, or read it back, before
+    // the upload overwrites it
     float dt = 0.f;
-    CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
-                             cudaMemcpyDeviceToHost, st()));
-    CFG_CUDA(cudaStreamSynchronize(st()));
+    if (dt_from_step_) {
+      CFG_CUDA(cudaEventSynchronize(ev_dt_));
+      dt = h_dt_pinned_[s];
+    } else {
+      CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
+                               cudaMemcpyDeviceToHost, st()));
+      CFG_CUDA(cudaStreamSynchronize(st()));
+    }
     if (dt > 0.f) sc.dtd = (double)dt;
   }
   sc.host.nx = sc.nx; sc.host.ny = sc.ny; sc.host.dx = (float)sc.dxd; sc.host.dt = (float)sc.dtd;
@@ -702,6 +716,7 @@ int Engine::set_cfl(int s, double cfl, double dt_cap) {
   if (cfl < 0 || !(dt_cap > 0)) return fail(CFG_ERR_INVAL, "cfl must be >= 0 and dt_cap > 0");
   scenes_[s].cfl = cfl; scenes_[s].dt_cap = dt_cap;
   graph_dirty_ = true;
+  dt_from_step_ = false;
   return CFG_OK;
 }
 int Engine::set_nray(int s, int nray) {
@@ -955,6 +970,11 @@ int Engine::max_lc() const {
   return m;
 }
 
+bool Engine::any_cfl() const {
+  for (auto& sc : scenes_) if (sc.cfl > 0) return true;
+  return false;
+}
+
 bool Engine::pcg_fused() const {
   // one scene: the folded update shortens the cycle's kernel chain; a batch is bound by
   // bandwidth instead, and the separate update kernel moves fewer bytes than the fold
@@ -1071,11 +1091,14 @@ void Engine::enqueue_factor_join(cudaStream_t s) {
 void Engine::enqueue_post_solve(cudaStream_t s) {
   const bool pipe = pipelined_coarse();
   if (pipe) cudaStreamWaitEvent(s, ev_join_, 0);
-  bool cfl = false;
-  for (auto& sc : scenes_) cfl = cfl || sc.cfl > 0;
+  const bool cfl = any_cfl();
   launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], any_fp64(), s, nscenes(), (pipe ? 1 : 0) | (cfl ? 2 : 0),
-                 d_dxd_, d_alpha_);
+                 d_dxd_, d_alpha_, d_dtv_);
   launches_++;
+  if (cfl) {   // the next dt to the host side, for cfg_write_params
+    cudaMemcpyAsync(h_dt_pinned_, d_dtv_, sizeof(float) * nscenes(), cudaMemcpyDeviceToHost, s);
+    cudaEventRecordWithFlags(ev_dt_, s, cudaEventRecordExternal);   // a node of the step graph when captured
+  }
 }
 
 void Engine::enqueue_bnorm(cudaStream_t s) {
@@ -1184,6 +1207,7 @@ int Engine::step(int nsteps) {
       }
       CFG_TRY(set_cond_mode(true));
       CFG_CUDA(cudaGraphLaunch(exec_, st()));
+      dt_from_step_ = dt_from_step_ || any_cfl();
     } else {
       CFG_TRY(set_cond_mode(false));
       launches_ = 0; vcycle_launches_ = 0;
@@ -1192,6 +1216,7 @@ int Engine::step(int nsteps) {
       CFG_TRY(host_pressure_loop());
       enqueue_post_solve(st());
       CFG_CUDA(cudaGetLastError());
+      dt_from_step_ = dt_from_step_ || any_cfl();
     }
     for (auto& sc : scenes_) if (sc.enabled) sc.time += sc.dtd;
   }
@@ -1248,6 +1273,7 @@ int Engine::step_profiled(float* ms) {
   CFG_TRY(host_pressure_loop());
   CFG_CUDA(cudaEventRecord(ev[6], s));
   enqueue_post_solve(s);
+  dt_from_step_ = dt_from_step_ || any_cfl();
   CFG_CUDA(cudaEventRecord(ev[7], s));
   CFG_CUDA(cudaEventSynchronize(ev[7]));
   for (int k = 0; k < 7; k++) CFG_CUDA(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
@@ -1259,6 +1285,7 @@ int Engine::step_profiled(float* ms) {
 int Engine::run_stage(const char* stage) {
   if (!stage) return fail(CFG_ERR_INVAL, "null stage");
   CFG_TRY(activate());
+  dt_from_step_ = false;   // a stage may change the device's dt (update_dt) without the step's copy
   const std::string st_(stage);
   cudaStream_t s = st();
   const bool fp64 = any_fp64();

@@ -179,6 +179,7 @@ class Engine {
   // Krylov mode with the update folded into the level-0 smoother kernels: an engine of one
   // scene whose coarse block starts below level 0
   bool pcg_fused() const;
+  bool any_cfl() const;
   int cycle_tail() const { return any_fp64() ? (krylov() ? (pcg_fused() ? 4 : 3) : 2) : 1; }
   void enqueue_loop_end(cudaStream_t s);
   void enqueue_fp64_tail(cudaStream_t s);
@@ -196,6 +197,12 @@ class Engine {
   SolveState* d_solve_ = nullptr;
   SolveCtl* d_ctl_ = nullptr;
   SolveCtl* h_ctl_pinned_ = nullptr;
+  // CFL steps: the step ends by copying each scene's next dt (d_dtv_) into pinned memory and
+  // recording ev_dt_, so cfg_write_params reads it once that event has passed instead of
+  // reading the descriptor back (dt_from_step_: no descriptor upload since that step)
+  float *h_dt_pinned_ = nullptr, *d_dtv_ = nullptr;
+  cudaEvent_t ev_dt_ = nullptr;
+  bool dt_from_step_ = false;
   double* d_dxd_ = nullptr;
   double* d_alpha_ = nullptr;
   double* d_scratch_ = nullptr;   // small FP64 outputs (budgets, norms)

@@ -28,7 +28,7 @@ __device__ __forceinline__ void cfl_next_dt(SceneDesc& S, double h, double alpha
 // next dt in the scene's last CTA (arrival on the scene's counter after its max|u|).
 template <bool FP64>
 __global__ void __launch_bounds__(256) k_project(SceneDesc* __restrict__ scenes, const Work* __restrict__ work, int nscenes,
-                                                 int post, const double* dxd, const double* alpha) {
+                                                 int post, const double* dxd, const double* alpha, float* dtv) {
   __shared__ float redm[32];
   __shared__ int s_last;
   const Work w = work[blockIdx.x];
@@ -107,6 +107,7 @@ __global__ void __launch_bounds__(256) k_project(SceneDesc* __restrict__ scenes,
   if (s_last && threadIdx.x == 0) {
     S.solve->counter = 0u;
     cfl_next_dt(S, dxd[w.scene], alpha[w.scene]);
+    if (dtv) dtv[w.scene] = S.P.dt;
   }
 }
 
@@ -335,10 +336,10 @@ __global__ void __launch_bounds__(1024) k_budgets(const SceneDesc* __restrict__ 
 }
 
 void launch_project(SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st, int nscenes, int post,
-                    const double* dxd, const double* alpha) {
+                    const double* dxd, const double* alpha, float* dtv) {
   if (ntiles <= 0) return;
-  if (fp64) k_project<true><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work, nscenes, post, dxd, alpha);
-  else k_project<false><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work, nscenes, post, dxd, alpha);
+  if (fp64) k_project<true><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work, nscenes, post, dxd, alpha, dtv);
+  else k_project<false><<<ntiles, PR_TX * PR_TY, 0, st>>>(scenes, work, nscenes, post, dxd, alpha, dtv);
 }
 void launch_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, const double* alpha, cudaStream_t st) {
   if (nscenes > 0) k_cfl_update<<<(nscenes + 127) / 128, 128, 0, st>>>(scenes, nscenes, dxd, alpha);

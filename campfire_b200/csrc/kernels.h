@@ -122,8 +122,9 @@ void launch_accum64(const SceneDesc* scenes, const Work* work, int ntiles, cudaS
 // (what k_cinv_swap and k_cfl_update do on their own), both after the projection's work
 // the coefficient restriction of every level from `level` down, one CTA per scene
 void launch_coef_restrict_tail(const SceneDesc* scenes, int nscenes, int level, cudaStream_t st);
+// (bit 1 also stores each CFL scene's next dt in dtv[scene] when dtv is given)
 void launch_project(SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st, int nscenes = 0,
-                    int post = 0, const double* dxd = nullptr, const double* alpha = nullptr);
+                    int post = 0, const double* dxd = nullptr, const double* alpha = nullptr, float* dtv = nullptr);
 void launch_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, const double* alpha, cudaStream_t st);
 void launch_geometry(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
 void launch_radiation(const SceneDesc* scenes, int scene, int ntargets, int nray, cudaStream_t st);
