@@ -1097,7 +1097,12 @@ void Engine::enqueue_post_solve(cudaStream_t s) {
   launches_++;
   if (cfl) {   // the next dt to the host side, for cfg_write_params
     cudaMemcpyAsync(h_dt_pinned_, d_dtv_, sizeof(float) * nscenes(), cudaMemcpyDeviceToHost, s);
-    cudaEventRecordWithFlags(ev_dt_, s, cudaEventRecordExternal);   // a node of the step graph when captured
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cap);
+    if (cap == cudaStreamCaptureStatusActive)
+      cudaEventRecordWithFlags(ev_dt_, s, cudaEventRecordExternal);   // a node of the step graph
+    else
+      cudaEventRecord(ev_dt_, s);
   }
 }
 
