@@ -174,6 +174,7 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   CFG_CUDA(cudaMallocHost(&h_ctl_pinned_, sizeof(SolveCtl)));
   CFG_CUDA(cudaMallocHost(&h_dt_pinned_, sizeof(float) * n));
   CFG_CUDA(cudaMalloc(&d_dtv_, sizeof(float) * n));
+  CFG_CUDA(cudaMemset(d_dtv_, 0, sizeof(float) * n));   // 0: no step has set a scene's dt yet
   CFG_CUDA(cudaMalloc(&d_dxd_, sizeof(double) * n));
   CFG_CUDA(cudaMalloc(&d_alpha_, sizeof(double) * n));
   CFG_CUDA(cudaMalloc(&d_scratch_, sizeof(double) * 64));
@@ -628,9 +629,9 @@ int Engine::write_params(int s) {
     // keep the device's CFL step: take the copy the last step made, or read it back, before
     // the upload overwrites it
     float dt = 0.f;
-    if (dt_from_step_) {
+    if (dt_from_step_ && sc.enabled) {
       CFG_CUDA(cudaEventSynchronize(ev_dt_));
-      dt = h_dt_pinned_[s];
+      dt = h_dt_pinned_[s];   // 0 (kept below) until a step of this scene has set it
     } else {
       CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
                                cudaMemcpyDeviceToHost, st()));
