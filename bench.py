@@ -121,18 +121,40 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
-def run_cpu(workload: str, steps: int, warmup: int, threads: int):
-    """The CPU restatement of the reference step (oracle, f32), same scene and solver."""
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    import campfire_b200 as cb
-    from campfire_b200.fluid import load_scene
-    from oracle import oracle
+def workload_config(workload: str, world: int) -> dict:
+    """The workload as both arms run it (scene, grid, solver, time step, L2 policy): the same dict in the
+    line of this implementation and of the reference arm."""
     nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
-    sc = cb.generate_scene(kind, nx, ny, 0.8, seed)
+    scene = {0: "3 logs", 1: "5-log tepee"}[kind]
+    return {"workload": f"{workload} gas step {nx}x{ny}, {scene}, FP32 V(2,2) in FP64 defect correction "
+                        f"to rel residual {tol:g}", "nx": nx, "ny": ny, "scene_kind": kind, "scene_seed": seed,
+            "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": maxc,
+                         "outer": "flexible preconditioned CG in FP64, FP32 V(2,2) as preconditioner",
+                         "coarsest": "direct: inverse factored beside the pressure loop, applied from the next "
+                                     "step (pipelined)"},
+            "dt": {"cfl": PLAIN_CFL, "cap_s": PLAIN_DT_CAP},
+            "l2": "flushed before every timed step (256 MB write)", "parallelism": f"replicas{world}"}
+
+
+def configure_solver(sim, workload: str) -> None:
+    """The workload's solver on a FluidSim or an OracleSim (same calls on both)."""
+    nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
+    sim.set_solver(mode, 1, tol, maxc)
+    sim.set_coarse_solve("pipelined")
+    sim.set_krylov(True)
+    sim.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)   # dt set by CFL 0.5 each step, capped at 2 ms
+
+
+def run_cpu(workload: str, steps: int, warmup: int, threads: int):
+    """The CPU restatement of the reference step (oracle, f32) on the same scene with the same solver.
+    Inputs come from the oracle's own scene restatement: the product library is not loaded."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle, scene_ref
+    nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
+    sc = scene_ref.generate_scene(kind, nx, ny, 0.8, seed)
     o = oracle.OracleSim(nx, ny, 0.8, sc["dt"])
-    load_scene(o, sc)
-    o.set_solver(mode, 1, tol, maxc)
-    o.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)
+    scene_ref.load_scene(o, sc)
+    configure_solver(o, workload)
     o.step(warmup)
     cyc = 0.0
     t0 = time.perf_counter()
@@ -183,11 +205,17 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     torch.cuda.synchronize(dev)
     b.synchronize()
     ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
-    cyc = [v.info()["last_cycles"] for v in b.scenes]
-    rel = max(v.info()["last_rel"] for v in b.scenes)
+    infos = [v.info() for v in b.scenes]
+    cyc = [i["last_cycles"] for i in infos]
+    rel = max(i["last_rel"] for i in infos)
     launches = b.launch_count()
     b.close()
     batched = cells * steps / (ms / 1e3)
+    # algorithmic bytes of the last step: each scene's cells x its own bytes per cell-update (its cycles)
+    step_bytes = sum(sc_["nx"] * sc_["ny"] * bytes_per_cell(i["diffSub"], i["last_cycles"], True)
+                     for sc_, i in zip(scenes, infos))
+    hbm, peak_kind = peaks()
+    achieved = step_bytes / (ms / steps / 1e3) / 1e9
 
     # the same scenes, one by one, through the plain single-scene step (same solver, same tolerance)
     plain_ms, plain_cells = 0.0, 0
@@ -222,123 +250,192 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
             "sizes": {f"{nx}x{ny}": sum(1 for s in scenes if (s["nx"], s["ny"]) == (nx, ny))
                       for nx, ny in BATCH_CLASSES},
             "plain_one_by_one": {"value": plain, "unit": METRIC, "steps_per_scene": plain_steps},
-            "batched_over_plain": batched / plain}
+            "batched_over_plain": batched / plain,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
+                         "step_bytes": step_bytes, "bytes_per_cell": step_bytes / cells,
+                         "basis": "algorithmic bytes of the last step (each scene's cycles) / mean ms per step"}}
 
 
-def field_errors(g, ref):
-    """max|gpu - ref| / max|ref| of T, u (U and V faces), Y_F and Y_S."""
+ERR_FIELDS = ("T", "u", "Y_F", "Y_S")
+
+
+def _err_arrays(read):
+    """T, u (U and V faces), Y_F and Y_S of a sim, as float64 arrays (`read`: readBuffer or OracleSim.read)."""
     import numpy as np
+    y = np.asarray(read("Y"), np.float64).reshape(-1, 4)
+    return {"T": np.asarray(read("T"), np.float64),
+            "u": np.concatenate([np.asarray(read("U"), np.float64), np.asarray(read("V"), np.float64)]),
+            "Y_F": y[:, 0], "Y_S": y[:, 3]}
+
+
+def field_errors(read_a, read_ref, detail: bool = False):
+    """Per field |a - ref| / max|ref|: its maximum, and with `detail` its 99.9th percentile and the fraction of
+    values above 1e-4 (a single cell whose limiter or chemistry branch flips under a rounding difference sets
+    the maximum; the percentile shows the rest of the field)."""
+    import numpy as np
+    a, b = _err_arrays(read_a), _err_arrays(read_ref)
     out = {}
-    for name, get in (("T", lambda s, r: (s("T"),)), ("u", lambda s, r: (s("U"), s("V"))),
-                      ("Y_F", lambda s, r: (s("Y").reshape(-1, 4)[:, 0],)),
-                      ("Y_S", lambda s, r: (s("Y").reshape(-1, 4)[:, 3],))):
-        a = np.concatenate([np.asarray(x, np.float64).ravel() for x in get(g.readBuffer, None)])
-        b = np.concatenate([np.asarray(x, np.float64).ravel() for x in get(ref.read, None)])
-        scale = float(np.max(np.abs(b))) or 1.0
-        out[name] = float(np.max(np.abs(a - b))) / scale
+    for f in ERR_FIELDS:
+        d = np.abs(a[f] - b[f]) / (float(np.max(np.abs(b[f]))) or 1.0)
+        out[f] = {"max": float(d.max()), "p99_9": float(np.quantile(d, 0.999)),
+                  "frac_above_1e-4": float(np.mean(d > 1e-4))} if detail else float(d.max())
     return out
 
 
 def run_fp64_error(dev, workload: str, steps: int, every: int, threads: int):
-    """The GPU step (FP32, FP64 defect correction) and the FP64 oracle (the same algorithm in
-    double precision) from the same scene, side by side; errors every `every` steps."""
+    """Accuracy of the GPU step (FP32 arithmetic, FP64 pressure to the workload's tolerance) against the FP64
+    oracle (the same algorithm in double precision), reported at step 1 and every `every` steps:
+      one_step    the step after the report, from the GPU's state: that state is copied into an FP64 oracle
+                  and into the CPU FP32 restatement, and all three take the step; errors against the FP64 one
+      trajectory  the GPU run and an FP64 oracle run from the same initial scene, and the FP32 restatement's
+                  own run against the FP64 one (the flame amplifies rounding: FP32 drift, not a defect)"""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     import campfire_b200 as cb
     from campfire_b200.fluid import load_scene
-    from oracle import oracle
+    from oracle import oracle, scene_ref
     nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
     sc = cb.generate_scene(kind, nx, ny, 0.8, seed)
     g = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
     load_scene(g, sc)
-    g.set_solver(mode, 1, tol, maxc)
-    g.set_coarse_solve("pipelined")
-    g.set_krylov(True)
-    g.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)
-    o = oracle.OracleSim(nx, ny, 0.8, sc["dt"], fp64=True)
-    load_scene(o, sc)
-    o.set_solver(mode, 1, tol, maxc)
-    o.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)
-    rows = []
-    for k in range(1, steps + 1):
+    configure_solver(g, workload)
+
+    def osim(fp64):
+        o = oracle.OracleSim(nx, ny, 0.8, sc["dt"], fp64=fp64)
+        scene_ref.load_scene(o, sc)
+        configure_solver(o, workload)
+        return o
+
+    traj64, traj32 = osim(True), osim(False)
+    t0 = time.perf_counter()
+    reports, probe, k = [], None, 0
+    while k < steps or probe is not None:   # the last report's probed step may run past `steps`
+        if probe is not None:    # the probed step: the GPU state copied into fresh oracles first
+            one64, one32 = osim(True), osim(False)
+            one64.copy_state_from(g, PLAIN_CFL, PLAIN_DT_CAP)
+            one32.copy_state_from(g, PLAIN_CFL, PLAIN_DT_CAP)
         g.step(1)
-        o.step(1)
-        if k % every == 0 or k == 1:
-            rows.append(dict(step=k, **field_errors(g, o)))
+        traj64.step(1)
+        traj32.step(1)
+        k += 1
+        if probe is not None:
+            one64.step(1)
+            one32.step(1)
+            probe["one_step"] = {"step": k, "gpu": field_errors(g.readBuffer, one64.read, detail=True),
+                                 "cpu_fp32": field_errors(one32.read, one64.read, detail=True),
+                                 "cycles": {"gpu": g.info()["last_cycles"], "fp64_oracle": one64.info()["last_cycles"]}}
+            one64.close()
+            one32.close()
+            probe = None
+        if k <= steps and (k == 1 or k % every == 0):
+            probe = {"step": k, "trajectory": {"gpu": field_errors(g.readBuffer, traj64.read),
+                                               "cpu_fp32": field_errors(traj32.read, traj64.read)},
+                     "one_step": None}
+            reports.append(probe)
     g.close()
-    return {"workload": workload, "steps": steps, "every": every, "errors": rows,
-            "metric": "max|gpu - fp64 oracle| / max|fp64 oracle| per field"}
+    return {"workload": workload, "steps": steps, "every": every, "reports": reports,
+            "steps_note": f"{steps} of the workload's 2000 steps (bounded so the line finishes in minutes)",
+            "metric": "|x - fp64 oracle| / max|fp64 oracle| per field (T; u = U and V faces; Y_F; Y_S)",
+            "cpu_threads": threads, "seconds": time.perf_counter() - t0}
 
 
 SERVE_CLASSES = ((96, 144), (128, 192), (192, 288), (256, 384), (512, 768))
 
 
-def served_jobs(lam: float, njobs: int, steps_lo: int, steps_hi: int, seed: int):
-    """Poisson arrivals at rate lam; size class uniform; tepee scenes (scene kind 1); N uniform."""
+def served_jobs(njobs: int, steps_lo: int, steps_hi: int, seed: int = 5):
+    """One job set for every arrival rate: size class uniform over the classes, tepee scenes (scene kind 1),
+    N uniform in [steps_lo, steps_hi]; `gap` holds unit-rate exponential inter-arrival gaps (divided by
+    lambda for a rate), so every rate serves the same jobs in the same order."""
     import numpy as np
     rng = np.random.default_rng(seed)
-    t, jobs = 0.0, []
+    jobs = []
     for k in range(njobs):
-        t += float(rng.exponential(1.0 / lam))
         jobs.append({"size_class": int(rng.integers(0, len(SERVE_CLASSES))), "kind": 1, "seed": 9000 + k,
-                     "nsteps": int(rng.integers(steps_lo, steps_hi + 1)), "arrival_s": t})
+                     "nsteps": int(rng.integers(steps_lo, steps_hi + 1)), "gap": float(rng.exponential(1.0))})
     return jobs
 
 
-def run_served(dev, stream, lams, njobs: int, steps_lo: int, steps_hi: int, slots: int, budget: float, tol: float):
-    """The serving loop (continuous batching, HBM-budget admission) at several arrival rates, against the
-    same jobs served one by one by the plain single-scene step (FIFO; each job's time from the measured
-    plain ms/step of its size class)."""
-    import numpy as np
-    import torch
+def diff_sub(dx: float, dt: float) -> int:
+    """Diffusion sub-steps for dt (js/fluid.js:190-198 with the default diffMult)."""
+    import math
+    tmax, rho_amb, t_amb = 2200.0, 101325 * 0.0289 / (8.314462 * 293.15), 293.15
+    mu = 1.716e-5 * (tmax / 273.15) ** 1.5 * 383.55 / (tmax + 110.4)
+    alpha = mu / 0.7 / (rho_amb * t_amb / tmax)
+    n = math.ceil(dt / (dx * dx / (4.5 * alpha)))
+    return max(1, min(5, n if n % 2 else n + 1))
+
+
+def run_one_by_one(dev, jobs, tol: float):
+    """Each job alone through the plain single-scene FluidSim (same scene, solver and step count as served):
+    wall seconds from generating its scene to its fields read back, one job after the other."""
     import campfire_b200 as cb
     from campfire_b200.fluid import load_scene
-    # plain per-step time of each size class (same solver), for the one-by-one schedule
-    plain_ms = {}
-    for c, (nx, ny) in enumerate(SERVE_CLASSES):
-        sc = cb.generate_scene(1, nx, ny, 0.8, 9000)
+    service = []
+    for j in jobs:
+        nx, ny = SERVE_CLASSES[j["size_class"]]
+        t0 = time.perf_counter()
+        sc = cb.generate_scene(j["kind"], nx, ny, 0.8, j["seed"])
         g = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
         load_scene(g, sc)
         g.set_solver(cb.SOLVE_FP64, 1, tol, 300)
         g.set_coarse_solve("pipelined")
         g.set_krylov(True)
-        g.set_stream(stream.cuda_stream)
-        g.step(3)
+        g.step(j["nsteps"])
         g.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        g.step(5)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        plain_ms[c] = e0.elapsed_time(e1) / 5
+        cb.field_hash(g)
+        service.append(time.perf_counter() - t0)
         g.close()
+    return service
+
+
+def run_served(dev, stream, lams, njobs: int, steps_lo: int, steps_hi: int, slots: int, budget: float, tol: float):
+    """The serving loop (continuous batching, HBM-budget admission) at several arrival rates, against the same
+    jobs run one by one through the plain single-scene step: each job's one-by-one service time is measured
+    (scene set-up, steps, fields read back), and each rate's first-come-first-served schedule is built from
+    those measured times and the rate's arrivals."""
+    import numpy as np
+    import campfire_b200 as cb
+    jobs = served_jobs(njobs, steps_lo, steps_hi)
+    service = run_one_by_one(dev, jobs, tol)
     srv = cb.Server(SERVE_CLASSES, [slots] * len(SERVE_CLASSES), budget, device=dev.index)
     srv.set_solver(cb.SOLVE_FP64, 1, tol, 300, "pipelined", krylov=True)
+    hbm, peak_kind = peaks()
+    cells = sum(SERVE_CLASSES[j["size_class"]][0] * SERVE_CLASSES[j["size_class"]][1] * j["nsteps"] for j in jobs)
     out = []
     for lam in lams:
-        jobs = served_jobs(lam, njobs, steps_lo, steps_hi, seed=int(lam) + 17)
-        res, wall, cu = srv.run(jobs)
+        t, run_jobs = 0.0, []
+        for j in jobs:
+            t += j["gap"] / lam
+            run_jobs.append(dict(j, arrival_s=t))
+        res, wall, cu = srv.run(run_jobs)
         lat = np.array([r["done_s"] - r["arrival_s"] for r in res])
-        # one by one, first come first served, with the plain step
         t_free, lat1 = 0.0, []
-        for j in sorted(jobs, key=lambda q: q["arrival_s"]):
-            start = max(j["arrival_s"], t_free)
-            t_free = start + j["nsteps"] * plain_ms[j["size_class"]] / 1e3
+        for j, svc in zip(run_jobs, service):          # arrival order
+            t_free = max(j["arrival_s"], t_free) + svc
             lat1.append(t_free - j["arrival_s"])
         lat1 = np.array(lat1)
-        cells = sum(SERVE_CLASSES[j["size_class"]][0] * SERVE_CLASSES[j["size_class"]][1] * j["nsteps"] for j in jobs)
-        out.append({"lambda_jobs_per_s": lam, "jobs": njobs, "value": cu / wall, "unit": METRIC,
+        # algorithmic bytes: each job's cells x steps x bytes per cell-update at its last solve's cycle count
+        byts = sum(SERVE_CLASSES[j["size_class"]][0] * SERVE_CLASSES[j["size_class"]][1] * j["nsteps"] *
+                   bytes_per_cell(diff_sub(0.8 / SERVE_CLASSES[j["size_class"]][0], 2e-3), r["last_cycles"], True)
+                   for j, r in zip(run_jobs, res))
+        value = cu / wall
+        one = cells / t_free
+        out.append({"lambda_jobs_per_s": lam, "jobs": njobs, "value": value, "unit": METRIC,
                     "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                     "wall_s": wall, "max_rel_residual": max(r["last_rel"] for r in res),
-                    "one_by_one": {"value": cells / t_free if t_free > 0 else None, "unit": METRIC,
+                    "roofline": {"achieved": byts / wall / 1e9, "peak": hbm, "unit": "GB/s",
+                                 "frac": byts / wall / 1e9 / hbm, "peak_source": f"{peak_kind} hbm_gbs"},
+                    "one_by_one": {"value": one, "unit": METRIC, "makespan_s": t_free,
                                    "p50_latency_s": float(np.percentile(lat1, 50)),
-                                   "p99_latency_s": float(np.percentile(lat1, 99))}})
+                                   "p99_latency_s": float(np.percentile(lat1, 99))},
+                    "served_over_one_by_one": value / one})
     srv.close()
     return {"classes": [f"{a}x{b}" for a, b in SERVE_CLASSES], "slots_per_class": slots, "budget_bytes": budget,
-            "steps_per_job": [steps_lo, steps_hi], "scene": "tepee (five logs of half 5 cm), FP64 defect correction "
-            f"to {tol:g}, pipelined direct coarsest", "one_by_one_model": "FIFO over the same jobs with each class's measured "
-            "plain single-scene ms/step", "plain_ms_per_step": {f"{a}x{b}": plain_ms[c] for c, (a, b) in
-                                                                enumerate(SERVE_CLASSES)},
-            "runs": out}
+            "jobs": njobs, "steps_per_job": [steps_lo, steps_hi], "job_steps_total": sum(j["nsteps"] for j in jobs),
+            "scene": f"tepee (five logs of half 5 cm), FP64 defect correction to {tol:g}, pipelined direct coarsest",
+            "one_by_one": "measured: each job alone through the plain FluidSim (scene set-up, steps, fields read "
+                          "back), first come first served at each rate's arrivals",
+            "one_by_one_service_s": float(sum(service)), "runs": out}
 
 
 APP_MODE = (224, 320, 0.003)    # the app's "balanced" grid (js/config.js:8), width 0.7 m
@@ -400,6 +497,141 @@ def run_app_frames(dev, stream, frames: int, warmup: int):
             "last_frame_stats": {"hrr_w_per_m": st["hrr"], "rad_w_per_m": st["rad"], "tmax_k": st["tmax"]}}
 
 
+def run_e2e(sim, sc, stream, flush, steps: int, barrier, dev, world: int) -> dict:
+    """Wall-clock steps through the C ABI with the host-side inputs and outputs of the app's frame (see main)."""
+    import torch
+    import torch.distributed as dist
+    import campfire_b200 as cb
+    L = cb.lib()
+    pin_pieces = torch.from_numpy(sc["pieces"].copy()).pin_memory()
+    acc = torch.zeros(528, dtype=torch.int32).pin_memory()
+    rad = torch.zeros(320 * 4, dtype=torch.float32).pin_memory()
+    fw = torch.zeros(256, dtype=torch.int32).pin_memory()
+    fptr = ctypes.cast(pin_pieces.data_ptr(), ctypes.POINTER(ctypes.c_float))
+    i32 = ctypes.POINTER(ctypes.c_int32)
+    accp, radp, fwp = (ctypes.cast(acc.data_ptr(), i32), ctypes.cast(rad.data_ptr(), ctypes.POINTER(ctypes.c_float)),
+                       ctypes.cast(fw.data_ptr(), i32))
+    tag, ready, slot = ctypes.c_uint64(), ctypes.c_int(), ctypes.c_int()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    collected, skipped, lag = 0, 0, []
+
+    def collect(k, wait):
+        nonlocal collected
+        while True:
+            if wait:
+                rc = L.cfg_readback_wait(sim._h, accp, radp, fwp, ctypes.byref(tag))
+                if rc == -2:
+                    return
+                cb._lib.check(rc)
+            else:
+                cb._lib.check(L.cfg_readback_poll(sim._h, accp, radp, fwp, ctypes.byref(tag), ctypes.byref(ready)))
+                if not ready.value:
+                    return
+            collected += 1
+            lag.append(k - tag.value)
+
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(steps):
+        ev[k][0].record(stream)
+        flush.fill_(float(k))
+        ev[k][1].record(stream)
+        cb._lib.check(L.cfg_upload_pieces(sim._h, fptr, sc["npieces"]))
+        cb._lib.check(L.cfg_write_params(sim._h))
+        cb._lib.check(L.cfg_step(sim._h, 1))
+        rc = L.cfg_readback_begin(sim._h, k, ctypes.byref(slot))
+        if rc == -16:
+            skipped += 1
+        else:
+            cb._lib.check(rc)
+        collect(k, False)
+    collect(steps, True)
+    wall = time.perf_counter() - t0
+    torch.cuda.synchronize(dev)
+    flush_s = sum(e0.elapsed_time(e1) for e0, e1 in ev) / 1e3
+    t = torch.tensor([wall - flush_s], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return {"steps": steps, "seconds": float(t.item()), "wall_s": wall, "flush_s": flush_s,
+            "collected": collected, "skipped_busy": skipped,
+            "lag_steps": {"max": max(lag) if lag else None, "mean": sum(lag) / len(lag) if lag else None}}
+
+
+def measure_gpu(dev, stream, flush, workload: str, steps: int, warmup: int, launch: str, coarse_cells: int,
+                world: int, rank: int, barrier, clocks=None) -> dict:
+    """The plain single-scene step of `workload` on this rank's GPU: `steps` steps timed one by one with CUDA
+    events on the library's stream after an L2 flush each; value = all ranks' cell-updates / max-over-ranks time."""
+    import torch
+    import torch.distributed as dist
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
+    sc = cb.generate_scene(kind, nx, ny, 0.8, seed + 1000 * rank)
+    sim = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(sim, sc)
+    configure_solver(sim, workload)
+    # smoother schedule picked by the autotuner (fused V-cycles timed on a scratch scene of this size)
+    if coarse_cells > 0:
+        sim.set_coarse_cells(coarse_cells)
+        schedule = {"coarse_cells": coarse_cells, "autotune": "skipped"}
+    else:
+        tune = cb.autotune([(nx, ny)], iters=20, device=dev.index, coarse_direct=True)
+        sim.set_coarse_cells(tune["best"])
+        schedule = {"coarse_cells": tune["best"],
+                    "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}}
+    sim.set_stream(stream.cuda_stream)
+    sim.set_graphs(launch == "graph")
+    sim.step(warmup)
+    sim.synchronize()
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if clocks:
+        clocks.start()
+    for k in range(steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        sim.step(1)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop() if clocks else None
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    info = sim.info()
+    sim.synchronize()
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return {"sim": sim, "scene": sc, "value": world * nx * ny * steps / (ms_max / 1e3), "ms_max": ms_max,
+            "info": info, "launches": sim.launch_count(), "schedule": schedule, "clocks": clk}
+
+
+def kernel_roofline(sim, workload: str, value_per_gpu: float, info: dict) -> dict:
+    """The dominant kernel's achieved HBM bandwidth (algorithmic bytes per launch / CUDA-event time of back-to-back
+    launches on the library's stream) and the whole step's (algorithmic bytes per cell-update x cell-updates/s)."""
+    import campfire_b200 as cb
+    L = cb.lib()
+    hbm, peak_kind = peaks()
+    kern = {}
+    for name in ("advect", "diffuse_sources", "forces", "mg_down0", "mg_up0", "mg_coarse", "pcg_step", "defect64",
+                 "project"):
+        m, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        cb._lib.check(L.cfg_time_kernel(sim._h, name.encode(), 50, ctypes.byref(m), ctypes.byref(b), ctypes.byref(n)))
+        kern[name] = {"ms": m.value, "bytes": b.value, "per_step": n.value, "share_ms": m.value * n.value}
+    dom = max(kern, key=lambda k: kern[k]["share_ms"])
+    dk = kern[dom]
+    achieved = dk["bytes"] / (dk["ms"] / 1e3) / 1e9
+    bpc = bytes_per_cell(info["diffSub"], info["last_cycles"], True)
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
+            "traffic": NCU_TRAFFIC.get((workload, dom)), "traffic_source": "ncu dram__bytes_read.sum + "
+            "dram__bytes_write.sum per launch, one capture of this workload",
+            "bytes_per_launch": dk["bytes"], "launch_ms": dk["ms"],
+            "step_bytes_per_cell": bpc, "step_achieved_gbs": value_per_gpu * bpc / 1e9,
+            "step_frac": value_per_gpu * bpc / 1e9 / hbm,
+            "kernels": {k: {"ms": round(v["ms"], 5), "per_step": v["per_step"]} for k, v in kern.items()}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -409,20 +641,24 @@ def main():
     ap.add_argument("--workload", default="plain", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batched-steps", type=int, default=10,
+    ap.add_argument("--fine-steps", type=int, default=20,
+                    help="timed steps of the 512x768 tepee workload (FP64 to 1e-10) added to the line as `fine` "
+                         "(0: skip; ignored with --workload fine)")
+    ap.add_argument("--batched-steps", type=int, default=500,
                     help="timed steps of the 64-scene batched measurement added to the line (0: skip)")
-    ap.add_argument("--served-jobs", type=int, default=40,
-                    help="jobs per arrival rate of the serving measurement added to the line (0: skip)")
-    ap.add_argument("--served-steps", type=int, nargs=2, default=(20, 200), metavar=("LO", "HI"),
+    ap.add_argument("--served-jobs", type=int, default=24,
+                    help="jobs of the serving measurement (the same jobs at every arrival rate; 0: skip)")
+    ap.add_argument("--served-steps", type=int, nargs=2, default=(100, 2000), metavar=("LO", "HI"),
                     help="steps per served job, uniform in [LO, HI]")
     ap.add_argument("--served-rates", type=float, nargs="+", default=(10.0, 100.0, 1000.0))
     ap.add_argument("--app-frames", type=int, default=120,
                     help="timed frames of the app frame measurement (wood coupling + gas steps + render) "
                          "added to the line (0: skip)")
-    ap.add_argument("--fp64-error-every", type=int, default=0,
-                    help="with --fp64-error-steps S: run the workload beside the FP64 oracle for S steps and "
-                         "report the field errors every this many steps (0: skip)")
-    ap.add_argument("--fp64-error-steps", type=int, default=2000)
+    ap.add_argument("--fp64-error-every", type=int, default=100,
+                    help="report the field errors against the FP64 oracle every this many steps (0: skip)")
+    ap.add_argument("--fp64-error-steps", type=int, default=200,
+                    help="steps of the FP64-oracle comparison (the workload defines 2000)")
+    ap.add_argument("--fp64-error-workload", default="fine", choices=sorted(WORKLOADS))
     ap.add_argument("--coarse-cells", type=int, default=0,
                     help="start the coarse block at the first level with at most this many cells instead of "
                          "autotuning (0: autotune); for profiling runs whose launch indices must not depend on "
@@ -438,32 +674,28 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[a.workload]
-    config = {"workload": f"{a.workload} gas step {nx}x{ny}, 3 logs, FP32 V(2,2) in FP64 defect correction "
-                          f"to rel residual {tol:g}", "nx": nx, "ny": ny, "scene_seed": seed,
-              "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": maxc},
-              "l2": "flushed before every timed step (256 MB write)", "parallelism": f"replicas{world}"}
+    config = workload_config(a.workload, world)
 
     if a.impl == "reference":
+        # the CPU restatement of the reference step on this box's host cores: oracle library only
         if rank != 0:
             return
         th = cpu_threads()
         val, secs, cyc = run_cpu(a.workload, a.steps, a.warmup, th)
         line = {"metric": METRIC, "value": val, "unit": METRIC, "impl": "reference", "n_gpus": a.gpus,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * secs / a.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(config, cycles_per_step=cyc),
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+                "solve": {"cycles_per_step": cyc, "arithmetic": "f32 (FP64 outer loop), host cores"},
                 "cpu_baseline": {"value": val, "unit": METRIC, "cores": th, "kind": "port",
                                  "sample": f"{a.steps} steps of the {nx}x{ny} workload after {a.warmup} warm-up steps "
-                                           "(C++ restatement of the reference WGSL, f32, OpenMP)"},
+                                           "(C++ restatement of the reference WGSL, f32, OpenMP, same solver)"},
                 "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
 
-    import numpy as np
     import torch
     import torch.distributed as dist
     import campfire_b200 as cb
-    from campfire_b200.fluid import load_scene
 
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
@@ -472,29 +704,6 @@ def main():
     # one non-default stream shared by the library, the L2 flush and the timing events
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
-
-    sc = cb.generate_scene(kind, nx, ny, 0.8, seed + 1000 * rank)
-    sim = cb.FluidSim(local, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
-    load_scene(sim, sc)
-    sim.set_solver(mode, 1, tol, maxc)
-    sim.set_coarse_solve("pipelined")
-    sim.set_krylov(True)
-    sim.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)   # dt set by CFL 0.5 each step, capped at 2 ms
-    config["dt"] = {"cfl": PLAIN_CFL, "cap_s": PLAIN_DT_CAP}
-    config["pressure"]["coarsest"] = "direct: inverse factored beside the pressure loop, applied from the next step (pipelined)"
-    config["pressure"]["outer"] = "flexible preconditioned CG in FP64, FP32 V(2,2) as preconditioner"
-    # smoother schedule picked by the autotuner (fused V-cycles timed on a scratch scene of this size)
-    if a.coarse_cells > 0:
-        sim.set_coarse_cells(a.coarse_cells)
-        config["schedule"] = {"coarse_cells": a.coarse_cells, "autotune": "skipped"}
-    else:
-        tune = cb.autotune([(nx, ny)], iters=20, device=local, coarse_direct=True)
-        sim.set_coarse_cells(tune["best"])
-        config["schedule"] = {"coarse_cells": tune["best"],
-                              "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}}
-    sim.set_stream(stream.cuda_stream)
-    sim.set_graphs(a.launch == "graph")
-    config["launch"] = a.launch
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def barrier():
@@ -502,86 +711,43 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    sim.step(a.warmup)
-    sim.synchronize()
-    barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    cycles = []
-    clocks = ClockSampler(local)
-    clocks.start()
-    for k in range(a.steps):
-        flush.fill_(float(k))
-        ev[k][0].record(stream)
-        sim.step(1)
-        ev[k][1].record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    clk = clocks.stop()
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
-    info = sim.info()
-    sim.synchronize()
-    launches = sim.launch_count()
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * nx * ny * a.steps / (ms_max / 1e3)
+    m = measure_gpu(dev, stream, flush, a.workload, a.steps, a.warmup, a.launch, a.coarse_cells, world, rank,
+                    barrier, ClockSampler(local))
+    sim, sc, value, ms_max, info = m["sim"], m["scene"], m["value"], m["ms_max"], m["info"]
 
-    # ---- end to end through the C ABI: per step upload params + pieces from pinned host
-    # memory, step, read the accumulators back (the frame data flow of js/main.js:266-283)
-    pin_pieces = torch.from_numpy(sc["pieces"].copy()).pin_memory()
-    acc = torch.zeros(528, dtype=torch.int32).pin_memory()
-    rad = torch.zeros(320 * 4, dtype=torch.float32).pin_memory()
-    fw = torch.zeros(256, dtype=torch.int32).pin_memory()
-    L = cb.lib()
-    fptr = ctypes.cast(pin_pieces.data_ptr(), ctypes.POINTER(ctypes.c_float))
-    i32 = ctypes.POINTER(ctypes.c_int32)
-    e2e_steps = max(5, min(50, a.steps // 4))
-    barrier()
-    e2e_s = 0.0
-    for k in range(e2e_steps):
-        flush.fill_(float(k))
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        cb._lib.check(L.cfg_upload_pieces(sim._h, fptr, sc["npieces"]))
-        cb._lib.check(L.cfg_write_params(sim._h))
-        cb._lib.check(L.cfg_step(sim._h, 1))
-        cb._lib.check(L.cfg_readback(sim._h, ctypes.cast(acc.data_ptr(), i32),
-                                     ctypes.cast(rad.data_ptr(), ctypes.POINTER(ctypes.c_float)),
-                                     ctypes.cast(fw.data_ptr(), i32)))
-        e2e_s += time.perf_counter() - t0
-    t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * nx * ny * e2e_steps / float(t.item())
+    # ---- end to end through the C ABI, the app's frame data flow (js/main.js:266-283): per step the piece
+    # buffer from pinned host memory and the parameter block go up, the step runs, and the step's
+    # accumulators, radiation output and face weights come back through the asynchronous readback ring
+    # (cfg_readback_begin / cfg_readback_poll, js/fluid.js:315-342), collected as they arrive. The host never
+    # waits for a step inside the loop; the timed region ends when the last readback has been collected.
+    # The L2 flush before each step (as in the device-timed loop) sits on the same stream and is timed with
+    # CUDA events; its device time is taken out of the wall time.
+    e2e = run_e2e(sim, sc, stream, flush, max(20, min(50, a.steps)), barrier, dev, world)
+    e2e_value = world * nx * ny * e2e["steps"] / e2e["seconds"]
 
-    # ---- roofline of the dominant kernel (device time per step share), measured after the timed region
-    hbm, peak_kind = peaks()
-    kern = {}
-    for name in ("advect", "diffuse_sources", "forces", "mg_down0", "mg_up0", "mg_coarse", "pcg_step", "defect64",
-                 "project"):
-        m, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-        cb._lib.check(L.cfg_time_kernel(sim._h, name.encode(), 50, ctypes.byref(m), ctypes.byref(b), ctypes.byref(n)))
-        kern[name] = {"ms": m.value, "bytes": b.value, "per_step": n.value, "share_ms": m.value * n.value}
-    dom = max(kern, key=lambda k: kern[k]["share_ms"])
-    dk = kern[dom]
-    achieved = dk["bytes"] / (dk["ms"] / 1e3) / 1e9
-    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
-            "traffic": NCU_TRAFFIC.get((a.workload, dom)), "traffic_source": "ncu dram__bytes_read.sum + "
-            "dram__bytes_write.sum, one capture of this workload (--set full)",
-            "bytes_per_launch": dk["bytes"], "launch_ms": dk["ms"],
-            "step_bytes_per_cell": bytes_per_cell(info["diffSub"], info["last_cycles"], True),
-            "step_frac": (value / world) * bytes_per_cell(info["diffSub"], info["last_cycles"], True) / 1e9 / hbm,
-            "kernels": {k: {"ms": round(v["ms"], 5), "per_step": v["per_step"]} for k, v in kern.items()}}
+    # ---- roofline of the dominant kernel, measured after the timed region
+    roof = kernel_roofline(sim, a.workload, value / world, info)
+    sim.close()
+
+    # ---- the 512x768 tepee workload (FP64 to 1e-10): the plain step where the roofline target is set
+    fine = None
+    if a.fine_steps > 0 and a.workload != "fine":
+        mf = measure_gpu(dev, stream, flush, "fine", a.fine_steps, a.warmup, a.launch, 0, world, rank, barrier)
+        fi = mf["info"]
+        fine = {"value": mf["value"], "unit": METRIC, "steps": a.fine_steps, "ms_per_step": mf["ms_max"] / a.fine_steps,
+                "config": workload_config("fine", world), "schedule": mf["schedule"],
+                "solve": {"cycles_last_step": fi["last_cycles"], "diff_sub": fi["diffSub"], "levels": fi["levels"],
+                          "last_rel": fi["last_rel"]},
+                "roofline": kernel_roofline(mf["sim"], "fine", mf["value"] / world, fi)}
+        mf["sim"].close()
 
     batched = None
     if a.batched_steps > 0:
-        batched = run_batched(dev, stream, flush, a.batched_steps, 3, 1e-10, 300, 3)
+        batched = run_batched(dev, stream, flush, a.batched_steps, 3, 1e-10, 300, 10)
 
     fp64_error = None
     if a.fp64_error_every > 0 and rank == 0:
-        fp64_error = run_fp64_error(dev, a.workload, a.fp64_error_steps, a.fp64_error_every, cpu_threads())
+        fp64_error = run_fp64_error(dev, a.fp64_error_workload, a.fp64_error_steps, a.fp64_error_every, cpu_threads())
 
     served = None
     if a.served_jobs > 0:
@@ -598,24 +764,27 @@ def main():
         val, secs, cyc = run_cpu(a.workload, a.cpu_sample, 1, th)
         cpu = {"value": val, "unit": METRIC, "cores": th, "kind": "port",
                "sample": f"{a.cpu_sample} steps of the same {nx}x{ny} workload after 1 warm-up step "
-                         f"(C++ restatement of the reference WGSL, f32, OpenMP; the reference's V-cycle and "
-                         f"coarsest sweeps in the plain FP64 defect correction to the same tolerance: "
+                         f"(C++ restatement of the reference WGSL, f32, OpenMP, same solver: "
                          f"{cyc:.1f} V-cycles/step)"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
                 "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(config, cycles_last_step=info["last_cycles"], diff_sub=info["diffSub"],
-                               levels=info["levels"]),
-                # H2D: the piece buffer, the descriptor's parameter block (uniform + step controls, 204 B)
-                # and dx/alpha of the diffusion rule (16 B); D2H: acc + rad + faceW
-                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 204 + 16,
-                        "d2h_bytes_per_step": 528 * 4 + 320 * 16 + 256 * 4},
-                "gpu_launches": launches * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "batched": batched, "served": served, "app_frame": app, "fp64_oracle_error": fp64_error}
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+                "launch": a.launch, "schedule": m["schedule"],
+                "solve": {"cycles_last_step": info["last_cycles"], "diff_sub": info["diffSub"],
+                          "levels": info["levels"], "last_rel": info["last_rel"]},
+                # H2D: the piece buffer, the descriptor's parameter block (uniform + step controls, 204 B, less
+                # the CFL step's dt and diffusion sub-steps, 12 B, which the device owns) and dx/alpha of the
+                # diffusion rule (16 B); D2H: acc + rad + faceW of every collected readback
+                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 192 + 16,
+                        "d2h_bytes_per_step": (528 * 4 + 320 * 16 + 256 * 4) * e2e["collected"] / e2e["steps"],
+                        "readback": "asynchronous ring of three pinned slots (js/fluid.js:315-342)",
+                        "readbacks": {k: e2e[k] for k in ("collected", "skipped_busy", "lag_steps")},
+                        "wall_s": e2e["wall_s"], "l2_flush_s_removed": e2e["flush_s"]},
+                "gpu_launches": m["launches"] * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": m["clocks"],
+                "fine": fine, "batched": batched, "served": served, "app_frame": app, "fp64_oracle_error": fp64_error}
         print(json.dumps(line))
-    sim.close()
     if world > 1:
         dist.destroy_process_group()
 

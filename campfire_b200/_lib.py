@@ -124,6 +124,9 @@ def lib():
         "cfg_geometry": [vp], "cfg_step": [vp, ci], "cfg_step_profiled": [vp, fp],
         "cfg_run_stage": [vp, cs], "cfg_vcycle": [vp, ci], "cfg_radiation": [vp],
         "cfg_set_frame": [vp, ctypes.c_uint32], "cfg_readback": [vp, i32p, fp, i32p],
+        "cfg_readback_begin": [vp, ctypes.c_uint64, ip],
+        "cfg_readback_poll": [vp, i32p, fp, i32p, ctypes.POINTER(ctypes.c_uint64), ip],
+        "cfg_readback_wait": [vp, i32p, fp, i32p, ctypes.POINTER(ctypes.c_uint64)],
         "cfg_field_size": [vp, cs, ctypes.POINTER(sz)], "cfg_read_field": [vp, cs, fp, sz],
         "cfg_write_field": [vp, cs, fp, sz], "cfg_read_p64": [vp, dp, sz],
         "cfg_get_info": [vp, ctypes.POINTER(CfgInfo)], "cfg_set_solver": [vp, ci, ci, cd, ci],

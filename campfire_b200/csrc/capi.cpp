@@ -88,6 +88,14 @@ int cfg_geometry(cfg_sim* sim) { SCENE_CALL(sim, geometry(sim->scene)); }
 int cfg_radiation(cfg_sim* sim) { SCENE_CALL(sim, radiation(sim->scene)); }
 int cfg_set_frame(cfg_sim* sim, uint32_t frame) { SCENE_CALL(sim, set_frame(sim->scene, frame)); }
 int cfg_readback(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW) { SCENE_CALL(sim, readback(sim->scene, acc, rad, faceW)); }
+int cfg_readback_begin(cfg_sim* sim, uint64_t tag, int* slot) { SCENE_CALL(sim, readback_begin(sim->scene, tag, slot)); }
+int cfg_readback_poll(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW, uint64_t* tag, int* ready) {
+  SCENE_CALL(sim, readback_collect(sim->scene, false, acc, rad, faceW, tag, ready));
+}
+int cfg_readback_wait(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW, uint64_t* tag) {
+  int ready = 0;
+  SCENE_CALL(sim, readback_collect(sim->scene, true, acc, rad, faceW, tag, &ready));
+}
 int cfg_render_defaults(cfg_sim* sim, cfg_render_params* rp) { SCENE_CALL(sim, render_defaults(sim->scene, rp)); }
 int cfg_render(cfg_sim* sim, const cfg_render_params* rp, const float* wood, int width, int height, float* rgba) {
   SIM_OK(sim);

@@ -86,6 +86,10 @@ Engine::~Engine() {
   destroy_graph();
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto& sc : scenes_) if (sc.arena) cudaFree(sc.arena);
+  for (auto& sc : scenes_) {
+    if (sc.ring.host) cudaFreeHost(sc.ring.host);
+    for (auto& e : sc.ring.ev) if (e) cudaEventDestroy(e);
+  }
   for (auto& w : d_wl_) if (w) cudaFree(w);
   if (d_scenes_) cudaFree(d_scenes_);
   if (d_solve_) cudaFree(d_solve_);
@@ -339,12 +343,12 @@ int Engine::checkpoint_save(int s, const char* path) {
   const Scene& sc = scenes_[s];
   int nstate = 0;
   for (auto& it : sc.items) nstate += it.state ? 1 : 0;
-  CkptHead h{1u, (uint32_t)sc.nx, (uint32_t)sc.ny, (uint32_t)sc.nlev, (uint32_t)nstate, sc.frame, (uint32_t)sc.nray, 0u,
-             sc.time, sc.dtd, sc.dt_cap, sc.cfl, sc.width};
   std::vector<char> dparams(kDescParamBytes);
   SolveState ss{};
   CFG_CUDA(cudaMemcpy(dparams.data(), d_scenes_ + s, kDescParamBytes, cudaMemcpyDeviceToHost));
   CFG_CUDA(cudaMemcpy(&ss, sc.desc.solve, sizeof ss, cudaMemcpyDeviceToHost));
+  CkptHead h{1u, (uint32_t)sc.nx, (uint32_t)sc.ny, (uint32_t)sc.nlev, (uint32_t)nstate, sc.frame, (uint32_t)sc.nray, 0u,
+             sc.cfl > 0 ? ss.time : sc.time, sc.dtd, sc.dt_cap, sc.cfl, sc.width};
   File out;
   out.f = std::fopen(path, "wb");
   if (!out.f) return fail(CFG_ERR_IO, std::string("cannot write ") + path);
@@ -415,6 +419,9 @@ int Engine::checkpoint_load(int s, const char* path) {
   const uint64_t expect = sum.h;
   if (std::fread(&digest, 1, 8, in.f) != 8 || digest != expect)
     return fail(CFG_ERR_INVAL, std::string("checkpoint checksum mismatch in ") + path);
+  // the handle's stream does not order against the legacy stream of the blocking copies
+  // below: let its queued work finish before the arrays are replaced
+  CFG_CUDA(cudaStreamSynchronize(st()));
   size_t k = 0;
   for (auto& it : sc.items) {
     if (!it.state) continue;
@@ -426,7 +433,11 @@ int Engine::checkpoint_load(int s, const char* path) {
   sc.time = h.time; sc.dtd = h.dt; sc.dt_cap = h.dt_cap; sc.cfl = h.cfl; sc.frame = h.frame; sc.nray = (int)h.nray;
   const double cfl = sc.cfl;
   sc.cfl = 0;   // write_params must not read the device's step back: it is restored below
+  sc.dt_on_device = false;
   CFG_TRY(write_params(s));
+  // write_params enqueues its parameter upload on the stream; it must land before the
+  // saved block is restored below (a blocking copy on the legacy stream)
+  CFG_CUDA(cudaStreamSynchronize(st()));
   sc.cfl = cfl;
   // the device's parameter block as saved (CFL step included); this slot's enabled flag kept
   SceneDesc tmp = sc.desc;
@@ -551,9 +562,23 @@ int Engine::upload_ctl() {
   return CFG_OK;
 }
 
+// Diffusion sub-steps for dt (js/fluid.js:190-198, JS double arithmetic)
+static int substeps(double dt, double dx, double alpha) {
+  int n = (int)std::ceil(dt / (dx * dx / (4.5 * alpha)));
+  n = std::min(5, n % 2 ? n : n + 1);
+  return n < 1 ? 1 : n;
+}
+
+// The largest diffusion sub-step count of the enabled scenes (the step graph's diffusion
+// kernel is instantiated for it). A CFL scene's device may move dt anywhere up to dt_cap
+// without the host seeing it, so its count at dt_cap counts too.
 int Engine::max_sub() const {
   int m = 1;
-  for (auto& sc : scenes_) if (sc.enabled) m = std::max(m, sc.diff_sub);
+  for (auto& sc : scenes_) {
+    if (!sc.enabled) continue;
+    m = std::max(m, sc.diff_sub);
+    if (sc.cfl > 0 && sc.alpha > 0) m = std::max(m, substeps(sc.dt_cap, sc.dxd, sc.alpha));
+  }
   return m;
 }
 int Engine::max_levels() const {
@@ -591,8 +616,10 @@ int Engine::reset(int s) {
   CFG_CUDA(cudaMemsetAsync(d.p64, 0, (size_t)sc.nx * sc.ny * 8, q));
   // no coarsest inverse of an earlier state survives a reset (direct_ok, cinv_cur, direct_ok_next)
   CFG_CUDA(cudaMemsetAsync(&d_solve_[s].direct_ok, 0, 3 * sizeof(int), q));
+  CFG_CUDA(cudaMemsetAsync(&d_solve_[s].time, 0, sizeof(double), q));   // the CFL step's device clock
   CFG_CUDA(cudaGetLastError());
   sc.time = 0;
+  sc.dt_on_device = false;
   return CFG_OK;
 }
 
@@ -618,6 +645,7 @@ int Engine::get_param(int s, const char* name, double* v) {
 int Engine::set_dt(int s, double dt) {
   if (!(dt > 0)) return fail(CFG_ERR_INVAL, "dt must be positive");
   scenes_[s].dtd = dt; scenes_[s].dt_cap = dt;
+  scenes_[s].dt_on_device = false;
   return CFG_OK;
 }
 
@@ -625,18 +653,24 @@ int Engine::set_dt(int s, double dt) {
 int Engine::write_params(int s) {
   CFG_TRY(activate());
   Scene& sc = scenes_[s];
-  if (sc.cfl > 0 && sc.desc.solve) {
-    // keep the device's CFL step: take the copy the last step made, or read it back, before
-    // the upload overwrites it
-    float dt = 0.f;
-    if (dt_from_step_ && sc.enabled) {
-      CFG_CUDA(cudaEventSynchronize(ev_dt_));
-      dt = h_dt_pinned_[s];   // 0 (kept below) until a step of this scene has set it
-    } else {
-      CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
-                               cudaMemcpyDeviceToHost, st()));
-      CFG_CUDA(cudaStreamSynchronize(st()));
+  // With a CFL step that a step of this scene has already taken, the device owns dt: the
+  // upload below leaves dt and the diffusion sub-steps as that step set them, so nothing
+  // here waits for the GPU. The host's copy of dt follows the step's pinned copy once it
+  // has landed. Otherwise (no step since set_cfl, a staged update) the device's dt is read
+  // back before the upload.
+  const bool device_dt = sc.cfl > 0 && sc.desc.solve && sc.dt_on_device && sc.enabled;
+  if (device_dt && dt_from_step_) {
+    const cudaError_t q = cudaEventQuery(ev_dt_);
+    if (q == cudaSuccess) {
+      if (h_dt_pinned_[s] > 0.f) sc.dtd = (double)h_dt_pinned_[s];
+    } else if (q != cudaErrorNotReady) {
+      return cuda_fail(q, "cudaEventQuery(step dt)");
     }
+  } else if (!device_dt && sc.cfl > 0 && sc.desc.solve) {
+    float dt = 0.f;
+    CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
+                             cudaMemcpyDeviceToHost, st()));
+    CFG_CUDA(cudaStreamSynchronize(st()));
     if (dt > 0.f) sc.dtd = (double)dt;
   }
   sc.host.nx = sc.nx; sc.host.ny = sc.ny; sc.host.dx = (float)sc.dxd; sc.host.dt = (float)sc.dtd;
@@ -644,9 +678,7 @@ int Engine::write_params(int s) {
   sc.P = sc.host;
   const double Tmax = 2200, mu = 1.716e-5 * std::pow(Tmax / 273.15, 1.5) * 383.55 / (Tmax + 110.4);
   sc.alpha = mu / PhysConst::Pr * (double)sc.host.diffMult / (PhysConst::rhoAmb() * PhysConst::Tamb / Tmax);
-  int n = (int)std::ceil(sc.dtd / (sc.dxd * sc.dxd / (4.5 * sc.alpha)));
-  n = std::min(5, n % 2 ? n : n + 1);
-  if (n < 1) n = 1;
+  const int n = substeps(sc.dtd, sc.dxd, sc.alpha);
   sc.diff_sub = n;
   sc.diff_dt = (float)(sc.dtd / n);
   SceneDesc& d = sc.desc;
@@ -655,7 +687,18 @@ int Engine::write_params(int s) {
   // only the leading scalar block changes here (the uniform and the step controls). The
   // sources are pageable host memory, which a copy has staged by the time it returns, so
   // the copies stay in stream order without a wait here.
-  CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &d, kDescParamBytes, cudaMemcpyHostToDevice, st()));
+  if (device_dt) {
+    // everything but P.dt and (diff_sub, diff_dt)
+    const size_t o_dt = offsetof(SceneDesc, P) + offsetof(cfg_params, dt);
+    const size_t o_sub = offsetof(SceneDesc, diff_sub), o_cfl = offsetof(SceneDesc, cfl);
+    char* dst = reinterpret_cast<char*>(d_scenes_ + s);
+    const char* src = reinterpret_cast<const char*>(&d);
+    CFG_CUDA(cudaMemcpyAsync(dst, src, o_dt, cudaMemcpyHostToDevice, st()));
+    CFG_CUDA(cudaMemcpyAsync(dst + o_dt + 4, src + o_dt + 4, o_sub - (o_dt + 4), cudaMemcpyHostToDevice, st()));
+    CFG_CUDA(cudaMemcpyAsync(dst + o_cfl, src + o_cfl, kDescParamBytes - o_cfl, cudaMemcpyHostToDevice, st()));
+  } else {
+    CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &d, kDescParamBytes, cudaMemcpyHostToDevice, st()));
+  }
   CFG_CUDA(cudaMemcpyAsync(d_dxd_ + s, &sc.dxd, 8, cudaMemcpyHostToDevice, st()));
   CFG_CUDA(cudaMemcpyAsync(d_alpha_ + s, &sc.alpha, 8, cudaMemcpyHostToDevice, st()));
   if (graph_sub_ >= 0 && max_sub() > graph_sub_) graph_dirty_ = true;
@@ -715,7 +758,18 @@ int Engine::radiation(int s) {
 int Engine::set_frame(int s, uint32_t f) { scenes_[s].frame = f; return CFG_OK; }
 int Engine::set_cfl(int s, double cfl, double dt_cap) {
   if (cfl < 0 || !(dt_cap > 0)) return fail(CFG_ERR_INVAL, "cfl must be >= 0 and dt_cap > 0");
-  scenes_[s].cfl = cfl; scenes_[s].dt_cap = dt_cap;
+  CFG_TRY(activate());
+  Scene& sc = scenes_[s];
+  if (cfl > 0 && !(sc.cfl > 0) && sc.desc.solve)   // the device clock starts from the host's
+    CFG_CUDA(cudaMemcpyAsync(&d_solve_[s].time, &sc.time, sizeof(double), cudaMemcpyHostToDevice, st()));
+  if (!(cfl > 0) && sc.cfl > 0 && sc.desc.solve) {  // and the host's from the device's
+    double t = 0;
+    CFG_CUDA(cudaMemcpyAsync(&t, &d_solve_[s].time, sizeof t, cudaMemcpyDeviceToHost, st()));
+    CFG_CUDA(cudaStreamSynchronize(st()));
+    sc.time = t;
+  }
+  sc.cfl = cfl; sc.dt_cap = dt_cap;
+  sc.dt_on_device = false;
   graph_dirty_ = true;
   dt_from_step_ = false;
   return CFG_OK;
@@ -736,6 +790,63 @@ int Engine::readback(int s, int32_t* acc, float* rad, int32_t* faceW) {
   if (faceW) CFG_CUDA(cudaMemcpyAsync(faceW, d.faceW, MAX_PIECES * 16, cudaMemcpyDeviceToHost, q));
   CFG_CUDA(cudaMemsetAsync(d.acc, 0, ACC_LEN * 4, q));
   CFG_CUDA(cudaStreamSynchronize(q));
+  return CFG_OK;
+}
+
+// encodeReadback (js/fluid.js:315-324) + afterSubmit (:327-342): the accumulators, the radiation
+// output and the face weights are copied on the stream into the ring's next pinned slot, then
+// acc is cleared; the slot's event marks the copies complete. When that slot still holds a
+// readback nobody has collected (three in flight), nothing is copied and acc keeps
+// accumulating (the reference's stageBusy skip): CFG_ERR_BUSY.
+int Engine::readback_begin(int s, uint64_t tag, int* slot) {
+  CFG_TRY(activate());
+  Scene& sc = scenes_[s];
+  Scene::Ring& R = sc.ring;
+  if (!R.host) {
+    CFG_CUDA(cudaMallocHost(&R.host, kRingSlots * kRingBytes));
+    for (auto& e : R.ev) CFG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const int i = R.idx;
+  if (R.busy[i]) return fail(CFG_ERR_BUSY, "readback ring slot still pending (three readbacks not collected)");
+  const SceneDesc& d = sc.desc;
+  cudaStream_t q = st();
+  char* h = R.host + (size_t)i * kRingBytes;
+  CFG_CUDA(cudaMemcpyAsync(h, d.acc, ACC_LEN * 4, cudaMemcpyDeviceToHost, q));
+  CFG_CUDA(cudaMemcpyAsync(h + ACC_LEN * 4, d.rad, RAD_LEN * 16, cudaMemcpyDeviceToHost, q));
+  CFG_CUDA(cudaMemcpyAsync(h + ACC_LEN * 4 + RAD_LEN * 16, d.faceW, MAX_PIECES * 16, cudaMemcpyDeviceToHost, q));
+  CFG_CUDA(cudaMemsetAsync(d.acc, 0, ACC_LEN * 4, q));
+  CFG_CUDA(cudaEventRecord(R.ev[i], q));
+  R.busy[i] = true;
+  R.tag[i] = tag;
+  R.seq[i] = R.next++;
+  R.idx = (i + 1) % kRingSlots;
+  if (slot) *slot = i;
+  return CFG_OK;
+}
+
+int Engine::readback_collect(int s, bool wait, int32_t* acc, float* rad, int32_t* faceW, uint64_t* tag, int* ready) {
+  if (!ready) return fail(CFG_ERR_INVAL, "null ready flag");
+  *ready = 0;
+  CFG_TRY(activate());
+  Scene::Ring& R = scenes_[s].ring;
+  int i = -1;
+  for (int k = 0; k < kRingSlots; k++)
+    if (R.busy[k] && (i < 0 || R.seq[k] < R.seq[i])) i = k;
+  if (i < 0) return wait ? fail(CFG_ERR_NOENT, "no readback pending") : CFG_OK;
+  if (wait) {
+    CFG_CUDA(cudaEventSynchronize(R.ev[i]));
+  } else {
+    const cudaError_t e = cudaEventQuery(R.ev[i]);
+    if (e == cudaErrorNotReady) return CFG_OK;
+    CFG_CUDA(e);
+  }
+  const char* h = R.host + (size_t)i * kRingBytes;
+  if (acc) std::memcpy(acc, h, ACC_LEN * 4);
+  if (rad) std::memcpy(rad, h + ACC_LEN * 4, RAD_LEN * 16);
+  if (faceW) std::memcpy(faceW, h + ACC_LEN * 4 + RAD_LEN * 16, MAX_PIECES * 16);
+  if (tag) *tag = R.tag[i];
+  R.busy[i] = false;
+  *ready = 1;
   return CFG_OK;
 }
 
@@ -880,7 +991,8 @@ int Engine::info(int s, cfg_info* o) {
   CFG_CUDA(cudaStreamSynchronize(st()));
   std::memset(o, 0, sizeof *o);
   o->nx = sc.nx; o->ny = sc.ny; o->levels = sc.nlev; o->diff_sub = sc.diff_sub;
-  o->dx = sc.dxd; o->dt = sc.cfl > 0 ? (double)dt : sc.dtd; o->height = sc.dxd * sc.ny; o->time = sc.time;
+  o->dx = sc.dxd; o->dt = sc.cfl > 0 ? (double)dt : sc.dtd; o->height = sc.dxd * sc.ny;
+  o->time = sc.cfl > 0 ? ss.time : sc.time;   // a CFL scene's clock runs on the device
   o->frame = sc.frame; o->last_cycles = ss.cycles; o->last_rel = ss.rel;
   for (int l = 0; l < MAX_LEVELS; l++) { o->level_nx[l] = l < sc.nlev ? sc.lnx[l] : 0; o->level_ny[l] = l < sc.nlev ? sc.lny[l] : 0; }
   return CFG_OK;
@@ -1089,22 +1201,29 @@ void Engine::enqueue_factor_join(cudaStream_t s) {
 
 // The step's tail: the projection, which also swaps the pipelined coarsest inverse
 // (after the factorisation's branch has joined) and sets the next CFL dt
-void Engine::enqueue_post_solve(cudaStream_t s) {
+// Returns the first failing CUDA call's status; on failure the pinned dt copy must not be
+// trusted (the caller leaves dt_from_step_ unset).
+cudaError_t Engine::enqueue_post_solve(cudaStream_t s) {
   const bool pipe = pipelined_coarse();
-  if (pipe) cudaStreamWaitEvent(s, ev_join_, 0);
+  if (pipe) {
+    const cudaError_t e = cudaStreamWaitEvent(s, ev_join_, 0);
+    if (e != cudaSuccess) return e;
+  }
   const bool cfl = any_cfl();
   launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], any_fp64(), s, nscenes(), (pipe ? 1 : 0) | (cfl ? 2 : 0),
                  d_dxd_, d_alpha_, d_dtv_);
   launches_++;
-  if (cfl) {   // the next dt to the host side, for cfg_write_params
-    cudaMemcpyAsync(h_dt_pinned_, d_dtv_, sizeof(float) * nscenes(), cudaMemcpyDeviceToHost, s);
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(s, &cap);
-    if (cap == cudaStreamCaptureStatusActive)
-      cudaEventRecordWithFlags(ev_dt_, s, cudaEventRecordExternal);   // a node of the step graph
-    else
-      cudaEventRecord(ev_dt_, s);
-  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !cfl) return e;
+  // the next dt to the host side, for cfg_write_params
+  e = cudaMemcpyAsync(h_dt_pinned_, d_dtv_, sizeof(float) * nscenes(), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return e;
+  if (cap == cudaStreamCaptureStatusActive)
+    return cudaEventRecordWithFlags(ev_dt_, s, cudaEventRecordExternal);   // a node of the step graph
+  return cudaEventRecord(ev_dt_, s);
 }
 
 void Engine::enqueue_bnorm(cudaStream_t s) {
@@ -1185,7 +1304,8 @@ int Engine::ensure_graph() {
   e = cudaStreamEndCapture(body_stream_, &body);
   if (e != cudaSuccess) return abort_capture(e, "cudaStreamEndCapture(body)");
   enqueue_loop_end(s);
-  enqueue_post_solve(s);
+  e = enqueue_post_solve(s);
+  if (e != cudaSuccess) return abort_capture(e, "enqueue_post_solve");
   e = cudaStreamEndCapture(s, &g);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
   graph_ = g;
@@ -1214,15 +1334,16 @@ int Engine::step(int nsteps) {
       CFG_TRY(set_cond_mode(true));
       CFG_CUDA(cudaGraphLaunch(exec_, st()));
       dt_from_step_ = dt_from_step_ || any_cfl();
+      mark_device_dt();
     } else {
       CFG_TRY(set_cond_mode(false));
       launches_ = 0; vcycle_launches_ = 0;
       enqueue_pre_solve(st(), 0ull, 0);
       CFG_CUDA(cudaGetLastError());
       CFG_TRY(host_pressure_loop());
-      enqueue_post_solve(st());
-      CFG_CUDA(cudaGetLastError());
+      CFG_CUDA(enqueue_post_solve(st()));
       dt_from_step_ = dt_from_step_ || any_cfl();
+      mark_device_dt();
     }
     for (auto& sc : scenes_) if (sc.enabled) sc.time += sc.dtd;
   }
@@ -1278,8 +1399,9 @@ int Engine::step_profiled(float* ms) {
   enqueue_factor(s);
   CFG_TRY(host_pressure_loop());
   CFG_CUDA(cudaEventRecord(ev[6], s));
-  enqueue_post_solve(s);
+  CFG_CUDA(enqueue_post_solve(s));
   dt_from_step_ = dt_from_step_ || any_cfl();
+  mark_device_dt();
   CFG_CUDA(cudaEventRecord(ev[7], s));
   CFG_CUDA(cudaEventSynchronize(ev[7]));
   for (int k = 0; k < 7; k++) CFG_CUDA(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));

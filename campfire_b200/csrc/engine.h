@@ -65,11 +65,28 @@ struct Scene {
   size_t arena_bytes = 0;
   SceneDesc desc{};              // host mirror of the device descriptor
   bool enabled = true;
+  // CFL step: a step has set this scene's dt on the device since the host last set it
+  // (reset, set_dt, set_cfl, checkpoint load): write_params then leaves dt to the device
+  bool dt_on_device = false;
   // the arena's arrays in allocation order; `state`: part of a checkpoint (not the
   // tensor maps, which hold this arena's addresses, nor per-step scratch)
   struct Item { void* ptr; size_t bytes; bool state; };
   std::vector<Item> items;
+  // The asynchronous readback ring (js/fluid.js:315-342): three pinned staging slots of
+  // acc, rad and faceW, each filled by copies on the stream and completed by its event,
+  // handed out oldest first. Allocated on the first cfg_readback_begin.
+  struct Ring {
+    char* host = nullptr;              // kRingSlots x kRingBytes, pinned
+    cudaEvent_t ev[3] = {};
+    uint64_t tag[3] = {}, seq[3] = {};
+    bool busy[3] = {};                 // copies enqueued, not yet handed out (stageBusy)
+    int idx = 0;                       // the next slot to fill (stageIdx)
+    uint64_t next = 0;                 // sequence number of the next fill
+  } ring;
 };
+
+constexpr int kRingSlots = 3;
+constexpr size_t kRingBytes = ACC_LEN * 4 + RAD_LEN * 16 + MAX_PIECES * 16;
 
 // Bytes of SceneDesc that cfg_write_params uploads: the uniform and the step
 // controls up to (not including) the tile counts and device pointers.
@@ -100,6 +117,10 @@ class Engine {
   int set_cfl(int s, double cfl, double dt_cap);
   int set_nray(int s, int nray);
   int readback(int s, int32_t* acc, float* rad, int32_t* faceW);
+  // encodeReadback + afterSubmit (js/fluid.js:315-342): CFG_ERR_BUSY when the next slot is still pending
+  int readback_begin(int s, uint64_t tag, int* slot);
+  // the oldest pending slot: *ready = 1 and its data once its copies have completed (wait: block for them)
+  int readback_collect(int s, bool wait, int32_t* acc, float* rad, int32_t* faceW, uint64_t* tag, int* ready);
   // render.wgsl's fragment stage into a host RGBA float image (wood: MAX_PIECES x 12 floats or null)
   int render(int s, const cfg_render_params& rp, const float* wood, int width, int height, float* rgba);
   int render_defaults(int s, cfg_render_params* rp);
@@ -180,11 +201,13 @@ class Engine {
   // scene whose coarse block starts below level 0
   bool pcg_fused() const;
   bool any_cfl() const;
+  // after a step's launch: every enabled CFL scene's dt now lives on the device
+  void mark_device_dt() { for (auto& sc : scenes_) if (sc.enabled && sc.cfl > 0) sc.dt_on_device = true; }
   int cycle_tail() const { return any_fp64() ? (krylov() ? (pcg_fused() ? 4 : 3) : 2) : 1; }
   void enqueue_loop_end(cudaStream_t s);
   void enqueue_fp64_tail(cudaStream_t s);
   void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
-  void enqueue_post_solve(cudaStream_t s);
+  cudaError_t enqueue_post_solve(cudaStream_t s);
   int host_pressure_loop();
   void enqueue_bnorm(cudaStream_t s);
 

@@ -49,6 +49,7 @@ struct SolveState {
   int pad;
   double delta, alpha, beta;   // Krylov FP64 mode: r.z of this cycle, the step length, the direction update
   double pi;                // Krylov FP64 mode: d.q of this cycle
+  double time;              // CFL step: the scene's clock, advanced on the device by each step's own dt
 };
 
 struct SceneDesc {

@@ -11,7 +11,9 @@ namespace cfg {
 // FP64: the FP64 pressure of the defect-correction loop, rounded once to f32.
 // CFL step for the next step: dt = min(dt_cap, cfl*dx/max|u|) and the diffusion
 // sub-step count of js/fluid.js:190-198 for that dt (one thread, after max|u| is complete)
-__device__ __forceinline__ void cfl_next_dt(SceneDesc& S, double h, double alpha) {
+// advance_clock: the step's own dt (P.dt, before it is replaced) is added to the scene's clock
+__device__ __forceinline__ void cfl_next_dt(SceneDesc& S, double h, double alpha, bool advance_clock) {
+  if (advance_clock) S.solve->time += (double)S.P.dt;
   const float m = __uint_as_float(S.solve->maxu);
   const float cand = m > 0.f ? S.cfl * S.P.dx / m : S.dt_cap;
   const float dt = fminf(S.dt_cap, cand);
@@ -106,7 +108,7 @@ __global__ void __launch_bounds__(256) k_project(SceneDesc* __restrict__ scenes,
   __syncthreads();
   if (s_last && threadIdx.x == 0) {
     S.solve->counter = 0u;
-    cfl_next_dt(S, dxd[w.scene], alpha[w.scene]);
+    cfl_next_dt(S, dxd[w.scene], alpha[w.scene], true);
     if (dtv) dtv[w.scene] = S.P.dt;
   }
 }
@@ -117,7 +119,7 @@ __global__ void k_cfl_update(SceneDesc* scenes, int nscenes, const double* dxd, 
   if (s >= nscenes) return;
   SceneDesc& S = scenes[s];
   if (!S.enabled || !(S.cfl > 0.f)) return;
-  cfl_next_dt(S, dxd[s], alpha[s]);
+  cfl_next_dt(S, dxd[s], alpha[s], false);
 }
 
 // geometry.wgsl:121-153: per cell the nearest piece (sdf, piece*4+face) and the

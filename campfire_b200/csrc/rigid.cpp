@@ -361,11 +361,11 @@ void RigidWorld::step(double dt) {
     m.tMass = 1 / (mA + mB + iA * rtA * rtA + iB * rtB * rtB);
   }
   for (int s = 0; s < ns; s++) {
-    for (auto& b : bodies_) {   // gravity (a held piece's weight is carried by the hand)
+    for (auto& b : bodies_) {   // gravity on every body the grip does not hold up
       if (b->dragging) continue;
       b->vx += p.gx * h; b->vy += p.gy * h;
     }
-    for (auto& m : manifolds_) {   // warm start
+    for (auto& m : manifolds_) {   // apply the impulses kept from the last collision step
       const double tx = m.ny, ty = -m.nx;
       for (int k = 0; k < m.npts; k++) apply_impulse(m.A, m.B, m.pts[k], m.pts[k].Pn * m.nx, m.pts[k].Pn * m.ny);
       apply_impulse(m.A, m.B, m, m.Pt * tx, m.Pt * ty);
@@ -378,7 +378,7 @@ void RigidWorld::step(double dt) {
       if (sp > vmax) { b->vx *= vmax / sp; b->vy *= vmax / sp; }
       b->x += b->vx * h; b->y += b->vy * h; b->a += b->w * h;
     }
-    solve_contacts(soft.biasRate, soft.massScale, soft.impulseScale, inv_h, false);   // relax
+    solve_contacts(soft.biasRate, soft.massScale, soft.impulseScale, inv_h, false);   // final velocity pass without position bias
   }
   // stick / slip state and anchor maintenance
   for (auto& m : manifolds_) {

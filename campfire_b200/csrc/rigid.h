@@ -24,8 +24,8 @@ double js_round(double x);
 
 struct RigidParams {                // RIGID_DEFAULTS, js/rigid.js:12-27
   double gx = 0, gy = -9.81;
-  double width = 0.7;               // wood-confining side walls at x = 0 and x = width
-  double dt = 1.0 / 480;            // collision step
+  double width = 0.7;               // walls that keep the pieces in [0, width]
+  double dt = 1.0 / 480;            // step of the collision solver (s)
   int substeps = 4;
   double slop = 0.0002;
   double contactHertz = 240, contactDamping = 10, maxPushout = 0.25;

@@ -71,7 +71,7 @@ void WoodPiece::step(double dt, const std::array<double, 4>& qConv, const std::a
   if (dead) return;
   using W = WoodK;
   const double Yc = ctl.charYield;
-  // char oxidation: remove mass, heat the surface
+  // burning char: its mass leaves the piece and its heat goes to the face
   std::array<double, 4> qChar{0, 0, 0, 0};
   for (int f = 0; f < 4; f++) {
     const double m = std::min(charBurnt[f], mc);
@@ -88,7 +88,7 @@ void WoodPiece::step(double dt, const std::array<double, 4>& qConv, const std::a
     const double s = side;
     const double dS = std::min(W::deltaS, s / 8), dP = std::min(W::deltaP, s / 8);
     const bool allChar = mv <= 1e-9;
-    // capacities (J/K per m)
+    // heat capacity of each layer, J/K per m of depth
     const double rcv = rhoV * W::cv, rcc = rhoC * W::cc;
     std::array<double, 4> Cs{}, Cp{};
     double Csum = 0;
@@ -100,7 +100,7 @@ void WoodPiece::step(double dt, const std::array<double, 4>& qConv, const std::a
     }
     const double Ctot = mv * W::cv + mc * W::cc;
     const double Cc = std::max(0.1 * Ctot, Ctot - Csum);
-    // pyrolysis
+    // virgin wood turning into gas and char
     const double A = W::pyroA * ctl.pyroMult;
     const double mFrontCap = rhoV * dP * s;
     double mFrontSum = 0;
@@ -112,7 +112,7 @@ void WoodPiece::step(double dt, const std::array<double, 4>& qConv, const std::a
     }
     const double rCore = A * std::exp(-W::pyroTa / Tc) * std::max(0.0, mv - mFrontSum);
     double rTot = rf[0] + rf[1] + rf[2] + rf[3] + rCore;
-    if (rTot * h > mv) {   // do not consume more than exists
+    if (rTot * h > mv) {   // cap the step's loss at the virgin mass left
       const double k = mv / (rTot * h);
       for (int f = 0; f < 4; f++) rf[f] *= k;
       rTot *= k;
@@ -123,13 +123,13 @@ void WoodPiece::step(double dt, const std::array<double, 4>& qConv, const std::a
     double coreIn = 0;
     for (int f = 0; f < 4; f++) {
       const double df = d[f];
-      // char conductivity with radiation across pores
+      // the char layer conducts by its solid and by radiation through its pores
       const double Tm = 0.5 * (Ts[f] + Tp[f]);
       const double kcEff = W::kc + 4 * W::eps * W::sigma * Tm * Tm * Tm * W::pore;
       const double Gsp = s / (df / kcEff + (dS + dP) / (2 * kvv));
       const double Lpc = std::max(0.5 * (0.5 * s - df), 0.001);
       const double Gpc = kvv * s / Lpc;
-      const double gas = (1 - Yc) * (rf[f] + 0.25 * rC);   // kg/s/m leaving this face
+      const double gas = (1 - Yc) * (rf[f] + 0.25 * rC);   // gas mass per second and m of depth through this face
       gasFace[f] += gas * h;
       const double Tsf = Ts[f], Tpf = Tp[f];
       const double eps = W::eps;
@@ -141,7 +141,7 @@ void WoodPiece::step(double dt, const std::array<double, 4>& qConv, const std::a
       const double qp = Gsp * (Tsf - Tpf) - Gpc * (Tpf - Tc) - W::dHpyro * rf[f];
       Tp[f] = Tpf + h * qp / (Cp[f] + h * (Gsp + Gpc));
       coreIn += Gpc * (Tpf - Tc);
-      // char layer grows into the virgin wood
+      // the charred depth advances by the char this face has made
       if (!allChar) d[f] = std::min(0.5 * s, d[f] + rf[f] * h / (rhoV * s));
     }
     Tc += h * (coreIn - W::dHpyro * rC) / Cc;
@@ -267,7 +267,7 @@ int WoodScene::readback(double sim_dt) {
     WoodSlot& p = slots_[s];
     if (!p.used) continue;
     for (int f = 0; f < 4; f++) {
-      // fraction of the face open to the gas (0 where pressed against wood or floor)
+      // share of the face that touches gas: none where it rests on the floor or another piece
       p.wood.exposure[f] = std::min(1.0, faceW[s * 4 + f] / 1e8 / std::max(p.wood.side, 1e-4));
       const int k = (s * 4 + f) * 2;
       p.qConv[f] = acc[k] / E_SCALE / sim_dt;

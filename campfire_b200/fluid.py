@@ -92,6 +92,39 @@ class _SceneOps:
         check(_lib.lib().cfg_readback(self._h, acc.ctypes.data_as(i32p), _fp(rad), fw.ctypes.data_as(i32p)))
         return {"acc": acc, "rad": rad, "faceW": fw}
 
+    def encodeReadback(self, tag: int = 0):
+        """encodeReadback + afterSubmit, asynchronous (cfg_readback_begin): the ring slot used, or None when
+        the next slot is still pending (the frame's readback is skipped and acc keeps accumulating)."""
+        slot = ctypes.c_int(-1)
+        rc = _lib.lib().cfg_readback_begin(self._h, tag, ctypes.byref(slot))
+        if rc == -16:
+            return None
+        check(rc)
+        return slot.value
+
+    def pollReadback(self, wait: bool = False):
+        """The oldest pending readback once its copies are done: (data, tag), data as readback() gives it;
+        None if nothing is ready (wait=True blocks for the oldest pending one)."""
+        acc = np.zeros(_lib.ACC_LEN, np.int32)
+        rad = np.zeros(_lib.RAD_LEN * 4, np.float32)
+        fw = np.zeros(_lib.MAX_PIECES * 4, np.int32)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        tag = ctypes.c_uint64()
+        L = _lib.lib()
+        if wait:
+            rc = L.cfg_readback_wait(self._h, acc.ctypes.data_as(i32p), _fp(rad), fw.ctypes.data_as(i32p),
+                                     ctypes.byref(tag))
+            if rc == -2:
+                return None
+            check(rc)
+        else:
+            ready = ctypes.c_int()
+            check(L.cfg_readback_poll(self._h, acc.ctypes.data_as(i32p), _fp(rad), fw.ctypes.data_as(i32p),
+                                      ctypes.byref(tag), ctypes.byref(ready)))
+            if not ready.value:
+                return None
+        return {"acc": acc, "rad": rad, "faceW": fw}, tag.value
+
     def field_size(self, name: str) -> int:
         n = ctypes.c_size_t()
         check(_lib.lib().cfg_field_size(self._h, name.encode(), ctypes.byref(n)))

@@ -47,7 +47,7 @@ extern "C" {
 #define CFG_ERR_NOENT (-2)     /* unknown parameter, field or stage name */
 #define CFG_ERR_IO (-5)        /* a CUDA call failed */
 #define CFG_ERR_NOMEM (-12)    /* device allocation failed or over the memory budget */
-#define CFG_ERR_BUSY (-16)     /* readback slot busy (js/fluid.js:317) */
+#define CFG_ERR_BUSY (-16)     /* readback ring slot still pending (js/fluid.js:317); server busy */
 #define CFG_ERR_NODEV (-19)    /* no CUDA device */
 #define CFG_ERR_INVAL (-22)    /* bad argument */
 #define CFG_ERR_RANGE (-34)    /* 'coarsest level too large' (js/fluid.js:91) */
@@ -132,6 +132,19 @@ int cfg_set_frame(cfg_sim* sim, uint32_t frame);
 /* encodeReadback + afterSubmit (js/fluid.js:315-342), synchronous: copies
  * acc[528] (i32), rad[320*4] (f32), faceW[256] (i32), then clears acc. Any pointer may be NULL. */
 int cfg_readback(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW);
+/* encodeReadback(enc) + afterSubmit(cb, tag) (js/fluid.js:315-342), asynchronous: enqueues on the
+ * stream the copy of acc[528], rad[320*4] and faceW[256] into the next of three pinned staging
+ * slots, then clears acc, and returns at once; *slot (may be NULL) receives the slot. When that
+ * slot still holds a readback not yet collected (three pending), it copies nothing, leaves acc
+ * accumulating and returns CFG_ERR_BUSY, as the reference skips a frame's readback while its
+ * staging buffer is mapped (:317). `tag` comes back with the data (the reference's tag). */
+int cfg_readback_begin(cfg_sim* sim, uint64_t tag, int* slot);
+/* afterSubmit's callback, polled: the oldest pending readback. *ready = 1 and acc/rad/faceW/tag
+ * filled (any pointer may be NULL) once its copies have completed, freeing its slot; *ready = 0
+ * if none is pending or the oldest is still in flight. Never waits. */
+int cfg_readback_poll(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW, uint64_t* tag, int* ready);
+/* the same, waiting for the oldest pending readback's copies; CFG_ERR_NOENT if none is pending */
+int cfg_readback_wait(cfg_sim* sim, int32_t* acc, float* rad, int32_t* faceW, uint64_t* tag);
 /* readBuffer(name) (js/fluid.js:345-355) and its inverse. Names: U V T Y SQ cellG fx fy
  * U2 V2 T2 Y2 p rhs ax ay, and p.L rhs.L ax.L ay.L for multigrid level L.
  * Uh Vh Th Yh are not kept by the fused kernels and read as CFG_ERR_NOENT. */

@@ -21,7 +21,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboracle_gas.so")
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libwgslref.so")
-REFERENCE_ROOT = "/root/reference"
+# the reference checkout, where one exists: CAMPFIRE_REF (environment); unset: the translated WGSL is not built
+REFERENCE_ROOT = os.environ.get("CAMPFIRE_REF", "")
 
 SOLVE_FIXED, SOLVE_TOL, SOLVE_FP64 = 0, 1, 2
 STAGES = ("advect", "diffuse", "sources", "forces", "coef_rhs", "pressure", "project")
@@ -34,10 +35,12 @@ def build(force: bool = False) -> str:
     return LIB_PATH
 
 
-def build_ref() -> str | None:
-    """Translate and compile the reference WGSL (only where the reference checkout exists)."""
-    if os.path.isdir(os.path.join(REFERENCE_ROOT, "shaders")):
-        subprocess.run(["make", "-C", _HERE, "ref"], check=True, stdout=subprocess.DEVNULL)
+def build_ref(checkout: str | None = None) -> str | None:
+    """Translate and compile the reference WGSL from the checkout at `checkout` (default: CAMPFIRE_REF);
+    nothing is built where no checkout exists."""
+    root = checkout or REFERENCE_ROOT
+    if root and os.path.isdir(os.path.join(root, "shaders")):
+        subprocess.run(["make", "-C", _HERE, "ref", f"REF={root}"], check=True, stdout=subprocess.DEVNULL)
     return REF_LIB_PATH if os.path.exists(REF_LIB_PATH) else None
 
 
@@ -243,6 +246,28 @@ class OracleSim:
         keys = ["nx", "ny", "dx", "dt", "time", "frame", "diffSub", "levels", "last_cycles",
                 "last_rel", "height", "last_rel0"]
         return dict(zip(keys, o[: len(keys)].tolist()))
+
+    def copy_state_from(self, sim, cfl: float = 0.0, dt_cap: float = 0.0):
+        """Take over the state of a FluidSim-like object (readBuffer / read_p64 / info): every field a step
+        reads or keeps (the gas fields and their advected copies, sources, geometry, the multigrid levels,
+        the FP64 pressure) and its time step, so that the next step starts from identical values (f32
+        values are exact in either arithmetic). cfl > 0: the CFL step with this cap continues."""
+        for f in ("T", "Y", "U", "V", "T2", "Y2", "U2", "V2", "SQ", "fx", "fy"):
+            self.write(f, sim.readBuffer(f))
+        cg = np.ascontiguousarray(sim.readBuffer("cellG"), np.float32)
+        g = np.empty(cg.size, np.float64)
+        g[0::2] = cg[0::2]
+        g[1::2] = cg.view(np.uint32)[1::2]          # bitcast<f32>(piece*4+face) -> its integer value
+        self.write("cellG", g)
+        for lvl in range(int(self.info()["levels"])):
+            for f in ("p", "rhs", "ax", "ay"):
+                name = f if lvl == 0 else f"{f}.{lvl}"
+                self.write(name, sim.readBuffer(name))
+        self.write("p64", sim.read_p64())
+        self.set_dt(float(sim.info()["dt"]))
+        if cfl > 0:
+            self.set_cfl(cfl, dt_cap)
+        self.write_params()
 
     def pressure_residual(self):
         v = ctypes.c_double()

@@ -4,7 +4,7 @@ The outputs come from the reference itself: its WGSL kernels (shaders/*.wgsl and
 the sampler text of js/gpu.js) translated mechanically to C++ by
 oracle/wgsl2cpp.py and driven in FluidSim's dispatch order (js/fluid.js) by
 oracle/wgsl_harness.cpp, built by `make -C oracle ref` into oracle/_ref/.
-Needs the reference checkout (default /root/reference, or $CAMPFIRE_REF) and
+Needs the reference checkout (its path in $CAMPFIRE_REF, or the first argument) and
 the product library for the scene generator; the fixtures themselves are
 self-contained (inputs and outputs), so the tests read only the .npz files.
 
@@ -20,7 +20,7 @@ Each fixture holds, for one seeded scene:
             per image k the 48-byte RP uniform rnd_rp_k and the RGB image rnd_img_k
             (row 0 at the top; alpha is 1), with the seeded wood buffer rnd_wood
 
-    python tests/golden/make_golden.py            # rewrite the fixtures
+    CAMPFIRE_REF=<reference checkout> python tests/golden/make_golden.py   # rewrite the fixtures
 """
 from __future__ import annotations
 
@@ -37,7 +37,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-REF = os.environ.get("CAMPFIRE_REF", "/root/reference")
+# the reference checkout: CAMPFIRE_REF (environment) or the first argument
+REF = os.environ.get("CAMPFIRE_REF") or (sys.argv[1] if len(sys.argv) > 1 else "")
+if not REF:
+    sys.exit("make_golden.py: set CAMPFIRE_REF (or pass the path) to the reference checkout")
 STATE = ("T", "Y", "U", "V", "T2", "Y2", "U2", "V2", "SQ", "p")
 STAGE_OUT = {
     "advect": ("T2", "Y2", "U2", "V2"),

@@ -1,0 +1,115 @@
+"""Parity of the benchmarked configurations: the exact solver settings the benchmark times,
+GPU against the CPU oracle from the same state.
+
+  plain  256x384, three logs: FP64 outer loop to ||r||/||rhs|| <= 1e-6 by flexible CG around the
+         FP32 V(2,2) cycle, the coarsest level's inverse factored beside the loop (pipelined),
+         the coarse block from the level of 1536 cells, CFL 0.5 capped at 2 ms, one CUDA graph
+         per step (the pressure loop a device-side WHILE node)
+  fine   512x768, five-log tepee: the same solver to 1e-10, seven multigrid levels (the
+         reference caps the hierarchy at six, js/fluid.js:72, 91; 512x768 needs seven to end
+         at <= 256 cells)
+
+The GPU runs a few steps from the generated scene first, so the pipelined coarsest inverse,
+the FP64 pressure and the CFL step are all carried over from earlier steps; its whole state
+(fields, geometry, multigrid levels, FP64 pressure, dt) is then copied into the oracle and
+both take the same steps. The FP32 oracle is the parity check (1e-4 per field, as the other
+full-step tests); the FP64 oracle is the accuracy check of the north-star workload.
+"""
+import numpy as np
+import pytest
+
+import campfire_b200 as cb
+from campfire_b200.fluid import load_scene
+from conftest import norm_err
+
+pytestmark = pytest.mark.gpu
+
+CFL, DT_CAP = 0.5, 2e-3
+WORKLOADS = {"plain": (256, 384, 0, 1235, 1e-6, 200), "fine": (512, 768, 1, 1236, 1e-10, 300)}
+
+
+def configure(sim, tol, max_cycles):
+    sim.set_solver(cb.SOLVE_FP64, 1, tol, max_cycles)
+    sim.set_coarse_solve("pipelined")
+    sim.set_krylov(True)
+    sim.set_cfl(CFL, DT_CAP)
+
+
+def gpu_run(name, warm_steps):
+    nx, ny, kind, seed, tol, maxc = WORKLOADS[name]
+    sc = cb.generate_scene(kind, nx, ny, 0.8, seed)
+    g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(g, sc)
+    configure(g, tol, maxc)
+    g.set_coarse_cells(1536)
+    g.set_graphs(True)
+    g.step(warm_steps)
+    return g, sc
+
+
+def oracle_from(oracle_mod, g, sc, name, fp64=False):
+    nx, ny, kind, seed, tol, maxc = WORKLOADS[name]
+    o = oracle_mod.OracleSim(nx, ny, 0.8, sc["dt"], fp64=fp64)
+    load_scene(o, sc)
+    configure(o, tol, maxc)
+    o.copy_state_from(g, CFL, DT_CAP)
+    return o
+
+
+def field_arrays(read):
+    y = np.asarray(read("Y"), np.float64).reshape(-1, 4)
+    return {"T": np.asarray(read("T"), np.float64),
+            "u": np.concatenate([np.asarray(read("U"), np.float64), np.asarray(read("V"), np.float64)]),
+            "Y_F": y[:, 0], "Y_S": y[:, 3]}
+
+
+def rel_errors(read_a, read_ref):
+    """per field: (max, 99.9th percentile) of |a - ref| / max|ref|"""
+    a, b = field_arrays(read_a), field_arrays(read_ref)
+    out = {}
+    for f in a:
+        d = np.abs(a[f] - b[f]) / max(float(np.max(np.abs(b[f]))), 1e-30)
+        out[f] = (float(d.max()), float(np.quantile(d, 0.999)))
+    return out
+
+
+@pytest.mark.parametrize("name,warm", [("plain", 4), ("fine", 3)])
+def test_benchmarked_solver_matches_oracle(oracle_mod, name, warm):
+    nx, ny, kind, seed, tol, maxc = WORKLOADS[name]
+    g, sc = gpu_run(name, warm)
+    o = oracle_from(oracle_mod, g, sc, name)
+    assert int(o.info()["levels"]) == g.info()["levels"] == (7 if name == "fine" else 6)
+    for k in range(2):
+        g.step(1)
+        o.step(1)
+        gi, oi = g.info(), o.info()
+        assert gi["last_rel"] <= tol and oi["last_rel"] <= tol, (k, gi["last_rel"], oi["last_rel"])
+        # the GPU's first step here uses the inverse factored in its previous step, the fresh
+        # oracle's the sweeps: the same converged pressure, up to a couple of cycles apart
+        assert abs(gi["last_cycles"] - oi["last_cycles"]) <= 2, (k, gi["last_cycles"], oi["last_cycles"])
+        assert abs(gi["dt"] - oi["dt"]) <= 1e-5 * oi["dt"], (k, gi["dt"], oi["dt"])
+        for f in ("T", "Y", "U", "V", "SQ"):
+            e = norm_err(g.readBuffer(f), o.read(f))
+            assert e <= 1e-4, (name, k, f, e)
+        assert norm_err(g.read_p64(), o.read("p64")) <= 1e-4
+    g.close()
+
+
+def test_fine_step_against_fp64_oracle(oracle_mod):
+    """One step of the 512x768 workload from the GPU's state: GPU (FP32 arithmetic, FP64 pressure to
+    1e-10) against the FP64 oracle. Fields within 1e-4 of the FP64 oracle, as the workload states; a
+    cell whose limiter or chemistry branch flips under a rounding difference may exceed it alone, so
+    the bound holds for the 99.9th percentile and the maximum may not exceed three times the CPU FP32
+    restatement's own maximum from the same state."""
+    g, sc = gpu_run("fine", 3)
+    o64 = oracle_from(oracle_mod, g, sc, "fine", fp64=True)
+    o32 = oracle_from(oracle_mod, g, sc, "fine")
+    g.step(1)
+    o64.step(1)
+    o32.step(1)
+    eg, e32 = rel_errors(g.readBuffer, o64.read), rel_errors(o32.read, o64.read)
+    for f in eg:
+        assert eg[f][1] <= 1e-4, (f, eg[f], e32[f])
+        assert eg[f][0] <= max(1e-4, 3 * e32[f][0]), (f, eg[f], e32[f])
+    assert g.info()["last_rel"] <= 1e-10
+    g.close()

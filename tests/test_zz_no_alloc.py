@@ -54,6 +54,61 @@ def test_noalloc_residual_matches_allocating_entry_point(nx, ny, kind, seed):
         sim.close()
 
 
+def _residual_fp64(p, rhs, ax, ay, nx, ny, h2):
+    """The residual sums of pressure.wgsl:77-101 in numpy: r in f32 with the kernel's operation order
+    (each product and sum rounded separately), the squares summed in FP64."""
+    f32 = np.float32
+    P = p.reshape(ny, nx)
+    AX = ax.reshape(ny, nx + 1)
+    AY = ay.reshape(ny + 1, nx)
+    w, e, s, n = AX[:, :-1], AX[:, 1:], AY[:-1, :], AY[1:, :]
+    off = np.zeros((ny, nx), f32)
+    diag = np.zeros((ny, nx), f32)
+    pl = np.zeros_like(P); pl[:, 1:] = P[:, :-1]
+    pr = np.zeros_like(P); pr[:, :-1] = P[:, 1:]
+    pb = np.zeros_like(P); pb[1:, :] = P[:-1, :]
+    pt = np.zeros_like(P); pt[:-1, :] = P[1:, :]
+    col = np.arange(nx)[None, :]
+    row = np.arange(ny)[:, None]
+    m = (col > 0)
+    off = np.where(m, off + w * pl, off); diag = np.where(m, diag + w, diag + f32(2) * w)
+    m = (col < nx - 1)
+    off = np.where(m, off + e * pr, off); diag = np.where(m, diag + e, diag + f32(2) * e)
+    m = (row > 0)
+    off = np.where(m, off + s * pb, off); diag = np.where(m, diag + s, diag)
+    m = (row < ny - 1)
+    off = np.where(m, off + n * pt, off); diag = np.where(m, diag + n, diag + f32(2) * n)
+    R = rhs.reshape(ny, nx)
+    r = np.where(diag <= 0, f32(0), R - (off - diag * P) / f32(h2)).astype(f32)
+    return float(np.sum(r.astype(np.float64) ** 2)), float(np.sum(R.astype(np.float64) ** 2))
+
+
+@pytest.mark.parametrize("nx,ny", [(1024, 1024), (700, 900)])
+def test_noalloc_residual_at_and_below_the_block_limit(nx, ny):
+    """1024x1024 fills exactly the 4096 blocks the scratch holds; 700x900 (2461 blocks) makes every
+    thread of the combine kernel sum several partials. Random coefficients with closed faces (zeros)."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(nx + ny)
+    f32 = np.float32
+    p = rng.standard_normal(nx * ny).astype(f32)
+    rhs = rng.standard_normal(nx * ny).astype(f32)
+    ax = (rng.random((nx + 1) * ny) * (rng.random((nx + 1) * ny) > 0.1)).astype(f32)
+    ay = (rng.random(nx * (ny + 1)) * (rng.random(nx * (ny + 1)) > 0.1)).astype(f32)
+    h2 = (0.8 / nx) ** 2
+    rr, bb = _residual_fp64(p, rhs, ax, ay, nx, ny, h2)
+    want = np.sqrt(rr / bb)
+    bufs = [_device_copy(torch, a, dev) for a in (p, rhs, ax, ay)]
+    torch.cuda.synchronize(dev)
+    L = cb.lib()
+    for call in range(2):
+        rel = ctypes.c_double(-1.0)
+        _lib.check(L.cfg_pressure_residual_noalloc(*[ctypes.c_void_p(b.data_ptr()) for b in bufs], nx, ny, h2,
+                                                   ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream),
+                                                   ctypes.byref(rel)))
+        assert abs(rel.value - want) <= REL_TOL * want, (call, rel.value, want)
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     torch = pytest.importorskip("torch")
     dev = torch.device("cuda", 0)
