@@ -192,6 +192,8 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     b.set_krylov(True)
     tune = cb.autotune([(s["nx"], s["ny"]) for s in scenes], iters=10, device=dev.index, coarse_direct=True)
     b.set_coarse_cells(tune["best"])
+    tt = cb.autotune_tiles([(s["nx"], s["ny"]) for s in scenes], iters=10, device=dev.index)
+    b.set_tiles(*tt["best"])
     b.set_stream(stream.cuda_stream)
     b.step(warmup)
     b.synchronize()
@@ -220,6 +222,7 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     # the same scenes, one by one, through the plain single-scene step (same solver, same tolerance)
     plain_ms, plain_cells = 0.0, 0
     best = {d: cb.autotune([d], iters=10, device=dev.index, coarse_direct=True)["best"] for d in BATCH_CLASSES}
+    best_tiles = {d: cb.autotune_tiles([d], iters=10, device=dev.index)["best"] for d in BATCH_CLASSES}
     for s in scenes:
         g = cb.FluidSim(dev.index, {"nx": s["nx"], "ny": s["ny"], "dt": s["dt"]}, width=0.8).init()
         load_scene(g, s)
@@ -227,6 +230,7 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
         g.set_coarse_solve("pipelined")
         g.set_krylov(True)
         g.set_coarse_cells(best[(s["nx"], s["ny"])])
+        g.set_tiles(*best_tiles[(s["nx"], s["ny"])])
         g.set_stream(stream.cuda_stream)
         g.step(warmup)
         g.synchronize()
@@ -243,7 +247,11 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     plain = plain_cells / (plain_ms / 1e3)
     return {"value": batched, "unit": METRIC, "scenes": len(scenes), "cells": cells, "steps": steps,
             "schedule": {"coarse_cells": tune["best"],
-                         "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}},
+                         "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()},
+                         "tiles": {"advect": cb.TILE_SHAPES[tt["best"][0]],
+                                   "diffuse_sources": cb.TILE_SHAPES[tt["best"][1]],
+                                   "forces": cb.TILE_SHAPES[tt["best"][2]],
+                                   "autotune_ms": {k: [round(x, 5) for x in v] for k, v in tt["ms"].items()}}},
             "ms_per_step": ms / steps, "launches_per_step": launches,
             "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": max_cycles,
                          "cycles_last_step": {"min": min(cyc), "max": max(cyc)}, "max_rel_residual": rel},
@@ -579,6 +587,12 @@ def measure_gpu(dev, stream, flush, workload: str, steps: int, warmup: int, laun
         sim.set_coarse_cells(tune["best"])
         schedule = {"coarse_cells": tune["best"],
                     "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()}}
+    # tile shapes of the advection, diffusion + sources and forces kernels (same bits for every shape)
+    tt = cb.autotune_tiles([(nx, ny)], iters=20, device=dev.index)
+    sim.set_tiles(*tt["best"])
+    schedule["tiles"] = {"advect": cb.TILE_SHAPES[tt["best"][0]], "diffuse_sources": cb.TILE_SHAPES[tt["best"][1]],
+                         "forces": cb.TILE_SHAPES[tt["best"][2]],
+                         "autotune_ms": {k: [round(x, 5) for x in v] for k, v in tt["ms"].items()}}
     sim.set_stream(stream.cuda_stream)
     sim.set_graphs(launch == "graph")
     sim.step(warmup)

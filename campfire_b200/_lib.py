@@ -146,6 +146,8 @@ def lib():
         "cfg_set_coarse_cluster": [vp, ci], "cfg_batch_set_coarse_cluster": [vp, ci],
         "cfg_autotune": [ci, ci, ip, ip, ci, ci, ip, ip, dp, ip],
         "cfg_set_coarse_solve": [vp, ci], "cfg_batch_set_coarse_solve": [vp, ci],
+        "cfg_set_tiles": [vp, ci, ci, ci], "cfg_batch_set_tiles": [vp, ci, ci, ci],
+        "cfg_autotune_tiles": [ci, ci, ip, ip, ci, ip, dp],
         "cfg_checkpoint_save": [vp, cs], "cfg_checkpoint_load": [vp, cs],
         "cfg_wood_piece_init": [ctypes.POINTER(CfgWoodPiece), cd, cd, cd],
         "cfg_wood_piece_preheat": [ctypes.POINTER(CfgWoodPiece), cd, cd, cd, cd],
@@ -154,6 +156,8 @@ def lib():
         "cfg_wood_add": [vp, cd, cd, cd, cd, cd, dp, dp, ip], "cfg_wood_remove": [vp, ci],
         "cfg_wood_frame": [vp, cd, ip], "cfg_wood_get": [vp, ci, ctypes.POINTER(CfgWoodPiece), dp, dp],
         "cfg_wood_stats": [vp, dp, dp, dp], "cfg_wood_render_data": [vp, fp],
+        "cfg_wood_set_readback_lag": [vp, ci],
+        "cfg_wood_readbacks": [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)],
         "cfg_render_defaults": [vp, ctypes.POINTER(CfgRenderParams)],
         "cfg_render": [vp, ctypes.POINTER(CfgRenderParams), fp, ci, ci, fp],
         "cfg_render_device": [vp, ctypes.POINTER(CfgRenderParams), fp, ci, ci, vp],

@@ -282,6 +282,29 @@ extern "C" int cfg_autotune(int device, int nscenes, const int* nx, const int* n
   });
 }
 
+extern "C" int cfg_set_tiles(cfg_sim* sim, int advect, int diffuse_sources, int forces) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->set_tiles(advect, diffuse_sources, forces); });
+}
+extern "C" int cfg_batch_set_tiles(cfg_batch* b, int advect, int diffuse_sources, int forces) {
+  if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
+  return guarded([&] { return b->eng->set_tiles(advect, diffuse_sources, forces); });
+}
+extern "C" int cfg_autotune_tiles(int device, int nscenes, const int* nx, const int* ny, int iters, int* best,
+                                  double* ms) {
+  if (nscenes < 1 || !nx || !ny || iters < 1 || !best) return cfg::fail(CFG_ERR_INVAL, "bad argument");
+  return guarded([&] {
+    std::vector<double> width(nscenes, 0.8), dt(nscenes, 0.002);
+    cfg::Engine eng;
+    CFG_TRY(eng.init(device, nscenes, nx, ny, width.data(), dt.data()));
+    for (int s = 0; s < nscenes; s++) CFG_TRY(cfg::load_generated_scene(eng, s, 0, 0.8, 1234 + s));
+    CFG_TRY(eng.set_solver(CFG_SOLVE_FP64, 1, 1e-6, 4));
+    CFG_TRY(eng.step(1));
+    CFG_TRY(eng.synchronize());
+    return eng.autotune_tiles(iters, best, ms);
+  });
+}
+
 extern "C" int cfg_set_coarse_solve(cfg_sim* sim, int direct) {
   SIM_OK(sim); OWNER_OK(sim);
   return guarded([&] { return sim->eng->set_coarse_solve(direct); });
@@ -398,7 +421,19 @@ int cfg_wood_create(cfg_sim* sim, double char_yield, double pyro_mult, cfg_wood*
   });
 }
 int cfg_wood_destroy(cfg_wood* w) {
+  // readbacks still on the ring are collected first, so the scene's ring is free again
+  const int rc = (w && w->scene) ? guarded([&] { return w->scene->set_readback_lag(0); }) : CFG_OK;
   delete w;
+  return rc;
+}
+int cfg_wood_set_readback_lag(cfg_wood* w, int lag) {
+  if (!w) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  return guarded([&] { return w->scene->set_readback_lag(lag); });
+}
+int cfg_wood_readbacks(cfg_wood* w, uint64_t* applied, uint64_t* skipped) {
+  if (!w) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  if (applied) *applied = w->scene->applied;
+  if (skipped) *skipped = w->scene->skipped;
   return CFG_OK;
 }
 int cfg_wood_add(cfg_wood* w, double x, double y, double angle, double side, double density, const double* preheat3,

@@ -165,6 +165,7 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   if (const char* v = std::getenv("CAMPFIRE_PDL")) set_pdl(v[0] != '0');
   CFG_CUDA(prepare_mg_coarse(coarse_smem_));
   CFG_CUDA(prepare_coarse_factor(cf_smem_));
+  CFG_CUDA(prepare_diffuse_sources());
   CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
   CFG_CUDA(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking));
@@ -464,9 +465,9 @@ int Engine::build_worklists() {
   };
   for (int s = 0; s < n; s++) {
     const Scene& sc = scenes_[s];
-    tiles(lists[WL_ADV], s, sc.nx, sc.ny, ADV_TX, ADV_TY);
-    tiles(lists[WL_DS], s, sc.nx, sc.ny, DS_TX, DS_TY);
-    tiles(lists[WL_FR], s, sc.nx, sc.ny, FR_TX, FR_TY);
+    tiles(lists[WL_ADV], s, sc.nx, sc.ny, TILE_TX[tiles_[TK_ADVECT]], TILE_TY[tiles_[TK_ADVECT]]);
+    tiles(lists[WL_DS], s, sc.nx, sc.ny, TILE_TX[tiles_[TK_DIFFSRC]], TILE_TY[tiles_[TK_DIFFSRC]]);
+    tiles(lists[WL_FR], s, sc.nx, sc.ny, TILE_TX[tiles_[TK_FORCES]], TILE_TY[tiles_[TK_FORCES]]);
     tiles(lists[WL_PR], s, sc.nx, sc.ny, PR_TX, PR_TY);
     tiles(lists[WL_GEO], s, sc.nx + 1, sc.ny + 1, GEO_TX, GEO_TY);
     tiles(lists[WL_MG0], s, sc.nx, sc.ny, MG_TX, MG_TY);
@@ -536,7 +537,66 @@ int Engine::set_coarse_cells(int cells) {
   return CFG_OK;
 }
 
+// Tile shapes of the advection, diffusion + sources and forces kernels (indices into
+// TILE_TX/TILE_TY): the work lists are rebuilt, and each scene's forces tile count (its
+// reduction's arrivals) follows. Every shape gives the same bits.
+int Engine::set_tiles(int advect, int diffsrc, int forces) {
+  for (int v : {advect, diffsrc, forces})
+    if (v < 0 || v >= kTileShapes) return fail(CFG_ERR_INVAL, "tile shape must be 0 (32x8), 1 (64x8) or 2 (32x16)");
+  CFG_TRY(activate());
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  tiles_[TK_ADVECT] = advect; tiles_[TK_DIFFSRC] = diffsrc; tiles_[TK_FORCES] = forces;
+  const int tx = TILE_TX[forces], ty = TILE_TY[forces];
+  for (int s = 0; s < nscenes(); s++) {
+    Scene& sc = scenes_[s];
+    sc.desc.nt_fr = ((sc.nx + tx - 1) / tx) * ((sc.ny + ty - 1) / ty);
+    // only the tile count changes: the device's parameter block (a CFL step's dt) stays
+    CFG_CUDA(cudaMemcpyAsync(&d_scenes_[s].nt_fr, &sc.desc.nt_fr, sizeof(int), cudaMemcpyHostToDevice, st()));
+  }
+  for (int k = 0; k < WL_COUNT; k++) {
+    if (d_wl_[k]) cudaFree(d_wl_[k]);
+    d_wl_[k] = nullptr;
+    nwl_[k] = 0;
+  }
+  CFG_TRY(build_worklists());
+  graph_dirty_ = true;
+  CFG_CUDA(cudaStreamSynchronize(st()));
+  return CFG_OK;
+}
+
+// The autotuner of the tile shapes: each of the three kernels is timed (`iters` launches
+// back to back, CUDA events on the stream) under every shape on the current state, and the
+// fastest shapes are kept. The kernels rewrite their outputs as they run, so the state
+// changes (use a scratch scene); ms[k * kTileShapes + s]: kernel k, shape s.
+int Engine::autotune_tiles(int iters, int* best, double* ms) {
+  if (iters < 1 || !best) return fail(CFG_ERR_INVAL, "bad argument");
+  const int keep[TK_COUNT] = {tiles_[0], tiles_[1], tiles_[2]};
+  const char* names[TK_COUNT] = {"advect", "diffuse_sources", "forces"};
+  double tbest[TK_COUNT] = {1e300, 1e300, 1e300};
+  for (int k = 0; k < TK_COUNT; k++) best[k] = keep[k];
+  for (int shape = 0; shape < kTileShapes; shape++) {
+    CFG_TRY(set_tiles(shape, shape, shape));
+    for (int k = 0; k < TK_COUNT; k++) {
+      double t = 0, b = 0, n = 0;
+      CFG_TRY(time_kernel(names[k], iters, &t, &b, &n));
+      if (ms) ms[k * kTileShapes + shape] = t;
+      if (t < tbest[k]) { tbest[k] = t; best[k] = shape; }
+    }
+  }
+  return set_tiles(best[0], best[1], best[2]);
+}
+
 int Engine::upload_desc(int s) {
+  // a CFL step the device owns survives a full descriptor upload
+  Scene& sc = scenes_[s];
+  if (sc.dt_on_device && sc.cfl > 0) {
+    SceneDesc dev;
+    CFG_CUDA(cudaMemcpyAsync(&dev, d_scenes_ + s, kDescParamBytes, cudaMemcpyDeviceToHost, st()));
+    CFG_CUDA(cudaStreamSynchronize(st()));
+    sc.desc.P.dt = dev.P.dt; sc.desc.diff_sub = dev.diff_sub; sc.desc.diff_dt = dev.diff_dt;
+    sc.P.dt = dev.P.dt; sc.diff_sub = dev.diff_sub; sc.diff_dt = dev.diff_dt;
+    sc.dtd = (double)dev.P.dt;
+  }
   dt_from_step_ = false;
   CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &scenes_[s].desc, sizeof(SceneDesc), cudaMemcpyHostToDevice, st()));
   return CFG_OK;
@@ -1039,9 +1099,9 @@ int Engine::set_solver(int mode, int ncycles, double tol, int max_cycles) {
 
 void Engine::enqueue_pre_solve(cudaStream_t s, unsigned long long h, int use_cond) {
   const bool fp64 = any_fp64();
-  launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s); launches_++;
-  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, s); launches_++;
-  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); launches_++;
+  launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], tiles_[TK_ADVECT], s); launches_++;
+  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, tiles_[TK_DIFFSRC], s); launches_++;
+  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, tiles_[TK_FORCES], s); launches_++;
   // the levels below the forces kernel's in-tile restriction, one block per scene
   if (FR_KMAX + 1 < max_levels()) { launch_coef_restrict_tail(d_scenes_, nscenes(), FR_KMAX, s); launches_++; }
   enqueue_factor(s);
@@ -1383,15 +1443,15 @@ int Engine::step_profiled(float* ms) {
   cudaEvent_t ev[8];
   for (auto& e : ev) CFG_CUDA(cudaEventCreate(&e));
   CFG_CUDA(cudaEventRecord(ev[0], s));
-  launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s);
+  launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], tiles_[TK_ADVECT], s);
   CFG_CUDA(cudaEventRecord(ev[1], s));
-  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), false, true, s);
+  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), false, true, tiles_[TK_DIFFSRC], s);
   CFG_CUDA(cudaEventRecord(ev[2], s));
-  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], 1, true, false, s);
+  launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], 1, true, false, tiles_[TK_DIFFSRC], s);
   CFG_CUDA(cudaEventRecord(ev[3], s));
-  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, false, any_fp64(), s);
+  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, false, any_fp64(), tiles_[TK_FORCES], s);
   CFG_CUDA(cudaEventRecord(ev[4], s));
-  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, false, true, any_fp64(), s);
+  launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, false, true, any_fp64(), tiles_[TK_FORCES], s);
   for (int l = FR_KMAX; l + 1 < max_levels(); l++)
     launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   CFG_CUDA(cudaEventRecord(ev[5], s));
@@ -1417,13 +1477,13 @@ int Engine::run_stage(const char* stage) {
   const std::string st_(stage);
   cudaStream_t s = st();
   const bool fp64 = any_fp64();
-  if (st_ == "advect") launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s);
-  else if (st_ == "diffuse") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), false, true, s);
-  else if (st_ == "sources") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], 1, true, false, s);
-  else if (st_ == "diffuse_sources") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, s);
-  else if (st_ == "forces") launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, false, fp64, s);
+  if (st_ == "advect") launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], tiles_[TK_ADVECT], s);
+  else if (st_ == "diffuse") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), false, true, tiles_[TK_DIFFSRC], s);
+  else if (st_ == "sources") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], 1, true, false, tiles_[TK_DIFFSRC], s);
+  else if (st_ == "diffuse_sources") launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, tiles_[TK_DIFFSRC], s);
+  else if (st_ == "forces") launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, false, fp64, tiles_[TK_FORCES], s);
   else if (st_ == "coef_rhs") {
-    launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, false, true, fp64, s);
+    launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, false, true, fp64, tiles_[TK_FORCES], s);
     for (int l = FR_KMAX; l + 1 < max_levels(); l++)
       launch_coef_restrict(d_scenes_, d_wl_[WL_MGC0 + l], nwl_[WL_MGC0 + l], l, s);
   } else if (st_ == "pressure") {
@@ -1456,12 +1516,12 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   const std::string n(name);
   std::function<void(int)> go;
   double b = 0, cnt = 1;
-  if (n == "advect") { go = [&](int) { launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], s); }; b = 156 * cells; }
+  if (n == "advect") { go = [&](int) { launch_advect(d_scenes_, d_wl_[WL_ADV], nwl_[WL_ADV], tiles_[TK_ADVECT], s); }; b = 156 * cells; }
   else if (n == "diffuse_sources") {
-    go = [&](int) { launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, s); };
+    go = [&](int) { launch_diffuse_sources(d_scenes_, d_wl_[WL_DS], nwl_[WL_DS], max_sub(), true, true, tiles_[TK_DIFFSRC], s); };
     b = (48.0 * sc.diff_sub + 68) * cells;
   } else if (n == "forces") {
-    go = [&](int) { launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, s); };
+    go = [&](int) { launch_forces(d_scenes_, d_wl_[WL_FR], nwl_[WL_FR], d_ctl_, true, true, fp64, tiles_[TK_FORCES], s); };
     b = (28 + 20 + 28 + 13.3) * cells;
   } else if (n == "relax0") {
     go = [&](int k) { launch_relax(d_scenes_, d_wl_[WL_MGV0], nwl_[WL_MGV0], 0, k & 1, s); };

@@ -162,9 +162,18 @@ class Engine {
   int set_coarse_solve(int direct);
   // FP64 mode: flexible preconditioned CG around the V-cycle (1) or plain defect correction (0)
   int set_krylov(int on);
+  // tile shapes of the advection, diffusion + sources and forces kernels (TILE_TX/TILE_TY index)
+  int set_tiles(int advect, int diffsrc, int forces);
+  int tiles(int k) const { return tiles_[k]; }
+  // times every shape of the three kernels on the current state and keeps the fastest
+  int autotune_tiles(int iters, int* best, double* ms);
   int scene_lc(int s) const { return scenes_[s].lc; }
   size_t arena_bytes(int s) const { return scenes_[s].arena_bytes; }
   int scene_nx(int s) const { return scenes_[s].nx; }
+  // the host's dt and frame counter of a scene, read without touching the device (a CFL scene's
+  // dt is the last one the host has seen)
+  double host_dt(int s) const { return scenes_[s].dtd; }
+  uint32_t host_frame(int s) const { return scenes_[s].frame; }
   int scene_ny(int s) const { return scenes_[s].ny; }
   cudaStream_t stream() const { return st(); }
   int nscenes() const { return (int)scenes_.size(); }
@@ -251,6 +260,7 @@ class Engine {
   int coarse_cells_ = COARSE_CELLS;
   int coarse_direct_ = 0;
   int krylov_ = 0;
+  int tiles_[TK_COUNT] = {0, 0, 0};       // tile shape of advection, diffusion + sources, forces
   unsigned long long cond_handle_ = 0;   // the step graph's WHILE-node handle
   int ctl_use_cond_ = 0;                 // SolveCtl::use_cond on the device (-1: stale)
   int set_cond_mode(bool graph);

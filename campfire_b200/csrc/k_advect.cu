@@ -183,8 +183,12 @@ __global__ void __launch_bounds__(256) k_advect(const SceneDesc* __restrict__ sc
   }
 }
 
-void launch_advect(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st) {
-  if (ntiles > 0) k_advect<ADV_TX, ADV_TY, ADV_H><<<ntiles, 256, 0, st>>>(scenes, work);
+void launch_advect(const SceneDesc* scenes, const Work* work, int ntiles, int shape, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  static_assert(TILE_TX[0] == ADV_TX && TILE_TY[0] == ADV_TY, "shape 0 is the default tile");
+  if (shape == 1) k_advect<TILE_TX[1], TILE_TY[1], ADV_H><<<ntiles, 256, 0, st>>>(scenes, work);
+  else if (shape == 2) k_advect<TILE_TX[2], TILE_TY[2], ADV_H><<<ntiles, 256, 0, st>>>(scenes, work);
+  else k_advect<ADV_TX, ADV_TY, ADV_H><<<ntiles, 256, 0, st>>>(scenes, work);
 }
 
 }  // namespace cfg

@@ -140,8 +140,11 @@ __device__ __forceinline__ SrcOut sources_cell(const SceneDesc& S, const cfg_par
 template <int TX, int TY, int NMAX, bool SOURCES, bool DIFFUSION>
 __global__ void __launch_bounds__(256) k_diffuse_sources(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work) {
   constexpr int RW = TX + 2 * NMAX, RH = TY + 2 * NMAX;
-  __shared__ float sT[2][RH * RW];
-  __shared__ float4 sY[2][RH * RW];
+  // the ping-pong state of tile + halo in dynamic shared memory (ds_smem_bytes: above 48 KB for
+  // the larger tiles at 5 sub-steps)
+  extern __shared__ __align__(16) unsigned char ds_smem[];
+  float4 (*sY)[RH * RW] = reinterpret_cast<float4 (*)[RH * RW]>(ds_smem);
+  float (*sT)[RH * RW] = reinterpret_cast<float (*)[RH * RW]>(ds_smem + 2 * RH * RW * sizeof(float4));
   __shared__ float rq[TY * TX], rr[TY * TX], rt[TY * TX];
 
   const Work w = work[blockIdx.x];
@@ -246,22 +249,60 @@ __global__ void __launch_bounds__(256) k_diffuse_sources(const SceneDesc* __rest
   }
 }
 
-void launch_diffuse_sources(const SceneDesc* scenes, const Work* work, int ntiles, int max_sub, bool with_sources,
+template <int TX, int TY, int NMAX>
+constexpr size_t ds_smem_bytes() { return (size_t)2 * (TX + 2 * NMAX) * (TY + 2 * NMAX) * (sizeof(float4) + sizeof(float)); }
+
+template <int TX, int TY, int NMAX, bool SRC, bool DIF>
+static void ds_launch(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st) {
+  k_diffuse_sources<TX, TY, NMAX, SRC, DIF><<<ntiles, 256, ds_smem_bytes<TX, TY, NMAX>(), st>>>(scenes, work);
+}
+template <int TX, int TY>
+static void ds_launch_shape(const SceneDesc* scenes, const Work* work, int ntiles, int max_sub, bool with_sources,
                             bool with_diffusion, cudaStream_t st) {
-  if (ntiles <= 0) return;
-  if (!with_diffusion) {
-    k_diffuse_sources<DS_TX, DS_TY, 1, true, false><<<ntiles, 256, 0, st>>>(scenes, work);
-    return;
-  }
+  if (!with_diffusion) { ds_launch<TX, TY, 1, true, false>(scenes, work, ntiles, st); return; }
   if (with_sources) {
-    if (max_sub <= 1) k_diffuse_sources<DS_TX, DS_TY, 1, true, true><<<ntiles, 256, 0, st>>>(scenes, work);
-    else if (max_sub <= 3) k_diffuse_sources<DS_TX, DS_TY, 3, true, true><<<ntiles, 256, 0, st>>>(scenes, work);
-    else k_diffuse_sources<DS_TX, DS_TY, 5, true, true><<<ntiles, 256, 0, st>>>(scenes, work);
+    if (max_sub <= 1) ds_launch<TX, TY, 1, true, true>(scenes, work, ntiles, st);
+    else if (max_sub <= 3) ds_launch<TX, TY, 3, true, true>(scenes, work, ntiles, st);
+    else ds_launch<TX, TY, 5, true, true>(scenes, work, ntiles, st);
   } else {
-    if (max_sub <= 1) k_diffuse_sources<DS_TX, DS_TY, 1, false, true><<<ntiles, 256, 0, st>>>(scenes, work);
-    else if (max_sub <= 3) k_diffuse_sources<DS_TX, DS_TY, 3, false, true><<<ntiles, 256, 0, st>>>(scenes, work);
-    else k_diffuse_sources<DS_TX, DS_TY, 5, false, true><<<ntiles, 256, 0, st>>>(scenes, work);
+    if (max_sub <= 1) ds_launch<TX, TY, 1, false, true>(scenes, work, ntiles, st);
+    else if (max_sub <= 3) ds_launch<TX, TY, 3, false, true>(scenes, work, ntiles, st);
+    else ds_launch<TX, TY, 5, false, true>(scenes, work, ntiles, st);
   }
+}
+template <int TX, int TY, int NMAX>
+static cudaError_t ds_allow_smem() {
+  const int b = (int)ds_smem_bytes<TX, TY, NMAX>();
+  cudaError_t e = cudaSuccess;
+  for (cudaError_t x : {cudaFuncSetAttribute(k_diffuse_sources<TX, TY, NMAX, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b),
+                        cudaFuncSetAttribute(k_diffuse_sources<TX, TY, NMAX, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b),
+                        cudaFuncSetAttribute(k_diffuse_sources<TX, TY, NMAX, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)})
+    if (x != cudaSuccess && e == cudaSuccess) e = x;
+  return e;
+}
+template <int TX, int TY>
+static cudaError_t ds_allow_shape() {
+  cudaError_t e = ds_allow_smem<TX, TY, 1>();
+  if (e == cudaSuccess) e = ds_allow_smem<TX, TY, 3>();
+  if (e == cudaSuccess) e = ds_allow_smem<TX, TY, 5>();
+  return e;
+}
+
+// the dynamic shared memory every instantiation may use (once per device, before any launch)
+cudaError_t prepare_diffuse_sources() {
+  static_assert(TILE_TX[0] == DS_TX && TILE_TY[0] == DS_TY, "shape 0 is the default tile");
+  cudaError_t e = ds_allow_shape<TILE_TX[0], TILE_TY[0]>();
+  if (e == cudaSuccess) e = ds_allow_shape<TILE_TX[1], TILE_TY[1]>();
+  if (e == cudaSuccess) e = ds_allow_shape<TILE_TX[2], TILE_TY[2]>();
+  return e;
+}
+
+void launch_diffuse_sources(const SceneDesc* scenes, const Work* work, int ntiles, int max_sub, bool with_sources,
+                            bool with_diffusion, int shape, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  if (shape == 1) ds_launch_shape<TILE_TX[1], TILE_TY[1]>(scenes, work, ntiles, max_sub, with_sources, with_diffusion, st);
+  else if (shape == 2) ds_launch_shape<TILE_TX[2], TILE_TY[2]>(scenes, work, ntiles, max_sub, with_sources, with_diffusion, st);
+  else ds_launch_shape<DS_TX, DS_TY>(scenes, work, ntiles, max_sub, with_sources, with_diffusion, st);
 }
 
 }  // namespace cfg

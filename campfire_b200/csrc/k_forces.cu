@@ -200,12 +200,20 @@ __global__ void __launch_bounds__(256) k_forces(const SceneDesc* __restrict__ sc
   }
 }
 
+template <int TX, int TY>
+static void launch_forces_t(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool forces,
+                            bool coef_rhs, bool fp64, cudaStream_t st) {
+  if (forces && coef_rhs) k_forces<TX, TY, true, true><<<ntiles, 256, 0, st>>>(scenes, work, ctl, fp64 ? 1 : 0);
+  else if (forces) k_forces<TX, TY, true, false><<<ntiles, 256, 0, st>>>(scenes, work, ctl, fp64 ? 1 : 0);
+  else if (coef_rhs) k_forces<TX, TY, false, true><<<ntiles, 256, 0, st>>>(scenes, work, ctl, fp64 ? 1 : 0);
+}
 void launch_forces(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool forces, bool coef_rhs,
-                   bool fp64, cudaStream_t st) {
+                   bool fp64, int shape, cudaStream_t st) {
   if (ntiles <= 0) return;
-  if (forces && coef_rhs) k_forces<FR_TX, FR_TY, true, true><<<ntiles, 256, 0, st>>>(scenes, work, ctl, fp64 ? 1 : 0);
-  else if (forces) k_forces<FR_TX, FR_TY, true, false><<<ntiles, 256, 0, st>>>(scenes, work, ctl, fp64 ? 1 : 0);
-  else if (coef_rhs) k_forces<FR_TX, FR_TY, false, true><<<ntiles, 256, 0, st>>>(scenes, work, ctl, fp64 ? 1 : 0);
+  static_assert(TILE_TX[0] == FR_TX && TILE_TY[0] == FR_TY, "shape 0 is the default tile");
+  if (shape == 1) launch_forces_t<TILE_TX[1], TILE_TY[1]>(scenes, work, ntiles, ctl, forces, coef_rhs, fp64, st);
+  else if (shape == 2) launch_forces_t<TILE_TX[2], TILE_TY[2]>(scenes, work, ntiles, ctl, forces, coef_rhs, fp64, st);
+  else launch_forces_t<FR_TX, FR_TY>(scenes, work, ntiles, ctl, forces, coef_rhs, fp64, st);
 }
 
 }  // namespace cfg

@@ -12,6 +12,15 @@ namespace cfg {
 constexpr int ADV_TX = 32, ADV_TY = 8, ADV_H = 2;    // advection (halo for |displacement| < 2 cells)
 constexpr int DS_TX = 32, DS_TY = 8;                 // diffusion + sources
 constexpr int FR_TX = 32, FR_TY = 8;                 // forces + coef + rhs0 (+ coefficient hierarchy)
+// Tile shapes the advection, diffusion + sources and forces kernels can run with (the
+// defaults above are shape 0). Every shape gives the same bits: each cell's arithmetic does
+// not depend on its tile, and the 8x8 blocks of the heat-release reduction stay whole.
+constexpr int kTileShapes = 3;
+constexpr int TILE_TX[kTileShapes] = {32, 64, 32}, TILE_TY[kTileShapes] = {8, 8, 16};
+enum TileKernel { TK_ADVECT = 0, TK_DIFFSRC, TK_FORCES, TK_COUNT };
+// diffusion + sources keeps its tile and halo state in dynamic shared memory (up to ~53 KB):
+// allowed once per device before the first launch
+cudaError_t prepare_diffuse_sources();
 constexpr int FR_KMAX = 3;                           // coarse coefficient levels built inside FR tiles
 constexpr int MG_TX = 32, MG_TY = 8;                 // single-pass multigrid kernels
 constexpr int MGF_TX = 32, MGF_TY = 16;              // fused (temporally blocked) multigrid kernels
@@ -56,13 +65,14 @@ bool pdl_enabled();
 // Work-list kinds (tiles per scene are built by the engine)
 enum WorkKind { WK_ADV, WK_DS, WK_FR, WK_PR, WK_GEO, WK_MG0 };
 
-void launch_advect(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
+// shape: an index into TILE_TX/TILE_TY, the shape the work list was built with
+void launch_advect(const SceneDesc* scenes, const Work* work, int ntiles, int shape, cudaStream_t st);
 // diffusion sub-steps (diff_sub of each scene) fused with the sources pass
 void launch_diffuse_sources(const SceneDesc* scenes, const Work* work, int ntiles, int max_sub,
-                            bool with_sources, bool with_diffusion, cudaStream_t st);
+                            bool with_sources, bool with_diffusion, int shape, cudaStream_t st);
 // forces (+ coef + rhs0 + coefficient levels 1..FR_KMAX + ||rhs|| reduction)
 void launch_forces(const SceneDesc* scenes, const Work* work, int ntiles, SolveCtl* ctl, bool forces,
-                   bool coef_rhs, bool fp64, cudaStream_t st);
+                   bool coef_rhs, bool fp64, int shape, cudaStream_t st);
 // coefficient restriction of level l -> l+1 for levels the FR tiles did not build
 void launch_coef_restrict(const SceneDesc* scenes, const Work* work, int ntiles, int level, cudaStream_t st);
 // single-pass multigrid (pressure.wgsl:87-129)

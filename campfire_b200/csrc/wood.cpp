@@ -176,6 +176,7 @@ int WoodScene::add(double x, double y, double angle, double side, double density
   WoodSlot& p = slots_[slot];
   p = WoodSlot{};
   p.used = true;
+  p.serial = next_serial_++;
   p.x = x; p.y = y; p.angle = angle;
   p.wood = WoodPiece(side, density);
   if (preheat3) p.wood.preheat(preheat3[0], preheat3[1], preheat3[2], ctl_.charYield);
@@ -259,13 +260,63 @@ int WoodScene::upload() {
 }
 
 int WoodScene::readback(double sim_dt) {
+  if (lag_ != 0) {
+    // encodeReadback + afterSubmit with the frame's tag {simDt, owners} (js/main.js:281-283)
+    Pending pd;
+    pd.simDt = sim_dt;
+    for (int s = 0; s < (int)slots_.size(); s++) pd.owners[s] = slots_[s].used ? slots_[s].serial : 0;
+    const uint64_t tag = next_tag_++;
+    const int rc = eng_->readback_begin(scene_, tag, nullptr);
+    if (rc == CFG_ERR_BUSY) { skipped++; return CFG_OK; }
+    CFG_TRY(rc);
+    pending_.emplace_back(tag, pd);
+    return CFG_OK;
+  }
   std::vector<int32_t> acc(ACC_LEN), faceW(MAX_PIECES * 4);
   std::vector<float> radv((size_t)RAD_LEN * 4);
   CFG_TRY(eng_->readback(scene_, acc.data(), radv.data(), faceW.data()));
-  if (sim_dt <= 0) return CFG_OK;
+  apply(acc.data(), radv.data(), faceW.data(), sim_dt, nullptr);
+  return CFG_OK;
+}
+
+// the readbacks in flight, oldest first: those with tags <= wait_upto are waited for, the
+// rest taken only if they have arrived (never, for a fixed lag: they wait their turn)
+int WoodScene::collect(uint64_t wait_upto) {
+  std::vector<int32_t> acc(ACC_LEN), faceW(MAX_PIECES * 4);
+  std::vector<float> radv((size_t)RAD_LEN * 4);
+  while (!pending_.empty()) {
+    const bool wait = pending_.front().first <= wait_upto;
+    if (!wait && lag_ > 0) return CFG_OK;
+    uint64_t tag = 0;
+    int ready = 0;
+    CFG_TRY(eng_->readback_collect(scene_, wait, acc.data(), radv.data(), faceW.data(), &tag, &ready));
+    if (!ready) return CFG_OK;
+    auto it = pending_.begin();
+    while (it != pending_.end() && it->first != tag) ++it;
+    if (it == pending_.end()) return fail(CFG_ERR_INVAL, "a readback arrived with an unknown tag");
+    const Pending pd = it->second;
+    pending_.erase(it);
+    apply(acc.data(), radv.data(), faceW.data(), pd.simDt, pd.owners.data());
+    applied++;
+  }
+  return CFG_OK;
+}
+
+int WoodScene::set_readback_lag(int lag) {
+  if (lag > 3) return fail(CFG_ERR_INVAL, "readback lag must be at most 3 frames (the ring's slots)");
+  if (!pending_.empty()) CFG_TRY(collect(~0ull));   // deliver what is in flight before switching
+  lag_ = lag < 0 ? -1 : lag;
+  return CFG_OK;
+}
+
+// onReadback (js/main.js:210-230): owners = the serials of the pieces that held the slots when
+// the readback's frame ran (null: the current ones)
+void WoodScene::apply(const int32_t* acc, const float* radv, const int32_t* faceW, double sim_dt,
+                      const uint64_t* owners) {
+  if (sim_dt <= 0) return;
   for (int s = 0; s < (int)slots_.size(); s++) {
     WoodSlot& p = slots_[s];
-    if (!p.used) continue;
+    if (!p.used || (owners && owners[s] != p.serial)) continue;
     for (int f = 0; f < 4; f++) {
       // share of the face that touches gas: none where it rests on the floor or another piece
       p.wood.exposure[f] = std::min(1.0, faceW[s * 4 + f] / 1e8 / std::max(p.wood.side, 1e-4));
@@ -279,20 +330,23 @@ int WoodScene::readback(double sim_dt) {
   hrr = acc[ACC_GLOBAL] / G_SCALE / sim_dt;
   rad = acc[ACC_GLOBAL + 1] / G_SCALE / sim_dt;
   tmax = acc[ACC_GLOBAL + 2];
-  return CFG_OK;
 }
 
 int WoodScene::frame(double sim_dt, int* nsteps) {
   if (!(sim_dt >= 0)) return fail(CFG_ERR_INVAL, "frame time must be >= 0");
-  cfg_info inf;
-  CFG_TRY(eng_->info(scene_, &inf));
-  const double dt = inf.dt;
+  // dt and the frame counter from the host side: a frame does not wait for the device
+  const double dt = eng_->host_dt(scene_);
+  const uint32_t frame_no = eng_->host_frame(scene_);
   // gas steps for this frame, capped at ceil(0.034 / dt) (js/main.js:252-257)
   sim_acc_ += sim_dt;
   const int maxSteps = (int)std::ceil(0.034 / dt);
   int n = (int)std::floor(sim_acc_ / dt);
   if (n > maxSteps) { n = maxSteps; sim_acc_ = 0; } else sim_acc_ -= n * dt;
   const double simDt = n * dt;
+  // readbacks of earlier frames, applied before this frame starts (the reference's callbacks run
+  // between frames; the tag of frame f is f + 1): with a fixed lag the one of the frame `lag`
+  // back, waited for; otherwise whatever has arrived
+  if (lag_ != 0) CFG_TRY(collect(lag_ > 0 && next_tag_ > (uint64_t)lag_ ? next_tag_ - (uint64_t)lag_ : 0));
   // the bodies move and touching pieces exchange heat (:262-263; the simulation runs, so
   // the rigid world advances by the frame's gas time)
   if (world_) {
@@ -323,7 +377,7 @@ int WoodScene::frame(double sim_dt, int* nsteps) {
   CFG_TRY(eng_->geometry(scene_));
   CFG_TRY(eng_->step(n));
   CFG_TRY(eng_->radiation(scene_));
-  CFG_TRY(eng_->set_frame(scene_, inf.frame + 1));
+  CFG_TRY(eng_->set_frame(scene_, frame_no + 1));
   if (nsteps) *nsteps = n;
   return readback(simDt);
 }

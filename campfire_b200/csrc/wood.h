@@ -44,6 +44,7 @@ struct WoodPiece {
 // wood; moving: a body of the scene's rigid world)
 struct WoodSlot {
   bool used = false;
+  uint64_t serial = 0;              // which piece holds the slot (a readback applies only to it)
   double x = 0, y = 0, angle = 0;
   int body = 0;                     // rigid body id (moving pieces), 0 when frozen
   WoodPiece wood;
@@ -72,10 +73,29 @@ class WoodScene {
   // the renderer's wood buffer built with the last upload (main.js:188-207): 64 x {Tp[4], d[4],
   // char fraction, Tcore, mean visible irradiance, has virgin wood}
   const std::vector<float>& render_wood() const { return render_wood_; }
+  // How a frame's readback reaches the wood. lag 0 (default): synchronously at the end of the
+  // frame. Otherwise the reference's way (encodeReadback + afterSubmit, js/fluid.js:315-342, with
+  // onReadback's tag, js/main.js:210-230): the frame enqueues its readback on the ring with a tag
+  // holding its gas time and the pieces that held the slots, and readbacks are applied at the
+  // start of later frames, before the wood steps, to those pieces only. lag < 0: whatever has
+  // arrived, never waiting (the reference; a frame whose ring slot is still pending skips its
+  // readback, and acc keeps accumulating); lag 1..3: the readback of the frame `lag` frames back,
+  // waited for (a fixed pipeline depth, the same from run to run; the ring never fills).
+  int set_readback_lag(int lag);
+  int readback_lag() const { return lag_; }
+  uint64_t applied = 0, skipped = 0;   // readbacks applied and skipped (lag != 0)
 
  private:
   int upload();
   int readback(double sim_dt);
+  // one readback's data applied with its frame's gas time to the pieces that still hold their slots
+  void apply(const int32_t* acc, const float* radv, const int32_t* faceW, double sim_dt, const uint64_t* owners);
+  // apply the readbacks that have arrived (wait_upto > 0: wait for every tag <= wait_upto first)
+  int collect(uint64_t wait_upto);
+  struct Pending { double simDt; std::array<uint64_t, 64> owners; };
+  int lag_ = 0;
+  uint64_t next_serial_ = 1, next_tag_ = 1;
+  std::vector<std::pair<uint64_t, Pending>> pending_;   // tags in flight on the ring
   Engine* eng_;
   int scene_;
   WoodCtl ctl_;

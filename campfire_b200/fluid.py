@@ -272,6 +272,10 @@ class FluidSim(_SceneOps):
         """FP64 mode: preconditioned CG around the V-cycle (True) or plain defect correction (False)."""
         check(_lib.lib().cfg_set_krylov(self._h, 1 if on else 0))
 
+    def set_tiles(self, advect: int, diffuse_sources: int, forces: int):
+        """Tile shapes (TILE_SHAPES indices) of the advection, diffusion + sources and forces kernels."""
+        check(_lib.lib().cfg_set_tiles(self._h, advect, diffuse_sources, forces))
+
     def set_solver(self, mode: int = _lib.SOLVE_FIXED, ncycles: int = 1, tol: float = 1e-6, max_cycles: int = 50):
         check(_lib.lib().cfg_set_solver(self._h, mode, ncycles, tol, max_cycles))
 
@@ -345,6 +349,9 @@ class Batch:
 
     def set_krylov(self, on: bool):
         check(_lib.lib().cfg_batch_set_krylov(self._h, 1 if on else 0))
+
+    def set_tiles(self, advect: int, diffuse_sources: int, forces: int):
+        check(_lib.lib().cfg_batch_set_tiles(self._h, advect, diffuse_sources, forces))
 
     def set_active(self, i: int, on: bool):
         check(_lib.lib().cfg_batch_set_active(self._h, i, 1 if on else 0))
@@ -473,6 +480,23 @@ def autotune(dims, iters: int = 20, device: int = 0, coarse_direct: bool = False
     check(_lib.lib().cfg_autotune(device, n, nx, ny, 1 if coarse_direct else 0, iters, ctypes.byref(best), cells, ms,
                                   ctypes.byref(k)))
     return {"best": best.value, "ms_per_cycle": {cells[i]: ms[i] for i in range(k.value)}}
+
+
+TILE_SHAPES = ((32, 8), (64, 8), (32, 16))
+
+
+def autotune_tiles(dims, iters: int = 20, device: int = 0) -> dict:
+    """Time the advection, diffusion + sources and forces kernels under every tile shape on a scratch
+    batch of these sizes (cfg_autotune_tiles); {"best": (advect, diffuse_sources, forces) shape indices,
+    "ms": {kernel: [ms per shape]}}."""
+    n = len(dims)
+    nx = (ctypes.c_int * n)(*[d[0] for d in dims])
+    ny = (ctypes.c_int * n)(*[d[1] for d in dims])
+    best = (ctypes.c_int * 3)()
+    ms = (ctypes.c_double * 9)()
+    check(_lib.lib().cfg_autotune_tiles(device, n, nx, ny, iters, best, ms))
+    names = ("advect", "diffuse_sources", "forces")
+    return {"best": tuple(best), "ms": {k: [ms[i * 3 + s] for s in range(3)] for i, k in enumerate(names)}}
 
 
 def generate_scene(kind: int, nx: int, ny: int, width: float = 0.8, seed: int = 1234) -> dict:

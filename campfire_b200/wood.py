@@ -108,6 +108,16 @@ class WoodScene:
         check(_lib.lib().cfg_wood_frame(self._h, sim_dt, ctypes.byref(n)))
         return n.value
 
+    def set_readback_lag(self, lag: int):
+        """0: synchronous readback; < 0: through the ring, applied when arrived (the reference);
+        1..3: applied exactly `lag` frames later (cfg_wood_set_readback_lag)."""
+        check(_lib.lib().cfg_wood_set_readback_lag(self._h, lag))
+
+    def readbacks(self) -> dict:
+        a, k = ctypes.c_uint64(), ctypes.c_uint64()
+        check(_lib.lib().cfg_wood_readbacks(self._h, ctypes.byref(a), ctypes.byref(k)))
+        return {"applied": a.value, "skipped": k.value}
+
     def piece(self, slot: int):
         """(state dict, qConv[4], qInc[4]) or None for an empty slot."""
         st = CfgWoodPiece()

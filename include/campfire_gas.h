@@ -231,6 +231,17 @@ int cfg_batch_set_krylov(cfg_batch* b, int on);
 int cfg_autotune(int device, int nscenes, const int* nx, const int* ny, int coarse_direct, int iters,
                  int* best_cells, int* cand_cells, double* cand_ms, int* ncand);
 
+/* Tile shapes of the advection, diffusion + sources and forces kernels (no counterpart in the
+ * reference, whose workgroups are 8x8): 0 = 32x8 cells (default), 1 = 64x8, 2 = 32x16. Every
+ * shape gives the same bits; only the time changes. Batch views: use cfg_batch_set_tiles. */
+int cfg_set_tiles(cfg_sim* sim, int advect, int diffuse_sources, int forces);
+int cfg_batch_set_tiles(cfg_batch* b, int advect, int diffuse_sources, int forces);
+/* Autotuner of those shapes (no counterpart in the reference): builds a scratch batch of these
+ * sizes on `device` with generated scenes, runs one step, then times `iters` launches of each
+ * kernel under each shape; best[3] receives the fastest shape of advection, diffusion + sources
+ * and forces, ms[k * 3 + s] (may be NULL) kernel k's mean time under shape s. */
+int cfg_autotune_tiles(int device, int nscenes, const int* nx, const int* ny, int iters, int* best, double* ms);
+
 /* Checkpoint / resume of one scene (no counterpart in the reference, which only resets,
  * js/fluid.js:162-176): every state array of the scene (fields, advected copies, sources,
  * geometry, pressure levels, FP64 pressure, accumulators, pieces), its host clock, dt and
@@ -294,6 +305,17 @@ int cfg_wood_add(cfg_wood* w, double x, double y, double angle, double side, dou
 int cfg_wood_remove(cfg_wood* w, int slot);
 /* one frame with `sim_dt` seconds of gas time (js/main.js:247-283); *nsteps gas steps run */
 int cfg_wood_frame(cfg_wood* w, double sim_dt, int* nsteps);
+/* How each frame's readback reaches the wood. lag 0 (default): synchronously at the end of the
+ * frame. Otherwise as the reference does it (encodeReadback + afterSubmit, js/fluid.js:315-342,
+ * and onReadback's tag, js/main.js:210-230): enqueued on the readback ring with the frame's gas
+ * time and the pieces that held the slots, and applied at the start of a later frame, before the
+ * wood steps, only to those pieces. lag < 0: whatever has arrived, never waiting (a frame whose
+ * ring slot is still pending skips its readback); lag 1..3: exactly the readback of the frame
+ * `lag` frames back, waited for (the same result from run to run). Pending readbacks are applied
+ * before the mode changes. */
+int cfg_wood_set_readback_lag(cfg_wood* w, int lag);
+/* readbacks applied and skipped (busy ring slot) in the lagged modes so far */
+int cfg_wood_readbacks(cfg_wood* w, uint64_t* applied, uint64_t* skipped);
 /* a piece's state and its last heat inputs (qConv W/m, qInc W/m^2); CFG_ERR_NOENT if the slot is empty */
 int cfg_wood_get(cfg_wood* w, int slot, cfg_wood_piece* out, double* qConv4, double* qInc4);
 /* heat release rate and radiative loss (W per m depth) and max T of the last frame (js/main.js:225-229) */

@@ -149,13 +149,18 @@ class WoodPiece:
 class WoodScene:
     """The frame loop of js/main.js for frozen pieces, over an OracleSim."""
 
-    def __init__(self, sim, charYield=0.25, pyroMult=1.0, world=None):
-        """world: an oracle.rigid_ref.RigidWorld for moving pieces (None: frozen)."""
+    def __init__(self, sim, charYield=0.25, pyroMult=1.0, world=None, lag=0):
+        """world: an oracle.rigid_ref.RigidWorld for moving pieces (None: frozen).
+        lag: 0 applies each frame's readback at its end; 1..3 applies it at the start of the frame `lag`
+        frames later, before the wood steps, with its own frame's gas time and only to the pieces that
+        held the slots then (afterSubmit's tag and onReadback, js/fluid.js:327-342, js/main.js:210-230,
+        with a fixed delay instead of the GPU's timing)."""
         self.sim, self.charYield, self.pyroMult, self.world = sim, charYield, pyroMult, world
         self.slots = [None] * 64
         self.simAcc = 0.0
         self.frame_no = 0
         self.hrr = self.rad = self.tmax = 0.0
+        self.lag, self.queue = lag, []
 
     def add(self, x, y, angle, side, density, preheat=None, faceT=None):
         s = self.slots.index(None)
@@ -203,6 +208,9 @@ class WoodScene:
         else:
             self.simAcc -= n * dt
         simDt = n * dt
+        while self.lag and len(self.queue) >= self.lag:   # the readback of the frame `lag` frames back
+            rb_, simDt_, owners_ = self.queue.pop(0)
+            self.apply(rb_, simDt_, owners_)
         if self.world is not None:   # js/main.js:262-263
             self.world.advance(simDt)
             exchange_contacts(self.world, simDt)
@@ -231,11 +239,19 @@ class WoodScene:
         self.sim.radiation()
         self.frame_no += 1
         rb = self.sim.readback()
+        if self.lag:
+            self.queue.append((rb, simDt, list(self.slots)))
+        else:
+            self.apply(rb, simDt, None)
+        return n
+
+    def apply(self, rb, simDt, owners):
+        """onReadback (js/main.js:210-230); owners: the slot contents when the readback's frame ran."""
         if simDt <= 0:
-            return n
+            return
         acc, rad, faceW = rb["acc"], rb["rad"], rb["faceW"]
         for s, p in enumerate(self.slots):
-            if p is None:
+            if p is None or (owners is not None and owners[s] is not p):
                 continue
             w = p["wood"]
             for f in range(4):
@@ -248,7 +264,6 @@ class WoodScene:
         self.hrr = int(acc[ACC_GLOBAL]) / G_SCALE / simDt
         self.rad = int(acc[ACC_GLOBAL + 1]) / G_SCALE / simDt
         self.tmax = float(acc[ACC_GLOBAL + 2])
-        return n
 
 
 def default_scene(scene, charYield=0.25, density=500.0):

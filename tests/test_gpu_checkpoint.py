@@ -98,3 +98,44 @@ def test_bad_checkpoints_are_rejected(tmp_path):
     assert e.value.code == -22
     assert state(a) == before   # a rejected file leaves the scene as it was
     a.close(); other.close()
+
+
+def test_resumed_scene_matches_oracle(tmp_path, oracle_mod):
+    """A checkpoint holds the whole state of a step: loaded into a fresh scene, its next steps equal the
+    CPU oracle's from that state (the benchmark's solver: FP64 outer loop by flexible CG, pipelined
+    coarsest inverse, CFL step), and the clock and dt come back as saved."""
+    from conftest import norm_err
+    nx, ny = 128, 192
+    sc = cb.generate_scene(0, nx, ny, 0.8, 1234)
+
+    def configure(s):
+        s.set_solver(cb.SOLVE_FP64, 1, 1e-8, 200)
+        s.set_coarse_solve("pipelined")
+        s.set_krylov(True)
+        s.set_cfl(0.5, 2e-3)
+
+    a = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(a, sc)
+    configure(a)
+    a.step(5)
+    saved = a.info()
+    path = str(tmp_path / "scene.ckpt")
+    a.save_checkpoint(path)
+    a.close()
+    c = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": 1e-3}, width=0.8).init()
+    configure(c)
+    c.load_checkpoint(path)
+    got = c.info()
+    assert got["dt"] == saved["dt"] and abs(got["time"] - saved["time"]) <= 1e-12
+    o = oracle_mod.OracleSim(nx, ny, 0.8, sc["dt"])
+    load_scene(o, sc)
+    configure(o)
+    o.copy_state_from(c, 0.5, 2e-3)
+    for k in range(2):
+        c.step(1)
+        o.step(1)
+        for f in ("T", "Y", "U", "V", "SQ"):
+            e = norm_err(c.readBuffer(f), o.read(f))
+            assert e <= 1e-4, (k, f, e)
+        assert norm_err(c.read_p64(), o.read("p64")) <= 1e-4
+    c.close()

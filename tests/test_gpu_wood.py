@@ -155,3 +155,60 @@ def test_moving_pieces_match_oracle(oracle_mod):
     assert ws.world.contacts()[0] >= 4               # and rests on the logs (floor + log contacts)
     assert abs(stick.vy) < 0.05
     ws.close(); g.close()
+
+
+def test_lagged_readbacks_match_the_oracle(oracle_mod):
+    """The reference applies each frame's readback when it arrives, frames later (afterSubmit's tag,
+    js/fluid.js:327-342, onReadback js/main.js:210-230). With a fixed lag of two frames the GPU loop
+    (readback ring, cfg_wood_set_readback_lag) and the oracle's loop apply the same readbacks at the
+    same frames, with their own frames' gas time; a piece removed meanwhile does not receive its old
+    slot's data."""
+    nx, ny = 96, 144
+    sc = cb.generate_scene(0, nx, ny, 0.8, 4242)
+    sc["npieces"] = 0
+    g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(g, sc)
+    o = oracle_mod.OracleSim(nx, ny, 0.8, sc["dt"])
+    load_scene(o, sc)
+    ws, rs = WoodScene(g), RefScene(o, lag=2)
+    ws.set_readback_lag(2)
+    for p in pieces():
+        assert ws.add(*p[:5], preheat=p[5]) == rs.add(*p[:5], preheat=p[5])
+    for k in range(5):
+        if k == 3:   # replace the stick: its old slot's readbacks in flight must not reach the new one
+            ws.remove(2)
+            rs.slots[2] = None
+            p = (0.41, 0.09, 0.0, 0.02, 500.0, None)
+            assert ws.add(*p[:5]) == rs.add(*p[:5]) == 2
+        assert ws.frame(1 / 60) == rs.frame(1 / 60)
+        sc_c = max(abs(q) for r in rs.slots[:3] for q in r["qConv"]) or 1.0
+        for s in range(3):
+            a, qc, qi = ws.piece(s)
+            r = rs.slots[s]
+            w = r["wood"]
+            for f in range(4):
+                assert rel(a["Ts"][f], w.Ts[f], 1.0) <= 1e-4, (k, s, f, a["Ts"][f], w.Ts[f])
+                assert abs(qc[f] - r["qConv"][f]) <= 5e-3 * sc_c, (k, s, f, qc[f], r["qConv"][f])
+    assert ws.readbacks() == {"applied": 3, "skipped": 0}   # frames 0-2 applied at the starts of 2-4
+    ws.close(); g.close()
+
+
+def test_readbacks_applied_when_they_arrive():
+    """lag < 0, the reference's own timing: frames never wait, every readback is applied once, in
+    order, or skipped while the ring is full; switching back to the synchronous mode delivers the rest."""
+    from campfire_b200.wood import default_scene
+    g = cb.FluidSim(0, {"nx": 224, "ny": 320, "dt": 0.003}, width=0.7).init()
+    g.writeParams()
+    g.reset()
+    ws = WoodScene(g)
+    default_scene(ws)
+    ws.set_readback_lag(-1)
+    frames = 40
+    for _ in range(frames):
+        ws.frame(1 / 60)
+    ws.set_readback_lag(0)
+    rb = ws.readbacks()
+    assert rb["applied"] + rb["skipped"] == frames and rb["applied"] >= frames // 2, rb
+    st = ws.stats()
+    assert st["hrr"] > 0 and 1000 < st["tmax"] < 3000, st
+    ws.close(); g.close()
