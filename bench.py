@@ -469,6 +469,7 @@ def run_app_frames(dev, stream, frames: int, warmup: int):
     sim.writeParams()
     sim.reset()
     ws = WoodScene(sim, rigid=app_rigid_options())
+    ws.set_readback_lag(-1)   # readbacks through the ring, applied when they arrive (js/fluid.js:315-342)
     npieces = len(default_scene(ws))
     ren = Renderer(sim)
     img = torch.empty(H * W * 4, dtype=torch.float32, device=dev)
@@ -493,11 +494,13 @@ def run_app_frames(dev, stream, frames: int, warmup: int):
             steps += n
     render_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
     st = ws.stats()
+    rbs = ws.readbacks()
     ws.close()
     sim.close()
     px = W * H
     return {"scene": f"the app's default fire ({npieces} moving pieces: 7 coals, 2 logs, 7 sticks), {nx}x{ny} "
                      f"cells, dt {dt}, one V-cycle per step", "frame_sim_dt_s": frame_dt, "frames": frames,
+            "readback": "asynchronous ring, applied when arrived", "readbacks": rbs,
             "warmup_frames": warmup, "image": [W, H], "frames_per_s": frames / wall,
             "ms_per_frame": 1e3 * wall / frames, "gas_steps_per_frame": steps / frames,
             "sim_time_per_wall_time": steps * dt / wall,
