@@ -138,7 +138,7 @@ def lib():
         "cfg_batch_create": [ci, ip, ip, dp, dp, ci, ctypes.POINTER(vp)], "cfg_batch_destroy": [vp],
         "cfg_batch_scene": [vp, ci, ctypes.POINTER(vp)], "cfg_batch_set_solver": [vp, ci, ci, cd, ci],
         "cfg_batch_set_active": [vp, ci, ci], "cfg_batch_step": [vp, ci], "cfg_batch_set_stream": [vp, vp],
-        "cfg_batch_synchronize": [vp], "cfg_batch_launch_count": [vp, ip], "cfg_batch_write_params": [vp],
+        "cfg_batch_synchronize": [vp], "cfg_batch_launch_count": [vp, ip], "cfg_batch_set_graphs": [vp, ci], "cfg_batch_write_params": [vp],
         "cfg_batch_geometry": [vp],
         "cfg_time_kernel": [vp, cs, ci, dp, dp, dp],
         "cfg_pressure_residual_noalloc": [vp, vp, vp, vp, ci, ci, cd, vp, dp],

@@ -174,6 +174,10 @@ int cfg_batch_set_active(cfg_batch* b, int i, int active) {
 int cfg_batch_step(cfg_batch* b, int nsteps) { BATCH_OK(b); return guarded([&] { return b->eng->step(nsteps); }); }
 int cfg_batch_set_stream(cfg_batch* b, void* stream) { BATCH_OK(b); return guarded([&] { return b->eng->set_stream((cudaStream_t)stream); }); }
 int cfg_batch_synchronize(cfg_batch* b) { BATCH_OK(b); return guarded([&] { return b->eng->synchronize(); }); }
+int cfg_batch_set_graphs(cfg_batch* b, int enable) {
+  if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
+  return b->eng->set_graphs(enable != 0);
+}
 int cfg_batch_launch_count(cfg_batch* b, int* per_step) {
   BATCH_OK(b);
   if (!per_step) return cfg::fail(CFG_ERR_INVAL, "null output");

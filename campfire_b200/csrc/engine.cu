@@ -822,14 +822,23 @@ int Engine::set_cfl(int s, double cfl, double dt_cap) {
   Scene& sc = scenes_[s];
   if (cfl > 0 && !(sc.cfl > 0) && sc.desc.solve)   // the device clock starts from the host's
     CFG_CUDA(cudaMemcpyAsync(&d_solve_[s].time, &sc.time, sizeof(double), cudaMemcpyHostToDevice, st()));
-  if (!(cfl > 0) && sc.cfl > 0 && sc.desc.solve) {  // and the host's from the device's
+  if (!(cfl > 0) && sc.cfl > 0 && sc.desc.solve) {  // and the host's clock and dt from the device's
     double t = 0;
+    float dt = 0.f;
     CFG_CUDA(cudaMemcpyAsync(&t, &d_solve_[s].time, sizeof t, cudaMemcpyDeviceToHost, st()));
+    CFG_CUDA(cudaMemcpyAsync(&dt, (char*)(d_scenes_ + s) + offsetof(SceneDesc, P) + offsetof(cfg_params, dt), 4,
+                             cudaMemcpyDeviceToHost, st()));
     CFG_CUDA(cudaStreamSynchronize(st()));
     sc.time = t;
+    if (dt > 0.f) sc.dtd = (double)dt;
   }
   sc.cfl = cfl; sc.dt_cap = dt_cap;
   sc.dt_on_device = false;
+  // the step controls take effect with the next step, as the solver settings do (not at the
+  // next cfg_write_params): the descriptor's cfl and dt_cap are updated on the device now
+  sc.desc.cfl = (float)cfl; sc.desc.dt_cap = (float)dt_cap;
+  static_assert(offsetof(SceneDesc, dt_cap) == offsetof(SceneDesc, cfl) + sizeof(float), "cfl, dt_cap adjacent");
+  CFG_CUDA(cudaMemcpyAsync(&d_scenes_[s].cfl, &sc.desc.cfl, 2 * sizeof(float), cudaMemcpyHostToDevice, st()));
   graph_dirty_ = true;
   dt_from_step_ = false;
   return CFG_OK;

@@ -353,6 +353,9 @@ class Batch:
     def set_tiles(self, advect: int, diffuse_sources: int, forces: int):
         check(_lib.lib().cfg_batch_set_tiles(self._h, advect, diffuse_sources, forces))
 
+    def set_graphs(self, on: bool):
+        check(_lib.lib().cfg_batch_set_graphs(self._h, 1 if on else 0))
+
     def set_active(self, i: int, on: bool):
         check(_lib.lib().cfg_batch_set_active(self._h, i, 1 if on else 0))
 

@@ -158,7 +158,9 @@ int cfg_get_info(cfg_sim* sim, cfg_info* out);
 /* ---- extensions (no counterpart in the reference) ---- */
 /* Pressure solve mode; see CFG_SOLVE_*. Defaults: CFG_SOLVE_FIXED, 1 cycle (the reference). */
 int cfg_set_solver(cfg_sim* sim, int mode, int ncycles, double tol, int max_cycles);
-/* CFL step: after each step dt = min(dt_cap, cfl*dx/max|u|); cfl = 0 keeps dt fixed. */
+/* CFL step: after each step dt = min(dt_cap, cfl*dx/max|u|); cfl = 0 keeps dt fixed. Takes effect
+ * from the next step. While it is on, the device owns dt: cfg_write_params leaves it as the last
+ * step set it (without waiting for the GPU) and cfg_get_info reads dt and the clock from the device. */
 int cfg_set_cfl(cfg_sim* sim, double cfl, double dt_cap);
 /* Rays per wood face / floor probe of the radiation pass (radiation.wgsl:22 fixes 64) */
 int cfg_set_nray(cfg_sim* sim, int nray);
@@ -275,6 +277,8 @@ int cfg_batch_step(cfg_batch* b, int nsteps);
 int cfg_batch_set_stream(cfg_batch* b, void* cuda_stream);
 int cfg_batch_synchronize(cfg_batch* b);
 int cfg_batch_launch_count(cfg_batch* b, int* per_step);
+/* as cfg_set_graphs, for the whole batch (off: kernel by kernel, e.g. for a profiler's launch list) */
+int cfg_batch_set_graphs(cfg_batch* b, int enable);
 int cfg_batch_write_params(cfg_batch* b);
 int cfg_batch_geometry(cfg_batch* b);
 int cfg_batch_set_coarse_cells(cfg_batch* b, int cells);

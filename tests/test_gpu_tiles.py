@@ -38,7 +38,7 @@ def test_tile_shapes_give_the_same_bits(nx, ny, dt, sub):
 
 
 def test_tile_shapes_in_an_uneven_batch():
-    dims = [(96, 144), (128, 192), (100, 150)]
+    dims = [(96, 144), (128, 192), (64, 96)]
     scenes = [cb.generate_scene(2, nx, ny, 0.8, 2000 + k) for k, (nx, ny) in enumerate(dims)]
     res = []
     for shape in SHAPES[:3]:

@@ -194,8 +194,11 @@ def test_lagged_readbacks_match_the_oracle(oracle_mod):
 
 
 def test_readbacks_applied_when_they_arrive():
-    """lag < 0, the reference's own timing: frames never wait, every readback is applied once, in
-    order, or skipped while the ring is full; switching back to the synchronous mode delivers the rest."""
+    """lag < 0, the reference's own timing: frames never wait for the GPU, every readback is applied
+    once, in order, or skipped while the ring is full; switching back to the synchronous mode delivers
+    the rest. Paced like the app (a frame every 8 ms, js/main.js's requestAnimationFrame), the GPU keeps
+    up and nearly every readback is applied, a frame or so late."""
+    import time
     from campfire_b200.wood import default_scene
     g = cb.FluidSim(0, {"nx": 224, "ny": 320, "dt": 0.003}, width=0.7).init()
     g.writeParams()
@@ -205,10 +208,13 @@ def test_readbacks_applied_when_they_arrive():
     ws.set_readback_lag(-1)
     frames = 40
     for _ in range(frames):
+        t0 = time.perf_counter()
         ws.frame(1 / 60)
+        assert time.perf_counter() - t0 < 0.5       # the frame enqueues its work; it does not wait for it
+        time.sleep(max(0.0, 0.008 - (time.perf_counter() - t0)))
     ws.set_readback_lag(0)
     rb = ws.readbacks()
-    assert rb["applied"] + rb["skipped"] == frames and rb["applied"] >= frames // 2, rb
+    assert rb["applied"] + rb["skipped"] == frames and rb["applied"] >= frames - 5, rb
     st = ws.stats()
     assert st["hrr"] > 0 and 1000 < st["tmax"] < 3000, st
     ws.close(); g.close()
