@@ -197,6 +197,23 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     b.set_stream(stream.cuda_stream)
     b.step(warmup)
     b.synchronize()
+    # the Krylov update: its own kernel per cycle, or folded into the level-0 smoother kernels (one
+    # launch fewer per cycle, more bytes): both timed over a few steps of the batch, the faster kept
+    fold_ms = {}
+    for mode in (3, 2):
+        b.set_krylov(mode)
+        b.step(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step(4)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        b.synchronize()
+        fold_ms[mode] = e0.elapsed_time(e1) / 4
+    fold = min(fold_ms, key=fold_ms.get)
+    b.set_krylov(fold)
+    b.step(1)
+    b.synchronize()
     torch.cuda.synchronize(dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for k in range(steps):
@@ -248,6 +265,8 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     return {"value": batched, "unit": METRIC, "scenes": len(scenes), "cells": cells, "steps": steps,
             "schedule": {"coarse_cells": tune["best"],
                          "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()},
+                         "krylov_update": "folded into the level-0 kernels" if fold == 2 else "own kernel",
+                         "krylov_update_ms_per_step": {"own kernel": fold_ms[3], "folded": fold_ms[2]},
                          "tiles": {"advect": cb.TILE_SHAPES[tt["best"][0]],
                                    "diffuse_sources": cb.TILE_SHAPES[tt["best"][1]],
                                    "forces": cb.TILE_SHAPES[tt["best"][2]],

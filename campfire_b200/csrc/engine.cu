@@ -1130,7 +1130,7 @@ int Engine::set_cond_mode(bool graph) {
 }
 
 int Engine::set_krylov(int on) {
-  if (on != 0 && on != 1) return fail(CFG_ERR_INVAL, "krylov must be 0 or 1");
+  if (on < 0 || on > 3) return fail(CFG_ERR_INVAL, "krylov must be 0 (off), 1 (on), 2 (on, update folded) or 3 (on, update kernel)");
   CFG_TRY(activate());
   krylov_ = on;
   graph_dirty_ = true;
@@ -1158,9 +1158,10 @@ bool Engine::any_cfl() const {
 }
 
 bool Engine::pcg_fused() const {
-  // one scene: the folded update shortens the cycle's kernel chain; a batch is bound by
-  // bandwidth instead, and the separate update kernel moves fewer bytes than the fold
-  if (!krylov() || scenes_.size() != 1) return false;
+  // krylov 1: one scene folds the update into the level-0 kernels (a shorter kernel chain); a
+  // batch, bound by bandwidth, keeps the separate update kernel, which moves fewer bytes.
+  // krylov 2 / 3 choose the fold / the kernel for any engine (the batch autotuner times both)
+  if (!krylov() || krylov_ == 3 || (krylov_ == 1 && scenes_.size() != 1)) return false;
   for (auto& sc : scenes_)
     if (sc.lc < 1) return false;
   return true;

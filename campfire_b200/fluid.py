@@ -268,9 +268,10 @@ class FluidSim(_SceneOps):
         inverse factored beside the previous step's solve ("pipelined")."""
         check(_lib.lib().cfg_set_coarse_solve(self._h, _coarse_mode(direct)))
 
-    def set_krylov(self, on: bool):
-        """FP64 mode: preconditioned CG around the V-cycle (True) or plain defect correction (False)."""
-        check(_lib.lib().cfg_set_krylov(self._h, 1 if on else 0))
+    def set_krylov(self, on):
+        """FP64 mode: preconditioned CG around the V-cycle (True) or plain defect correction (False);
+        2 / 3: CG with its update folded into the level-0 kernels / as its own kernel."""
+        check(_lib.lib().cfg_set_krylov(self._h, int(on)))
 
     def set_tiles(self, advect: int, diffuse_sources: int, forces: int):
         """Tile shapes (TILE_SHAPES indices) of the advection, diffusion + sources and forces kernels."""
@@ -347,8 +348,10 @@ class Batch:
     def set_coarse_cluster(self, cs: int):
         check(_lib.lib().cfg_batch_set_coarse_cluster(self._h, int(cs)))
 
-    def set_krylov(self, on: bool):
-        check(_lib.lib().cfg_batch_set_krylov(self._h, 1 if on else 0))
+    def set_krylov(self, on):
+        """True / 1: on (the update kernel for a batch); 2: on, update folded into the level-0 kernels;
+        3: on, separate update kernel; False / 0: plain defect correction."""
+        check(_lib.lib().cfg_batch_set_krylov(self._h, int(on)))
 
     def set_tiles(self, advect: int, diffuse_sources: int, forces: int):
         check(_lib.lib().cfg_batch_set_tiles(self._h, advect, diffuse_sources, forces))

@@ -221,7 +221,10 @@ int cfg_batch_set_coarse_solve(cfg_batch* b, int direct);
 /* FP64 mode outer loop (no counterpart in the reference): 0 (default) plain defect correction
  * (p64 += V-cycle(f32(r)) per cycle); 1 flexible preconditioned conjugate gradients on the
  * level-0 operator in FP64 with the same FP32 V-cycle as preconditioner (Polak-Ribiere
- * direction update), which needs about half the cycles for the same tolerance. */
+ * direction update), which needs about half the cycles for the same tolerance. With 1 the
+ * direction update is folded into the level-0 smoother kernels for one scene and runs as its
+ * own kernel for a batch; 2 folds it and 3 keeps the kernel whatever the engine (one launch per
+ * cycle fewer, against more bytes per cycle; the same iteration up to rounding). */
 int cfg_set_krylov(cfg_sim* sim, int on);
 int cfg_batch_set_krylov(cfg_batch* b, int on);
 /* Autotuner of that schedule (no counterpart in the reference): builds a scratch batch of

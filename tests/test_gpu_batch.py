@@ -55,3 +55,32 @@ def test_inactive_scene_is_left_untouched():
     b.step(1)
     assert not np.array_equal(b.scenes[1].readBuffer("T"), before)
     b.close()
+
+
+def test_batch_krylov_update_folded_matches_its_own_kernel():
+    """The Krylov direction update of a batch folded into the level-0 smoother kernels (krylov 2) or
+    run as its own kernel per cycle (krylov 3): the same iteration, so the same cycle counts (within
+    one: the stopping test's rounding) and pressures to 1e-7, with one launch per cycle fewer."""
+    from conftest import norm_err
+    dims = [(96, 144), (128, 192), (64, 96)]
+    scenes = [cb.generate_scene(2, nx, ny, 0.8, 2100 + k) for k, (nx, ny) in enumerate(dims)]
+    out = {}
+    for mode in (3, 2):
+        b = cb.Batch(dims, 0.8, [s["dt"] for s in scenes])
+        for v, s in zip(b.scenes, scenes):
+            load_scene(v, s)
+        b.set_solver(cb.SOLVE_FP64, 1, 1e-9, 100)
+        b.set_coarse_solve("pipelined")
+        b.set_coarse_cells(1536)
+        b.set_krylov(mode)
+        b.step(3)
+        b.synchronize()
+        out[mode] = ([v.info()["last_cycles"] for v in b.scenes], [v.read_p64() for v in b.scenes],
+                     [{f: v.readBuffer(f) for f in ("T", "U", "V")} for v in b.scenes], b.launch_count())
+        b.close()
+    for k in range(len(dims)):
+        assert abs(out[2][0][k] - out[3][0][k]) <= 1, (k, out[2][0], out[3][0])
+        assert norm_err(out[2][1][k], out[3][1][k]) <= 1e-7, k
+        for f in ("T", "U", "V"):
+            assert norm_err(out[2][2][k][f], out[3][2][k][f]) <= 1e-6, (k, f)
+    assert out[2][3] < out[3][3], (out[2][3], out[3][3])
