@@ -316,7 +316,9 @@ def run_fp64_error(dev, workload: str, steps: int, every: int, threads: int):
       one_step    the step after the report, from the GPU's state: that state is copied into an FP64 oracle
                   and into the CPU FP32 restatement, and all three take the step; errors against the FP64 one
       trajectory  the GPU run and an FP64 oracle run from the same initial scene, and the FP32 restatement's
-                  own run against the FP64 one (the flame amplifies rounding: FP32 drift, not a defect)"""
+                  own run against the FP64 one (the flame amplifies rounding: FP32 drift, not a defect; the
+                  FP64 oracle also rasterises the pieces in FP64, so a face that is barely open in FP32 can
+                  be closed there, which moves u at that face from the first step on)"""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     import campfire_b200 as cb
     from campfire_b200.fluid import load_scene

@@ -1302,13 +1302,15 @@ void Engine::enqueue_bnorm(cudaStream_t s) {
 
 // Pressure loop driven from the host (launches outside a graph): the device
 // decides per cycle and mirrors the decision into SolveCtl::any_active.
-int Engine::host_pressure_loop() {
+// started: the step's pre-solve kernels already launched the first FP64 defect and reset the
+// cycle counter (the stream-launched step); false for the staged calls that run the loop alone
+int Engine::host_pressure_loop(bool started) {
   cudaStream_t s = st();
   int guard = 0;
-  if (any_fp64()) {
-    launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s);
+  if (!started) {
+    if (any_fp64()) launch_defect64(d_scenes_, nscenes(), d_wl_[WL_MG0], nwl_[WL_MG0], d_ctl_, 1, s);
+    CFG_CUDA(cudaMemsetAsync(&d_ctl_->iter, 0, sizeof(int), s));
   }
-  CFG_CUDA(cudaMemsetAsync(&d_ctl_->iter, 0, sizeof(int), s));
   CFG_CUDA(cudaMemcpyAsync(h_ctl_pinned_, d_ctl_, sizeof(SolveCtl), cudaMemcpyDeviceToHost, s));
   CFG_CUDA(cudaStreamSynchronize(s));
   int any = any_fp64() ? h_ctl_pinned_->any_active : 1;
@@ -1410,7 +1412,7 @@ int Engine::step(int nsteps) {
       launches_ = 0; vcycle_launches_ = 0;
       enqueue_pre_solve(st(), 0ull, 0);
       CFG_CUDA(cudaGetLastError());
-      CFG_TRY(host_pressure_loop());
+      CFG_TRY(host_pressure_loop(true));
       CFG_CUDA(enqueue_post_solve(st()));
       dt_from_step_ = dt_from_step_ || any_cfl();
       mark_device_dt();
@@ -1467,7 +1469,7 @@ int Engine::step_profiled(float* ms) {
   CFG_CUDA(cudaEventRecord(ev[5], s));
   CFG_TRY(set_cond_mode(false));
   enqueue_factor(s);
-  CFG_TRY(host_pressure_loop());
+  CFG_TRY(host_pressure_loop(false));
   CFG_CUDA(cudaEventRecord(ev[6], s));
   CFG_CUDA(enqueue_post_solve(s));
   dt_from_step_ = dt_from_step_ || any_cfl();
@@ -1500,7 +1502,7 @@ int Engine::run_stage(const char* stage) {
     CFG_TRY(set_cond_mode(false));
     enqueue_factor(s);
     enqueue_bnorm(s);
-    CFG_TRY(host_pressure_loop());
+    CFG_TRY(host_pressure_loop(false));
     enqueue_factor_join(s);
   } else if (st_ == "project") launch_project(d_scenes_, d_wl_[WL_PR], nwl_[WL_PR], fp64, s);
   else if (st_ == "update_dt") launch_cfl_update(d_scenes_, nscenes(), d_dxd_, d_alpha_, s);

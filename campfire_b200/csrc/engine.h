@@ -217,7 +217,7 @@ class Engine {
   void enqueue_fp64_tail(cudaStream_t s);
   void enqueue_cycle_tail(cudaStream_t s, unsigned long long h, int use_cond);
   cudaError_t enqueue_post_solve(cudaStream_t s);
-  int host_pressure_loop();
+  int host_pressure_loop(bool started);
   void enqueue_bnorm(cudaStream_t s);
 
   int device_ = 0;
