@@ -47,7 +47,8 @@ B_FIXED = 156 + 68 + 28 + 20 + 28 + 13.3 + 32
 
 
 # DRAM bytes (read + write) per launch of a kernel, from one ncu capture of the workload
-NCU_TRAFFIC = {("plain", "mg_coarse"): 123904, ("plain", "advect"): 2967808}
+NCU_TRAFFIC = {("plain", "mg_coarse"): 123904, ("plain", "advect"): 2967808,
+               ("batched", "mg_down0"): 43902464}
 
 
 def bytes_per_cell(diff_sub: int, cycles: float, fp64: bool) -> float:
@@ -281,7 +282,11 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth)",
                          "step_bytes": step_bytes, "bytes_per_cell": step_bytes / cells,
-                         "basis": "algorithmic bytes of the last step (each scene's cycles) / mean ms per step"}}
+                         "basis": "algorithmic bytes of the last step (each scene's cycles) / mean ms per step",
+                         "traffic": {"kernel": "mg_down0", "bytes": NCU_TRAFFIC[("batched", "mg_down0")],
+                                     "algorithmic_bytes": 82.0 * cells,
+                                     "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of "
+                                               "the level-0 down kernel of this batch (cold replay)"}}}
 
 
 ERR_FIELDS = ("T", "u", "Y_F", "Y_S")
