@@ -47,6 +47,19 @@ class _SceneOps:
     """Per-scene FluidSim surface shared by FluidSim and batch scene views."""
 
     _h: Optional[int]
+    _cfl = 0.0
+
+    # FluidSim.time (js/fluid.js:252): advanced by dt per step on the host; with a CFL step the
+    # device owns dt and the clock, so it is read from the device (cfg_get_info)
+    @property
+    def time(self) -> float:
+        if self._cfl > 0 and getattr(self, "_h", None):
+            return self.info()["time"]
+        return self.__dict__.get("_time", 0.0)
+
+    @time.setter
+    def time(self, v: float):
+        self.__dict__["_time"] = float(v)
 
     # -- FluidSim methods
     def reset(self):
@@ -172,7 +185,11 @@ class _SceneOps:
         self.dt = float(dt)
 
     def set_cfl(self, cfl: float, dt_cap: float):
+        t = self.time   # the clock so far (the device's while a CFL step was on)
         check(_lib.lib().cfg_set_cfl(self._h, float(cfl), float(dt_cap)))
+        self._cfl = float(cfl)
+        if cfl <= 0:
+            self.time = t
 
     def set_nray(self, n: int):
         check(_lib.lib().cfg_set_nray(self._h, int(n)))
@@ -237,7 +254,8 @@ class FluidSim(_SceneOps):
     def encodeStep(self, pass_=None, n: int = 1):
         """One gas step (js/fluid.js:225-253); time += dt."""
         check(_lib.lib().cfg_step(self._h, int(n)))
-        self.time += n * self.dt
+        if self._cfl <= 0:
+            self.time += n * self.dt
 
     def step(self, n: int = 1):
         self.encodeStep(n=n)
@@ -246,7 +264,8 @@ class FluidSim(_SceneOps):
         """One step with per-stage device ms, names of js/fluid.js:291."""
         ms = np.zeros(7, np.float32)
         check(_lib.lib().cfg_step_profiled(self._h, _fp(ms)))
-        self.time += self.dt
+        if self._cfl <= 0:
+            self.time += self.dt
         return dict(zip(STAGES, ms.tolist()))
 
     def vcycle(self, pass_=None, nu: int = 2):

@@ -24,6 +24,11 @@ def _run(graphs, steps=4):
         g.step(1)
     g.synchronize()
     out = {f: g.readBuffer(f) for f in ("T", "U", "V")}
+    # the clock: the sum of the dt each step used, kept on the device (and by the Python mirror)
+    t = 0.0
+    for d in dts:
+        t += d
+    assert g.info()["time"] == t and g.time == t
     g.close()
     return out, dts
 
