@@ -1553,6 +1553,18 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   } else if (n == "mg_up0") {
     go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 0, d_ctl_, s); };
     b = (17 + 4 * 16) * cells; cnt = cyc;   // prolongation + 4 colour passes
+  } else if (n == "mg_down0_krylov" || n == "mg_up0_krylov") {
+    // the level-0 kernels as the step runs them in the fused Krylov mode (the update folded in):
+    // the V-cycle's bytes plus half of the FP64 iteration's 40 B per cell each
+    if (!pcg_fused()) return fail(CFG_ERR_NOENT, n + ": the Krylov update is not folded in this engine");
+    if (n == "mg_down0_krylov") {
+      go = [&](int) { launch_mg_down(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, d_ctl_, 0, 1, s); };
+      b = (4 * 16 + 18 + 20) * cells;
+    } else {
+      go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 4, d_ctl_, s); };
+      b = (17 + 4 * 16 + 20) * cells;
+    }
+    cnt = cyc;
   } else if (n == "mg_coarse") {
     go = [&](int) {
       if (coarse_cluster_ > 0) launch_mg_cluster(d_scenes_, nscenes(), d_ctl_, coarse_cluster_, 0, cluster_smem_, s);

@@ -272,11 +272,11 @@ __device__ __forceinline__ void pcg_down_apply(const SceneDesc& S, const LevelDe
 // ------------------------------------------------------------------ down: 4 passes + restrict
 // PCG: the fused Krylov update on level 0 (above)
 template <int TX, int TY, bool PCG>
-// CTAs per SM: the fused Krylov variants (level 0) at three (at most 85 registers a thread,
-// 44 bytes of spill in the down kernel): 512x768's 768 level-0 tiles then run in two waves
-// instead of three (measured: -5% per Krylov cycle at 512x768); the plain variants at four (they
-// need 56 registers; a bound of three let them take 69 and cost a CTA per SM in batches)
-__global__ void __launch_bounds__(256, PCG ? 3 : 4) k_mg_down(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
+// three CTAs per SM (at most 85 registers a thread; 44 bytes of spill in the fused Krylov
+// variant): 512x768's 768 level-0 tiles run in two waves instead of three (measured: -5% per
+// Krylov cycle at 512x768). Four for the plain variants (62 registers) was measured 3-4% slower
+// per step at 256x384 and 512x768 and no faster for the batch.
+__global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                  int level, SolveCtl* ctl, int count_iter) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
   __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256, PCG ? 3 : 4) k_mg_down(const SceneDesc* _
 // mode (the pending r, q update first; the loop decision from the recurrence for ||r||),
 // compiled into the KRY instance only
 template <int TX, int TY, bool KRY>
-__global__ void __launch_bounds__(256, KRY ? 3 : 4) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
+__global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, int tail, SolveCtl* ctl) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
   constexpr int RW = TX + 2 * MGF_H, RH = TY + 2 * MGF_H;

@@ -309,7 +309,7 @@ int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int 
   if (server_busy(s)) return cfg::fail(CFG_ERR_BUSY, "the server is running jobs: drain it first");
   CFG_TRY(s->eng.set_solver(mode, ncycles, tol, max_cycles));
   CFG_TRY(s->eng.set_coarse_solve(coarse_direct));
-  CFG_TRY(s->eng.set_krylov(krylov ? 1 : 0));
+  CFG_TRY(s->eng.set_krylov(krylov));   // 0-3 as cfg_set_krylov
   if (coarse_cells > 0) CFG_TRY(s->eng.set_coarse_cells(coarse_cells));
   return CFG_OK;
 }

@@ -427,7 +427,7 @@ class Server:
     def set_solver(self, mode=_lib.SOLVE_FP64, ncycles=1, tol=1e-10, max_cycles=300, coarse_direct=True,
                    coarse_cells=0, krylov=False):
         check(_lib.lib().cfg_server_set_solver(self._h, mode, ncycles, tol, max_cycles, _coarse_mode(coarse_direct),
-                                               coarse_cells, 1 if krylov else 0))
+                                               coarse_cells, int(krylov)))
 
     def slot_bytes(self, size_class: int) -> int:
         b = ctypes.c_size_t()

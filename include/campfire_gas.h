@@ -193,7 +193,10 @@ int cfg_launch_count(cfg_sim* sim, int* per_step);
  * stream), its algorithmic bytes per launch and its launches per step.
  * Kernels: "advect", "diffuse_sources", "forces", "relax0", "restrict0",
  * "prolong0", "coarsest", "resnorm", "mg_down0", "mg_up0", "mg_coarse", "vcycle"
- * (one fused V-cycle), "defect64", "project". The state changes as the kernel runs. */
+ * (one fused V-cycle), "defect64", "project", "mg_downL" / "mg_upL" (level L below the coarse
+ * block), "mg_down0_krylov" / "mg_up0_krylov" (the level-0 kernels with the Krylov update folded
+ * in, as the step runs them when it is), "pcg_step", "coarse_factor". The state changes as the
+ * kernel runs. */
 int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, double* mean_ms, double* bytes_per_launch,
                     double* launches_per_step);
 
@@ -432,7 +435,7 @@ int cfg_server_create(int device, int nclasses, const int* nx, const int* ny, co
                       double width, cfg_server** out);
 int cfg_server_destroy(cfg_server* s);
 /* solver of every slot (as cfg_set_solver, cfg_set_coarse_solve, cfg_set_coarse_cells (cells <= 0
- * keeps it) and cfg_set_krylov) */
+ * keeps it) and cfg_set_krylov, whose 0-3 it takes) */
 int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int max_cycles, int coarse_direct,
                           int coarse_cells, int krylov);
 /* device bytes of one slot of a size class */

@@ -152,6 +152,23 @@ def test_submitted_jobs_match_the_batch_run():
     s.close()
 
 
+@pytest.mark.parametrize("krylov", [1, 2])
+def test_krylov_results_do_not_depend_on_the_mix(krylov):
+    """The FP64 loop by flexible CG, with its update as its own kernel (1) or folded into the
+    level-0 kernels (2): each scene still decides its own solve, so a job's bits do not depend
+    on the jobs beside it."""
+    js = jobs()[:4]
+    s = cb.Server(CLASSES, [2, 2], 64e9)
+    s.set_solver(**dict(SOLVER, coarse_direct="pipelined", coarse_cells=1536, krylov=krylov))
+    mixed, _, _ = s.run(js)
+    alone = []
+    for j in js:
+        r, _, _ = s.run([dict(j, arrival_s=0.0)])
+        alone.append(r[0]["hash"])
+    s.close()
+    assert [r["hash"] for r in mixed] == alone
+
+
 def test_pipelined_coarse_solve_keeps_results_independent_of_the_mix():
     """With the pipelined coarsest inverse a slot's inverse belongs to its own scene: a job
     admitted into a used slot starts without one (reset), so mixes and reuse change nothing."""
