@@ -720,11 +720,15 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     mbar_wait(&bar, 0);
     return;
   }
-  if (*act == 0) return;
+  // the scene's flag and level lc's rhs are read together (two L2 round trips overlapped): the
+  // loads land in shared memory whether or not the scene still cycles, then every thread leaves
+  // together if it does not
+  const int still = *act;
   float* sres = smem + s_res;   // residual scratch (level lc size)
   for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.rhs[e] = __ldcg(grhs + e);
   if (lc == 0)   // warm start
     for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.p[e] = __ldcg(s_gp + e);
+  if (still == 0) return;
   __syncthreads();
   // ---- down: smoothing, then per coarse cell the residuals of its four fine cells
   // (pressure.wgsl:96-101) summed in the restriction's order (pressure.wgsl:104-113)
