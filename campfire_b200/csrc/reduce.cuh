@@ -154,9 +154,23 @@ __device__ __forceinline__ bool scene_reduce_n(const SceneDesc& S, int tile, int
   if (!s_lastn) return false;
   #pragma unroll
   for (int m = 0; m < N; m++) v[m] = 0.0;
-  for (int k = threadIdx.x; k < ntiles; k += blockDim.x)
+  // two tiles' partials loaded before either is added (their L2 round trips overlap); the sums
+  // keep the order of one tile after the other
+  const int stride = blockDim.x;
+  for (int k = threadIdx.x; k < ntiles; k += 2 * stride) {
+    double a[N], b[N];
+    const bool two = k + stride < ntiles;
     #pragma unroll
-    for (int m = 0; m < N; m++) v[m] += __ldcg(S.part + N * k + m);
+    for (int m = 0; m < N; m++) {
+      a[m] = __ldcg(S.part + N * k + m);
+      b[m] = two ? __ldcg(S.part + N * (k + stride) + m) : 0.0;
+    }
+    #pragma unroll
+    for (int m = 0; m < N; m++) {
+      v[m] += a[m];
+      if (two) v[m] += b[m];
+    }
+  }
   block_sum_t<N>(v, sh);
   if (threadIdx.x == 0) S.solve->counter = 0u;
   return true;
