@@ -38,6 +38,13 @@ WORKLOADS = {
     "plain": (256, 384, 0, 1235, 2, 1e-6, 200),
     "fine": (512, 768, 1, 1236, 2, 1e-10, 300),
 }
+# cycle shape of each workload's pressure loop: the W tail (the level two above the coarsest visits the
+# level below it twice per cycle, inside the one-CTA coarse block) when that level has at most this many
+# cells; 0: the reference's V(2,2) cycle. On the tepee scenes the coarse levels limit the FP64 loop's
+# convergence: the W tail takes ~19% fewer cycles to 1e-10 at 512x768 (oracle: 18.8 -> 15.2 per step) for
+# a few more coarse-block phases per cycle; the three-log scene at 1e-6 gains nothing.
+W_CELLS = {"plain": 0, "fine": 1536}
+SERVE_W_CELLS = 1536                  # the served jobs are tepee scenes too
 METRIC = "cell-updates/s"
 PLAIN_CFL, PLAIN_DT_CAP = 0.5, 2e-3   # the plain workload's time step: CFL 0.5, at most 2 ms
 # algorithmic bytes per cell-update (reference schedule, one read + one write per element at storage width):
@@ -67,16 +74,49 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region: NVML read every 2 ms
+    from a thread (read-only queries), so that even a timed region of a few tens of milliseconds holds
+    samples; nvidia-smi at its 20 ms period when NVML is not importable."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index, self.proc, self.lines = index, None, []
+        self.nvml, self.samples, self.reasons, self.max_mhz = None, [], set(), None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = self._handle(pynvml, index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                         "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                         "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                         "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+        except Exception:
+            self.nvml = None
+
+    @staticmethod
+    def _handle(pynvml, index: int):
+        """The NVML handle of CUDA device `index` (matched by PCI bus id: NVML numbers every GPU of the
+        machine, CUDA only the visible ones)."""
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(index)
 
     def start(self):
+        if self.nvml is not None:
+            self.stop_evt = threading.Event()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "20"],
@@ -86,11 +126,34 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _sample(self):
+        nv = self.nvml
+        self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+        r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+        for n, b in self.bits.items():
+            if r & b:
+                self.reasons.add(n)
+
+    def _poll(self):
+        try:
+            while True:
+                self._sample()
+                if self.stop_evt.wait(0.002):
+                    break
+        except Exception:
+            pass
+
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_evt.set()
+            self.t.join(timeout=5)
+            sm = sorted(self.samples)
+            return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(self.reasons), "samples": len(sm), "source": "nvml, 2 ms period"}
         if self.proc:
             self.proc.terminate()
             try:
@@ -98,7 +161,6 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 7:
@@ -107,12 +169,12 @@ class ClockSampler:
                 sm.append(float(f[0])); mx = float(f[1])
             except ValueError:
                 continue
-            for n, v in zip(names, f[3:7]):
+            for n, v in zip(self.NAMES, f[3:7]):
                 if v.lower() == "active":
                     reasons.add(n)
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 20 ms period"}
 
 
 def cpu_threads() -> int:
@@ -130,20 +192,29 @@ def workload_config(workload: str, world: int) -> dict:
     return {"workload": f"{workload} gas step {nx}x{ny}, {scene}, FP32 V(2,2) in FP64 defect correction "
                         f"to rel residual {tol:g}", "nx": nx, "ny": ny, "scene_kind": kind, "scene_seed": seed,
             "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": maxc,
-                         "outer": "flexible preconditioned CG in FP64, FP32 V(2,2) as preconditioner",
+                         "outer": "flexible preconditioned CG in FP64, FP32 multigrid cycle as preconditioner",
+                         "cycle": cycle_name(W_CELLS[workload]),
                          "coarsest": "direct: inverse factored beside the pressure loop, applied from the next "
                                      "step (pipelined)"},
             "dt": {"cfl": PLAIN_CFL, "cap_s": PLAIN_DT_CAP},
             "l2": "flushed before every timed step (256 MB write)", "parallelism": f"replicas{world}"}
 
 
-def configure_solver(sim, workload: str) -> None:
-    """The workload's solver on a FluidSim or an OracleSim (same calls on both)."""
+def configure_solver(sim, workload: str, w_cells=None) -> None:
+    """The workload's solver on a FluidSim or an OracleSim (same calls on both); w_cells overrides the
+    workload's cycle shape."""
     nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
     sim.set_solver(mode, 1, tol, maxc)
     sim.set_coarse_solve("pipelined")
     sim.set_krylov(True)
     sim.set_cfl(PLAIN_CFL, PLAIN_DT_CAP)   # dt set by CFL 0.5 each step, capped at 2 ms
+    sim.set_coarse_w(W_CELLS[workload] if w_cells is None else w_cells)
+
+
+def cycle_name(w_cells: int) -> str:
+    return ("V(2,2)" if w_cells <= 0 else
+            f"V(2,2) with a W tail: the level two above the coarsest (at most {w_cells} cells) visits the level "
+            "below it twice per cycle (inside the one-CTA coarse block)")
 
 
 def run_cpu(workload: str, steps: int, warmup: int, threads: int):
@@ -414,6 +485,7 @@ def run_one_by_one(dev, jobs, tol: float):
         g.set_solver(cb.SOLVE_FP64, 1, tol, 300)
         g.set_coarse_solve("pipelined")
         g.set_krylov(True)
+        g.set_coarse_w(SERVE_W_CELLS)
         g.step(j["nsteps"])
         g.synchronize()
         cb.field_hash(g)
@@ -432,7 +504,8 @@ def run_served(dev, stream, lams, njobs: int, steps_lo: int, steps_hi: int, slot
     jobs = served_jobs(njobs, steps_lo, steps_hi)
     service = run_one_by_one(dev, jobs, tol)
     srv = cb.Server(SERVE_CLASSES, [slots] * len(SERVE_CLASSES), budget, device=dev.index)
-    srv.set_solver(cb.SOLVE_FP64, 1, tol, 300, "pipelined", krylov=2)   # the Krylov update folded (as the batch)
+    srv.set_solver(cb.SOLVE_FP64, 1, tol, 300, "pipelined", krylov=2,   # the Krylov update folded (as the batch)
+                   coarse_w=SERVE_W_CELLS)
     hbm, peak_kind = peaks()
     cells = sum(SERVE_CLASSES[j["size_class"]][0] * SERVE_CLASSES[j["size_class"]][1] * j["nsteps"] for j in jobs)
     out = []
@@ -466,7 +539,8 @@ def run_served(dev, stream, lams, njobs: int, steps_lo: int, steps_hi: int, slot
     srv.close()
     return {"classes": [f"{a}x{b}" for a, b in SERVE_CLASSES], "slots_per_class": slots, "budget_bytes": budget,
             "jobs": njobs, "steps_per_job": [steps_lo, steps_hi], "job_steps_total": sum(j["nsteps"] for j in jobs),
-            "scene": f"tepee (five logs of half 5 cm), FP64 defect correction to {tol:g}, pipelined direct coarsest",
+            "scene": f"tepee (five logs of half 5 cm), FP64 defect correction to {tol:g}, pipelined direct coarsest, "
+                     f"cycle {cycle_name(SERVE_W_CELLS)}",
             "one_by_one": "measured: each job alone through the plain FluidSim (scene set-up, steps, fields read "
                           "back), first come first served at each rate's arrivals",
             "one_by_one_service_s": float(sum(service)), "runs": out}
@@ -599,7 +673,7 @@ def run_e2e(sim, sc, stream, flush, steps: int, barrier, dev, world: int) -> dic
 
 
 def measure_gpu(dev, stream, flush, workload: str, steps: int, warmup: int, launch: str, coarse_cells: int,
-                world: int, rank: int, barrier, clocks=None) -> dict:
+                world: int, rank: int, barrier, clocks=None, w_cells=None) -> dict:
     """The plain single-scene step of `workload` on this rank's GPU: `steps` steps timed one by one with CUDA
     events on the library's stream after an L2 flush each; value = all ranks' cell-updates / max-over-ranks time."""
     import torch
@@ -610,7 +684,7 @@ def measure_gpu(dev, stream, flush, workload: str, steps: int, warmup: int, laun
     sc = cb.generate_scene(kind, nx, ny, 0.8, seed + 1000 * rank)
     sim = cb.FluidSim(dev.index, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
     load_scene(sim, sc)
-    configure_solver(sim, workload)
+    configure_solver(sim, workload, w_cells)
     # smoother schedule picked by the autotuner (fused V-cycles timed on a scratch scene of this size)
     if coarse_cells > 0:
         sim.set_coarse_cells(coarse_cells)
@@ -661,7 +735,7 @@ def kernel_roofline(sim, workload: str, value_per_gpu: float, info: dict) -> dic
     hbm, peak_kind = peaks()
     kern = {}
     for name in ("advect", "diffuse_sources", "forces", "mg_down0_krylov", "mg_up0_krylov", "mg_down0", "mg_up0",
-                 "mg_coarse", "pcg_step", "defect64", "project"):
+                 "mg_coarse", "pcg_decide", "pcg_step", "defect64", "project"):
         m, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         rc = L.cfg_time_kernel(sim._h, name.encode(), 50, ctypes.byref(m), ctypes.byref(b), ctypes.byref(n))
         if rc == -2:   # a variant this engine does not run (the folded Krylov kernels, or the plain ones)
@@ -785,14 +859,22 @@ def main():
     # ---- the 512x768 tepee workload (FP64 to 1e-10): the plain step where the roofline target is set
     fine = None
     if a.fine_steps > 0 and a.workload != "fine":
-        mf = measure_gpu(dev, stream, flush, "fine", a.fine_steps, a.warmup, a.launch, 0, world, rank, barrier)
+        mf = measure_gpu(dev, stream, flush, "fine", a.fine_steps, a.warmup, a.launch, 0, world, rank, barrier,
+                         ClockSampler(local))
         fi = mf["info"]
         fine = {"value": mf["value"], "unit": METRIC, "steps": a.fine_steps, "ms_per_step": mf["ms_max"] / a.fine_steps,
                 "config": workload_config("fine", world), "schedule": mf["schedule"],
                 "solve": {"cycles_last_step": fi["last_cycles"], "diff_sub": fi["diffSub"], "levels": fi["levels"],
                           "last_rel": fi["last_rel"]},
-                "roofline": kernel_roofline(mf["sim"], "fine", mf["value"] / world, fi)}
+                "roofline": kernel_roofline(mf["sim"], "fine", mf["value"] / world, fi), "clocks": mf["clocks"]}
         mf["sim"].close()
+        # the same workload with the V(2,2) cycle throughout (the cycle shape's effect)
+        mv = measure_gpu(dev, stream, flush, "fine", a.fine_steps, a.warmup, a.launch, 0, world, rank, barrier,
+                         w_cells=0)
+        fine["v_cycle"] = {"value": mv["value"], "unit": METRIC, "ms_per_step": mv["ms_max"] / a.fine_steps,
+                           "cycle": cycle_name(0), "cycles_last_step": mv["info"]["last_cycles"],
+                           "last_rel": mv["info"]["last_rel"]}
+        mv["sim"].close()
 
     batched = None
     if a.batched_steps > 0:

@@ -144,6 +144,7 @@ def lib():
         "cfg_pressure_residual_noalloc": [vp, vp, vp, vp, ci, ci, cd, vp, dp],
         "cfg_set_coarse_cells": [vp, ci], "cfg_batch_set_coarse_cells": [vp, ci],
         "cfg_set_coarse_cluster": [vp, ci], "cfg_batch_set_coarse_cluster": [vp, ci],
+        "cfg_set_coarse_w": [vp, ci], "cfg_batch_set_coarse_w": [vp, ci], "cfg_server_set_coarse_w": [vp, ci],
         "cfg_autotune": [ci, ci, ip, ip, ci, ci, ip, ip, dp, ip],
         "cfg_set_coarse_solve": [vp, ci], "cfg_batch_set_coarse_solve": [vp, ci],
         "cfg_set_tiles": [vp, ci, ci, ci], "cfg_batch_set_tiles": [vp, ci, ci, ci],

@@ -203,6 +203,14 @@ extern "C" int cfg_batch_set_coarse_cells(cfg_batch* b, int cells) {
   if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
   return guarded([&] { return b->eng->set_coarse_cells(cells); });
 }
+extern "C" int cfg_set_coarse_w(cfg_sim* sim, int cells) {
+  SIM_OK(sim); OWNER_OK(sim);
+  return guarded([&] { return sim->eng->set_coarse_w(cells); });
+}
+extern "C" int cfg_batch_set_coarse_w(cfg_batch* b, int cells) {
+  if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
+  return guarded([&] { return b->eng->set_coarse_w(cells); });
+}
 extern "C" int cfg_set_coarse_cluster(cfg_sim* sim, int cs) {
   SIM_OK(sim); OWNER_OK(sim);
   return guarded([&] { return sim->eng->set_coarse_cluster(cs); });

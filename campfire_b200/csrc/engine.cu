@@ -260,7 +260,7 @@ int Engine::alloc_scene(Scene& sc) {
   const int nt_fr = ((sc.nx + FR_TX - 1) / FR_TX) * ((sc.ny + FR_TY - 1) / FR_TY);
   const int nt_mg0 = ((sc.nx + MG_TX - 1) / MG_TX) * ((sc.ny + MG_TY - 1) / MG_TY);
   const int nt_up0 = ((sc.nx + MGF_TX - 1) / MGF_TX) * ((sc.ny + MGF_TY - 1) / MGF_TY);
-  d.nt_fr = nt_fr; d.nt_mg0 = nt_mg0; d.nt_up0 = nt_up0; d.lc = sc.lc;
+  d.nt_fr = nt_fr; d.nt_mg0 = nt_mg0; d.nt_up0 = nt_up0; d.lc = sc.lc; d.lw = std::min(sc.lw, sc.nlev);
   struct Item { void** ptr; size_t bytes; };
   std::vector<Item> items = {
     {(void**)&d.U, Uf * 4}, {(void**)&d.U2, Uf * 4}, {(void**)&d.fx, Uf * 4},
@@ -503,11 +503,19 @@ int Engine::set_coarse_cells(int cells) {
   CFG_TRY(activate());
   CFG_CUDA(cudaStreamSynchronize(st()));
   const int cs = coarse_cluster_;
+  if (cs > 0 && w_cells_ > 0) return fail(CFG_ERR_INVAL, "the W tail runs in the one-CTA coarse block only");
   size_t smem = 0;
-  std::vector<int> lcs(scenes_.size());
+  std::vector<int> lcs(scenes_.size()), lws(scenes_.size());
   for (size_t s = 0; s < scenes_.size(); s++) {
     const Scene& sc = scenes_[s];
-    lcs[s] = choose_lc(sc, cells, cs);
+    // the W tail: level nlev - 3 (two above the coarsest) visits level nlev - 2 twice when it has
+    // at most w_cells_ cells; it starts the coarse block at the latest
+    int lw = MAX_LEVELS;
+    if (w_cells_ > 0 && sc.nlev >= 3 && sc.lnx[sc.nlev - 3] * sc.lny[sc.nlev - 3] <= w_cells_) lw = sc.nlev - 3;
+    lws[s] = lw;
+    lcs[s] = choose_lc(sc, std::max(cells, lw < sc.nlev ? sc.lnx[lw] * sc.lny[lw] : 0), cs);
+    if (lw < sc.nlev && lcs[s] > lw)
+      return fail(CFG_ERR_RANGE, "the W tail's levels do not fit in the coarse block's shared memory");
     smem = std::max(smem, cs > 0 ? cluster_smem_bytes(sc.lnx, sc.lny, lcs[s], sc.nlev, cs)
                                  : coarse_smem_bytes(sc.lnx, sc.lny, lcs[s], sc.nlev));
   }
@@ -524,6 +532,8 @@ int Engine::set_coarse_cells(int cells) {
   for (size_t s = 0; s < scenes_.size(); s++) {
     scenes_[s].lc = lcs[s];
     scenes_[s].desc.lc = lcs[s];
+    scenes_[s].lw = lws[s];
+    scenes_[s].desc.lw = std::min(lws[s], scenes_[s].nlev);
     CFG_TRY(upload_desc((int)s));
   }
   for (int k = 0; k < WL_COUNT; k++) {
@@ -535,6 +545,21 @@ int Engine::set_coarse_cells(int cells) {
   graph_dirty_ = true;
   CFG_CUDA(cudaStreamSynchronize(st()));
   return CFG_OK;
+}
+
+// The pressure loop's cycle shape: the W tail when the level two above the coarsest has at most
+// `cells` cells (0: the V-cycle). The coarse block is re-chosen so that it holds that level.
+int Engine::set_coarse_w(int cells) {
+  if (cells < 0) return fail(CFG_ERR_INVAL, "W cells must be >= 0");
+  if (cells > 0 && coarse_cluster_ > 0) return fail(CFG_ERR_INVAL, "the W tail runs in the one-CTA coarse block only");
+  const int prev = w_cells_;
+  w_cells_ = cells;
+  const int rc = set_coarse_cells(coarse_cells_);
+  if (rc != CFG_OK) {
+    w_cells_ = prev;
+    set_coarse_cells(coarse_cells_);
+  }
+  return rc;
 }
 
 // Tile shapes of the advection, diffusion + sources and forces kernels (indices into
@@ -1195,6 +1220,10 @@ void Engine::enqueue_vcycle(cudaStream_t s, int tail, int count_iter) {
     launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0 + l], nwl_[WL_MGD0 + l], l, l == 0 ? tail : 0, d_ctl_, s);
     vcycle_launches_++;
   }
+  if (tail == 4) {   // the fused Krylov mode's sums and decision
+    launch_pcg_decide(d_scenes_, nscenes(), d_ctl_, s);
+    vcycle_launches_++;
+  }
 }
 
 // FluidSim.vcycle (js/fluid.js:294-312), nu = 2: one kernel per reference dispatch
@@ -1564,6 +1593,14 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
       go = [&](int) { launch_mg_up(d_scenes_, nscenes(), d_wl_[WL_MGD0], nwl_[WL_MGD0], 0, 4, d_ctl_, s); };
       b = (17 + 4 * 16 + 20) * cells;
     }
+    cnt = cyc;
+  } else if (n == "pcg_decide") {
+    // the fused Krylov mode's per-scene sums and decision: nine partials per level-0 tile read
+    if (!pcg_fused()) return fail(CFG_ERR_NOENT, n + ": the Krylov update is not folded in this engine");
+    go = [&](int) { launch_pcg_decide(d_scenes_, nscenes(), d_ctl_, s); };
+    b = 0;
+    for (int k = 0; k < nscenes(); k++)
+      b += 72.0 * ((scenes_[k].nx + MGF_TX - 1) / MGF_TX) * ((scenes_[k].ny + MGF_TY - 1) / MGF_TY);
     cnt = cyc;
   } else if (n == "mg_coarse") {
     go = [&](int) {

@@ -61,6 +61,7 @@ struct Scene {
   double alpha = 0;              // alpha(2200 K) of the diffusion sub-step rule
   int lnx[MAX_LEVELS] = {}, lny[MAX_LEVELS] = {};
   int lc = 0;                    // first level of the one-CTA coarse block
+  int lw = MAX_LEVELS;           // nlev - 3 with the W tail, else MAX_LEVELS
   void* arena = nullptr;
   size_t arena_bytes = 0;
   SceneDesc desc{};              // host mirror of the device descriptor
@@ -154,6 +155,11 @@ class Engine {
   // most `cells` cells (levels above it run as tiled down/up kernels)
   int set_coarse_cells(int cells);
   int coarse_cells() const { return coarse_cells_; }
+  // cycle shape of the pressure loop: with cells > 0, the level two above the coarsest visits
+  // its coarser level twice per cycle (the W tail) when it has at most `cells` cells; that
+  // level always runs inside the one-CTA coarse block
+  int set_coarse_w(int cells);
+  int coarse_w() const { return w_cells_; }
   // the coarse phase on one CTA (0) or on a cluster of cs CTAs per scene (2..16, from level 1)
   int set_coarse_cluster(int cs);
   int coarse_cluster() const { return coarse_cluster_; }
@@ -258,6 +264,7 @@ class Engine {
   size_t cluster_smem_ = 0;
   int cf_bw_ = 0;               // the widest coarsest level (k_coarse_factor's register window)
   int coarse_cells_ = COARSE_CELLS;
+  int w_cells_ = 0;             // set_coarse_w
   int coarse_direct_ = 0;
   int krylov_ = 0;
   int tiles_[TK_COUNT] = {0, 0, 0};       // tile shape of advection, diffusion + sources, forces

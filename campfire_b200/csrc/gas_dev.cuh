@@ -63,6 +63,7 @@ struct SceneDesc {
   int nt_fr, nt_mg0;        // tiles of this scene in the forces and level-0 multigrid work lists
   int nt_up0;               // tiles of this scene in the level-0 fused up-smoother work list
   int lc;                   // first level of the one-CTA coarse block (levels lc..nlev-1)
+  int lw;                   // nlev - 3: the coarse block's W tail (that level visits the next twice); nlev: none
   float *U, *V, *U2, *V2, *T, *T2, *Tw;   // Tw: diffusion ping-pong buffer
   float4 *Y, *Y2, *Yw;
   float2 *SQ, *cellG;

@@ -208,8 +208,10 @@ __device__ __forceinline__ void tile_passes(const Tile& t, const LevelDesc& L, i
 // new rhs0 = f32(r - alpha q) on pass 1's region from the stored r, q, Lz (read only
 // there, so no CTA reads a value another rewrites); the next up kernel rewrites r and q on
 // its tile before its dot products; the update of the last cycle is applied by
-// k_pcg_finish after the loop. The up kernel also returns ||r_c||^2 = r.r - 2 alpha r.q_c +
-// alpha^2 q_c.q_c (q_c = Lz + beta q) from its dot products, for the loop decision.
+// k_pcg_finish after the loop. The up kernel's tiles leave their nine dot products as
+// partials; k_pcg_decide (one CTA per scene, the next kernel) sums them, forms the cycle's
+// alpha and beta, and ||r_c||^2 = r.r - 2 alpha r.q_c + alpha^2 q_c.q_c (q_c = Lz + beta q)
+// for the loop decision.
 // This thread's share of the down kernel's update: up to 4 cells of pass 1's region and
 // 2 tile cells, with their stored values loaded right after the wait.
 struct PcgDown {
@@ -389,11 +391,9 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
   const bool live = *(volatile int*)&ss->active != 0;
   // fused Krylov mode: the solve state and this thread's stored r, q, Lz, read beside the copies
   PcgPrev pv{};
-  DecideIn din{};
   double r0[2] = {0.0, 0.0}, q0[2] = {0.0, 0.0}, lz0[2] = {0.0, 0.0};
   if (KRY) {
     pv = pcg_load(ss);
-    din = decide_load(ctl, ss);
     #pragma unroll
     for (int m = 0; m < 2; m++) {
       const int e = threadIdx.x + 256 * m;
@@ -445,17 +445,13 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
       v[0] += r * z; v[1] += q * z; v[2] += z * lz;
       v[3] += r * r; v[4] += r * lz; v[5] += r * q; v[6] += lz * lz; v[7] += lz * q; v[8] += q * q;
     }
+    // the tile's nine partials, quantity-major (part[m * nt_up0 + tile]); k_pcg_decide sums
+    // them once this kernel has completed (no arrival, no fence in these CTAs)
     __shared__ double redt[9 * 256 + 9];
     block_sum_t<9>(v, redt);
-    if (scene_reduce_n<9>(S, w.tile, S.nt_up0, v, redt) && threadIdx.x == 0) {
-      double alpha, beta;
-      pcg_coef(ss, pv, v[0], v[1], v[2], &alpha, &beta);
-      // ||r - alpha (Lz + beta q)||^2 from the dot products
-      const double rq = v[4] + beta * v[5];
-      const double qq = v[6] + 2.0 * beta * v[7] + beta * beta * v[8];
-      const double r2 = v[3] - 2.0 * alpha * rq + alpha * alpha * qq;
-      solve_decide(ctl, ss, din, r2 > 0.0 ? r2 : 0.0, true);
-    }
+    if (threadIdx.x == 0)
+      #pragma unroll
+      for (int m = 0; m < 9; m++) S.part[m * S.nt_up0 + w.tile] = v[m];
     return;
   }
   double part = 0.0, part2 = 0.0, part3 = 0.0;
@@ -493,6 +489,54 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
   const double bp = block_sum(part, red);
   double total = 0.0;
   if (scene_reduce(S, w.tile, S.nt_up0, bp, red, &total) && threadIdx.x == 0) solve_decide(ctl, ss, total, true);
+}
+
+// ------------------------------------------------------------------ fused Krylov mode: the loop decision
+// One CTA per scene, after the level-0 up kernel has completed: the nine sums over the scene's
+// tiles (thread t adds tiles t, t + 256, ... in that order, four tiles' loads in flight at a
+// time; then block_sum_t's fixed order), the cycle's coefficients and the decision. A scene
+// that is disabled or no longer cycles wrote no partials and does not decide.
+__global__ void __launch_bounds__(256) k_pcg_decide(const SceneDesc* __restrict__ scenes, SolveCtl* ctl) {
+  const SceneDesc& S = scenes[blockIdx.x];
+  pdl_trigger();
+  const bool on = S.enabled;   // host-written, constant during the step
+  const int nt = S.nt_up0;
+  SolveState* ss = S.solve;
+  pdl_wait();
+  // the flag, the solve state and the partials are read together (the partial array is always
+  // allocated; a scene that stopped leaves stale values, which are loaded but not used)
+  const int act = *(volatile int*)&ss->active;
+  PcgPrev pv{};
+  DecideIn din{};
+  if (threadIdx.x == 0) {
+    pv = pcg_load(ss);
+    din = decide_load(ctl, ss);
+  }
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k0 = threadIdx.x; k0 < nt; k0 += 4 * 256) {
+    double a[4][9];
+    #pragma unroll
+    for (int j = 0; j < 4; j++)
+      #pragma unroll
+      for (int m = 0; m < 9; m++) a[j][m] = k0 + 256 * j < nt ? __ldcg(S.part + (size_t)m * nt + k0 + 256 * j) : 0.0;
+    #pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (k0 + 256 * j < nt)
+        #pragma unroll
+        for (int m = 0; m < 9; m++) v[m] += a[j][m];
+  }
+  if (!on || act == 0) return;   // the same in every thread of the CTA
+  __shared__ double redt[9 * 256 + 9];
+  block_sum_t<9>(v, redt);
+  if (threadIdx.x == 0) {
+    double alpha, beta;
+    pcg_coef(ss, pv, v[0], v[1], v[2], &alpha, &beta);
+    // ||r - alpha (Lz + beta q)||^2 from the dot products
+    const double rq = v[4] + beta * v[5];
+    const double qq = v[6] + 2.0 * beta * v[7] + beta * beta * v[8];
+    const double r2 = v[3] - 2.0 * alpha * rq + alpha * alpha * qq;
+    solve_decide(ctl, ss, din, r2 > 0.0 ? r2 : 0.0, true);
+  }
 }
 
 // ------------------------------------------------------------------ coarse block: levels lc..coarsest in one CTA
@@ -620,6 +664,128 @@ __device__ __forceinline__ void smooth_visit(const LvS& L, int first) {
   const LinMap mh(half, L.mhalf);
   for (int k = 0; k < 2; k++) { pass_d(L, first, mh); __syncthreads(); pass_d(L, 1 - first, mh); __syncthreads(); }
 }
+// The coarse block's level visits (k_mg_coarse), and what they read beside the block's shared
+// memory.
+struct CbCtx {
+  float* smem;
+  const LvO* lvo;     // level offsets in smem (shared)
+  float* sres;        // residual scratch (level lc size)
+  const SceneDesc* S;
+  int nl, s_dir, s_inv, s_A;
+};
+// level l's visit on the way down: smoothing, then per coarse cell the residuals of its four
+// fine cells summed in the restriction's order
+__device__ __forceinline__ void cb_down(const CbCtx c, int l) {
+  float* const smem = c.smem;
+  const LvO* const lvo = c.lvo;
+    const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
+    smooth_visit(F, 0);
+    auto res = [&](int i, int j) {
+      float off, diag; stencil_d(F, i, j, off, diag);
+      const int e = j * F.pc + i;
+      return diag <= 0.f ? 0.f : F.rhs[e] - div_by_rcp(off - diag * F.p[e], F.h2, F.rh2);
+    };
+    const LinMap mc(Cc.nx, Cc.mnx);
+    if (mc.R)
+    for (int J = mc.j0; J < Cc.ny; J += mc.R)
+      for (int I = mc.i0; I < Cc.nx; I += mc.di(Cc.nx)) {
+        const float r = res(2 * I, 2 * J) + res(2 * I + 1, 2 * J) + res(2 * I, 2 * J + 1) + res(2 * I + 1, 2 * J + 1);
+        Cc.rhs[J * Cc.pc + I] = 0.25f * r;
+        Cc.p[J * Cc.pc + I] = 0.f;
+      }
+    __syncthreads();
+}
+// the coarsest level's solve (its p overwritten: the inverse's product, or sweeps from zero)
+__device__ __forceinline__ void cb_coarsest(const CbCtx c) {
+  float* const smem = c.smem;
+  const LvO* const lvo = c.lvo;
+  float* const sres = c.sres;
+  const SceneDesc& S = *c.S;
+  const int nl = c.nl, s_dir = c.s_dir, s_inv = c.s_inv, s_A = c.s_A;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // ---- coarsest (pressure.wgsl:132-156): 120 red-black sweeps from zero. Row-major
+    // cells 2t and 2t+1 have opposite colours for any nx (even nx: same row, adjacent;
+    // odd nx: colour = index parity), so thread t owns one cell of each colour and every
+    // thread works in every pass; the ceil(n/2) threads (<= 128, rounded up to warps)
+    // sync on a named barrier while the other warps wait at the block barrier below.
+    // Stencils, diagonals and their reciprocals stay in registers for all sweeps.
+    if (s_dir) {
+      // direct coarse solve (TOL/FP64 modes): p = A^-1 b with b = -rhs h2 (0 in closed cells),
+      // each row's dot product as 8 strided partial sums combined pairwise (the oracle's order)
+      const LvS L = lvs_at(smem, lvo[nl - 1]);
+      const int n = L.nx * L.ny;
+      for (int k = threadIdx.x; k < n; k += CB_THREADS) {
+        const int j = fdiv(k, L.mnx), i = k - j * L.nx;
+        sres[k] = L.rc[k] > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
+      }
+      __syncthreads();
+      const int q = lane & 7;
+      const bool staged = s_inv != 0;
+      // the global copy is addressed only when the inverse is not staged
+      const float* Ag = staged ? nullptr : S.cinv + (size_t)S.solve->cinv_cur * n * n;
+      const float* As = smem + s_A;
+      for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
+        const int k = base + (lane >> 3);
+        float sum = 0.f;
+        if (k < n) {
+          if (staged) {
+            #pragma unroll 4
+            for (int m = q; m < n; m += 8) sum = __fmaf_rn(As[k * n + m], sres[m], sum);
+          } else {
+            #pragma unroll 4
+            for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(Ag + (size_t)k * n + m), sres[m], sum);
+          }
+        }
+        sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+        sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+        sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+        if (k < n && q == 0) { const int j = fdiv(k, L.mnx); L.p[j * L.pc + k - j * L.nx] = sum; }
+      }
+    } else {
+      const LvS L = lvs_at(smem, lvo[nl - 1]);
+      const int npair = (L.nx * L.ny + 1) >> 1;
+      const int nthr = (npair + 31) & ~31;
+      if ((int)threadIdx.x < nthr) {
+        const CCell a = coarsest_cell(L, 2 * threadIdx.x), b = coarsest_cell(L, 2 * threadIdx.x + 1);
+        if (a.act) L.p[a.kp] = 0.f;
+        if (b.act) L.p[b.kp] = 0.f;
+        // colour of cell 2t: (i + j) & 1
+        const int k0 = 2 * threadIdx.x;
+        const int j0 = fdiv(k0, L.mnx);
+        const bool a_red = ((k0 - j0 * L.nx + j0) & 1) == 0;
+        const CCell c0 = a_red ? a : b, c1 = a_red ? b : a;
+        float* p = L.p;
+        bar_coarsest(nthr);
+        #pragma unroll 1
+        for (int it = 0; it < 120; it++) {
+          coarsest_update(p, L.pc, c0);
+          bar_coarsest(nthr);
+          coarsest_update(p, L.pc, c1);
+          bar_coarsest(nthr);
+        }
+      }
+    }
+    __syncthreads();
+}
+// level l's visit on the way up: prolongation of level l + 1's p, then smoothing
+__device__ __forceinline__ void cb_up(const CbCtx c, int l) {
+  float* const smem = c.smem;
+  const LvO* const lvo = c.lvo;
+    const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
+    const LinMap mp(F.nx, F.mnx);
+    if (mp.R)
+    for (int j = mp.j0; j < F.ny; j += mp.R)
+      for (int i = mp.i0; i < F.nx; i += mp.di(F.nx)) {
+        const int I = i / 2, J = j / 2;
+        const int I2 = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), Cc.nx - 1);
+        const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), Cc.ny - 1);
+        const float c = 0.5625f * Cc.p[J * Cc.pc + I] + 0.1875f * (Cc.p[J * Cc.pc + I2] + Cc.p[J2 * Cc.pc + I]) +
+                        0.0625f * Cc.p[J2 * Cc.pc + I2];
+        F.p[j * F.pc + i] += F.rc[j * F.nx + i] > 0.f ? c : 0.f;
+      }
+    __syncthreads();
+    smooth_visit(F, 1);
+}
 }  // namespace
 
 // smem_floats: the launch's dynamic shared memory in floats; past the levels and the residual
@@ -730,106 +896,20 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
     for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.p[e] = __ldcg(s_gp + e);
   if (still == 0) return;
   __syncthreads();
-  // ---- down: smoothing, then per coarse cell the residuals of its four fine cells
-  // (pressure.wgsl:96-101) summed in the restriction's order (pressure.wgsl:104-113)
-  for (int l = lc; l < nl - 1; l++) {
-    const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
-    smooth_visit(F, 0);
-    auto res = [&](int i, int j) {
-      float off, diag; stencil_d(F, i, j, off, diag);
-      const int e = j * F.pc + i;
-      return diag <= 0.f ? 0.f : F.rhs[e] - div_by_rcp(off - diag * F.p[e], F.h2, F.rh2);
-    };
-    const LinMap mc(Cc.nx, Cc.mnx);
-    if (mc.R)
-    for (int J = mc.j0; J < Cc.ny; J += mc.R)
-      for (int I = mc.i0; I < Cc.nx; I += mc.di(Cc.nx)) {
-        const float r = res(2 * I, 2 * J) + res(2 * I + 1, 2 * J) + res(2 * I, 2 * J + 1) + res(2 * I + 1, 2 * J + 1);
-        Cc.rhs[J * Cc.pc + I] = 0.25f * r;
-        Cc.p[J * Cc.pc + I] = 0.f;
-      }
-    __syncthreads();
+  const CbCtx cbx{smem, lvo, sres, &S, nl, s_dir, s_inv, s_A};
+  // The cycle over levels lc..nl-1: the V(2,2) cycle of js/fluid.js:294-312, straight down, the
+  // coarsest, straight up. With the W tail (S.lw = nl - 3) level nl - 3 visits level nl - 2
+  // twice: after the first visit has come back up through level nl - 2, that level is smoothed
+  // from its p and restricted again (its rhs stays) and the coarsest solved again. Straight-line
+  // code: the visits keep their registers to themselves.
+  for (int l = lc; l < nl - 1; l++) cb_down(cbx, l);
+  cb_coarsest(cbx);
+  if (S.lw == nl - 3 && nl - 3 >= lc) {
+    cb_up(cbx, nl - 2);
+    cb_down(cbx, nl - 2);
+    cb_coarsest(cbx);
   }
-  // ---- coarsest (pressure.wgsl:132-156): 120 red-black sweeps from zero. Row-major
-  // cells 2t and 2t+1 have opposite colours for any nx (even nx: same row, adjacent;
-  // odd nx: colour = index parity), so thread t owns one cell of each colour and every
-  // thread works in every pass; the ceil(n/2) threads (<= 128, rounded up to warps)
-  // sync on a named barrier while the other warps wait at the block barrier below.
-  // Stencils, diagonals and their reciprocals stay in registers for all sweeps.
-  if (s_dir) {
-    // direct coarse solve (TOL/FP64 modes): p = A^-1 b with b = -rhs h2 (0 in closed cells),
-    // each row's dot product as 8 strided partial sums combined pairwise (the oracle's order)
-    const LvS L = lvs_at(smem, lvo[nl - 1]);
-    const int n = L.nx * L.ny;
-    for (int k = threadIdx.x; k < n; k += CB_THREADS) {
-      const int j = fdiv(k, L.mnx), i = k - j * L.nx;
-      sres[k] = L.rc[k] > 0.f ? -(L.rhs[j * L.pc + i] * L.h2) : 0.f;
-    }
-    __syncthreads();
-    const int q = lane & 7;
-    const bool staged = s_inv != 0;
-    // the global copy is addressed only when the inverse is not staged
-    const float* Ag = staged ? nullptr : S.cinv + (size_t)S.solve->cinv_cur * n * n;
-    const float* As = smem + s_A;
-    for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
-      const int k = base + (lane >> 3);
-      float sum = 0.f;
-      if (k < n) {
-        if (staged) {
-          #pragma unroll 4
-          for (int m = q; m < n; m += 8) sum = __fmaf_rn(As[k * n + m], sres[m], sum);
-        } else {
-          #pragma unroll 4
-          for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(Ag + (size_t)k * n + m), sres[m], sum);
-        }
-      }
-      sum += __shfl_xor_sync(0xffffffffu, sum, 1);
-      sum += __shfl_xor_sync(0xffffffffu, sum, 2);
-      sum += __shfl_xor_sync(0xffffffffu, sum, 4);
-      if (k < n && q == 0) { const int j = fdiv(k, L.mnx); L.p[j * L.pc + k - j * L.nx] = sum; }
-    }
-  } else {
-    const LvS L = lvs_at(smem, lvo[nl - 1]);
-    const int npair = (L.nx * L.ny + 1) >> 1;
-    const int nthr = (npair + 31) & ~31;
-    if ((int)threadIdx.x < nthr) {
-      const CCell a = coarsest_cell(L, 2 * threadIdx.x), b = coarsest_cell(L, 2 * threadIdx.x + 1);
-      if (a.act) L.p[a.kp] = 0.f;
-      if (b.act) L.p[b.kp] = 0.f;
-      // colour of cell 2t: (i + j) & 1
-      const int k0 = 2 * threadIdx.x;
-      const int j0 = fdiv(k0, L.mnx);
-      const bool a_red = ((k0 - j0 * L.nx + j0) & 1) == 0;
-      const CCell c0 = a_red ? a : b, c1 = a_red ? b : a;
-      float* p = L.p;
-      bar_coarsest(nthr);
-      #pragma unroll 1
-      for (int it = 0; it < 120; it++) {
-        coarsest_update(p, L.pc, c0);
-        bar_coarsest(nthr);
-        coarsest_update(p, L.pc, c1);
-        bar_coarsest(nthr);
-      }
-    }
-  }
-  __syncthreads();
-  // ---- up
-  for (int l = nl - 2; l >= lc; l--) {
-    const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
-    const LinMap mp(F.nx, F.mnx);
-    if (mp.R)
-    for (int j = mp.j0; j < F.ny; j += mp.R)
-      for (int i = mp.i0; i < F.nx; i += mp.di(F.nx)) {
-        const int I = i / 2, J = j / 2;
-        const int I2 = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), Cc.nx - 1);
-        const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), Cc.ny - 1);
-        const float c = 0.5625f * Cc.p[J * Cc.pc + I] + 0.1875f * (Cc.p[J * Cc.pc + I2] + Cc.p[J2 * Cc.pc + I]) +
-                        0.0625f * Cc.p[J2 * Cc.pc + I2];
-        F.p[j * F.pc + i] += F.rc[j * F.nx + i] > 0.f ? c : 0.f;
-      }
-    __syncthreads();
-    smooth_visit(F, 1);
-  }
+  for (int l = nl - 2; l >= lc; l--) cb_up(cbx, l);
   // ---- write level lc back; when the block covers level 0, finish the cycle here
   float* const gp = s_gp;
   const int gpc = s_gpc, gnx = V0.nx;
@@ -1071,6 +1151,9 @@ void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int nt
   if (ntiles > 0)
     launch_pdl(pdl_enabled(), tail == 4 ? k_mg_up<MGF_TX, MGF_TY, true> : k_mg_up<MGF_TX, MGF_TY, false>, dim3(ntiles),
                dim3(256), 0, st, scenes, nscenes, work, level, tail, ctl);
+}
+void launch_pcg_decide(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, cudaStream_t st) {
+  if (nscenes > 0) launch_pdl(pdl_enabled(), k_pcg_decide, dim3(nscenes), dim3(256), 0, st, scenes, ctl);
 }
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
                       cudaStream_t st) {

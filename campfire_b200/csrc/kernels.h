@@ -104,6 +104,9 @@ void launch_mg_down(const SceneDesc* scenes, int nscenes, const Work* work, int 
                     int count_iter, int pcg, cudaStream_t st);
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st);
+// after the level-0 up kernel with tail 4: each scene's dot products summed, the coefficients
+// and the loop decision (one CTA per scene)
+void launch_pcg_decide(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, cudaStream_t st);
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
                       cudaStream_t st);
 size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);

@@ -314,6 +314,12 @@ int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int 
   return CFG_OK;
 }
 
+int cfg_server_set_coarse_w(cfg_server* s, int cells) {
+  if (!s) return cfg::fail(CFG_ERR_INVAL, "null cfg_server handle");
+  if (server_busy(s)) return cfg::fail(CFG_ERR_BUSY, "the server is running jobs: drain it first");
+  return s->eng.set_coarse_w(cells);
+}
+
 int cfg_server_slot_bytes(cfg_server* s, int size_class, size_t* bytes) {
   if (!s || !bytes) return cfg::fail(CFG_ERR_INVAL, "null argument");
   for (size_t k = 0; k < s->slot_class.size(); k++)

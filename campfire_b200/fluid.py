@@ -282,6 +282,11 @@ class FluidSim(_SceneOps):
         """The coarse phase on one CTA (0) or on a cluster of cs CTAs (2, 4, 8, 16); bit-identical."""
         check(_lib.lib().cfg_set_coarse_cluster(self._h, int(cs)))
 
+    def set_coarse_w(self, cells: int):
+        """Cycle shape: the W tail (the level two above the coarsest, if it has <= cells cells, visits the
+        next level twice per cycle); 0: the V-cycle."""
+        check(_lib.lib().cfg_set_coarse_w(self._h, int(cells)))
+
     def set_coarse_solve(self, direct):
         """TOL/FP64 modes: the coarsest level by its inverse (True), by 120 sweeps (False), or by the
         inverse factored beside the previous step's solve ("pipelined")."""
@@ -367,6 +372,9 @@ class Batch:
     def set_coarse_cluster(self, cs: int):
         check(_lib.lib().cfg_batch_set_coarse_cluster(self._h, int(cs)))
 
+    def set_coarse_w(self, cells: int):
+        check(_lib.lib().cfg_batch_set_coarse_w(self._h, int(cells)))
+
     def set_krylov(self, on):
         """True / 1: on (the update kernel for a batch); 2: on, update folded into the level-0 kernels;
         3: on, separate update kernel; False / 0: plain defect correction."""
@@ -425,9 +433,10 @@ class Server:
             pass
 
     def set_solver(self, mode=_lib.SOLVE_FP64, ncycles=1, tol=1e-10, max_cycles=300, coarse_direct=True,
-                   coarse_cells=0, krylov=False):
+                   coarse_cells=0, krylov=False, coarse_w=0):
         check(_lib.lib().cfg_server_set_solver(self._h, mode, ncycles, tol, max_cycles, _coarse_mode(coarse_direct),
                                                coarse_cells, int(krylov)))
+        check(_lib.lib().cfg_server_set_coarse_w(self._h, int(coarse_w)))
 
     def slot_bytes(self, size_class: int) -> int:
         b = ctypes.c_size_t()

@@ -195,8 +195,8 @@ int cfg_launch_count(cfg_sim* sim, int* per_step);
  * "prolong0", "coarsest", "resnorm", "mg_down0", "mg_up0", "mg_coarse", "vcycle"
  * (one fused V-cycle), "defect64", "project", "mg_downL" / "mg_upL" (level L below the coarse
  * block), "mg_down0_krylov" / "mg_up0_krylov" (the level-0 kernels with the Krylov update folded
- * in, as the step runs them when it is), "pcg_step", "coarse_factor". The state changes as the
- * kernel runs. */
+ * in, as the step runs them when it is), "pcg_decide" (that mode's per-scene sums and loop decision),
+ * "pcg_step", "coarse_factor". The state changes as the kernel runs. */
 int cfg_time_kernel(cfg_sim* sim, const char* kernel, int iters, double* mean_ms, double* bytes_per_launch,
                     double* launches_per_step);
 
@@ -210,6 +210,18 @@ int cfg_set_coarse_cells(cfg_sim* sim, int cells);
  * at the earliest; level 0 stays tiled). Results are bit-identical for every choice. */
 int cfg_set_coarse_cluster(cfg_sim* sim, int cs);
 int cfg_batch_set_coarse_cluster(cfg_batch* b, int cs);
+/* Cycle shape of the pressure loop (no counterpart in the reference, whose V(2,2) cycle of
+ * js/fluid.js:294-312 is the default, cells = 0): the W tail. When the level two above the
+ * coarsest has at most `cells` cells, it visits the level below it twice per cycle: after the
+ * first visit has come back up, that level is smoothed on from its result and restricted
+ * again, and the coarsest is solved again. The level runs inside the one-CTA coarse block,
+ * which then starts there at the latest; results do not depend on cfg_set_coarse_cells. A
+ * better coarse correction per cycle for the FP64 loop's preconditioner (fewer cycles to the
+ * same tolerance on scenes whose coarse levels limit the convergence) for a few block phases.
+ * CFG_ERR_INVAL with a cluster coarse phase; CFG_ERR_RANGE if that level does not fit in one
+ * CTA's shared memory. */
+int cfg_set_coarse_w(cfg_sim* sim, int cells);
+int cfg_batch_set_coarse_w(cfg_batch* b, int cells);
 /* Coarsest-level solve of the TOL and FP64 modes (no counterpart in the reference, which runs
  * one fixed cycle): 0 (default) the reference's 120 red-black sweeps; 1 the level's operator
  * inverted once per step (f32 banded Cholesky and column solves, after the coefficients are
@@ -438,6 +450,8 @@ int cfg_server_destroy(cfg_server* s);
  * keeps it) and cfg_set_krylov, whose 0-3 it takes) */
 int cfg_server_set_solver(cfg_server* s, int mode, int ncycles, double tol, int max_cycles, int coarse_direct,
                           int coarse_cells, int krylov);
+/* cycle shape of every slot (as cfg_set_coarse_w); CFG_ERR_BUSY while jobs run */
+int cfg_server_set_coarse_w(cfg_server* s, int cells);
 /* device bytes of one slot of a size class */
 int cfg_server_slot_bytes(cfg_server* s, int size_class, size_t* bytes);
 /* run the jobs to completion in real time (arrivals are honoured by the host clock);

@@ -164,6 +164,7 @@ struct Sim {
   // runs one fixed cycle with the 120-sweep coarsest level)
   int coarse_direct = 0;
   int krylov = 0;   // FP64 mode: flexible preconditioned CG around the FP32 V-cycle (extension)
+  long w_cells = 0; // cycle shape of the solve loop (extension): the W tail (cycle_at)
   std::vector<R> cinv;
   bool cinv_ok = false;
   std::vector<double> p64, rhs64;   // FP64 defect correction state (level 0)
@@ -869,6 +870,23 @@ struct Sim {
       for (int s = 0; s < nu; s++) { relax(l, 1); relax(l, 0); }
     }
   }
+  // The solve loop's cycle (extension of the library): the V-cycle above, or with w_cells > 0 the
+  // W tail: the level two above the coarsest, if it has at most w_cells cells, visits the next
+  // level twice per visit (the second visit smooths on from the first one's p; that level's rhs
+  // is restricted once)
+  void cycle_at(int l, bool direct) {
+    const int NL = (int)lv.size();
+    if (l == NL - 1) { if (direct) coarsest_direct(NL - 1); else coarsest(NL - 1); return; }
+    for (int s = 0; s < 2; s++) { relax(l, 0); relax(l, 1); }
+    restrictRes(l);
+    const int g = (l == NL - 3 && (long)lv[l].nx * lv[l].ny <= w_cells) ? 2 : 1;
+    for (int k = 0; k < g; k++) cycle_at(l + 1, direct);
+    prolong(l);
+    for (int s = 0; s < 2; s++) { relax(l, 1); relax(l, 0); }
+  }
+  void cycle(bool direct = false) {
+    if (w_cells > 0) cycle_at(0, direct); else vcycle(2, direct);
+  }
   // :159-180
   void project() {
     const std::vector<R>& p = lv[0].p;
@@ -963,7 +981,7 @@ struct Sim {
     int c = 0;
     while (b > 0 && rn / b > tol && c < max_cycles) {
       for (size_t k = 0; k < n; k++) { L0.rhs[k] = R((float)r[k]); L0.p[k] = R(0); }
-      vcycle(2, direct);
+      cycle(direct);
       for (size_t k = 0; k < n; k++) z[k] = (double)L0.p[k];
       lap64(z, lz);
       // delta = r.z, eta = q.z, zeta = z.Lz; beta (Polak-Ribiere); d.q = zeta + 2 beta eta +
@@ -1034,7 +1052,7 @@ struct Sim {
   }
   void pressure_solve_inner() {
     if (mode == SOLVE_FIXED) {
-      for (int c = 0; c < ncycles; c++) vcycle();
+      for (int c = 0; c < ncycles; c++) cycle();
       last_cycles = ncycles;
       const double b = rhs_norm(); last_rel = b > 0 ? res_norm() / b : 0.0;
       return;
@@ -1044,7 +1062,7 @@ struct Sim {
     if (mode == SOLVE_TOL) {
       const double b = rhs_norm();
       int c = 0; double rel = 0;
-      do { vcycle(2, direct); c++; rel = b > 0 ? res_norm() / b : 0.0; } while (rel > tol && c < max_cycles);
+      do { cycle(direct); c++; rel = b > 0 ? res_norm() / b : 0.0; } while (rel > tol && c < max_cycles);
       last_cycles = c; last_rel = rel;
       return;
     }
@@ -1059,7 +1077,7 @@ struct Sim {
     Level& L0 = lv[0];
     while (b > 0 && rn / b > tol && c < max_cycles) {
       for (size_t k = 0; k < r.size(); k++) { L0.rhs[k] = R((float)r[k]); L0.p[k] = R(0); }
-      vcycle(2, direct); c++;
+      cycle(direct); c++;
       for (size_t k = 0; k < r.size(); k++) p64[k] += (double)L0.p[k];
       rn = res64(r);
     }

@@ -63,6 +63,7 @@ def _declare(L, pfx):
                      ctypes.POINTER(ctypes.c_int32)],
         "budgets": [vp, dp], "info": [vp, dp], "level_dims": [vp, ci, ctypes.POINTER(ctypes.c_int)],
         "pressure_residual": [vp, dp], "set_coarse_solve": [vp, ci], "set_krylov": [vp, ci],
+        "set_coarse_w": [vp, ci],
         "render": [vp, vp, ctypes.POINTER(ctypes.c_float), ci, ci, ctypes.POINTER(ctypes.c_float)],
     }
     for name, args in sigs.items():
@@ -170,6 +171,10 @@ class OracleSim:
 
     def set_krylov(self, on):
         self._chk(self._f.set_krylov(self._h, 1 if on else 0))
+
+    def set_coarse_w(self, cells: int):
+        """The solve loop's cycle: the W tail when the level two above the coarsest has <= cells cells (0: V-cycle)."""
+        self._chk(self._f.set_coarse_w(self._h, int(cells)))
 
     def upload_pieces(self, data, n):
         a = np.zeros(64 * 20, np.float32)

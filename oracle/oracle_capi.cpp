@@ -163,6 +163,7 @@ int orc_set_solver(void* h, int mode, int ncycles, double tol, int max_cycles) {
 }
 int orc_set_coarse_solve(void* h, int direct) { DISPATCH(h, s.coarse_direct = direct; return 0); }
 int orc_set_krylov(void* h, int on) { DISPATCH(h, s.krylov = on; return 0); }
+int orc_set_coarse_w(void* h, int cells) { DISPATCH(h, s.w_cells = cells; return 0); }
 int orc_upload_pieces(void* h, const float* data, int n) {
   DISPATCH(h, {
     if (n < 0 || n > MAX_PIECES) { g_err = "piece count out of range"; return -22; }

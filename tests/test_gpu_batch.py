@@ -60,7 +60,9 @@ def test_inactive_scene_is_left_untouched():
 def test_batch_krylov_update_folded_matches_its_own_kernel():
     """The Krylov direction update of a batch folded into the level-0 smoother kernels (krylov 2) or
     run as its own kernel per cycle (krylov 3): the same iteration, so the same cycle counts (within
-    one: the stopping test's rounding) and pressures to 1e-7, with one launch per cycle fewer."""
+    one: the stopping test's rounding) and pressures to 1e-7. Each cycle ends with one kernel in
+    both forms (the folded form's per-scene sums and decision, or the update kernel); the folded
+    form adds one launch per step, its last update after the loop."""
     from conftest import norm_err
     dims = [(96, 144), (128, 192), (64, 96)]
     scenes = [cb.generate_scene(2, nx, ny, 0.8, 2100 + k) for k, (nx, ny) in enumerate(dims)]
@@ -83,4 +85,5 @@ def test_batch_krylov_update_folded_matches_its_own_kernel():
         assert norm_err(out[2][1][k], out[3][1][k]) <= 1e-7, k
         for f in ("T", "U", "V"):
             assert norm_err(out[2][2][k][f], out[3][2][k][f]) <= 1e-6, (k, f)
-    assert out[2][3] < out[3][3], (out[2][3], out[3][3])
+    if out[2][0][0] == out[3][0][0]:   # launches per step are counted with scene 0's cycles
+        assert out[2][3] == out[3][3] + 1, (out[2][3], out[3][3])

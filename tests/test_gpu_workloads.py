@@ -7,7 +7,8 @@ GPU against the CPU oracle from the same state.
          per step (the pressure loop a device-side WHILE node)
   fine   512x768, five-log tepee: the same solver to 1e-10, seven multigrid levels (the
          reference caps the hierarchy at six, js/fluid.js:72, 91; 512x768 needs seven to end
-         at <= 256 cells)
+         at <= 256 cells), the cycle with the W tail (the 1536-cell level visits the next one
+         twice, inside the coarse block); also with the V-cycle throughout
 
 The GPU runs a few steps from the generated scene first, so the pipelined coarsest inverse,
 the FP64 pressure and the CFL step are all carried over from earlier steps; its whole state
@@ -25,33 +26,35 @@ from conftest import norm_err
 pytestmark = pytest.mark.gpu
 
 CFL, DT_CAP = 0.5, 2e-3
-WORKLOADS = {"plain": (256, 384, 0, 1235, 1e-6, 200), "fine": (512, 768, 1, 1236, 1e-10, 300)}
+# name: nx, ny, scene kind, seed, tol, max cycles, W cells (the cycle shape the benchmark times)
+WORKLOADS = {"plain": (256, 384, 0, 1235, 1e-6, 200, 0), "fine": (512, 768, 1, 1236, 1e-10, 300, 1536)}
 
 
-def configure(sim, tol, max_cycles):
+def configure(sim, tol, max_cycles, w_cells):
     sim.set_solver(cb.SOLVE_FP64, 1, tol, max_cycles)
     sim.set_coarse_solve("pipelined")
     sim.set_krylov(True)
     sim.set_cfl(CFL, DT_CAP)
+    sim.set_coarse_w(w_cells)
 
 
-def gpu_run(name, warm_steps):
-    nx, ny, kind, seed, tol, maxc = WORKLOADS[name]
+def gpu_run(name, warm_steps, w_cells=None):
+    nx, ny, kind, seed, tol, maxc, w = WORKLOADS[name]
     sc = cb.generate_scene(kind, nx, ny, 0.8, seed)
     g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
     load_scene(g, sc)
-    configure(g, tol, maxc)
     g.set_coarse_cells(1536)
+    configure(g, tol, maxc, w if w_cells is None else w_cells)
     g.set_graphs(True)
     g.step(warm_steps)
     return g, sc
 
 
-def oracle_from(oracle_mod, g, sc, name, fp64=False):
-    nx, ny, kind, seed, tol, maxc = WORKLOADS[name]
+def oracle_from(oracle_mod, g, sc, name, fp64=False, w_cells=None):
+    nx, ny, kind, seed, tol, maxc, w = WORKLOADS[name]
     o = oracle_mod.OracleSim(nx, ny, 0.8, sc["dt"], fp64=fp64)
     load_scene(o, sc)
-    configure(o, tol, maxc)
+    configure(o, tol, maxc, w if w_cells is None else w_cells)
     o.copy_state_from(g, CFL, DT_CAP)
     return o
 
@@ -73,11 +76,11 @@ def rel_errors(read_a, read_ref):
     return out
 
 
-@pytest.mark.parametrize("name,warm", [("plain", 4), ("fine", 3)])
-def test_benchmarked_solver_matches_oracle(oracle_mod, name, warm):
-    nx, ny, kind, seed, tol, maxc = WORKLOADS[name]
-    g, sc = gpu_run(name, warm)
-    o = oracle_from(oracle_mod, g, sc, name)
+@pytest.mark.parametrize("name,warm,w_cells", [("plain", 4, None), ("fine", 3, None), ("fine", 3, 0)])
+def test_benchmarked_solver_matches_oracle(oracle_mod, name, warm, w_cells):
+    nx, ny, kind, seed, tol, maxc, w = WORKLOADS[name]
+    g, sc = gpu_run(name, warm, w_cells)
+    o = oracle_from(oracle_mod, g, sc, name, w_cells=w_cells)
     assert int(o.info()["levels"]) == g.info()["levels"] == (7 if name == "fine" else 6)
     for k in range(2):
         g.step(1)
