@@ -1182,6 +1182,11 @@ bool Engine::any_cfl() const {
   return false;
 }
 
+bool Engine::any_wtail() const {
+  for (auto& sc : scenes_) if (sc.lw < sc.nlev) return true;
+  return false;
+}
+
 bool Engine::pcg_fused() const {
   // krylov 1: one scene folds the update into the level-0 kernels (a shorter kernel chain); a
   // batch, bound by bandwidth, keeps the separate update kernel, which moves fewer bytes.
@@ -1213,7 +1218,7 @@ void Engine::enqueue_vcycle(cudaStream_t s, int tail, int count_iter) {
   if (coarse_cluster_ > 0)
     launch_mg_cluster(d_scenes_, nscenes(), d_ctl_, coarse_cluster_, count_iter, cluster_smem_, s);
   else
-    launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, count_iter, coarse_smem_, s);
+    launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, count_iter, coarse_smem_, any_wtail(), s);
   vcycle_launches_++;
   for (int l = LD - 1; l >= 0; l--) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
@@ -1605,7 +1610,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   } else if (n == "mg_coarse") {
     go = [&](int) {
       if (coarse_cluster_ > 0) launch_mg_cluster(d_scenes_, nscenes(), d_ctl_, coarse_cluster_, 0, cluster_smem_, s);
-      else launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, 0, coarse_smem_, s);
+      else launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, 0, coarse_smem_, any_wtail(), s);
     };
     // the reference schedule's V-cycle bytes of the levels the block covers (163 B per level cell)
     b = 0;

@@ -160,6 +160,7 @@ class Engine {
   // level always runs inside the one-CTA coarse block
   int set_coarse_w(int cells);
   int coarse_w() const { return w_cells_; }
+  bool any_wtail() const;       // some scene's coarse block runs the W tail
   // the coarse phase on one CTA (0) or on a cluster of cs CTAs per scene (2..16, from level 1)
   int set_coarse_cluster(int cs);
   int coarse_cluster() const { return coarse_cluster_; }

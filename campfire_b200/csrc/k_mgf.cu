@@ -790,6 +790,8 @@ __device__ __forceinline__ void cb_up(const CbCtx c, int l) {
 
 // smem_floats: the launch's dynamic shared memory in floats; past the levels and the residual
 // scratch, the coarsest inverse of the direct solve is staged there when it fits
+// WT: compiled with the W tail (an engine whose scenes have one); without it the V-cycle's code alone
+template <bool WT>
 __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __restrict__ scenes, int nscenes, SolveCtl* ctl, int tail,
                                                          int count_iter, int smem_floats) {
   extern __shared__ __align__(128) float smem[];
@@ -904,7 +906,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // code: the visits keep their registers to themselves.
   for (int l = lc; l < nl - 1; l++) cb_down(cbx, l);
   cb_coarsest(cbx);
-  if (S.lw == nl - 3 && nl - 3 >= lc) {
+  if (WT && S.lw == nl - 3 && nl - 3 >= lc) {
     cb_up(cbx, nl - 2);
     cb_down(cbx, nl - 2);
     cb_coarsest(cbx);
@@ -1156,10 +1158,10 @@ void launch_pcg_decide(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, cuda
   if (nscenes > 0) launch_pdl(pdl_enabled(), k_pcg_decide, dim3(nscenes), dim3(256), 0, st, scenes, ctl);
 }
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
-                      cudaStream_t st) {
+                      int wtail, cudaStream_t st) {
   if (nscenes > 0)
-    launch_pdl(pdl_enabled(), k_mg_coarse, dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail,
-               count_iter, (int)(smem / 4));
+    launch_pdl(pdl_enabled(), wtail ? k_mg_coarse<true> : k_mg_coarse<false>, dim3(nscenes), dim3(CB_THREADS), smem,
+               st, scenes, nscenes, ctl, tail, count_iter, (int)(smem / 4));
 }
 // bw: the widest coarsest level of the batch (the register window's bound)
 void launch_coarse_factor(const SceneDesc* scenes, int nscenes, size_t smem, int bw, int pipelined, cudaStream_t st) {
@@ -1182,8 +1184,10 @@ cudaError_t prepare_coarse_factor(size_t smem) {
 }
 cudaError_t prepare_mg_coarse(size_t smem) {
   // the kernel's attribute, shared by every engine: the largest size any schedule can ask for
-  return cudaFuncSetAttribute(k_mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)std::max(smem, kCoarseSmemMax));
+  const int bytes = (int)std::max(smem, kCoarseSmemMax);
+  const cudaError_t e = cudaFuncSetAttribute(k_mg_coarse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_mg_coarse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 }  // namespace cfg
