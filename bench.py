@@ -55,7 +55,7 @@ B_FIXED = 156 + 68 + 28 + 20 + 28 + 13.3 + 32
 
 # DRAM bytes (read + write) per launch of a kernel, from one ncu capture of the workload
 NCU_TRAFFIC = {("plain", "mg_coarse"): 123904, ("plain", "advect"): 2967808,
-               ("fine", "mg_up0_krylov"): 16272896, ("batched", "mg_down0"): 43902464}
+               ("fine", "mg_up0_krylov"): 16264960, ("batched", "mg_down0"): 43902464}
 
 
 def bytes_per_cell(diff_sub: int, cycles: float, fp64: bool) -> float:
@@ -758,6 +758,26 @@ def kernel_roofline(sim, workload: str, value_per_gpu: float, info: dict) -> dic
             "kernels": {k: {"ms": round(v["ms"], 5), "per_step": v["per_step"]} for k, v in kern.items()}}
 
 
+def profile_steps(workload: str, warm: int, w_cells) -> None:
+    """The workload's scene and solver launched kernel by kernel: `warm` steps, then one more, synchronised
+    between (a profiler's capture selects launches of the last step by skipping the earlier ones)."""
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
+    sc = cb.generate_scene(kind, nx, ny, 0.8, seed)
+    g = cb.FluidSim(0, {"nx": nx, "ny": ny, "dt": sc["dt"]}, width=0.8).init()
+    load_scene(g, sc)
+    configure_solver(g, workload, w_cells)
+    g.set_coarse_cells(1536)
+    g.set_graphs(False)
+    g.step(warm)
+    g.synchronize()
+    g.step(1)
+    g.synchronize()
+    print(json.dumps({"workload": workload, "profile_steps": warm + 1, "cycles_last_step": g.info()["last_cycles"]}))
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -793,8 +813,17 @@ def main():
                     help="graph: one CUDA graph per step (pressure loop as a device-side WHILE node); "
                          "stream: kernel by kernel, the host polling the loop decision (for profilers that "
                          "do not list kernels inside conditional graph nodes)")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling driver: step the workload's scene this many times, then once more, kernel by "
+                         "kernel (stream launches, coarse block from 1536 cells, no autotuning), print its cycle "
+                         "count and exit without a benchmark line (for ncu's launch lists and captures)")
+    ap.add_argument("--w-cells", type=int, default=None,
+                    help="override the workload's cycle shape (cfg_set_coarse_w; 0: the V-cycle)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
+    if a.profile_steps > 0:
+        profile_steps(a.workload, a.profile_steps, a.w_cells)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
