@@ -268,14 +268,15 @@ int Engine::alloc_scene(Scene& sc) {
     {(void**)&d.T, C * 4}, {(void**)&d.T2, C * 4}, {(void**)&d.Tw, C * 4},
     {(void**)&d.Y, C * 16}, {(void**)&d.Y2, C * 16}, {(void**)&d.Yw, C * 16},
     {(void**)&d.SQ, C * 8}, {(void**)&d.cellG, C * 8},
-    {(void**)&d.acc, ACC_LEN * 4}, {(void**)&d.faceW, MAX_PIECES * 4 * 4},
-    {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4}, {(void**)&d.rad, RAD_LEN * 16},
+    // acc, rad, faceW in this order: the readback ring copies them in one piece (kRingBytes)
+    {(void**)&d.acc, ACC_LEN * 4}, {(void**)&d.rad, RAD_LEN * 16}, {(void**)&d.faceW, MAX_PIECES * 4 * 4},
+    {(void**)&d.pieces, MAX_PIECES * PIECE_FLOATS * 4},
     {(void**)&d.p64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.rhs64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.part, (size_t)std::max(std::max(nt_fr, nt_mg0), nt_up0) * 72},   // up to 9 sums per tile
     {(void**)&d.r64, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.dA, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.dB, (size_t)sc.nx * sc.ny * 8}, {(void**)&d.q64, (size_t)sc.nx * sc.ny * 8},
     {(void**)&d.tmap, (size_t)MAX_LEVELS * TM_PER_LEVEL * TMAP_BYTES},
-    {(void**)&d.cinv, (size_t)2 * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * 4},
+    {(void**)&d.cinv, (size_t)2 * sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1] * cinv_ld(sc.lnx[sc.nlev - 1] * sc.lny[sc.nlev - 1]) * 4},
   };
   double h = sc.dxd;
   for (int l = 0; l < sc.nlev; l++) {
@@ -308,11 +309,13 @@ int Engine::alloc_scene(Scene& sc) {
     const bool scratch = it.ptr == (void**)&d.tmap || it.ptr == (void**)&d.part;
     sc.items.push_back({*it.ptr, it.bytes, !scratch});
   }
+  if ((char*)d.rad != (char*)d.acc + kRbRadOff || (char*)d.faceW != (char*)d.acc + kRbFaceWOff)
+    return fail(CFG_ERR_INVAL, "readback arrays not laid out as the ring expects");
   return build_tmaps(sc);
 }
 
 // ------------------------------------------------------------------ checkpoints
-// File: "CFGCKPT1", u32 version 1, nx, ny, nlev, nitems; f64 time, dt, dt_cap, cfl,
+// File: "CFGCKPT1", u32 version 2, nx, ny, nlev, nitems; f64 time, dt, dt_cap, cfl,
 // width; u32 frame, nray; the host params (cfg_params); the host pieces
 // (64 x 20 f32); the device's parameter block (the uniform and step controls,
 // which the CFL step updates on the device); the scene's SolveState; then per
@@ -320,6 +323,8 @@ int Engine::alloc_scene(Scene& sc) {
 // the bytes; last u64 FNV-1a of everything after the magic.
 namespace {
 constexpr char kCkptMagic[8] = {'C', 'F', 'G', 'C', 'K', 'P', 'T', '1'};
+// 2: the solve state carries the device clock; acc, rad, faceW adjacent in the arena
+constexpr uint32_t kCkptVersion = 2u;
 struct CkptHead {
   uint32_t version, nx, ny, nlev, nitems, frame, nray, pad;
   double time, dt, dt_cap, cfl, width;
@@ -348,7 +353,7 @@ int Engine::checkpoint_save(int s, const char* path) {
   SolveState ss{};
   CFG_CUDA(cudaMemcpy(dparams.data(), d_scenes_ + s, kDescParamBytes, cudaMemcpyDeviceToHost));
   CFG_CUDA(cudaMemcpy(&ss, sc.desc.solve, sizeof ss, cudaMemcpyDeviceToHost));
-  CkptHead h{1u, (uint32_t)sc.nx, (uint32_t)sc.ny, (uint32_t)sc.nlev, (uint32_t)nstate, sc.frame, (uint32_t)sc.nray, 0u,
+  CkptHead h{kCkptVersion, (uint32_t)sc.nx, (uint32_t)sc.ny, (uint32_t)sc.nlev, (uint32_t)nstate, sc.frame, (uint32_t)sc.nray, 0u,
              sc.cfl > 0 ? ss.time : sc.time, sc.dtd, sc.dt_cap, sc.cfl, sc.width};
   File out;
   out.f = std::fopen(path, "wb");
@@ -403,7 +408,7 @@ int Engine::checkpoint_load(int s, const char* path) {
     return fail(CFG_ERR_IO, std::string("truncated checkpoint ") + path);
   int nstate = 0;
   for (auto& it : sc.items) nstate += it.state ? 1 : 0;
-  if (h.version != 1u) return fail(CFG_ERR_INVAL, "unsupported checkpoint version");
+  if (h.version != kCkptVersion) return fail(CFG_ERR_INVAL, "unsupported checkpoint version");
   if ((int)h.nx != sc.nx || (int)h.ny != sc.ny || (int)h.nlev != sc.nlev || (int)h.nitems != nstate)
     return fail(CFG_ERR_RANGE, "checkpoint grid " + std::to_string(h.nx) + "x" + std::to_string(h.ny) +
                                    " does not match this scene");
@@ -905,9 +910,7 @@ int Engine::readback_begin(int s, uint64_t tag, int* slot) {
   const SceneDesc& d = sc.desc;
   cudaStream_t q = st();
   char* h = R.host + (size_t)i * kRingBytes;
-  CFG_CUDA(cudaMemcpyAsync(h, d.acc, ACC_LEN * 4, cudaMemcpyDeviceToHost, q));
-  CFG_CUDA(cudaMemcpyAsync(h + ACC_LEN * 4, d.rad, RAD_LEN * 16, cudaMemcpyDeviceToHost, q));
-  CFG_CUDA(cudaMemcpyAsync(h + ACC_LEN * 4 + RAD_LEN * 16, d.faceW, MAX_PIECES * 16, cudaMemcpyDeviceToHost, q));
+  CFG_CUDA(cudaMemcpyAsync(h, d.acc, kRingBytes, cudaMemcpyDeviceToHost, q));   // acc, rad, faceW at once
   CFG_CUDA(cudaMemsetAsync(d.acc, 0, ACC_LEN * 4, q));
   CFG_CUDA(cudaEventRecord(R.ev[i], q));
   R.busy[i] = true;
@@ -936,8 +939,8 @@ int Engine::readback_collect(int s, bool wait, int32_t* acc, float* rad, int32_t
   }
   const char* h = R.host + (size_t)i * kRingBytes;
   if (acc) std::memcpy(acc, h, ACC_LEN * 4);
-  if (rad) std::memcpy(rad, h + ACC_LEN * 4, RAD_LEN * 16);
-  if (faceW) std::memcpy(faceW, h + ACC_LEN * 4 + RAD_LEN * 16, MAX_PIECES * 16);
+  if (rad) std::memcpy(rad, h + kRbRadOff, RAD_LEN * 16);
+  if (faceW) std::memcpy(faceW, h + kRbFaceWOff, MAX_PIECES * 16);
   if (tag) *tag = R.tag[i];
   R.busy[i] = false;
   *ready = 1;

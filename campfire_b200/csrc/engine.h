@@ -87,7 +87,11 @@ struct Scene {
 };
 
 constexpr int kRingSlots = 3;
-constexpr size_t kRingBytes = ACC_LEN * 4 + RAD_LEN * 16 + MAX_PIECES * 16;
+// One readback is one copy: acc, rad and faceW sit next to each other in the scene arena (each
+// array's start rounded up to 256 bytes), and a ring slot mirrors that layout.
+constexpr size_t kRbRadOff = (ACC_LEN * 4 + 255) / 256 * 256;
+constexpr size_t kRbFaceWOff = kRbRadOff + (RAD_LEN * 16 + 255) / 256 * 256;
+constexpr size_t kRingBytes = kRbFaceWOff + MAX_PIECES * 16;
 
 // Bytes of SceneDesc that cfg_write_params uploads: the uniform and the step
 // controls up to (not including) the tile counts and device pointers.

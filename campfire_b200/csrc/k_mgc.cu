@@ -213,9 +213,10 @@ __global__ void __launch_bounds__(CC_THREADS) k_mg_cluster(const SceneDesc* __re
   // this CTA's rows of the coarsest inverse (constant during the step)
   if (direct) {
     const LvC& C = lv[nl - 1];
-    const float* A = S.cinv + (size_t)S.solve->cinv_cur * ncs * ncs + (size_t)C.r0 * C.nx * ncs;
+    const int ld = cinv_ld(ncs);   // the inverse's row stride in global memory
+    const float* A = S.cinv + (size_t)S.solve->cinv_cur * ncs * ld + (size_t)C.r0 * C.nx * ld;
     const int na = (C.r1 - C.r0) * C.nx * ncs;
-    for (int e = threadIdx.x; e < na; e += CC_THREADS) arow[e] = __ldg(A + e);
+    for (int e = threadIdx.x; e < na; e += CC_THREADS) arow[e] = __ldg(A + (size_t)(e / ncs) * ld + e % ncs);
   }
   const bool ok = mbar_wait(&bar, 0);
   if (threadIdx.x == 0) s_ok = ok ? 1 : 0;

@@ -722,7 +722,8 @@ __device__ __forceinline__ void cb_coarsest(const CbCtx c) {
       const int q = lane & 7;
       const bool staged = s_inv != 0;
       // the global copy is addressed only when the inverse is not staged
-      const float* Ag = staged ? nullptr : S.cinv + (size_t)S.solve->cinv_cur * n * n;
+      const int ld = cinv_ld(n);
+      const float* Ag = staged ? nullptr : S.cinv + (size_t)S.solve->cinv_cur * n * ld;
       const float* As = smem + s_A;
       for (int base = warp * 4; base < n; base += CB_WARPS * 4) {
         const int k = base + (lane >> 3);
@@ -730,10 +731,10 @@ __device__ __forceinline__ void cb_coarsest(const CbCtx c) {
         if (k < n) {
           if (staged) {
             #pragma unroll 4
-            for (int m = q; m < n; m += 8) sum = __fmaf_rn(As[k * n + m], sres[m], sum);
+            for (int m = q; m < n; m += 8) sum = __fmaf_rn(As[k * ld + m], sres[m], sum);
           } else {
             #pragma unroll 4
-            for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(Ag + (size_t)k * n + m), sres[m], sum);
+            for (int m = q; m < n; m += 8) sum = __fmaf_rn(__ldg(Ag + (size_t)k * ld + m), sres[m], sum);
           }
         }
         sum += __shfl_xor_sync(0xffffffffu, sum, 1);
@@ -846,8 +847,9 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       for (int l = lc; l < nl; l++) bytes += (S.lev[l].ny * S.lev[l].pu + (S.lev[l].ny + 1) * S.lev[l].pc) * 4;
       const int n = S.lev[nl - 1].nx * S.lev[nl - 1].ny;
       s_dir = ctl->coarse_direct && S.solve->direct_ok;   // both fixed for the loop
-      const bool inv = s_dir && (n % 2) == 0 && n <= kStagedInverseMax && s_A + n * n <= smem_floats;
-      if (inv) bytes += (uint32_t)(n * n * 4);
+      const int ld = cinv_ld(n);
+      const bool inv = s_dir && (n % 2) == 0 && n <= kStagedInverseMax && s_A + n * ld <= smem_floats;
+      if (inv) bytes += (uint32_t)(n * ld * 4);
       mbar_arrive_expect_tx(&bar, bytes);
       for (int l = lc; l < nl; l++) {
         const LevelDesc& G = S.lev[l];
@@ -855,7 +857,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
         bulk_g2s(smem + lvo[l].yo, G.ay, (G.ny + 1) * G.pc * 4, &bar);
       }
       if (inv) {
-        bulk_g2s(smem + s_A, S.cinv + (size_t)S.solve->cinv_cur * n * n, (uint32_t)(n * n * 4), &bar);
+        bulk_g2s(smem + s_A, S.cinv + (size_t)S.solve->cinv_cur * n * ld, (uint32_t)(n * ld * 4), &bar);
         s_inv = 1;
       }
     }
@@ -915,6 +917,16 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // ---- write level lc back; when the block covers level 0, finish the cycle here
   float* const gp = s_gp;
   const int gpc = s_gpc, gnx = V0.nx;
+  if (lc > 0) {
+    // the shared copy of level lc's p has the global pitch: one bulk copy (the last visit ended
+    // with a block barrier); the next kernel reads it after this grid has completed
+    if (threadIdx.x == 0) {
+      proxy_fence_shared();
+      bulk_s2g(gp, V0.p, (uint32_t)(V0.ny * gpc * 4));
+      bulk_wait_read();
+    }
+    return;
+  }
   double part = 0.0, part2 = 0.0, part3 = 0.0;
   const LinMap mw(V0.nx, V0.mnx);
   if (mw.R)
@@ -995,7 +1007,8 @@ __global__ void __launch_bounds__(CF_THREADS) k_coarse_factor(const SceneDesc* _
   const LevelDesc L = S.lev[S.nlev - 1];
   const int n = L.nx * L.ny, bw = L.nx, W = bw + 1;
   int* ok_flag = pipelined ? &S.solve->direct_ok_next : &S.solve->direct_ok;
-  float* cinv = S.cinv + (size_t)(pipelined ? 1 - S.solve->cinv_cur : S.solve->cinv_cur) * n * n;
+  const int ld = cinv_ld(n);
+  float* cinv = S.cinv + (size_t)(pipelined ? 1 - S.solve->cinv_cur : S.solve->cinv_cur) * n * ld;
   if (n > CF_THREADS || bw > BWM) {
     if (threadIdx.x == 0) *ok_flag = 0;
     return;
@@ -1101,7 +1114,7 @@ __global__ void __launch_bounds__(CF_THREADS) k_coarse_factor(const SceneDesc* _
         for (int m = 0; m < BWM; m++)
           if (m < bw && i + 1 + m <= n - 1) sum = __fmaf_rn(-band[(i + 1 + m) * W + (m + 1)], win[m], sum);
         const float xi = sum * rinv[i];
-        cinv[(size_t)i * n + c] = xi;
+        cinv[(size_t)i * ld + c] = xi;
 #pragma unroll
         for (int m = BWM - 1; m > 0; m--) win[m] = win[m - 1];
         win[0] = xi;
@@ -1138,7 +1151,8 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
   f += (size_t)round_up((int)cells, 32);
   // room for the coarsest inverse of the direct solve when it fits
   const size_t n = (size_t)lnx[nlev - 1] * lny[nlev - 1];
-  if (n % 2 == 0 && n <= (size_t)kStagedInverseMax && (f + n * n) * 4 <= kCoarseSmemMax) f += n * n;
+  const size_t ld = (size_t)cinv_ld((int)n);
+  if (n % 2 == 0 && n <= (size_t)kStagedInverseMax && (f + n * ld) * 4 <= kCoarseSmemMax) f += n * ld;
   return f * 4;
 }
 

@@ -124,6 +124,10 @@ cudaError_t prepare_mg_coarse(size_t smem);
 void launch_coarse_factor(const SceneDesc* scenes, int nscenes, size_t smem, int bw, int pipelined, cudaStream_t st);
 // pipelined coarse solve: switch every enabled scene to the inverse factored during the step
 void launch_cinv_swap(const SceneDesc* scenes, int nscenes, cudaStream_t st);
+// Row stride (floats) of the coarsest inverse of n unknowns: the smallest ld >= n with ld = 8
+// (mod 32), so that the four rows a warp reads at once in the coarse block's product fall in
+// different shared-memory banks (ld * 4 bytes stays a multiple of 16 for the bulk copies)
+__host__ __device__ constexpr int cinv_ld(int n) { return n <= 8 ? 8 : (n - 8 + 31) / 32 * 32 + 8; }
 // dynamic shared memory of k_coarse_factor for a coarsest level of n cells and band width bw
 size_t coarse_factor_smem(int n, int bw);
 cudaError_t prepare_coarse_factor(size_t smem);

@@ -31,6 +31,18 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// shared -> global bulk copy (one bulk async-group per call): both addresses and `bytes`
+// multiples of 16. The caller makes the block's shared-memory writes visible to the copy
+// first (a block barrier, then proxy_fence_shared in the issuing thread) and waits with
+// bulk_wait_read before that shared memory is written again or the block exits.
+__device__ __forceinline__ void proxy_fence_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
 // 2D tiled tensor copy global -> shared of the box at (x, y) of `tmap` (a CUtensorMap
 // in global memory); out-of-range elements are zero-filled. x * element size must be
 // a multiple of 16 bytes; the destination 128-byte aligned.
