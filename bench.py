@@ -269,21 +269,35 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
     b.set_stream(stream.cuda_stream)
     b.step(warmup)
     b.synchronize()
-    # the Krylov update: its own kernel per cycle, or folded into the level-0 smoother kernels (one
-    # launch fewer per cycle, more bytes): both timed over a few steps of the batch, the faster kept
-    fold_ms = {}
-    for mode in (3, 2):
-        b.set_krylov(mode)
-        b.step(1)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        b.step(4)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        b.synchronize()
-        fold_ms[mode] = e0.elapsed_time(e1) / 4
-    fold = min(fold_ms, key=fold_ms.get)
-    b.set_krylov(fold)
+    # the Krylov update: its own kernel per cycle, or folded into the level-0 smoother kernels (a
+    # one-CTA-per-scene decision kernel ends each cycle), which needs every scene's coarse block
+    # below level 0. Candidates: the autotuner's coarse level with the update kernel, and the
+    # largest timed coarse level below every scene's level 0 with the fold; each timed over
+    # whole steps, interleaved (the scenes' cycle counts drift from step to step), the faster kept
+    min_cells = min(s["nx"] * s["ny"] for s in scenes)
+    cands = [(tune["best"], 3)]
+    below = [c for c in tune["ms_per_cycle"] if c < min_cells]
+    if below:
+        cands.append((max(below), 2))
+    cand_ms = {c: 0.0 for c in cands}
+    folded = {}
+    for rnd in range(2):
+        for c in cands:
+            b.set_coarse_cells(c[0])
+            b.set_krylov(c[1])
+            folded[c] = b.krylov_folded()
+            b.step(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.step(3)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            b.synchronize()
+            cand_ms[c] += e0.elapsed_time(e1) / 6
+    kept = min(cand_ms, key=cand_ms.get)
+    b.set_coarse_cells(kept[0])
+    b.set_krylov(kept[1])
+    fold = kept[1] if folded[kept] else 3
     b.step(1)
     b.synchronize()
     torch.cuda.synchronize(dev)
@@ -335,10 +349,11 @@ def run_batched(dev, stream, flush, steps: int, warmup: int, tol: float, max_cyc
         g.close()
     plain = plain_cells / (plain_ms / 1e3)
     return {"value": batched, "unit": METRIC, "scenes": len(scenes), "cells": cells, "steps": steps,
-            "schedule": {"coarse_cells": tune["best"],
+            "schedule": {"coarse_cells": kept[0],
                          "autotune_ms_per_cycle": {str(k): round(v, 5) for k, v in tune["ms_per_cycle"].items()},
                          "krylov_update": "folded into the level-0 kernels" if fold == 2 else "own kernel",
-                         "krylov_update_ms_per_step": {"own kernel": fold_ms[3], "folded": fold_ms[2]},
+                         "candidates_ms_per_step": {f"coarse {c[0]}, " + ("folded" if folded[c] else "own kernel"):
+                                                    round(v, 4) for c, v in cand_ms.items()},
                          "tiles": {"advect": cb.TILE_SHAPES[tt["best"][0]],
                                    "diffuse_sources": cb.TILE_SHAPES[tt["best"][1]],
                                    "forces": cb.TILE_SHAPES[tt["best"][2]],

@@ -179,6 +179,7 @@ def lib():
         "cfg_server_create": [ci, ci, ip, ip, ip, cd, cd, ctypes.POINTER(vp)], "cfg_server_destroy": [vp],
         "cfg_server_set_solver": [vp, ci, ci, cd, ci, ci, ci, ci],
         "cfg_set_krylov": [vp, ci], "cfg_batch_set_krylov": [vp, ci],
+        "cfg_krylov_folded": [vp, ctypes.POINTER(ci)], "cfg_batch_krylov_folded": [vp, ctypes.POINTER(ci)],
         "cfg_server_slot_bytes": [vp, ci, ctypes.POINTER(sz)],
         "cfg_server_run": [vp, ctypes.POINTER(CfgJob), ci, ctypes.POINTER(CfgJobResult), dp, dp],
         "cfg_server_submit": [vp, ctypes.POINTER(CfgJob), ctypes.POINTER(ctypes.c_uint64)],

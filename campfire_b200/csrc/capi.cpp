@@ -343,6 +343,17 @@ extern "C" int cfg_batch_set_krylov(cfg_batch* b, int on) {
   if (!b || !b->eng) return cfg::fail(CFG_ERR_INVAL, "null cfg_batch handle");
   return guarded([&] { return b->eng->set_krylov(on); });
 }
+extern "C" int cfg_krylov_folded(cfg_sim* sim, int* folded) {
+  SIM_OK(sim);
+  if (!folded) return cfg::fail(CFG_ERR_INVAL, "null output");
+  *folded = sim->eng->krylov_folded() ? 1 : 0;
+  return CFG_OK;
+}
+extern "C" int cfg_batch_krylov_folded(cfg_batch* b, int* folded) {
+  if (!b || !b->eng || !folded) return cfg::fail(CFG_ERR_INVAL, "null argument");
+  *folded = b->eng->krylov_folded() ? 1 : 0;
+  return CFG_OK;
+}
 
 // ------------------------------------------------------------------ wood
 struct cfg_rigid {

@@ -165,6 +165,7 @@ class Engine {
   int set_coarse_w(int cells);
   int coarse_w() const { return w_cells_; }
   bool any_wtail() const;       // some scene's coarse block runs the W tail
+  bool krylov_folded() const { return pcg_fused(); }   // the loop folds the Krylov update
   // the coarse phase on one CTA (0) or on a cluster of cs CTAs per scene (2..16, from level 1)
   int set_coarse_cluster(int cs);
   int coarse_cluster() const { return coarse_cluster_; }
@@ -217,8 +218,8 @@ class Engine {
   void enqueue_factor(cudaStream_t s);
   void enqueue_factor_join(cudaStream_t s);
   bool krylov() const { return mode_ == CFG_SOLVE_FP64 && krylov_ != 0; }
-  // Krylov mode with the update folded into the level-0 smoother kernels: an engine of one
-  // scene whose coarse block starts below level 0
+  // Krylov mode with the update folded into the level-0 smoother kernels (krylov 1: one scene,
+  // 2: any engine), when every scene's coarse block starts below level 0
   bool pcg_fused() const;
   bool any_cfl() const;
   // after a step's launch: every enabled CFL scene's dt now lives on the device

@@ -297,6 +297,12 @@ class FluidSim(_SceneOps):
         2 / 3: CG with its update folded into the level-0 kernels / as its own kernel."""
         check(_lib.lib().cfg_set_krylov(self._h, int(on)))
 
+    def krylov_folded(self) -> bool:
+        """Whether the pressure loop folds the Krylov update into the level-0 kernels."""
+        f = ctypes.c_int()
+        check(_lib.lib().cfg_krylov_folded(self._h, ctypes.byref(f)))
+        return bool(f.value)
+
     def set_tiles(self, advect: int, diffuse_sources: int, forces: int):
         """Tile shapes (TILE_SHAPES indices) of the advection, diffusion + sources and forces kernels."""
         check(_lib.lib().cfg_set_tiles(self._h, advect, diffuse_sources, forces))
@@ -379,6 +385,11 @@ class Batch:
         """True / 1: on (the update kernel for a batch); 2: on, update folded into the level-0 kernels;
         3: on, separate update kernel; False / 0: plain defect correction."""
         check(_lib.lib().cfg_batch_set_krylov(self._h, int(on)))
+
+    def krylov_folded(self) -> bool:
+        f = ctypes.c_int()
+        check(_lib.lib().cfg_batch_krylov_folded(self._h, ctypes.byref(f)))
+        return bool(f.value)
 
     def set_tiles(self, advect: int, diffuse_sources: int, forces: int):
         check(_lib.lib().cfg_batch_set_tiles(self._h, advect, diffuse_sources, forces))

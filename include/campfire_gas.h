@@ -238,10 +238,17 @@ int cfg_batch_set_coarse_solve(cfg_batch* b, int direct);
  * level-0 operator in FP64 with the same FP32 V-cycle as preconditioner (Polak-Ribiere
  * direction update), which needs about half the cycles for the same tolerance. With 1 the
  * direction update is folded into the level-0 smoother kernels for one scene and runs as its
- * own kernel for a batch; 2 folds it and 3 keeps the kernel whatever the engine (one launch per
- * cycle fewer, against more bytes per cycle; the same iteration up to rounding). */
+ * own kernel for a batch; 2 folds it and 3 keeps the kernel whatever the engine (the folded
+ * form reads more bytes per cycle and ends each cycle with a one-CTA decision kernel in place
+ * of the update kernel; the same iteration up to rounding). The fold needs every scene's
+ * coarse block below level 0, else the update kernel runs (cfg_krylov_folded says which). */
 int cfg_set_krylov(cfg_sim* sim, int on);
 int cfg_batch_set_krylov(cfg_batch* b, int on);
+/* *folded = 1 when the pressure loop runs the Krylov update folded into the level-0 smoother
+ * kernels (with a per-scene decision kernel after them): the mode asks for it and every
+ * scene's coarse block starts below level 0 (cfg_set_coarse_cells); 0 otherwise */
+int cfg_krylov_folded(cfg_sim* sim, int* folded);
+int cfg_batch_krylov_folded(cfg_batch* b, int* folded);
 /* Autotuner of that schedule (no counterpart in the reference): builds a scratch batch of
  * these sizes on `device` with generated scenes, runs one step to build the coefficients
  * (and, with coarse_direct, the coarsest inverse), then times `iters` fused V-cycles for

@@ -75,6 +75,7 @@ def test_batch_krylov_update_folded_matches_its_own_kernel():
         b.set_coarse_solve("pipelined")
         b.set_coarse_cells(1536)
         b.set_krylov(mode)
+        assert b.krylov_folded() == (mode == 2)
         b.step(3)
         b.synchronize()
         out[mode] = ([v.info()["last_cycles"] for v in b.scenes], [v.read_p64() for v in b.scenes],
@@ -87,3 +88,20 @@ def test_batch_krylov_update_folded_matches_its_own_kernel():
             assert norm_err(out[2][2][k][f], out[3][2][k][f]) <= 1e-6, (k, f)
     if out[2][0][0] == out[3][0][0]:   # launches per step are counted with scene 0's cycles
         assert out[2][3] == out[3][3] + 1, (out[2][3], out[3][3])
+
+
+def test_krylov_fold_needs_every_coarse_block_below_level_0():
+    """The fold asked for (krylov 2) runs only while every scene's coarse block starts below level 0:
+    a coarse block that covers a scene's level 0 falls back to the update kernel, and says so."""
+    dims = [(96, 144), (64, 96)]
+    b = cb.Batch(dims, 0.8, [1e-3, 1e-3])
+    b.set_solver(cb.SOLVE_FP64, 1, 1e-9, 100)
+    b.set_krylov(2)
+    b.set_coarse_cells(1536)
+    assert b.krylov_folded()
+    b.set_coarse_cells(6144)          # 64x96 is 6144 cells: its whole hierarchy in the block
+    assert not b.krylov_folded()
+    b.set_krylov(3)
+    b.set_coarse_cells(1536)
+    assert not b.krylov_folded()
+    b.close()
