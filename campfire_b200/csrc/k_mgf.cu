@@ -134,10 +134,11 @@ __device__ __forceinline__ bool tile_wait2(uint64_t* bar, SolveCtl* ctl, F&& bet
 // (1..4) covers [x0-H+k, x0+TX+H-k) x [y0-H+k, y0+TY+H-k) clipped to the level, with colour
 // (first + k - 1) & 1; thread t owns slots t and t + 256 of each colour in pass 1's region
 // (the largest; 20 cells of a colour per row). tile_stencils builds their stencils from the
-// coefficients alone (coefficients, neighbour flags, diagonal, its correctly rounded
-// reciprocal, the passes that include the cell); tile_passes adds rhs h2 once the state
-// has landed and updates the cells by pressure.wgsl:87-94, dividing by div_by_rcp.
-struct TCell { float w, e, s, n, rh, diag, rcp; int kp, fl; };   // fl: 1 w, 2 e, 4 s, 8 n; 16 << k: pass k
+// coefficients alone (the four coefficients, zero for a neighbour outside the level, the
+// diagonal, its correctly rounded reciprocal, the passes that include the cell, whether it
+// is a tile cell); tile_passes adds rhs h2 once the state has landed and updates the cells
+// by pressure.wgsl:87-94, dividing by div_by_rcp.
+struct TCell { float w, e, s, n, rh, diag, rcp; int kp, fl; };   // fl: 1 a tile cell; 16 << k: pass k
 constexpr int SM_W1 = MGF_TX + 2 * MGF_H - 2, SM_H1 = MGF_TY + 2 * MGF_H - 2;   // pass 1's region
 __device__ __forceinline__ void tile_stencils(const Tile& t, const LevelDesc& L, int x0, int y0, int first,
                                               TCell (&c)[2][2]) {
@@ -154,25 +155,42 @@ __device__ __forceinline__ void tile_stencils(const Tile& t, const LevelDesc& L,
       if (sl >= HALF * SM_H1) continue;
       const int r = sl / HALF, j = jb + r, i = ib + ((ib + j + col) & 1) + 2 * (sl - r * HALF);
       if (i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
-      int pm = 0;
-      #pragma unroll
-      for (int k = 1; k <= 4; k++)
-        if (((first + k - 1) & 1) == col && i >= x0 - MGF_H + k && i < x0 + MGF_TX + MGF_H - k &&
-            j >= y0 - MGF_H + k && j < y0 + MGF_TY + MGF_H - k)
-          pm |= 16 << k;
+      // pass k (1..4) covers the cells at distance >= k from the edge of the region
+      // [x0-H, x0+TX+H) x [y0-H, y0+TY+H), and has colour (first + k - 1) & 1: passes 1, 3
+      // or 2, 4 for this cell's colour, up to its distance; distance >= H: a tile cell
+      const int d = min(min(i - (x0 - MGF_H), x0 + MGF_TX + MGF_H - 1 - i),
+                        min(j - (y0 - MGF_H), y0 + MGF_TY + MGF_H - 1 - j));
+      const int pm = (((first ^ col) & 1) ? (64 | 256) : (32 | 128)) & (((2 << min(d, 4)) - 2) << 4);
       if (!pm) continue;
       const int k = t.c(i, j);
       q.kp = k;
-      q.w = t.ax[k]; q.e = t.ax[k + 1]; q.s = t.ay[k]; q.n = t.ay[k + MGF_BW];
+      const float w = t.ax[k], e = t.ax[k + 1], s = t.ay[k], n = t.ay[k + MGF_BW];
       float diag = 0.f;
-      if (i > 0) diag += q.w; else diag += 2.f * q.w;
-      if (i < L.nx - 1) diag += q.e; else diag += 2.f * q.e;
-      if (j > 0) diag += q.s;
-      if (j < L.ny - 1) diag += q.n; else diag += 2.f * q.n;
+      if (i > 0) diag += w; else diag += 2.f * w;
+      if (i < L.nx - 1) diag += e; else diag += 2.f * e;
+      if (j > 0) diag += s;
+      if (j < L.ny - 1) diag += n; else diag += 2.f * n;
       q.diag = diag;
       q.rcp = diag > 0.f ? __frcp_rn(diag) : 0.f;
-      q.fl = pm | (i > 0 ? 1 : 0) | (i < L.nx - 1 ? 2 : 0) | (j > 0 ? 4 : 0) | (j < L.ny - 1 ? 8 : 0);
+      // a neighbour outside the level contributes nothing (pressure.wgsl:77-85): its
+      // coefficient is zero in the passes' sums, whose values outside the level are zero
+      q.w = i > 0 ? w : 0.f;
+      q.e = i < L.nx - 1 ? e : 0.f;
+      q.s = j > 0 ? s : 0.f;
+      q.n = j < L.ny - 1 ? n : 0.f;
+      q.fl = pm | (d >= MGF_H ? 1 : 0);
     }
+}
+// off of pressure.wgsl:77-85 from the slot's stencil: every neighbour's term is added in the
+// reference's order (west, east, south, north); a missing neighbour's term is an exact zero,
+// and adding it to a sum that started at +0 leaves the sum's bits unchanged
+__device__ __forceinline__ float tcell_off(const Tile& t, const TCell& q) {
+  float off = 0.f;
+  off += q.w * t.p[q.kp - 1];
+  off += q.e * t.p[q.kp + 1];
+  off += q.s * t.p[q.kp - MGF_BW];
+  off += q.n * t.p[q.kp + MGF_BW];
+  return off;
 }
 __device__ __forceinline__ void tile_passes(const Tile& t, const LevelDesc& L, int first, TCell (&c)[2][2]) {
   #pragma unroll
@@ -188,11 +206,7 @@ __device__ __forceinline__ void tile_passes(const Tile& t, const LevelDesc& L, i
     for (int m = 0; m < 2; m++) {
       const TCell& q = c[col][m];
       if (!(q.fl & (16 << k))) continue;
-      float off = 0.f;
-      if (q.fl & 1) off += q.w * t.p[q.kp - 1];
-      if (q.fl & 2) off += q.e * t.p[q.kp + 1];
-      if (q.fl & 4) off += q.s * t.p[q.kp - MGF_BW];
-      if (q.fl & 8) off += q.n * t.p[q.kp + MGF_BW];
+      const float off = tcell_off(t, q);
       v[m] = q.diag > 0.f ? mgc::div_by_rcp(off - q.rh, q.diag, q.rcp) : 0.f;
     }
     #pragma unroll
@@ -328,14 +342,24 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
     }
   }
   tile_passes(t, L, 0, c);   // colours 0, 1, 0, 1 (js/fluid.js:298-301)
-  // residual of the tile cells (pressure.wgsl:96-101) and the smoothed p
+  // residual of the tile cells (pressure.wgsl:96-101) from the slots' stencils (every tile cell
+  // of the level is a slot of some thread); the quotient by h2 from RN(1/h2), the IEEE one
+  const float rh2 = __frcp_rn(L.h2);
+  #pragma unroll
+  for (int col = 0; col < 2; col++)
+    #pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const TCell& q = c[col][m];
+      if (!(q.fl & 1)) continue;
+      const int bj = q.kp / MGF_BW, bi = q.kp - bj * MGF_BW;   // box row and column
+      const float off = tcell_off(t, q);
+      sr[(bj - MGF_H) * TX + (bi - MGF_SX)] =
+          q.diag <= 0.f ? 0.f : t.rhs[q.kp] - mgc::div_by_rcp(off - q.diag * t.p[q.kp], L.h2, rh2);
+    }
+  // the smoothed p
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
-    if (i >= L.nx || j >= L.ny) continue;
-    float off, diag; stencil_s(t, L.nx, L.ny, i, j, off, diag);
-    const int k = t.c(i, j);
-    sr[e] = diag <= 0.f ? 0.f : t.rhs[k] - (off - diag * t.p[k]) / L.h2;
-    L.pb[j * L.pc + i] = t.p[k];
+    if (i < L.nx && j < L.ny) L.pb[j * L.pc + i] = t.p[t.c(i, j)];
   }
   __syncthreads();
   // restriction (pressure.wgsl:104-113)
