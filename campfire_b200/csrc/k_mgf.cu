@@ -50,16 +50,19 @@ __device__ __forceinline__ void stencil_s(const Tile& t, int nx, int ny, int i, 
   if (j < ny - 1) { off += n * t.p[k + MGF_BW]; diag += n; } else { diag += 2.f * n; }
 }
 // (L z)_ij in FP64 from the tile's f32 z and coefficients (pressure.wgsl:77-85 promoted,
-// as the FP64 defect: (off - diag z) / h2, 0 in closed cells)
-__device__ __forceinline__ double lap_tile64(const Tile& t, const LevelDesc& L, int i, int j) {
+// as the FP64 defect: (off - diag z) / h2, 0 in closed cells). The products of two f32 values
+// are exact in FP64, so the fused multiply-adds round as the separate products and sums
+// would; the division is a product with rh2 = 1 / h2 (FP64, one rounding more: the Krylov
+// loop's own operator, the same in every kernel that forms it)
+__device__ __forceinline__ double lap_tile64(const Tile& t, const LevelDesc& L, int i, int j, double rh2) {
   const int k = t.c(i, j);
   const double w = t.ax[k], e = t.ax[k + 1], s = t.ay[k], n = t.ay[k + MGF_BW];
   double off = 0.0, diag = 0.0;
-  if (i > 0) { off += w * (double)t.p[k - 1]; diag += w; } else diag += 2.0 * w;
-  if (i < L.nx - 1) { off += e * (double)t.p[k + 1]; diag += e; } else diag += 2.0 * e;
-  if (j > 0) { off += s * (double)t.p[k - MGF_BW]; diag += s; }
-  if (j < L.ny - 1) { off += n * (double)t.p[k + MGF_BW]; diag += n; } else diag += 2.0 * n;
-  return diag > 0.0 ? (off - diag * (double)t.p[k]) / (double)L.h2 : 0.0;
+  if (i > 0) { off = __fma_rn(w, (double)t.p[k - 1], off); diag += w; } else diag += 2.0 * w;
+  if (i < L.nx - 1) { off = __fma_rn(e, (double)t.p[k + 1], off); diag += e; } else diag += 2.0 * e;
+  if (j > 0) { off = __fma_rn(s, (double)t.p[k - MGF_BW], off); diag += s; }
+  if (j < L.ny - 1) { off = __fma_rn(n, (double)t.p[k + MGF_BW], off); diag += n; } else diag += 2.0 * n;
+  return diag > 0.0 ? __fma_rn(-diag, (double)t.p[k], off) * rh2 : 0.0;
 }
 __device__ __forceinline__ float diag_s(const Tile& t, int nx, int ny, int i, int j) {
   const int k = t.c(i, j);
@@ -403,7 +406,10 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
   SolveState* ss = S.solve;
   const bool spec = nscenes == 1;   // as in k_mg_down
   if (on && spec) stage_coef(S, level, t, bar);
+  __shared__ double s_rh2;   // the FP64 operator's 1 / h2 (tails 3 and 4)
+  if (threadIdx.x == 0) s_rh2 = 1.0 / (double)L.h2;
   __syncthreads();
+  const double rh2 = s_rh2;
   pdl_wait();
   if (!on) return;
   if (!spec) {
@@ -464,10 +470,11 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
         S.r64[kk] = r;
       }
       const double z = (double)t.p[k];
-      const double lz = lap_tile64(t, L, i, j);
+      const double lz = lap_tile64(t, L, i, j, rh2);
       S.dB[kk] = lz;
-      v[0] += r * z; v[1] += q * z; v[2] += z * lz;
-      v[3] += r * r; v[4] += r * lz; v[5] += r * q; v[6] += lz * lz; v[7] += lz * q; v[8] += q * q;
+      v[0] = __fma_rn(r, z, v[0]); v[1] = __fma_rn(q, z, v[1]); v[2] = __fma_rn(z, lz, v[2]);
+      v[3] = __fma_rn(r, r, v[3]); v[4] = __fma_rn(r, lz, v[4]); v[5] = __fma_rn(r, q, v[5]);
+      v[6] = __fma_rn(lz, lz, v[6]); v[7] = __fma_rn(lz, q, v[7]); v[8] = __fma_rn(q, q, v[8]);
     }
     // the tile's nine partials, quantity-major (part[m * nt_up0 + tile]); k_pcg_decide sums
     // them once this kernel has completed (no arrival, no fence in these CTAs)
@@ -494,7 +501,7 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
       // z = the cycle's p; Lz from the tile (its ring is exact after the fourth pass), in FP64
       const int kk = j * L.nx + i;
       const double z = (double)t.p[k];
-      const double lz = lap_tile64(t, L, i, j);
+      const double lz = lap_tile64(t, L, i, j, rh2);
       S.dB[kk] = lz;
       part += S.r64[kk] * z;
       part2 += S.q64[kk] * z;
