@@ -18,8 +18,9 @@ namespace {
 // sources.wgsl:34-157 for one gas cell; returns false for a cell inside wood
 struct SrcOut { float T; float4 Y; float S, qrel, qrad, tpeak; bool solid; };
 
+// Tamb4 = powf(P.Tamb, 4) (the radiation's ambient term, the same for every cell of the scene)
 __device__ __forceinline__ SrcOut sources_cell(const SceneDesc& S, const cfg_params& P, int i, int j, float Tc, float4 Yc,
-                                               float Tadv) {
+                                               float Tadv, float Tamb4) {
   SrcOut o; o.qrel = 0.f; o.qrad = 0.f; o.tpeak = 0.f; o.solid = false; o.S = 0.f;
   const int k = j * S.pc + i;
   const float2 g = __ldg(S.cellG + k);
@@ -110,7 +111,7 @@ __device__ __forceinline__ SrcOut sources_cell(const SceneDesc& S, const cfg_par
   const float fv = r1 * Yc.w / P.sootDensity;
   const float kap = P.kappaSootC * fv * Tc + P.kappaGas * Yc.z;
   const float T3 = Tc * Tc * Tc;
-  o.qrad = 4.f * kap * P.sigma * (T3 * Tc - powf(P.Tamb, 4.f));
+  o.qrad = 4.f * kap * P.sigma * (T3 * Tc - Tamb4);
   const float dTr = o.qrad * dt / (r1 * P.cp) / (1.f + 16.f * kap * P.sigma * T3 * dt / (r1 * P.cp));
   Tc -= dTr;
   // :140-148 entrainment of ambient air through the front/back faces
@@ -206,6 +207,7 @@ __global__ void __launch_bounds__(256) k_diffuse_sources(const SceneDesc* __rest
   }
 
   // ---- sources on the tile cells (or write the diffused state)
+  const float Tamb4 = powf(P.Tamb, 4.f);
   for (int e = threadIdx.x; e < TX * TY; e += blockDim.x) {
     const int i = x0 + e % TX, j = y0 + e / TX;
     float q = 0.f, qr = 0.f, tp = 0.f;
@@ -214,7 +216,7 @@ __global__ void __launch_bounds__(256) k_diffuse_sources(const SceneDesc* __rest
       const int k = j * pc + i;
       const float Tc = sT[cur][r]; const float4 Yc = sY[cur][r];
       if (SOURCES) {
-        const SrcOut o = sources_cell(S, P, i, j, Tc, Yc, __ldg(S.T2 + k));
+        const SrcOut o = sources_cell(S, P, i, j, Tc, Yc, __ldg(S.T2 + k), Tamb4);
         S.T[k] = o.T; S.Y[k] = o.Y;
         S.SQ[k] = o.solid ? make_float2(0.f, 0.f) : make_float2(o.S, o.qrel);
         q = o.qrel; qr = o.qrad; tp = o.tpeak;

@@ -29,7 +29,9 @@ template <int TX, int TY, bool FORCES, bool COEF>
 __global__ void __launch_bounds__(256) k_forces(const SceneDesc* __restrict__ scenes, const Work* __restrict__ work,
                                                SolveCtl* ctl, int fp64) {
   constexpr int AXW = TX + 1, AYH = TY + 1;
+  constexpr int MW = TX + 2, MH = TY + 2;   // cell viscosities of the tile and a one-cell ring
   __shared__ float sU[TY * AXW], sV[AYH * TX];
+  __shared__ float sMu[FORCES ? MH * MW : 1];
   __shared__ float sAx[2][TY * AXW], sAy[2][AYH * TX];
   __shared__ double red[32];
 
@@ -51,6 +53,15 @@ __global__ void __launch_bounds__(256) k_forces(const SceneDesc* __restrict__ sc
   auto v2 = [&](int i, int j) { const int k = j * pc + i; return __ldg(fya + k) > 0.f ? __ldg(V2 + k) : 0.f; };
   const LevelDesc L0 = S.lev[0];
 
+  // each cell's viscosity once (a cell's mu enters the two U faces and the two V faces beside
+  // it); the ring's indices clamp as Tc's do
+  if (FORCES) {
+    for (int e = threadIdx.x; e < MH * MW; e += blockDim.x)
+      sMu[e] = muOf(P, Tc(x0 - 1 + e % MW, y0 - 1 + e / MW));
+    __syncthreads();
+  }
+  auto muC = [&](int i, int j) { return sMu[(j - y0 + 1) * MW + (i - x0 + 1)]; };
+
   // ---- U faces: x in [x0, x0+TX], y in [y0, y0+TY)
   for (int e = threadIdx.x; e < TY * AXW; e += blockDim.x) {
     const int i = x0 + e % AXW, j = y0 + e / AXW;
@@ -66,11 +77,12 @@ __global__ void __launch_bounds__(256) k_forces(const SceneDesc* __restrict__ sc
         const float u = __ldg(U2 + k);
         const float TL = Tc(i - 1, j), TR = Tc(i, j);
         const float rhoF = rhoOf(P, 0.5f * (TL + TR));
-        const float muE = muOf(P, TR), muW = muOf(P, TL);
-        float uN = u, muN = muOf(P, 0.5f * (TL + TR));
+        const float muE = muC(i, j), muW = muC(i - 1, j);
+        float uN = u, muN, uS = -u, muS;
         if (j < ny - 1) { uN = u2(i, j + 1); muN = muOf(P, 0.25f * (TL + TR + Tc(i - 1, j + 1) + Tc(i, j + 1))); }
-        float uS = -u, muS = muOf(P, 0.5f * (TL + TR));
+        else muN = muOf(P, 0.5f * (TL + TR));
         if (j > 0) { uS = u2(i, j - 1); muS = muOf(P, 0.25f * (TL + TR + Tc(i - 1, j - 1) + Tc(i, j - 1))); }
+        else muS = muOf(P, 0.5f * (TL + TR));
         const float visc = (muE * (u2(i + 1, j) - u) + muW * (u2(i - 1, j) - u) + muN * (uN - u) + muS * (uS - u)) * idx2 / rhoF;
         const float vAvg = 0.25f * (__ldg(V2 + j * pc + i - 1) + __ldg(V2 + j * pc + i) + __ldg(V2 + (j + 1) * pc + i - 1) +
                                     __ldg(V2 + (j + 1) * pc + i));
@@ -103,11 +115,12 @@ __global__ void __launch_bounds__(256) k_forces(const SceneDesc* __restrict__ sc
         const float TB = Tc(i, j - 1), TT = Tc(i, j);
         const float Tf = 0.5f * (TB + TT);
         const float rhoF = rhoOf(P, Tf);
-        const float muN = muOf(P, TT), muS = muOf(P, TB);
-        float vE = v, muE = muOf(P, Tf);
+        const float muN = muC(i, j), muS = muC(i, j - 1);
+        float vE = v, muE, vW = v, muW;
         if (i < nx - 1) { vE = v2(i + 1, j); muE = muOf(P, 0.25f * (TB + TT + Tc(i + 1, j - 1) + Tc(i + 1, j))); }
-        float vW = v, muW = muOf(P, Tf);
+        else muE = muOf(P, Tf);
         if (i > 0) { vW = v2(i - 1, j); muW = muOf(P, 0.25f * (TB + TT + Tc(i - 1, j - 1) + Tc(i - 1, j))); }
+        else muW = muOf(P, Tf);
         const float visc = (muN * (v2(i, j + 1) - v) + muS * (v2(i, j - 1) - v) + muE * (vE - v) + muW * (vW - v)) * idx2 / rhoF;
         const float buoy = P.grav * (Tf / P.Tamb - 1.f);
         const float uAvg = 0.25f * (__ldg(U2 + (j - 1) * pu + i) + __ldg(U2 + (j - 1) * pu + i + 1) + __ldg(U2 + j * pu + i) +
