@@ -244,12 +244,25 @@ __device__ __forceinline__ void minmax4(const F& f, float gx, float gy, float4& 
   lo = min4(min4(A, C), min4(D, E)); hi = max4(max4(A, C), max4(D, E));
 }
 
-// advect.wgsl:28-34: vel = (s_U, s_V)/dx; RK2 midpoint back-trace (dt < 0 traces forward)
+// x / d rounded to nearest from r = RN(1/d): q0 = RN(x r), q = RN(q0 + r (x - d q0)),
+// the residual x - d q0 exact by FMA (Markstein, IBM J. Res. Dev. 34(1), 1990). Equal
+// to the IEEE quotient for quotients in the normal range (and for x = +0); for x = -0 it
+// gives +0. It replaces the division subroutine where the divisor is fixed for many
+// quotients (smoother diagonals, h2, dx).
+__device__ __forceinline__ float div_by_rcp(float x, float d, float r) {
+  const float q0 = __fmul_rn(x, r);
+  const float e = __fmaf_rn(-q0, d, x);
+  return __fmaf_rn(e, r, q0);
+}
+
+// advect.wgsl:28-34: vel = (s_U, s_V)/dx; RK2 midpoint back-trace (dt < 0 traces forward).
+// The quotient by dx from rdx = RN(1/dx): the IEEE one, except that a velocity of -0 comes
+// out +0, which moves no trace point (g - h * (+-0) = g)
 struct VelSampler {
-  UField u; VField v; float dx;
+  UField u; VField v; float dx, rdx;
   __device__ __forceinline__ void vel(float gx, float gy, float& vx, float& vy) const {
-    vx = sample(u, gx, gy, 0.f, 0.5f) / dx;
-    vy = sample(v, gx, gy, 0.5f, 0.f) / dx;
+    vx = div_by_rcp(sample(u, gx, gy, 0.f, 0.5f), dx, rdx);
+    vy = div_by_rcp(sample(v, gx, gy, 0.5f, 0.f), dx, rdx);
   }
   __device__ __forceinline__ void trace(float gx, float gy, float tdt, float& ox, float& oy) const {
     float vx, vy; vel(gx, gy, vx, vy);

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(256) k_advect(const SceneDesc* __restrict__ sc
   vs.u = UField{S.U, nx, ny, pu};
   vs.v = VField{S.V, nx, ny, pc};
   vs.dx = dx;
+  vs.rdx = __frcp_rn(dx);
   const CField Tf{S.T, nx, ny, pc, S.P.Tamb};
   const C4Field Yf{S.Y, nx, ny, pc, ambY(S.P)};
 

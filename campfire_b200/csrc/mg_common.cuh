@@ -83,15 +83,7 @@ __device__ __forceinline__ double lap_block64(const LvS& L, int i, int j) {
 }
 __device__ __forceinline__ void bar_coarsest(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
 
-// x / d rounded to nearest from r = RN(1/d): q0 = RN(x r), q = RN(q0 + r (x - d q0)),
-// the residual x - d q0 exact by FMA (Markstein, IBM J. Res. Dev. 34(1), 1990). Equal
-// to the IEEE quotient for quotients in the normal range; it replaces the division
-// subroutine on the coarsest level, whose diagonals stay fixed for all its sweeps.
-__device__ __forceinline__ float div_by_rcp(float x, float d, float r) {
-  const float q0 = __fmul_rn(x, r);
-  const float e = __fmaf_rn(-q0, d, x);
-  return __fmaf_rn(e, r, q0);
-}
+using cfg::div_by_rcp;   // gas_dev.cuh
 
 // One coarsest-level cell with its fixed stencil (pressure.wgsl:132-156).
 struct CCell {
