@@ -134,17 +134,13 @@ __device__ __forceinline__ void loop_count(SolveCtl* ctl) {
 
 // ------------------------------------------------------------- common.wgsl
 __device__ __forceinline__ float rhoOf(const cfg_params& P, float T) { return P.rhoAmb * P.Tamb / T; }   // :33
-// x^1.5 as x sqrt(x) (x > 0): one rounding of the product after the correctly rounded root,
-// within the error of a general power routine (the stages that use it are checked against
-// the oracle to a tolerance, as every transcendental is)
-__device__ __forceinline__ float pow1_5(float x) { return x * sqrtf(x); }
 // :36-38 Sutherland viscosity
 __device__ __forceinline__ float muOf(const cfg_params& P, float T) {
-  return 1.716e-5f * pow1_5(T / 273.15f) * (float)(273.15 + 110.4) / (T + 110.4f) * P.viscMult;
+  return 1.716e-5f * powf(T / 273.15f, 1.5f) * (float)(273.15 + 110.4) / (T + 110.4f) * P.viscMult;
 }
 // :40-42 rho*D = k/cp
 __device__ __forceinline__ float rhoDOf(const cfg_params& P, float T) {
-  return 1.716e-5f * pow1_5(T / 273.15f) * (float)(273.15 + 110.4) / (T + 110.4f) / P.Pr * P.diffMult;
+  return 1.716e-5f * powf(T / 273.15f, 1.5f) * (float)(273.15 + 110.4) / (T + 110.4f) / P.Pr * P.diffMult;
 }
 __device__ __forceinline__ float4 ambY(const cfg_params& P) { return make_float4(0.f, P.YOamb, 0.f, 0.f); }  // :44
 // WGSL mix(a, b, t) = a * (1 - t) + b * t
