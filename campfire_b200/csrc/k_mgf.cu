@@ -649,8 +649,10 @@ __device__ __forceinline__ RCell rcell_of(const LvS& L, int i, int j) {
   c.fl = (i > 0 ? 1 : 0) | (i < L.nx - 1 ? 2 : 0) | (j > 0 ? 4 : 0) | (j < L.ny - 1 ? 8 : 0);
   return c;
 }
+// res (the down visit's residuals, or null): after the sweeps, each thread writes the residual
+// of its cells (pressure.wgsl:96-101, with the stencils it holds) to res[j * pc + i]
 template <int NPER>
-__device__ __forceinline__ void smooth_regs(const LvS& L, int first) {
+__device__ __forceinline__ void smooth_regs(const LvS& L, int first, float* res = nullptr) {
   const int half = (L.nx + 1) >> 1;
   RCell c[2][NPER];
   bool act[2][NPER];
@@ -685,15 +687,32 @@ __device__ __forceinline__ void smooth_regs(const LvS& L, int first) {
         if (act[col][m]) L.p[c[col][m].kp] = v[m];
       __syncthreads();
     }
+  if (!res) return;
+  #pragma unroll
+  for (int col = 0; col < 2; col++)
+    #pragma unroll
+    for (int m = 0; m < NPER; m++) {
+      if (!act[col][m]) continue;
+      const RCell& q = c[col][m];
+      float off = 0.f;
+      if (q.fl & 1) off += q.w * L.p[q.kp - 1];
+      if (q.fl & 2) off += q.e * L.p[q.kp + 1];
+      if (q.fl & 4) off += q.s * L.p[q.kp - L.pc];
+      if (q.fl & 8) off += q.n * L.p[q.kp + L.pc];
+      res[q.kp] = q.diag <= 0.f ? 0.f : L.rhs[q.kp] - div_by_rcp(off - q.diag * L.p[q.kp], L.h2, L.rh2);
+    }
+  __syncthreads();
 }
 // both sweeps of a level visit (colour `first` first in each sweep, a block barrier after
-// every pass): in registers when each thread owns at most two cells of a colour
-__device__ __forceinline__ void smooth_visit(const LvS& L, int first) {
+// every pass): in registers when each thread owns at most two cells of a colour. With res
+// (a down visit), true when the residuals were also written there (the register path)
+__device__ __forceinline__ bool smooth_visit(const LvS& L, int first, float* res = nullptr) {
   const int half = (L.nx + 1) >> 1, nslot = half * L.ny;
-  if (nslot <= CB_THREADS) { smooth_regs<1>(L, first); return; }
-  if (nslot <= 2 * CB_THREADS) { smooth_regs<2>(L, first); return; }
+  if (nslot <= CB_THREADS) { smooth_regs<1>(L, first, res); return res != nullptr; }
+  if (nslot <= 2 * CB_THREADS) { smooth_regs<2>(L, first, res); return res != nullptr; }
   const LinMap mh(half, L.mhalf);
   for (int k = 0; k < 2; k++) { pass_d(L, first, mh); __syncthreads(); pass_d(L, 1 - first, mh); __syncthreads(); }
+  return false;
 }
 // The coarse block's level visits (k_mg_coarse), and what they read beside the block's shared
 // memory.
@@ -709,22 +728,35 @@ struct CbCtx {
 __device__ __forceinline__ void cb_down(const CbCtx c, int l) {
   float* const smem = c.smem;
   const LvO* const lvo = c.lvo;
-    const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
-    smooth_visit(F, 0);
-    auto res = [&](int i, int j) {
-      float off, diag; stencil_d(F, i, j, off, diag);
-      const int e = j * F.pc + i;
-      return diag <= 0.f ? 0.f : F.rhs[e] - div_by_rcp(off - diag * F.p[e], F.h2, F.rh2);
-    };
-    const LinMap mc(Cc.nx, Cc.mnx);
+  const LvS F = lvs_at(smem, lvo[l]), Cc = lvs_at(smem, lvo[l + 1]);
+  const LinMap mc(Cc.nx, Cc.mnx);
+  // the residuals from the smoothing's register stencils (pitched like F in the scratch), or
+  // recomputed per coarse cell on the shared-memory path of large levels
+  if (smooth_visit(F, 0, c.sres)) {
+    const float* r = c.sres;
     if (mc.R)
     for (int J = mc.j0; J < Cc.ny; J += mc.R)
       for (int I = mc.i0; I < Cc.nx; I += mc.di(Cc.nx)) {
-        const float r = res(2 * I, 2 * J) + res(2 * I + 1, 2 * J) + res(2 * I, 2 * J + 1) + res(2 * I + 1, 2 * J + 1);
-        Cc.rhs[J * Cc.pc + I] = 0.25f * r;
+        const int e = 2 * J * F.pc + 2 * I;
+        Cc.rhs[J * Cc.pc + I] = 0.25f * (r[e] + r[e + 1] + r[e + F.pc] + r[e + F.pc + 1]);
         Cc.p[J * Cc.pc + I] = 0.f;
       }
     __syncthreads();
+    return;
+  }
+  auto res = [&](int i, int j) {
+    float off, diag; stencil_d(F, i, j, off, diag);
+    const int e = j * F.pc + i;
+    return diag <= 0.f ? 0.f : F.rhs[e] - div_by_rcp(off - diag * F.p[e], F.h2, F.rh2);
+  };
+  if (mc.R)
+  for (int J = mc.j0; J < Cc.ny; J += mc.R)
+    for (int I = mc.i0; I < Cc.nx; I += mc.di(Cc.nx)) {
+      const float r = res(2 * I, 2 * J) + res(2 * I + 1, 2 * J) + res(2 * I, 2 * J + 1) + res(2 * I + 1, 2 * J + 1);
+      Cc.rhs[J * Cc.pc + I] = 0.25f * r;
+      Cc.p[J * Cc.pc + I] = 0.f;
+    }
+  __syncthreads();
 }
 // the coarsest level's solve (its p overwritten: the inverse's product, or sweeps from zero)
 __device__ __forceinline__ void cb_coarsest(const CbCtx c) {
@@ -851,7 +883,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
       lvo[l] = o;
     }
     s_res = q;
-    const int nres = S.lev[lc].nx * S.lev[lc].ny;
+    const int nres = S.lev[lc].ny * S.lev[lc].pc;   // the largest level's pitched size
     q += round_up(nres > COARSEST_SCRATCH ? nres : COARSEST_SCRATCH, 32);   // residual scratch
     for (int l = lc; l < nl; l++) { lvo[l].to = q; q += S.lev[l].nx * S.lev[l].ny; }
     q = round_up(q, 32);
@@ -1176,7 +1208,7 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
     const size_t pc = (size_t)round_up(lnx[l], 32), pu = (size_t)round_up(lnx[l] + 1, 32);
     f += 2 * lny[l] * pc + lny[l] * pu + (lny[l] + 1) * pc;
   }
-  f += (size_t)round_up(std::max(lnx[lc] * lny[lc], COARSEST_SCRATCH), 32);
+  f += (size_t)round_up(std::max(round_up(lnx[lc], 32) * lny[lc], COARSEST_SCRATCH), 32);
   size_t cells = 0;   // the 1/diag table of every level
   for (int l = lc; l < nlev; l++) cells += (size_t)lnx[l] * lny[l];
   f += (size_t)round_up((int)cells, 32);
