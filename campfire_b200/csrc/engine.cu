@@ -789,8 +789,14 @@ int Engine::write_params(int s) {
   } else {
     CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &d, kDescParamBytes, cudaMemcpyHostToDevice, st()));
   }
-  CFG_CUDA(cudaMemcpyAsync(d_dxd_ + s, &sc.dxd, 8, cudaMemcpyHostToDevice, st()));
-  CFG_CUDA(cudaMemcpyAsync(d_alpha_ + s, &sc.alpha, 8, cudaMemcpyHostToDevice, st()));
+  if (sc.dxd != sc.up_dxd) {
+    CFG_CUDA(cudaMemcpyAsync(d_dxd_ + s, &sc.dxd, 8, cudaMemcpyHostToDevice, st()));
+    sc.up_dxd = sc.dxd;
+  }
+  if (sc.alpha != sc.up_alpha) {
+    CFG_CUDA(cudaMemcpyAsync(d_alpha_ + s, &sc.alpha, 8, cudaMemcpyHostToDevice, st()));
+    sc.up_alpha = sc.alpha;
+  }
   if (graph_sub_ >= 0 && max_sub() > graph_sub_) graph_dirty_ = true;
   return CFG_OK;
 }

@@ -62,6 +62,9 @@ struct Scene {
   int lnx[MAX_LEVELS] = {}, lny[MAX_LEVELS] = {};
   int lc = 0;                    // first level of the one-CTA coarse block
   int lw = MAX_LEVELS;           // nlev - 3 with the W tail, else MAX_LEVELS
+  // the dx and diffusion alpha last copied to the device (write_params copies them only when
+  // they change; nothing on the device writes them)
+  double up_dxd = -1.0, up_alpha = -1.0;
   void* arena = nullptr;
   size_t arena_bytes = 0;
   SceneDesc desc{};              // host mirror of the device descriptor
