@@ -184,16 +184,17 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
-def workload_config(workload: str, world: int) -> dict:
+def workload_config(workload: str, world: int, w_cells=None) -> dict:
     """The workload as both arms run it (scene, grid, solver, time step, L2 policy): the same dict in the
-    line of this implementation and of the reference arm."""
+    line of this implementation and of the reference arm (w_cells: the cycle shape's override)."""
     nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[workload]
+    w = W_CELLS[workload] if w_cells is None else w_cells
     scene = {0: "3 logs", 1: "5-log tepee"}[kind]
     return {"workload": f"{workload} gas step {nx}x{ny}, {scene}, FP32 V(2,2) in FP64 defect correction "
                         f"to rel residual {tol:g}", "nx": nx, "ny": ny, "scene_kind": kind, "scene_seed": seed,
             "pressure": {"mode": "fp64_defect_correction", "tol": tol, "max_cycles": maxc,
                          "outer": "flexible preconditioned CG in FP64, FP32 multigrid cycle as preconditioner",
-                         "cycle": cycle_name(W_CELLS[workload]),
+                         "cycle": cycle_name(w),
                          "coarsest": "direct: inverse factored beside the pressure loop, applied from the next "
                                      "step (pipelined)"},
             "dt": {"cfl": PLAIN_CFL, "cap_s": PLAIN_DT_CAP},
@@ -217,7 +218,7 @@ def cycle_name(w_cells: int) -> str:
             "below it twice per cycle (inside the one-CTA coarse block)")
 
 
-def run_cpu(workload: str, steps: int, warmup: int, threads: int):
+def run_cpu(workload: str, steps: int, warmup: int, threads: int, w_cells=None):
     """The CPU restatement of the reference step (oracle, f32) on the same scene with the same solver.
     Inputs come from the oracle's own scene restatement: the product library is not loaded."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
@@ -226,7 +227,7 @@ def run_cpu(workload: str, steps: int, warmup: int, threads: int):
     sc = scene_ref.generate_scene(kind, nx, ny, 0.8, seed)
     o = oracle.OracleSim(nx, ny, 0.8, sc["dt"])
     scene_ref.load_scene(o, sc)
-    configure_solver(o, workload)
+    configure_solver(o, workload, w_cells)
     o.step(warmup)
     cyc = 0.0
     t0 = time.perf_counter()
@@ -839,7 +840,8 @@ def main():
                          "kernel (stream launches, coarse block from 1536 cells, no autotuning), print its cycle "
                          "count and exit without a benchmark line (for ncu's launch lists and captures)")
     ap.add_argument("--w-cells", type=int, default=None,
-                    help="override the workload's cycle shape (cfg_set_coarse_w; 0: the V-cycle)")
+                    help="override the main workload's cycle shape (cfg_set_coarse_w; 0: the V-cycle) in both "
+                         "arms, the profiling driver included")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     if a.profile_steps > 0:
@@ -850,14 +852,14 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nx, ny, kind, seed, mode, tol, maxc = WORKLOADS[a.workload]
-    config = workload_config(a.workload, world)
+    config = workload_config(a.workload, world, a.w_cells)
 
     if a.impl == "reference":
         # the CPU restatement of the reference step on this box's host cores: oracle library only
         if rank != 0:
             return
         th = cpu_threads()
-        val, secs, cyc = run_cpu(a.workload, a.steps, a.warmup, th)
+        val, secs, cyc = run_cpu(a.workload, a.steps, a.warmup, th, a.w_cells)
         line = {"metric": METRIC, "value": val, "unit": METRIC, "impl": "reference", "n_gpus": a.gpus,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * secs / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
@@ -888,7 +890,7 @@ def main():
         torch.cuda.synchronize(dev)
 
     m = measure_gpu(dev, stream, flush, a.workload, a.steps, a.warmup, a.launch, a.coarse_cells, world, rank,
-                    barrier, ClockSampler(local))
+                    barrier, ClockSampler(local), w_cells=a.w_cells)
     sim, sc, value, ms_max, info = m["sim"], m["scene"], m["value"], m["ms_max"], m["info"]
 
     # ---- end to end through the C ABI, the app's frame data flow (js/main.js:266-283): per step the piece
@@ -946,7 +948,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         th = cpu_threads()
-        val, secs, cyc = run_cpu(a.workload, a.cpu_sample, 1, th)
+        val, secs, cyc = run_cpu(a.workload, a.cpu_sample, 1, th, a.w_cells)
         cpu = {"value": val, "unit": METRIC, "cores": th, "kind": "port",
                "sample": f"{a.cpu_sample} steps of the same {nx}x{ny} workload after 1 warm-up step "
                          f"(C++ restatement of the reference WGSL, f32, OpenMP, same solver: "
