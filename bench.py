@@ -780,6 +780,30 @@ def kernel_roofline(sim, workload: str, value_per_gpu: float, info: dict) -> dic
             "kernels": {k: {"ms": round(v["ms"], 5), "per_step": v["per_step"]} for k, v in kern.items()}}
 
 
+def profile_batch(warm: int, coarse_cells: int, krylov: int) -> None:
+    """The batched workload (the 64 scenes of run_batched, FP64 to 1e-10, pipelined coarsest inverse) launched
+    kernel by kernel with a fixed schedule: `warm` steps, then one more."""
+    import campfire_b200 as cb
+    from campfire_b200.fluid import load_scene
+    scenes = batch_scenes()
+    b = cb.Batch([(s["nx"], s["ny"]) for s in scenes], 0.8, [s["dt"] for s in scenes])
+    for v, s in zip(b.scenes, scenes):
+        load_scene(v, s)
+    b.set_solver(cb.SOLVE_FP64, 1, 1e-10, 300)
+    b.set_coarse_solve("pipelined")
+    b.set_coarse_cells(coarse_cells)
+    b.set_krylov(krylov)
+    b.set_graphs(False)
+    b.step(warm)
+    b.synchronize()
+    b.step(1)
+    b.synchronize()
+    print(json.dumps({"workload": "batched", "profile_steps": warm + 1, "coarse_cells": coarse_cells,
+                      "krylov_folded": b.krylov_folded(),
+                      "cycles_last_step": max(v.info()["last_cycles"] for v in b.scenes)}))
+    b.close()
+
+
 def profile_steps(workload: str, warm: int, w_cells) -> None:
     """The workload's scene and solver launched kernel by kernel: `warm` steps, then one more, synchronised
     between (a profiler's capture selects launches of the last step by skipping the earlier ones)."""
@@ -839,13 +863,19 @@ def main():
                     help="profiling driver: step the workload's scene this many times, then once more, kernel by "
                          "kernel (stream launches, coarse block from 1536 cells, no autotuning), print its cycle "
                          "count and exit without a benchmark line (for ncu's launch lists and captures)")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="with --profile-steps: the batched workload (coarse block from 6144 cells, the Krylov "
+                         "update folded, as the benchmark's batch keeps it in its runs) instead of --workload")
     ap.add_argument("--w-cells", type=int, default=None,
                     help="override the main workload's cycle shape (cfg_set_coarse_w; 0: the V-cycle) in both "
                          "arms, the profiling driver included")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     if a.profile_steps > 0:
-        profile_steps(a.workload, a.profile_steps, a.w_cells)
+        if a.profile_batch:
+            profile_batch(a.profile_steps, 6144, 2)
+        else:
+            profile_steps(a.workload, a.profile_steps, a.w_cells)
         return
 
     rank = int(os.environ.get("RANK", "0"))
