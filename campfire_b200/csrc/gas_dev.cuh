@@ -178,6 +178,9 @@ __device__ __forceinline__ uint32_t faceOf(float px, float py, const Piece& pc) 
 }
 
 // ------------------------------------------------------------- samplers (js/gpu.js:16-65)
+// at(i, j) applies the boundary rules; quad(i, j, ...) reads the 2x2 block (i..i+1, j..j+1)
+// directly when every corner of it is an ordinary value (the same values at() returns) and
+// says whether it did
 // C fields: open sides/top sample the ambient, the floor is zero-gradient (:32-35)
 struct CField {
   const float* a; int nx, ny, pc; float amb;
@@ -185,12 +188,24 @@ struct CField {
     if (i < 0 || i >= nx || j >= ny) return amb;
     return __ldg(a + max(j, 0) * pc + i);
   }
+  __device__ __forceinline__ bool quad(int i, int j, float& A, float& C, float& D, float& E) const {
+    if ((unsigned)i >= (unsigned)(nx - 1) || (unsigned)j >= (unsigned)(ny - 1)) return false;
+    const float* q = a + j * pc + i;
+    A = __ldg(q); C = __ldg(q + 1); D = __ldg(q + pc); E = __ldg(q + pc + 1);
+    return true;
+  }
 };
 struct C4Field {
   const float4* a; int nx, ny, pc; float4 amb;
   __device__ __forceinline__ float4 at(int i, int j) const {
     if (i < 0 || i >= nx || j >= ny) return amb;
     return __ldg(a + max(j, 0) * pc + i);
+  }
+  __device__ __forceinline__ bool quad(int i, int j, float4& A, float4& C, float4& D, float4& E) const {
+    if ((unsigned)i >= (unsigned)(nx - 1) || (unsigned)j >= (unsigned)(ny - 1)) return false;
+    const float4* q = a + j * pc + i;
+    A = __ldg(q); C = __ldg(q + 1); D = __ldg(q + pc); E = __ldg(q + pc + 1);
+    return true;
   }
 };
 // U: still air outside, no-slip floor ghost -U(i,0) (:44-46)
@@ -201,6 +216,12 @@ struct UField {
     if (j < 0) return -__ldg(a + i);
     return __ldg(a + j * pu + i);
   }
+  __device__ __forceinline__ bool quad(int i, int j, float& A, float& C, float& D, float& E) const {
+    if ((unsigned)i >= (unsigned)nx || (unsigned)j >= (unsigned)(ny - 1)) return false;
+    const float* q = a + j * pu + i;
+    A = __ldg(q); C = __ldg(q + 1); D = __ldg(q + pu); E = __ldg(q + pu + 1);
+    return true;
+  }
 };
 // V: still air outside, clamp at the floor (:47-48)
 struct VField {
@@ -209,34 +230,52 @@ struct VField {
     if (i < 0 || i >= nx || j > ny) return 0.f;
     return __ldg(a + max(j, 0) * pc + i);
   }
+  __device__ __forceinline__ bool quad(int i, int j, float& A, float& C, float& D, float& E) const {
+    if ((unsigned)i >= (unsigned)(nx - 1) || (unsigned)j >= (unsigned)ny) return false;
+    const float* q = a + j * pc + i;
+    A = __ldg(q); C = __ldg(q + 1); D = __ldg(q + pc); E = __ldg(q + pc + 1);
+    return true;
+  }
 };
 
 // s_<name>: bilinear at g - off (cell units); off = (0.5,0.5) C, (0,0.5) U, (0.5,0) V
+// the four corners of the 2x2 block at (i, j), directly when the field allows it
+template <class F, class T>
+__device__ __forceinline__ void corners(const F& f, int i, int j, T& A, T& C, T& D, T& E) {
+  if (f.quad(i, j, A, C, D, E)) return;
+  A = f.at(i, j); C = f.at(i + 1, j); D = f.at(i, j + 1); E = f.at(i + 1, j + 1);
+}
 template <class F>
 __device__ __forceinline__ float sample(const F& f, float gx, float gy, float ox, float oy) {
   const float fxp = gx - ox, fyp = gy - oy;
   const float bx = floorf(fxp), by = floorf(fyp), tx = fxp - bx, ty = fyp - by;
   const int i = wgsl_i32(bx), j = wgsl_i32(by);
-  return mixf(mixf(f.at(i, j), f.at(i + 1, j), tx), mixf(f.at(i, j + 1), f.at(i + 1, j + 1), tx), ty);
+  float A, C, D, E;
+  corners(f, i, j, A, C, D, E);
+  return mixf(mixf(A, C, tx), mixf(D, E, tx), ty);
 }
 template <class F>
 __device__ __forceinline__ float4 sample4(const F& f, float gx, float gy) {
   const float fxp = gx - 0.5f, fyp = gy - 0.5f;
   const float bx = floorf(fxp), by = floorf(fyp), tx = fxp - bx, ty = fyp - by;
   const int i = wgsl_i32(bx), j = wgsl_i32(by);
-  return mix4(mix4(f.at(i, j), f.at(i + 1, j), tx), mix4(f.at(i, j + 1), f.at(i + 1, j + 1), tx), ty);
+  float4 A, C, D, E;
+  corners(f, i, j, A, C, D, E);
+  return mix4(mix4(A, C, tx), mix4(D, E, tx), ty);
 }
 // mm_<name>: min/max of the 4 corners
 template <class F>
 __device__ __forceinline__ void minmax(const F& f, float gx, float gy, float ox, float oy, float& lo, float& hi) {
   const int i = wgsl_i32(floorf(gx - ox)), j = wgsl_i32(floorf(gy - oy));
-  const float A = f.at(i, j), C = f.at(i + 1, j), D = f.at(i, j + 1), E = f.at(i + 1, j + 1);
+  float A, C, D, E;
+  corners(f, i, j, A, C, D, E);
   lo = fminf(fminf(A, C), fminf(D, E)); hi = fmaxf(fmaxf(A, C), fmaxf(D, E));
 }
 template <class F>
 __device__ __forceinline__ void minmax4(const F& f, float gx, float gy, float4& lo, float4& hi) {
   const int i = wgsl_i32(floorf(gx - 0.5f)), j = wgsl_i32(floorf(gy - 0.5f));
-  const float4 A = f.at(i, j), C = f.at(i + 1, j), D = f.at(i, j + 1), E = f.at(i + 1, j + 1);
+  float4 A, C, D, E;
+  corners(f, i, j, A, C, D, E);
   lo = min4(min4(A, C), min4(D, E)); hi = max4(max4(A, C), max4(D, E));
 }
 

@@ -16,8 +16,21 @@ namespace cfg {
 
 namespace {
 
+// at(i, j): the first-order value from shared memory, recomputed from global memory outside
+// the staged region; quad(i, j, ...): the 2x2 block straight from shared memory when all four
+// corners are inside the level (no boundary rule applies) and inside the staged region
+__device__ __forceinline__ bool staged_block(int i, int j, int nx1, int ny1, int rx0, int ry0, int RW, int RH) {
+  return (unsigned)i < (unsigned)nx1 && (unsigned)j < (unsigned)ny1 && (unsigned)(i - rx0) < (unsigned)(RW - 1) &&
+         (unsigned)(j - ry0) < (unsigned)(RH - 1);
+}
 struct ThLookup {
   const float* sm; int rx0, ry0, RW, RH; const VelSampler* vs; const CField* T; float dt;
+  __device__ __forceinline__ bool quad(int i, int j, float& A, float& C, float& D, float& E) const {
+    if (!staged_block(i, j, T->nx - 1, T->ny - 1, rx0, ry0, RW, RH)) return false;
+    const float* q = sm + (j - ry0) * RW + (i - rx0);
+    A = q[0]; C = q[1]; D = q[RW]; E = q[RW + 1];
+    return true;
+  }
   __device__ __forceinline__ float at(int i, int j) const {
     if (i < 0 || i >= T->nx || j >= T->ny) return T->amb;
     j = max(j, 0);
@@ -29,6 +42,12 @@ struct ThLookup {
 };
 struct YhLookup {
   const float4* sm; int rx0, ry0, RW, RH; const VelSampler* vs; const C4Field* Y; float dt;
+  __device__ __forceinline__ bool quad(int i, int j, float4& A, float4& C, float4& D, float4& E) const {
+    if (!staged_block(i, j, Y->nx - 1, Y->ny - 1, rx0, ry0, RW, RH)) return false;
+    const float4* q = sm + (j - ry0) * RW + (i - rx0);
+    A = q[0]; C = q[1]; D = q[RW]; E = q[RW + 1];
+    return true;
+  }
   __device__ __forceinline__ float4 at(int i, int j) const {
     if (i < 0 || i >= Y->nx || j >= Y->ny) return Y->amb;
     j = max(j, 0);
@@ -40,6 +59,12 @@ struct YhLookup {
 };
 struct UhLookup {
   const float* sm; int rx0, ry0, RW, RH; const VelSampler* vs; float dt;
+  __device__ __forceinline__ bool quad(int i, int j, float& A, float& C, float& D, float& E) const {
+    if (!staged_block(i, j, vs->u.nx, vs->u.ny - 1, rx0, ry0, RW, RH)) return false;
+    const float* q = sm + (j - ry0) * RW + (i - rx0);
+    A = q[0]; C = q[1]; D = q[RW]; E = q[RW + 1];
+    return true;
+  }
   __device__ __forceinline__ float at(int i, int j) const {
     const UField& u = vs->u;
     if (i < 0 || i > u.nx || j >= u.ny) return 0.f;
@@ -54,6 +79,12 @@ struct UhLookup {
 };
 struct VhLookup {
   const float* sm; int rx0, ry0, RW, RH; const VelSampler* vs; float dt;
+  __device__ __forceinline__ bool quad(int i, int j, float& A, float& C, float& D, float& E) const {
+    if (!staged_block(i, j, vs->v.nx - 1, vs->v.ny, rx0, ry0, RW, RH)) return false;
+    const float* q = sm + (j - ry0) * RW + (i - rx0);
+    A = q[0]; C = q[1]; D = q[RW]; E = q[RW + 1];
+    return true;
+  }
   __device__ __forceinline__ float at(int i, int j) const {
     const VField& v = vs->v;
     if (i < 0 || i >= v.nx || j > v.ny) return 0.f;
