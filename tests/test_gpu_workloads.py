@@ -14,7 +14,7 @@ The GPU runs a few steps from the generated scene first, so the pipelined coarse
 the FP64 pressure and the CFL step are all carried over from earlier steps; its whole state
 (fields, geometry, multigrid levels, FP64 pressure, dt) is then copied into the oracle and
 both take the same steps. The FP32 oracle is the parity check (1e-4 per field, as the other
-full-step tests); the FP64 oracle is the accuracy check of the north-star workload.
+full-step tests); the FP64 oracle is the accuracy check of the 512x768 five-log workload.
 """
 import numpy as np
 import pytest
