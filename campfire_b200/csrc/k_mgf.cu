@@ -83,8 +83,9 @@ __device__ __forceinline__ const void* tmap_of(const SceneDesc& S, int level, in
 }
 
 // Tile staging on two barriers around the wait on the previous kernel. stage_coef
-// (before the wait in a one-scene engine, else once the scene's flag says it still cycles):
-// one thread initialises both barriers and requests the coefficients
+// (before the wait in a one-scene engine, which also waits for them and builds the stencils
+// before the wait, with the state copies' tensor maps prefetched; else once the scene's flag
+// says it still cycles): one thread initialises both barriers and requests the coefficients
 // ax, ay on bar[0]; they are built before the pressure loop and written by no loop kernel
 // (the loop is entered through a full dependency: a graph node or a memset). stage_state
 // (after the wait): p from map `pkind`, rhs and the coarse p under the tile on bar[1]; with
@@ -99,6 +100,14 @@ __device__ __forceinline__ void stage_coef(const SceneDesc& S, int level, const 
     mbar_arrive_expect_tx(&bar[0], BOX_BYTES + BOX_AY_BYTES);
     tma_load_2d(t.ax, tmap_of(S, level, TM_AX), t.sx, t.sy, &bar[0]);
     tma_load_2d(t.ay, tmap_of(S, level, TM_AY), t.sx, t.sy, &bar[0]);
+  }
+}
+// the tensor maps of stage_state's copies into the descriptor cache (before the wait)
+__device__ __forceinline__ void prefetch_state_maps(const SceneDesc& S, int level, int pkind, bool coarse) {
+  if (threadIdx.x == 0) {
+    tmap_prefetch(tmap_of(S, level, pkind));
+    tmap_prefetch(tmap_of(S, level, TM_RHS));
+    if (coarse) tmap_prefetch(tmap_of(S, level + 1, TM_PC));
   }
 }
 __device__ __forceinline__ void stage_state(const SceneDesc& S, int level, int pkind, const Tile& t, bool copy,
@@ -315,11 +324,18 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
   // one scene: its flag only ends the loop, so the tile is requested before it is read;
   // several: a scene that stopped loads nothing
   const bool spec = nscenes == 1;
-  if (on && spec) stage_coef(S, level, t, bar);
+  if (on && spec) {
+    stage_coef(S, level, t, bar);
+    prefetch_state_maps(S, level, TM_P, false);
+  }
   __syncthreads();
+  // one scene: the stencils, which depend on the coefficients alone, are built before the wait
+  TCell c[2][2];
+  bool ok = true;
+  if (on && spec && (ok = tile_wait(&bar[0], ctl))) tile_stencils(t, L, x0, y0, 0, c);
   pdl_wait();
   if (count_iter && blockIdx.x == 0 && threadIdx.x == 0) loop_count(ctl);
-  if (!on) return;
+  if (!on || !ok) return;
   if (!spec) {
     if (*(volatile int*)&ss->active == 0) return;
     stage_coef(S, level, t, bar);
@@ -334,8 +350,8 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
   const bool live = *(volatile int*)&ss->active != 0;
   const bool upd = PCG && pv.cycles >= 1;   // an update of the previous cycle is pending
   stage_state(S, level, TM_P, t, !upd, nullptr, 0, 0, bar);
-  TCell c[2][2];
-  if (!tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 0, c); }) || !live) return;
+  if (!(spec ? tile_wait(&bar[1], ctl) : tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 0, c); })) || !live)
+    return;
   if (upd) {
     pcg_down_apply(S, L, t, x0, y0, pv, u);
     __syncthreads();
@@ -405,13 +421,19 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
   const bool on = S.enabled;   // host-written, constant during the step
   SolveState* ss = S.solve;
   const bool spec = nscenes == 1;   // as in k_mg_down
-  if (on && spec) stage_coef(S, level, t, bar);
+  if (on && spec) {
+    stage_coef(S, level, t, bar);
+    prefetch_state_maps(S, level, TM_PB, true);
+  }
   __shared__ double s_rh2;   // the FP64 operator's 1 / h2 (tails 3 and 4)
   if (threadIdx.x == 0) s_rh2 = 1.0 / (double)L.h2;
   __syncthreads();
   const double rh2 = s_rh2;
+  TCell c[2][2];
+  bool ok = true;
+  if (on && spec && (ok = tile_wait(&bar[0], ctl))) tile_stencils(t, L, x0, y0, 1, c);
   pdl_wait();
-  if (!on) return;
+  if (!on || !ok) return;
   if (!spec) {
     if (*(volatile int*)&ss->active == 0) return;
     stage_coef(S, level, t, bar);
@@ -434,8 +456,8 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
       }
     }
   }
-  TCell c[2][2];
-  if (!tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 1, c); }) || !live) return;
+  if (!(spec ? tile_wait(&bar[1], ctl) : tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 1, c); })) || !live)
+    return;
   // prolongation (pressure.wgsl:116-129) on the whole region
   for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
     const int i = x0 - MGF_H + e % RW, j = y0 - MGF_H + e / RW;

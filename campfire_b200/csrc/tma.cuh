@@ -54,6 +54,12 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, 
       : "memory");
 }
 
+// fetch a tensor map (a CUtensorMap in global memory that no kernel writes) into the
+// descriptor cache ahead of the copies that name it
+__device__ __forceinline__ void tmap_prefetch(const void* tmap) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
