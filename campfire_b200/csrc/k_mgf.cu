@@ -89,7 +89,8 @@ __device__ __forceinline__ const void* tmap_of(const SceneDesc& S, int level, in
 // ax, ay on bar[0]; they are built before the pressure loop and written by no loop kernel
 // (the loop is entered through a full dependency: a graph node or a memset). stage_state
 // (after the wait): p from map `pkind`, rhs and the coarse p under the tile on bar[1]; with
-// `copy` false nothing is requested and bar[1] completes on its arrival. The copies are
+// `copy` false nothing is requested and bar[1] completes on its arrival; with `pload` false p
+// is not copied (the caller zero-fills its box). The copies are
 // issued whether or not the scene still cycles, so the read of its `active` flag overlaps
 // them. tile_wait: all threads wait for one barrier (bounded); false in every thread if a
 // wait ran out, after recording the error and waiting once more for the copies in flight.
@@ -111,11 +112,11 @@ __device__ __forceinline__ void prefetch_state_maps(const SceneDesc& S, int leve
   }
 }
 __device__ __forceinline__ void stage_state(const SceneDesc& S, int level, int pkind, const Tile& t, bool copy,
-                                            float* cp, int cx, int cy, uint64_t* bar) {
+                                            float* cp, int cx, int cy, uint64_t* bar, bool pload = true) {
   if (threadIdx.x == 0) {
-    mbar_arrive_expect_tx(&bar[1], copy ? 2 * BOX_BYTES + (cp ? CBOX_BYTES : 0u) : 0u);
+    mbar_arrive_expect_tx(&bar[1], copy ? (pload ? 2 : 1) * BOX_BYTES + (cp ? CBOX_BYTES : 0u) : 0u);
     if (copy) {
-      tma_load_2d(t.p, tmap_of(S, level, pkind), t.sx, t.sy, &bar[1]);
+      if (pload) tma_load_2d(t.p, tmap_of(S, level, pkind), t.sx, t.sy, &bar[1]);
       tma_load_2d(t.rhs, tmap_of(S, level, TM_RHS), t.sx, t.sy, &bar[1]);
       if (cp) tma_load_2d(cp, tmap_of(S, level + 1, TM_PC), cx, cy, &bar[1]);
     }
@@ -228,6 +229,58 @@ __device__ __forceinline__ void tile_passes(const Tile& t, const LevelDesc& L, i
   }
 }
 
+// The up kernel's prolongation (pressure.wgsl:116-129) over the region [x0-H, x0+TX+H) x
+// [y0-H, y0+TY+H); with one scene split in two. prolong_plan (from the coefficients and the level
+// sizes alone, beside the stencils before the wait) packs for element e = threadIdx.x + 256 m: the fine cell's box index
+// (bits 0-10), the index in the coarse box of its own coarse cell (11-19), the steps to the other
+// coarse column and row of its bilinear stencil plus one (20-21, 22-23), whether the cell is open
+// (24) and whether it lies in the level (25). prolong_apply adds the interpolated correction once
+// the coarse box has landed: a closed cell adds +0, as pressure.wgsl:129 has it.
+constexpr int PR_W = MGF_TX + 2 * MGF_H, PR_H = MGF_TY + 2 * MGF_H, PR_N = (PR_W * PR_H + 255) / 256;
+static_assert(MGF_BW * MGF_BH <= 2048 && MGF_CBW * MGF_CBH <= 512, "plan fields");
+__device__ __forceinline__ void prolong_plan(const Tile& t, const LevelDesc& L, const LevelDesc& C, int x0, int y0,
+                                             int cx, int cy, uint32_t (&pl)[PR_N]) {
+  #pragma unroll
+  for (int m = 0; m < PR_N; m++) {
+    const int e = threadIdx.x + 256 * m;
+    const int i = x0 - MGF_H + e % PR_W, j = y0 - MGF_H + e / PR_W;
+    pl[m] = 0u;
+    if (e >= PR_W * PR_H || i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
+    const int I = i / 2, J = j / 2;
+    const int dI = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), C.nx - 1) - I;
+    const int dJ = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), C.ny - 1) - J;
+    const int a = (J - cy) * MGF_CBW + I - cx;
+    pl[m] = (uint32_t)t.c(i, j) | (uint32_t)a << 11 | (uint32_t)(dI + 1) << 20 | (uint32_t)(dJ + 1) << 22 |
+            (diag_s(t, L.nx, L.ny, i, j) > 0.f ? 1u << 24 : 0u) | 1u << 25;
+  }
+}
+// the same additions computed in one pass after the coarse box has landed (several scenes: the
+// plan would only add instructions after the wait)
+__device__ __forceinline__ void prolong_direct(const Tile& t, const LevelDesc& L, const LevelDesc& C, int x0, int y0,
+                                               int cx, int cy, const float* scp) {
+  for (int e = threadIdx.x; e < PR_W * PR_H; e += 256) {
+    const int i = x0 - MGF_H + e % PR_W, j = y0 - MGF_H + e / PR_W;
+    if (i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
+    const int I = i / 2, J = j / 2;
+    const int I2 = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), C.nx - 1);
+    const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), C.ny - 1);
+    const int r0 = (J - cy) * MGF_CBW, r1 = (J2 - cy) * MGF_CBW;
+    const float c_ = 0.5625f * scp[r0 + I - cx] + 0.1875f * (scp[r0 + I2 - cx] + scp[r1 + I - cx]) +
+                     0.0625f * scp[r1 + I2 - cx];
+    t.p[t.c(i, j)] += diag_s(t, L.nx, L.ny, i, j) > 0.f ? c_ : 0.f;
+  }
+}
+__device__ __forceinline__ void prolong_apply(const Tile& t, const float* scp, const uint32_t (&pl)[PR_N]) {
+  #pragma unroll
+  for (int m = 0; m < PR_N; m++) {
+    const uint32_t q = pl[m];
+    if (!(q & (1u << 25))) continue;
+    const int a = (q >> 11) & 511, dI = (int)((q >> 20) & 3) - 1, dJ = ((int)((q >> 22) & 3) - 1) * MGF_CBW;
+    const float c_ = 0.5625f * scp[a] + 0.1875f * (scp[a + dI] + scp[a + dJ]) + 0.0625f * scp[a + dI + dJ];
+    t.p[q & 2047] += (q & (1u << 24)) ? c_ : 0.f;
+  }
+}
+
 // Fused Krylov mode on level 0 (all scenes' coarse blocks start below it). The update of
 // cycle c (d = z + beta d, q = Lz + beta q, p64 += alpha d, r -= alpha q with cycle c's
 // alpha, beta) is split: the next cycle's down kernel forms d and p64 on its tile and the
@@ -299,7 +352,8 @@ __device__ __forceinline__ void pcg_down_apply(const SceneDesc& S, const LevelDe
 
 // ------------------------------------------------------------------ down: 4 passes + restrict
 // PCG: the fused Krylov update on level 0 (above)
-template <int TX, int TY, bool PCG>
+// ONE: compiled for an engine of one scene (nscenes == 1), whose flag only ends the loop
+template <int TX, int TY, bool PCG, bool ONE>
 // three CTAs per SM (at most 85 registers a thread; 44 bytes of spill in the fused Krylov
 // variant): 512x768's 768 level-0 tiles run in two waves instead of three (measured: -5% per
 // Krylov cycle at 512x768). Four for the plain variants (62 registers) was measured 3-4% slower
@@ -323,11 +377,16 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
   SolveState* ss = S.solve;
   // one scene: its flag only ends the loop, so the tile is requested before it is read;
   // several: a scene that stopped loads nothing
-  const bool spec = nscenes == 1;
+  constexpr bool spec = ONE;
   if (on && spec) {
     stage_coef(S, level, t, bar);
     prefetch_state_maps(S, level, TM_P, false);
   }
+  // below level 0 the level's p is zero on entry (the restriction above zeroes it): with one
+  // scene its box is zero-filled before the wait instead of copied after it
+  const bool pz = spec && level > 0;
+  if (pz)
+    for (int e = threadIdx.x; e < MGF_BW * MGF_BH; e += 256) t.p[e] = 0.f;
   __syncthreads();
   // one scene: the stencils, which depend on the coefficients alone, are built before the wait
   TCell c[2][2];
@@ -349,7 +408,7 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
   }
   const bool live = *(volatile int*)&ss->active != 0;
   const bool upd = PCG && pv.cycles >= 1;   // an update of the previous cycle is pending
-  stage_state(S, level, TM_P, t, !upd, nullptr, 0, 0, bar);
+  stage_state(S, level, TM_P, t, !upd, nullptr, 0, 0, bar, !pz);
   if (!(spec ? tile_wait(&bar[1], ctl) : tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 0, c); })) || !live)
     return;
   if (upd) {
@@ -398,11 +457,10 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
 // 3 r.z, q.z, z.Lz -> the direction update (Krylov FP64 mode), 4 the same in the fused Krylov
 // mode (the pending r, q update first; the loop decision from the recurrence for ||r||),
 // compiled into the KRY instance only
-template <int TX, int TY, bool KRY>
+template <int TX, int TY, bool KRY, bool ONE>   // ONE: as in k_mg_down
 __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, int tail, SolveCtl* ctl) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
-  constexpr int RW = TX + 2 * MGF_H, RH = TY + 2 * MGF_H;
   __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
   __shared__ __align__(128) float srhs[MGF_BH * MGF_BW];
   __shared__ __align__(128) float sax[MGF_BH * MGF_BW];
@@ -420,7 +478,7 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
   const int cx = x0 / 2 - 8, cy = y0 / 2 - 4;
   const bool on = S.enabled;   // host-written, constant during the step
   SolveState* ss = S.solve;
-  const bool spec = nscenes == 1;   // as in k_mg_down
+  constexpr bool spec = ONE;   // as in k_mg_down
   if (on && spec) {
     stage_coef(S, level, t, bar);
     prefetch_state_maps(S, level, TM_PB, true);
@@ -430,8 +488,12 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
   __syncthreads();
   const double rh2 = s_rh2;
   TCell c[2][2];
+  uint32_t pl[PR_N];
   bool ok = true;
-  if (on && spec && (ok = tile_wait(&bar[0], ctl))) tile_stencils(t, L, x0, y0, 1, c);
+  if (on && spec && (ok = tile_wait(&bar[0], ctl))) {
+    tile_stencils(t, L, x0, y0, 1, c);
+    prolong_plan(t, L, C, x0, y0, cx, cy, pl);
+  }
   pdl_wait();
   if (!on || !ok) return;
   if (!spec) {
@@ -459,17 +521,10 @@ __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ 
   if (!(spec ? tile_wait(&bar[1], ctl) : tile_wait2(bar, ctl, [&] { tile_stencils(t, L, x0, y0, 1, c); })) || !live)
     return;
   // prolongation (pressure.wgsl:116-129) on the whole region
-  for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
-    const int i = x0 - MGF_H + e % RW, j = y0 - MGF_H + e / RW;
-    if (i < 0 || i >= L.nx || j < 0 || j >= L.ny) continue;
-    const int I = i / 2, J = j / 2;
-    const int I2 = min(max(I + ((i & 1) == 1 ? 1 : -1), 0), C.nx - 1);
-    const int J2 = min(max(J + ((j & 1) == 1 ? 1 : -1), 0), C.ny - 1);
-    const int r0_ = (J - cy) * MGF_CBW, r1 = (J2 - cy) * MGF_CBW;
-    const float c_ = 0.5625f * scp[r0_ + I - cx] + 0.1875f * (scp[r0_ + I2 - cx] + scp[r1 + I - cx]) +
-                     0.0625f * scp[r1 + I2 - cx];
-    t.p[t.c(i, j)] += diag_s(t, L.nx, L.ny, i, j) > 0.f ? c_ : 0.f;
-  }
+  if (spec)
+    prolong_apply(t, scp, pl);
+  else
+    prolong_direct(t, L, C, x0, y0, cx, cy, scp);
   __syncthreads();
   tile_passes(t, L, 1, c);   // colours 1, 0, 1, 0 (js/fluid.js:307-310)
   if (KRY) {
@@ -1244,14 +1299,18 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
 void launch_mg_down(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, SolveCtl* ctl,
                     int count_iter, int pcg, cudaStream_t st) {
   if (ntiles > 0)
-    launch_pdl(pdl_enabled(), pcg ? k_mg_down<MGF_TX, MGF_TY, true> : k_mg_down<MGF_TX, MGF_TY, false>, dim3(ntiles),
-               dim3(256), 0, st, scenes, nscenes, work, level, ctl, count_iter);
+    launch_pdl(pdl_enabled(),
+               nscenes == 1 ? (pcg ? k_mg_down<MGF_TX, MGF_TY, true, true> : k_mg_down<MGF_TX, MGF_TY, false, true>)
+                            : (pcg ? k_mg_down<MGF_TX, MGF_TY, true, false> : k_mg_down<MGF_TX, MGF_TY, false, false>),
+               dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, ctl, count_iter);
 }
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {
   if (ntiles > 0)
-    launch_pdl(pdl_enabled(), tail == 4 ? k_mg_up<MGF_TX, MGF_TY, true> : k_mg_up<MGF_TX, MGF_TY, false>, dim3(ntiles),
-               dim3(256), 0, st, scenes, nscenes, work, level, tail, ctl);
+    launch_pdl(pdl_enabled(),
+               nscenes == 1 ? (tail == 4 ? k_mg_up<MGF_TX, MGF_TY, true, true> : k_mg_up<MGF_TX, MGF_TY, false, true>)
+                            : (tail == 4 ? k_mg_up<MGF_TX, MGF_TY, true, false> : k_mg_up<MGF_TX, MGF_TY, false, false>),
+               dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, tail, ctl);
 }
 void launch_pcg_decide(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, cudaStream_t st) {
   if (nscenes > 0) launch_pdl(pdl_enabled(), k_pcg_decide, dim3(nscenes), dim3(256), 0, st, scenes, ctl);
