@@ -47,8 +47,8 @@ def _compile(src: str, force: bool, extra: list[str]) -> str:
         return obj
     cmd = [nvcc()] + NVCC_FLAGS + extra + ["-x", "cu" if src.endswith(".cu") else "c++", "-c", path, "-o", obj]
     if src.endswith(".cpp"):
-        cmd = [nvcc(), "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off", "-I" + os.path.join(HERE, "..", "include"),
-               "-x", "c++", "-c", path, "-o", obj]
+        cmd = [nvcc()] + ARCH + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                                 "-I" + os.path.join(HERE, "..", "include"), "-x", "c++", "-c", path, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")

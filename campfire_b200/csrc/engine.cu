@@ -1196,6 +1196,11 @@ bool Engine::any_wtail() const {
   return false;
 }
 
+bool Engine::any_block_level0() const {
+  for (auto& sc : scenes_) if (sc.lc == 0) return true;
+  return false;
+}
+
 bool Engine::pcg_fused() const {
   // krylov 1: one scene folds the update into the level-0 kernels (a shorter kernel chain); a
   // batch, bound by bandwidth, keeps the separate update kernel, which moves fewer bytes.
@@ -1227,7 +1232,7 @@ void Engine::enqueue_vcycle(cudaStream_t s, int tail, int count_iter) {
   if (coarse_cluster_ > 0)
     launch_mg_cluster(d_scenes_, nscenes(), d_ctl_, coarse_cluster_, count_iter, cluster_smem_, s);
   else
-    launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, count_iter, coarse_smem_, any_wtail(), s);
+    launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, tail, count_iter, coarse_smem_, any_wtail(), any_block_level0(), s);
   vcycle_launches_++;
   for (int l = LD - 1; l >= 0; l--) {
     if (nwl_[WL_MGD0 + l] == 0) continue;
@@ -1619,7 +1624,7 @@ int Engine::time_kernel(const char* name, int iters, double* ms, double* bytes, 
   } else if (n == "mg_coarse") {
     go = [&](int) {
       if (coarse_cluster_ > 0) launch_mg_cluster(d_scenes_, nscenes(), d_ctl_, coarse_cluster_, 0, cluster_smem_, s);
-      else launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, 0, coarse_smem_, any_wtail(), s);
+      else launch_mg_coarse(d_scenes_, nscenes(), d_ctl_, 0, 0, coarse_smem_, any_wtail(), any_block_level0(), s);
     };
     // the reference schedule's V-cycle bytes of the levels the block covers (163 B per level cell)
     b = 0;

@@ -168,6 +168,7 @@ class Engine {
   int set_coarse_w(int cells);
   int coarse_w() const { return w_cells_; }
   bool any_wtail() const;       // some scene's coarse block runs the W tail
+  bool any_block_level0() const;   // some scene's coarse block covers level 0
   bool krylov_folded() const { return pcg_fused(); }   // the loop folds the Krylov update
   // the coarse phase on one CTA (0) or on a cluster of cs CTAs per scene (2..16, from level 1)
   int set_coarse_cluster(int cs);

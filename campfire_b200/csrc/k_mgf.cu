@@ -455,12 +455,15 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
 // ------------------------------------------------------------------ up: prolong + 4 passes (+ level-0 tail)
 // tail: 0 none, 1 residual norm + loop decision (FP32 modes), 2 p64 += p (FP64 defect correction),
 // 3 r.z, q.z, z.Lz -> the direction update (Krylov FP64 mode), 4 the same in the fused Krylov
-// mode (the pending r, q update first; the loop decision from the recurrence for ||r||),
-// compiled into the KRY instance only
-template <int TX, int TY, bool KRY, bool ONE>   // ONE: as in k_mg_down
+// mode (the pending r, q update first; the loop decision from the recurrence for ||r||); one
+// instance per tail (levels below 0: tail 0)
+template <int TX, int TY, int TAIL, bool ONE>   // ONE: as in k_mg_down
 __global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
-                                               int level, int tail, SolveCtl* ctl) {
+                                               int level, SolveCtl* ctl) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
+  static_assert(TAIL >= 0 && TAIL <= 4, "tails 0-4");
+  constexpr bool KRY = TAIL == 4;
+  constexpr int tail = TAIL;
   __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
   __shared__ __align__(128) float srhs[MGF_BH * MGF_BW];
   __shared__ __align__(128) float sax[MGF_BH * MGF_BW];
@@ -932,7 +935,8 @@ __device__ __forceinline__ void cb_up(const CbCtx c, int l) {
 // smem_floats: the launch's dynamic shared memory in floats; past the levels and the residual
 // scratch, the coarsest inverse of the direct solve is staged there when it fits
 // WT: compiled with the W tail (an engine whose scenes have one); without it the V-cycle's code alone
-template <bool WT>
+// L0: compiled with the level-0 ends of the cycle (an engine where some scene's block covers level 0)
+template <bool WT, bool L0>
 __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __restrict__ scenes, int nscenes, SolveCtl* ctl, int tail,
                                                          int count_iter, int smem_floats) {
   extern __shared__ __align__(128) float smem[];
@@ -944,7 +948,6 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   const SceneDesc& S = scenes[blockIdx.x];
   pdl_trigger();
   const int lc = S.lc, nl = S.nlev;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     int q = 0;
     for (int l = lc; l < nl; l++) {
@@ -1036,7 +1039,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   const int still = *act;
   float* sres = smem + s_res;   // residual scratch (level lc size)
   for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.rhs[e] = __ldcg(grhs + e);
-  if (lc == 0)   // warm start
+  if (L0 && lc == 0)   // warm start
     for (int e = threadIdx.x; e < V0.ny * V0.pc; e += CB_THREADS) V0.p[e] = __ldcg(s_gp + e);
   if (still == 0) return;
   __syncthreads();
@@ -1057,7 +1060,7 @@ __global__ void __launch_bounds__(CB_THREADS) k_mg_coarse(const SceneDesc* __res
   // ---- write level lc back; when the block covers level 0, finish the cycle here
   float* const gp = s_gp;
   const int gpc = s_gpc, gnx = V0.nx;
-  if (lc > 0) {
+  if (!L0 || lc > 0) {
     // the shared copy of level lc's p has the global pitch: one bulk copy (the last visit ended
     // with a block barrier); the next kernel reads it after this grid has completed
     if (threadIdx.x == 0) {
@@ -1296,6 +1299,17 @@ size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev) {
   return f * 4;
 }
 
+using UpKernel = void (*)(const SceneDesc*, int, const Work*, int, SolveCtl*);
+template <bool ONE>
+static UpKernel up_kernel(int tail) {
+  switch (tail) {
+    case 1: return k_mg_up<MGF_TX, MGF_TY, 1, ONE>;
+    case 2: return k_mg_up<MGF_TX, MGF_TY, 2, ONE>;
+    case 3: return k_mg_up<MGF_TX, MGF_TY, 3, ONE>;
+    case 4: return k_mg_up<MGF_TX, MGF_TY, 4, ONE>;
+    default: return k_mg_up<MGF_TX, MGF_TY, 0, ONE>;
+  }
+}
 void launch_mg_down(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, SolveCtl* ctl,
                     int count_iter, int pcg, cudaStream_t st) {
   if (ntiles > 0)
@@ -1307,19 +1321,19 @@ void launch_mg_down(const SceneDesc* scenes, int nscenes, const Work* work, int 
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {
   if (ntiles > 0)
-    launch_pdl(pdl_enabled(),
-               nscenes == 1 ? (tail == 4 ? k_mg_up<MGF_TX, MGF_TY, true, true> : k_mg_up<MGF_TX, MGF_TY, false, true>)
-                            : (tail == 4 ? k_mg_up<MGF_TX, MGF_TY, true, false> : k_mg_up<MGF_TX, MGF_TY, false, false>),
-               dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, tail, ctl);
+    launch_pdl(pdl_enabled(), nscenes == 1 ? up_kernel<true>(tail) : up_kernel<false>(tail), dim3(ntiles), dim3(256), 0,
+               st, scenes, nscenes, work, level, ctl);
 }
 void launch_pcg_decide(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, cudaStream_t st) {
   if (nscenes > 0) launch_pdl(pdl_enabled(), k_pcg_decide, dim3(nscenes), dim3(256), 0, st, scenes, ctl);
 }
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
-                      int wtail, cudaStream_t st) {
+                      int wtail, int level0, cudaStream_t st) {
   if (nscenes > 0)
-    launch_pdl(pdl_enabled(), wtail ? k_mg_coarse<true> : k_mg_coarse<false>, dim3(nscenes), dim3(CB_THREADS), smem,
-               st, scenes, nscenes, ctl, tail, count_iter, (int)(smem / 4));
+    launch_pdl(pdl_enabled(),
+               wtail ? (level0 ? k_mg_coarse<true, true> : k_mg_coarse<true, false>)
+                     : (level0 ? k_mg_coarse<false, true> : k_mg_coarse<false, false>),
+               dim3(nscenes), dim3(CB_THREADS), smem, st, scenes, nscenes, ctl, tail, count_iter, (int)(smem / 4));
 }
 // bw: the widest coarsest level of the batch (the register window's bound)
 void launch_coarse_factor(const SceneDesc* scenes, int nscenes, size_t smem, int bw, int pipelined, cudaStream_t st) {
@@ -1343,9 +1357,11 @@ cudaError_t prepare_coarse_factor(size_t smem) {
 cudaError_t prepare_mg_coarse(size_t smem) {
   // the kernel's attribute, shared by every engine: the largest size any schedule can ask for
   const int bytes = (int)std::max(smem, kCoarseSmemMax);
-  const cudaError_t e = cudaFuncSetAttribute(k_mg_coarse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_mg_coarse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaFuncSetAttribute(k_mg_coarse<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mg_coarse<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mg_coarse<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mg_coarse<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
 }
 
 }  // namespace cfg

@@ -107,9 +107,11 @@ void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int nt
 // after the level-0 up kernel with tail 4: each scene's dot products summed, the coefficients
 // and the loop decision (one CTA per scene)
 void launch_pcg_decide(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, cudaStream_t st);
-// wtail: some scene has the W tail (SceneDesc::lw), else the V-cycle's instance
+// wtail: some scene has the W tail (SceneDesc::lw), else the V-cycle's instance; level0: some
+// scene's block covers level 0 (the cycle's level-0 ends: warm start, `tail`), else an instance
+// without them
 void launch_mg_coarse(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, int tail, int count_iter, size_t smem,
-                      int wtail, cudaStream_t st);
+                      int wtail, int level0, cudaStream_t st);
 size_t coarse_smem_bytes(const int* lnx, const int* lny, int lc, int nlev);
 // the cluster coarse phase (k_mgc.cu): levels lc..coarsest of each scene on a cluster of cs CTAs
 constexpr size_t kClusterSmemMax = 232448 - 2048;
