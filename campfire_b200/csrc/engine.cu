@@ -29,6 +29,9 @@ namespace cfg {
 
 // bench.py counts these bytes as the per-step parameter upload of cfg_write_params
 static_assert(kDescParamBytes == 204, "parameter block of SceneDesc");
+static_assert(kDescParamBytes == 4 * PARAM_WORDS && sizeof(ParamWords) == kDescParamBytes, "parameter words");
+static_assert(sizeof(PieceFloats) == sizeof(Scene::pieces), "piece block");
+static_assert(kRingBytes % 4 == 0, "readback words");
 
 namespace {
 thread_local std::string g_err;
@@ -100,8 +103,7 @@ Engine::~Engine() {
   if (d_rwood_) cudaFree(d_rwood_);
   if (d_image_) cudaFree(d_image_);
   if (h_ctl_pinned_) cudaFreeHost(h_ctl_pinned_);
-  if (h_dt_pinned_) cudaFreeHost(h_dt_pinned_);
-  if (d_dtv_) cudaFree(d_dtv_);
+  if (h_dt_pinned_) cudaFreeHost(h_dt_pinned_);   // d_dtv_ is its device address
   if (ev_dt_) cudaEventDestroy(ev_dt_);
   if (stream_) cudaStreamDestroy(stream_);
   if (body_stream_) cudaStreamDestroy(body_stream_);
@@ -177,9 +179,9 @@ int Engine::init(int device, int n, const int* nx, const int* ny, const double* 
   CFG_CUDA(cudaMemset(d_solve_, 0, sizeof(SolveState) * n));
   CFG_CUDA(cudaMalloc(&d_ctl_, sizeof(SolveCtl)));
   CFG_CUDA(cudaMallocHost(&h_ctl_pinned_, sizeof(SolveCtl)));
-  CFG_CUDA(cudaMallocHost(&h_dt_pinned_, sizeof(float) * n));
-  CFG_CUDA(cudaMalloc(&d_dtv_, sizeof(float) * n));
-  CFG_CUDA(cudaMemset(d_dtv_, 0, sizeof(float) * n));   // 0: no step has set a scene's dt yet
+  CFG_CUDA(cudaHostAlloc(&h_dt_pinned_, sizeof(float) * n, cudaHostAllocMapped | cudaHostAllocPortable));
+  std::memset(h_dt_pinned_, 0, sizeof(float) * n);   // 0: no step has set a scene's dt yet
+  CFG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d_dtv_), h_dt_pinned_, 0));
   CFG_CUDA(cudaMalloc(&d_dxd_, sizeof(double) * n));
   CFG_CUDA(cudaMalloc(&d_alpha_, sizeof(double) * n));
   CFG_CUDA(cudaMalloc(&d_scratch_, sizeof(double) * 64));
@@ -774,20 +776,20 @@ int Engine::write_params(int s) {
   SceneDesc& d = sc.desc;
   d.P = sc.P; d.diff_sub = n; d.diff_dt = sc.diff_dt;
   d.cfl = (float)sc.cfl; d.dt_cap = (float)sc.dt_cap; d.nray = sc.nray; d.enabled = sc.enabled ? 1 : 0;
-  // only the leading scalar block changes here (the uniform and the step controls). The
-  // sources are pageable host memory, which a copy has staged by the time it returns, so
-  // the copies stay in stream order without a wait here.
-  if (device_dt) {
-    // everything but P.dt and (diff_sub, diff_dt)
-    const size_t o_dt = offsetof(SceneDesc, P) + offsetof(cfg_params, dt);
-    const size_t o_sub = offsetof(SceneDesc, diff_sub), o_cfl = offsetof(SceneDesc, cfl);
-    char* dst = reinterpret_cast<char*>(d_scenes_ + s);
-    const char* src = reinterpret_cast<const char*>(&d);
-    CFG_CUDA(cudaMemcpyAsync(dst, src, o_dt, cudaMemcpyHostToDevice, st()));
-    CFG_CUDA(cudaMemcpyAsync(dst + o_dt + 4, src + o_dt + 4, o_sub - (o_dt + 4), cudaMemcpyHostToDevice, st()));
-    CFG_CUDA(cudaMemcpyAsync(dst + o_cfl, src + o_cfl, kDescParamBytes - o_cfl, cudaMemcpyHostToDevice, st()));
-  } else {
-    CFG_CUDA(cudaMemcpyAsync(d_scenes_ + s, &d, kDescParamBytes, cudaMemcpyHostToDevice, st()));
+  // only the leading scalar block changes here (the uniform and the step controls): one kernel
+  // on the stream with the block as its parameter (no copy engine, nothing to wait for), which
+  // with a step-owned dt leaves P.dt and (diff_sub, diff_dt) as the step set them
+  {
+    ParamWords b;
+    std::memcpy(b.w, &d, kDescParamBytes);
+    int skip = -1, s0 = -1, s1 = -1;
+    if (device_dt) {
+      skip = (int)((offsetof(SceneDesc, P) + offsetof(cfg_params, dt)) / 4);
+      s0 = (int)(offsetof(SceneDesc, diff_sub) / 4);
+      s1 = (int)(offsetof(SceneDesc, cfl) / 4);
+    }
+    launch_write_params(reinterpret_cast<uint32_t*>(d_scenes_ + s), b, skip, s0, s1, st());
+    CFG_CUDA(cudaGetLastError());
   }
   if (sc.dxd != sc.up_dxd) {
     CFG_CUDA(cudaMemcpyAsync(d_dxd_ + s, &sc.dxd, 8, cudaMemcpyHostToDevice, st()));
@@ -814,8 +816,11 @@ int Engine::upload_pieces(int s, const float* data, int n) {
   sc.host.nPieces = n;
   std::memset(sc.pieces, 0, sizeof sc.pieces);
   if (data) std::memcpy(sc.pieces, data, sizeof sc.pieces);
-  // pageable source: staged by the time the copy returns (no wait needed)
-  CFG_CUDA(cudaMemcpyAsync(sc.desc.pieces, sc.pieces, sizeof sc.pieces, cudaMemcpyHostToDevice, st()));
+  // the block as the parameter of one kernel on the stream (no copy engine, no wait)
+  PieceFloats b;
+  std::memcpy(b.f, sc.pieces, sizeof sc.pieces);
+  launch_write_pieces(sc.desc.pieces, b, st());
+  CFG_CUDA(cudaGetLastError());
   return CFG_OK;
 }
 
@@ -908,16 +913,19 @@ int Engine::readback_begin(int s, uint64_t tag, int* slot) {
   Scene& sc = scenes_[s];
   Scene::Ring& R = sc.ring;
   if (!R.host) {
-    CFG_CUDA(cudaMallocHost(&R.host, kRingSlots * kRingBytes));
+    CFG_CUDA(cudaHostAlloc(&R.host, kRingSlots * kRingBytes, cudaHostAllocMapped | cudaHostAllocPortable));
+    CFG_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&R.dev), R.host, 0));
     for (auto& e : R.ev) CFG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   const int i = R.idx;
   if (R.busy[i]) return fail(CFG_ERR_BUSY, "readback ring slot still pending (three readbacks not collected)");
   const SceneDesc& d = sc.desc;
   cudaStream_t q = st();
-  char* h = R.host + (size_t)i * kRingBytes;
-  CFG_CUDA(cudaMemcpyAsync(h, d.acc, kRingBytes, cudaMemcpyDeviceToHost, q));   // acc, rad, faceW at once
-  CFG_CUDA(cudaMemsetAsync(d.acc, 0, ACC_LEN * 4, q));
+  // acc, rad, faceW (contiguous on the device) written into the slot by one kernel, which then
+  // clears the accumulators
+  launch_readback(reinterpret_cast<uint32_t*>(d.acc), reinterpret_cast<uint32_t*>(R.dev + (size_t)i * kRingBytes),
+                  (int)(kRingBytes / 4), ACC_LEN, q);
+  CFG_CUDA(cudaGetLastError());
   CFG_CUDA(cudaEventRecord(R.ev[i], q));
   R.busy[i] = true;
   R.tag[i] = tag;
@@ -1319,7 +1327,7 @@ void Engine::enqueue_factor_join(cudaStream_t s) {
 
 // The step's tail: the projection, which also swaps the pipelined coarsest inverse
 // (after the factorisation's branch has joined) and sets the next CFL dt
-// Returns the first failing CUDA call's status; on failure the pinned dt copy must not be
+// Returns the first failing CUDA call's status; on failure the pinned dt must not be
 // trusted (the caller leaves dt_from_step_ unset).
 cudaError_t Engine::enqueue_post_solve(cudaStream_t s) {
   const bool pipe = pipelined_coarse();
@@ -1333,9 +1341,7 @@ cudaError_t Engine::enqueue_post_solve(cudaStream_t s) {
   launches_++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !cfl) return e;
-  // the next dt to the host side, for cfg_write_params
-  e = cudaMemcpyAsync(h_dt_pinned_, d_dtv_, sizeof(float) * nscenes(), cudaMemcpyDeviceToHost, s);
-  if (e != cudaSuccess) return e;
+  // the projection wrote the next dt to the host side (mapped pinned memory) for cfg_write_params
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   e = cudaStreamIsCapturing(s, &cap);
   if (e != cudaSuccess) return e;

@@ -80,7 +80,8 @@ struct Scene {
   // acc, rad and faceW, each filled by copies on the stream and completed by its event,
   // handed out oldest first. Allocated on the first cfg_readback_begin.
   struct Ring {
-    char* host = nullptr;              // kRingSlots x kRingBytes, pinned
+    char* host = nullptr;              // kRingSlots x kRingBytes, pinned and mapped
+    char* dev = nullptr;               // the same memory in the device's address space
     cudaEvent_t ev[3] = {};
     uint64_t tag[3] = {}, seq[3] = {};
     bool busy[3] = {};                 // copies enqueued, not yet handed out (stageBusy)
@@ -245,9 +246,10 @@ class Engine {
   SolveState* d_solve_ = nullptr;
   SolveCtl* d_ctl_ = nullptr;
   SolveCtl* h_ctl_pinned_ = nullptr;
-  // CFL steps: the step ends by copying each scene's next dt (d_dtv_) into pinned memory and
-  // recording ev_dt_, so cfg_write_params reads it once that event has passed instead of
-  // reading the descriptor back (dt_from_step_: no descriptor upload since that step)
+  // CFL steps: the projection writes each scene's next dt into pinned host memory mapped into
+  // the device's address space (d_dtv_ is its device address) and the step records ev_dt_, so
+  // cfg_write_params reads it once that event has passed instead of reading the descriptor back
+  // (dt_from_step_: no descriptor upload since that step)
   float *h_dt_pinned_ = nullptr, *d_dtv_ = nullptr;
   cudaEvent_t ev_dt_ = nullptr;
   bool dt_from_step_ = false;

@@ -109,7 +109,10 @@ __global__ void __launch_bounds__(256) k_project(SceneDesc* __restrict__ scenes,
   if (s_last && threadIdx.x == 0) {
     S.solve->counter = 0u;
     cfl_next_dt(S, dxd[w.scene], alpha[w.scene], true);
-    if (dtv) dtv[w.scene] = S.P.dt;
+    if (dtv) {   // pinned host memory: visible to the host once the step's event has passed
+      dtv[w.scene] = S.P.dt;
+      __threadfence_system();
+    }
   }
 }
 
@@ -337,6 +340,39 @@ __global__ void __launch_bounds__(1024) k_budgets(const SceneDesc* __restrict__ 
   if (threadIdx.x == 0) out[7] = (double)tm;
 }
 
+// ------------------------------------------------------------------ host blocks by value, readback
+// A scene's parameter block (writeParams, js/fluid.js:180-199) and its pieces (uploadPieces,
+// js/fluid.js:201-204) arrive as kernel parameters: one launch each instead of copy-engine
+// transfers beside the compute stream, and the host's copy is free again once the launch returns.
+// k_write_params leaves out word `skip` and words [s0, s1) (the step-owned dt and diffusion
+// sub-steps of a CFL scene; -1: none).
+__global__ void k_write_params(uint32_t* __restrict__ dst, const ParamWords b, int skip, int s0, int s1) {
+  for (int k = threadIdx.x; k < PARAM_WORDS; k += blockDim.x)
+    if (k != skip && (k < s0 || k >= s1)) dst[k] = b.w[k];
+}
+__global__ void k_write_pieces(float* __restrict__ dst, const PieceFloats b) {
+  for (int k = threadIdx.x; k < MAX_PIECES * PIECE_FLOATS; k += blockDim.x) dst[k] = b.f[k];
+}
+// The readback (js/fluid.js:315-342): nwords words from src into pinned host memory mapped into the
+// device's address space, then the first nzero of them (the accumulators) cleared on the device;
+// each thread clears only words it has read. The host reads the slot after the event that follows.
+__global__ void k_readback(uint32_t* __restrict__ src, uint32_t* __restrict__ host, int nwords, int nzero) {
+  for (int k = threadIdx.x; k < nwords; k += blockDim.x) {
+    host[k] = src[k];
+    if (k < nzero) src[k] = 0u;
+  }
+  __threadfence_system();
+}
+
+void launch_write_params(uint32_t* dst, const ParamWords& b, int skip, int s0, int s1, cudaStream_t st) {
+  k_write_params<<<1, 64, 0, st>>>(dst, b, skip, s0, s1);
+}
+void launch_write_pieces(float* dst, const PieceFloats& b, cudaStream_t st) {
+  k_write_pieces<<<1, 256, 0, st>>>(dst, b);
+}
+void launch_readback(uint32_t* src, uint32_t* host, int nwords, int nzero, cudaStream_t st) {
+  k_readback<<<1, 512, 0, st>>>(src, host, nwords, nzero);
+}
 void launch_project(SceneDesc* scenes, const Work* work, int ntiles, bool fp64, cudaStream_t st, int nscenes, int post,
                     const double* dxd, const double* alpha, float* dtv) {
   if (ntiles <= 0) return;

@@ -93,6 +93,15 @@ void launch_pcg_step(const SceneDesc* scenes, int nscenes, const Work* work, int
 void launch_pcg_finish(const SceneDesc* scenes, const Work* work, int ntiles, cudaStream_t st);
 // end of a loop iteration: count it and set the WHILE node's condition (bounded by SolveCtl::hard_cap)
 void launch_loop_guard(SolveCtl* ctl, unsigned long long cond_handle, int use_cond, cudaStream_t st);
+// a scene's parameter block (the leading PARAM_WORDS words of SceneDesc) and its pieces, passed by value
+constexpr int PARAM_WORDS = 51;
+struct ParamWords { uint32_t w[PARAM_WORDS]; };
+struct PieceFloats { float f[MAX_PIECES * PIECE_FLOATS]; };
+// dst[k] = b.w[k] except word `skip` and words [s0, s1) (-1: none)
+void launch_write_params(uint32_t* dst, const ParamWords& b, int skip, int s0, int s1, cudaStream_t st);
+void launch_write_pieces(float* dst, const PieceFloats& b, cudaStream_t st);
+// nwords words of src to mapped pinned host memory, then the first nzero cleared on the device
+void launch_readback(uint32_t* src, uint32_t* host, int nwords, int nzero, cudaStream_t st);
 // fused V(2,2) cycle: per fine level a down kernel (4 passes + restriction) and an
 // up kernel (prolongation + 4 passes; level 0 tail: 1 residual norm + decision,
 // 2 p64 += p, 3 the Krylov dot products, 4 the fused Krylov mode's), and one CTA per
