@@ -54,7 +54,7 @@ B_FIXED = 156 + 68 + 28 + 20 + 28 + 13.3 + 32
 
 
 # DRAM bytes (read + write) per launch of a kernel, from one ncu capture of the workload
-NCU_TRAFFIC = {("plain", "mg_coarse"): 123904, ("plain", "advect"): 2967808,
+NCU_TRAFFIC = {("plain", "mg_coarse"): 157440, ("plain", "advect"): 2967808,
                ("fine", "mg_up0_krylov"): 16266752, ("fine", "mg_down0_krylov"): 20596736,
                ("batched", "mg_down0"): 43902464}
 
