@@ -353,12 +353,14 @@ __device__ __forceinline__ void pcg_down_apply(const SceneDesc& S, const LevelDe
 // ------------------------------------------------------------------ down: 4 passes + restrict
 // PCG: the fused Krylov update on level 0 (above)
 // ONE: compiled for an engine of one scene (nscenes == 1), whose flag only ends the loop
-template <int TX, int TY, bool PCG, bool ONE>
+// MINB: resident CTAs per SM the registers are sized for (3; 2 for a level-0 Krylov kernel whose
+// tiles fit in one wave at two per SM: no spill)
+template <int TX, int TY, bool PCG, bool ONE, int MINB = 3>
 // three CTAs per SM (at most 85 registers a thread; 44 bytes of spill in the fused Krylov
 // variant): 512x768's 768 level-0 tiles run in two waves instead of three (measured: -5% per
 // Krylov cycle at 512x768). Four for the plain variants (62 registers) was measured 3-4% slower
 // per step at 256x384 and 512x768 and no faster for the batch.
-__global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
+__global__ void __launch_bounds__(256, MINB) k_mg_down(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                  int level, SolveCtl* ctl, int count_iter) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
   __shared__ __align__(128) float sp[MGF_BH * MGF_BW];
@@ -457,8 +459,8 @@ __global__ void __launch_bounds__(256, 3) k_mg_down(const SceneDesc* __restrict_
 // 3 r.z, q.z, z.Lz -> the direction update (Krylov FP64 mode), 4 the same in the fused Krylov
 // mode (the pending r, q update first; the loop decision from the recurrence for ||r||); one
 // instance per tail (levels below 0: tail 0)
-template <int TX, int TY, int TAIL, bool ONE>   // ONE: as in k_mg_down
-__global__ void __launch_bounds__(256, 3) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
+template <int TX, int TY, int TAIL, bool ONE, int MINB = 3>   // ONE, MINB: as in k_mg_down
+__global__ void __launch_bounds__(256, MINB) k_mg_up(const SceneDesc* __restrict__ scenes, int nscenes, const Work* __restrict__ work,
                                                int level, SolveCtl* ctl) {
   static_assert(TX == MGF_TX && TY == MGF_TY, "the tensor-map boxes are built for the MGF tile");
   static_assert(TAIL >= 0 && TAIL <= 4, "tails 0-4");
@@ -1310,19 +1312,33 @@ static UpKernel up_kernel(int tail) {
     default: return k_mg_up<MGF_TX, MGF_TY, 0, ONE>;
   }
 }
+// whether `ntiles` CTAs fit in one wave at two per SM (this process's device)
+static bool one_wave_at_two(int ntiles) {
+  static const int sms = [] {
+    int d = 0, n = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d) != cudaSuccess)
+      n = 0;
+    return n;
+  }();
+  return ntiles <= 2 * sms;
+}
 void launch_mg_down(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, SolveCtl* ctl,
                     int count_iter, int pcg, cudaStream_t st) {
-  if (ntiles > 0)
-    launch_pdl(pdl_enabled(),
-               nscenes == 1 ? (pcg ? k_mg_down<MGF_TX, MGF_TY, true, true> : k_mg_down<MGF_TX, MGF_TY, false, true>)
-                            : (pcg ? k_mg_down<MGF_TX, MGF_TY, true, false> : k_mg_down<MGF_TX, MGF_TY, false, false>),
-               dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, ctl, count_iter);
+  if (ntiles <= 0) return;
+  const auto k = nscenes == 1
+                     ? (pcg ? (one_wave_at_two(ntiles) ? k_mg_down<MGF_TX, MGF_TY, true, true, 2>
+                                                       : k_mg_down<MGF_TX, MGF_TY, true, true>)
+                            : k_mg_down<MGF_TX, MGF_TY, false, true>)
+                     : (pcg ? k_mg_down<MGF_TX, MGF_TY, true, false> : k_mg_down<MGF_TX, MGF_TY, false, false>);
+  launch_pdl(pdl_enabled(), k, dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, ctl, count_iter);
 }
 void launch_mg_up(const SceneDesc* scenes, int nscenes, const Work* work, int ntiles, int level, int tail, SolveCtl* ctl,
                   cudaStream_t st) {
-  if (ntiles > 0)
-    launch_pdl(pdl_enabled(), nscenes == 1 ? up_kernel<true>(tail) : up_kernel<false>(tail), dim3(ntiles), dim3(256), 0,
-               st, scenes, nscenes, work, level, ctl);
+  if (ntiles <= 0) return;
+  const UpKernel k = nscenes != 1 ? up_kernel<false>(tail)
+                     : tail == 4 && one_wave_at_two(ntiles) ? k_mg_up<MGF_TX, MGF_TY, 4, true, 2>
+                                                            : up_kernel<true>(tail);
+  launch_pdl(pdl_enabled(), k, dim3(ntiles), dim3(256), 0, st, scenes, nscenes, work, level, ctl);
 }
 void launch_pcg_decide(const SceneDesc* scenes, int nscenes, SolveCtl* ctl, cudaStream_t st) {
   if (nscenes > 0) launch_pdl(pdl_enabled(), k_pcg_decide, dim3(nscenes), dim3(256), 0, st, scenes, ctl);
