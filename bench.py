@@ -625,8 +625,10 @@ def run_app_frames(dev, stream, frames: int, warmup: int):
             "last_frame_stats": {"hrr_w_per_m": st["hrr"], "rad_w_per_m": st["rad"], "tmax_k": st["tmax"]}}
 
 
-def run_e2e(sim, sc, stream, flush, steps: int, barrier, dev, world: int) -> dict:
-    """Wall-clock steps through the C ABI with the host-side inputs and outputs of the app's frame (see main)."""
+def run_e2e(sim, sc, stream, flush, steps: int, barrier, dev, world: int, ckpt=None) -> dict:
+    """Wall-clock steps through the C ABI with the host-side inputs and outputs of the app's frame (see main).
+    ckpt: the state measure_gpu saved two warm-up steps before its timed steps; it is loaded and the two steps are
+    taken the same way untimed, so that the timed steps are the device-timed ones."""
     import torch
     import torch.distributed as dist
     import campfire_b200 as cb
@@ -640,6 +642,15 @@ def run_e2e(sim, sc, stream, flush, steps: int, barrier, dev, world: int) -> dic
     accp, radp, fwp = (ctypes.cast(acc.data_ptr(), i32), ctypes.cast(rad.data_ptr(), ctypes.POINTER(ctypes.c_float)),
                        ctypes.cast(fw.data_ptr(), i32))
     tag, ready, slot = ctypes.c_uint64(), ctypes.c_int(), ctypes.c_int()
+    if ckpt:
+        sim.load_checkpoint(ckpt)
+        for k in range(2):
+            flush.fill_(float(k))
+            cb._lib.check(L.cfg_upload_pieces(sim._h, fptr, sc["npieces"]))
+            cb._lib.check(L.cfg_write_params(sim._h))
+            cb._lib.check(L.cfg_step(sim._h, 1))
+            cb._lib.check(L.cfg_readback_begin(sim._h, k, ctypes.byref(slot)))
+            cb._lib.check(L.cfg_readback_wait(sim._h, accp, radp, fwp, ctypes.byref(tag)))
     collected, skipped, lag = 0, 0, []
     # the L2 flush's device time, measured apart (so that the timed loop carries no extra events)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -696,9 +707,11 @@ def run_e2e(sim, sc, stream, flush, steps: int, barrier, dev, world: int) -> dic
 
 
 def measure_gpu(dev, stream, flush, workload: str, steps: int, warmup: int, launch: str, coarse_cells: int,
-                world: int, rank: int, barrier, clocks=None, w_cells=None) -> dict:
+                world: int, rank: int, barrier, clocks=None, w_cells=None, ckpt=None) -> dict:
     """The plain single-scene step of `workload` on this rank's GPU: `steps` steps timed one by one with CUDA
-    events on the library's stream after an L2 flush each; value = all ranks' cell-updates / max-over-ranks time."""
+    events on the library's stream after an L2 flush each; value = all ranks' cell-updates / max-over-ranks time.
+    ckpt: a file that receives the scene's state two warm-up steps before the timed steps (cfg_checkpoint_save),
+    so that the end-to-end measurement can take the same steps."""
     import torch
     import torch.distributed as dist
     import campfire_b200 as cb
@@ -725,7 +738,13 @@ def measure_gpu(dev, stream, flush, workload: str, steps: int, warmup: int, laun
                          "autotune_ms": {k: [round(x, 5) for x in v] for k, v in tt["ms"].items()}}
     sim.set_stream(stream.cuda_stream)
     sim.set_graphs(launch == "graph")
-    sim.step(warmup)
+    if ckpt:
+        sim.step(warmup - 2)
+        sim.synchronize()
+        sim.save_checkpoint(ckpt)
+        sim.step(2)
+    else:
+        sim.step(warmup)
     sim.synchronize()
     barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
@@ -920,8 +939,11 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
+    import tempfile
+    fd, ckpt = tempfile.mkstemp(prefix="campfire_bench_", suffix=".ckpt")
+    os.close(fd)
     m = measure_gpu(dev, stream, flush, a.workload, a.steps, a.warmup, a.launch, a.coarse_cells, world, rank,
-                    barrier, ClockSampler(local), w_cells=a.w_cells)
+                    barrier, ClockSampler(local), w_cells=a.w_cells, ckpt=ckpt)
     sim, sc, value, ms_max, info = m["sim"], m["scene"], m["value"], m["ms_max"], m["info"]
 
     # ---- end to end through the C ABI, the app's frame data flow (js/main.js:266-283): per step the piece
@@ -932,7 +954,9 @@ def main():
     # three steps queued ahead of the GPU). The timed region ends when the last readback has been collected.
     # The L2 flush before each step (as in the device-timed loop) sits on the same stream; its device time,
     # measured with CUDA events over the same number of flushes just before, is taken out of the wall time.
-    e2e = run_e2e(sim, sc, stream, flush, max(20, min(50, a.steps)), barrier, dev, world)
+    # The timed steps are the device-timed ones: the scene resumes from the state saved before them.
+    e2e = run_e2e(sim, sc, stream, flush, a.steps, barrier, dev, world, ckpt=ckpt)
+    os.unlink(ckpt)
     e2e_value = world * nx * ny * e2e["steps"] / e2e["seconds"]
 
     # ---- roofline of the dominant kernel, measured after the timed region
@@ -992,11 +1016,12 @@ def main():
                 "launch": a.launch, "schedule": m["schedule"],
                 "solve": {"cycles_last_step": info["last_cycles"], "diff_sub": info["diffSub"],
                           "levels": info["levels"], "last_rel": info["last_rel"]},
-                # H2D: the piece buffer, the descriptor's parameter block (uniform + step controls, 204 B, less
-                # the CFL step's dt and diffusion sub-steps, 12 B, which the device owns) and dx/alpha of the
-                # diffusion rule (16 B); D2H: acc + rad + faceW of every collected readback
-                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 192 + 16,
+                # H2D: the piece buffer and the descriptor's parameter block (uniform + step controls, 204 B), each
+                # the parameter of a one-CTA kernel (dx and alpha of the diffusion rule go up only when they change);
+                # D2H: acc + rad + faceW of every collected readback
+                "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 64 * 20 * 4 + 204,
                         "d2h_bytes_per_step": (528 * 4 + 320 * 16 + 256 * 4) * e2e["collected"] / e2e["steps"],
+                        "steps": e2e["steps"], "steps_timed": "the device-timed steps, resumed from a checkpoint",
                         "readback": "asynchronous ring of three pinned slots (js/fluid.js:315-342)",
                         "readbacks": {k: e2e[k] for k in ("collected", "waited_on_full_ring", "lag_steps")},
                         "wall_s": e2e["wall_s"], "l2_flush_s_removed": e2e["flush_s"]},
